@@ -1,0 +1,576 @@
+// api.cu — the C ABI of libfopis_gpu.so (include/fopis_gpu.h).
+//
+// Every entry point catches C++ exceptions and returns an fopis_status; the
+// message of the last failure is kept per context (fopis_last_error).
+#include "internal.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+namespace fopis {
+void unet_free(Ctx& c);
+int unet_set_training(Ctx& c, int enable, double lr);
+int unet_get_state(Ctx& c, double* loss, int64_t* steps);
+int unet_predict(Ctx& c);            // writes the guess into phi, 0 when unavailable
+void unet_observe(Ctx& c);           // records a (rho, phi^{n-1}, phi^{n-2}) -> phi^n pair and trains
+}
+
+using namespace fopis;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+constexpr uint32_t kFatalBits = FOPIS_DEV_PARTICLE_OVERFLOW | FOPIS_DEV_ABSORB_OVERFLOW | FOPIS_DEV_BAD_CMAT_NODE |
+                                FOPIS_DEV_NONFINITE;
+
+template <typename F>
+int guarded(void* h, F&& f) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return FOPIS_ERR_ARG;
+    try {
+        return f(*c);
+    } catch (const CudaError& e) {
+        c->err = std::string("CUDA error ") + cudaGetErrorString(e.code) + " at " + e.where;
+        return FOPIS_ERR_CUDA;
+    } catch (const ApiError& e) {
+        c->err = e.msg;
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        c->err = "host allocation failed";
+        return FOPIS_ERR_NOMEM;
+    } catch (const std::exception& e) {
+        c->err = e.what();
+        return FOPIS_ERR_ARG;
+    }
+}
+
+// Reads the device scalars and turns latched device errors into a status.
+int check_device(Ctx& c) {
+    sync_scalars(c);
+    const uint32_t st = c.h_sc->status;
+    if (st & (FOPIS_DEV_PARTICLE_OVERFLOW | FOPIS_DEV_ABSORB_OVERFLOW)) {
+        c.err = "particle or absorbed-list capacity exceeded (device status " + std::to_string(st) + ")";
+        return FOPIS_ERR_CAPACITY;
+    }
+    if (st & kFatalBits) {
+        c.err = "device status " + std::to_string(st) + ": invalid surface node or non-finite particle state";
+        return FOPIS_ERR_DEVICE;
+    }
+    return FOPIS_OK;
+}
+
+void update_currents(Ctx& c) {
+    for (size_t o = 0; o < c.objs.size(); ++o)
+        for (int s = 0; s < c.nsp; ++s) {
+            const double q = c.p.species[s].charge * c.p.species[s].size;
+            c.objs[o].current[s] =
+                q * ((double)c.h_sc->absorbed_by[o][s] - (double)c.h_sc->emitted_by[o][s]);
+        }
+    int64_t ab = 0, em = 0;
+    for (size_t o = 0; o < c.objs.size(); ++o)
+        for (int s = 0; s < c.nsp; ++s) { ab += c.h_sc->absorbed_by[o][s]; em += c.h_sc->emitted_by[o][s]; }
+    c.absorbed_step = ab;
+    c.emitted_step = em;
+}
+
+void step_begin(Ctx& c) {
+    objects_step_begin(c);
+    FOPIS_CUDA(cudaMemsetAsync(c.d_sc->energy, 0, sizeof(c.d_sc->energy), c.st));
+    c.step_vcycles = 0;
+    c.step_solves = 0;
+}
+
+double solve_tol(const Ctx& c) { return c.p.poisson_tol > 0 ? c.p.poisson_tol : 1e-8; }
+int solve_cap(const Ctx& c) { return c.p.max_vcycles > 0 ? c.p.max_vcycles : 100; }
+
+// One Poisson solve with the start guess of the context's mode; a solve that
+// fails to converge from the learned guess is redone from the previous phi,
+// and one from the previous phi is redone from zero.
+int solve(Ctx& c, bool first_of_step) {
+    int mode = c.p.guess_mode;
+    if (mode == FOPIS_GUESS_ZERO) FOPIS_CUDA(cudaMemsetAsync(c.phi, 0, sizeof(double) * c.N, c.st));
+    bool learned = false;
+    if (mode == FOPIS_GUESS_LEARNED && first_of_step) learned = unet_predict(c) != 0;
+    c.learned_used = learned ? 1 : 0;
+    int rc = mg_solve(c, solve_tol(c), solve_cap(c));
+    if (rc == FOPIS_ERR_NOT_CONVERGED && learned) {
+        FOPIS_CUDA(cudaMemcpyAsync(c.phi, c.phi_prev, sizeof(double) * c.N, cudaMemcpyDeviceToDevice, c.st));
+        rc = mg_solve(c, solve_tol(c), solve_cap(c));
+        c.learned_used = 0;
+    }
+    if (rc == FOPIS_ERR_NOT_CONVERGED && mode != FOPIS_GUESS_ZERO) {
+        FOPIS_CUDA(cudaMemsetAsync(c.phi, 0, sizeof(double) * c.N, c.st));
+        rc = mg_solve(c, solve_tol(c), solve_cap(c));
+    }
+    return rc;
+}
+
+// RootGrid::updateRho after the per-particle pass: fold and convert, the
+// object charge sums, and with objects the first solve plus the
+// redistribution (RootGridField.cpp:1198-1243).
+int rho_tail(Ctx& c, int* solve_rc) {
+    launch_absorb(c);
+    rho_finalize(c);
+    int rc = FOPIS_OK;
+    if (!c.objs.empty()) {
+        objects_step_end(c);
+        rc = solve(c, true);
+        redistribute(c);
+    }
+    *solve_rc = rc;
+    return FOPIS_OK;
+}
+
+void record(Ctx& c, int k) {
+    if (c.ev[k]) FOPIS_CUDA(cudaEventRecord(c.ev[k], c.st));
+}
+
+// The fused RootGrid::mainLoopES (RootGrid.cpp:82-143).
+int one_step(Ctx& c) {
+    step_begin(c);
+    FOPIS_CUDA(cudaMemsetAsync(&c.d_sc->absorbed_n, 0, sizeof(unsigned long long), c.st));
+    rho_zero(c);
+    record(c, 0);
+    launch_push(c, true, true, true);
+    record(c, 1);
+    launch_emit(c, true);
+    record(c, 2);
+    launch_inject(c, true);
+    record(c, 3);
+    int rc1 = FOPIS_OK;
+    rho_tail(c, &rc1);
+    record(c, 5);
+    const bool learned_first = c.objs.empty();
+    int rc2 = solve(c, learned_first);
+    record(c, 6);
+    efield_update(c);
+    record(c, 7);
+    if (c.unet) unet_observe(c);
+    const int si = c.p.sort_interval > 0 ? c.p.sort_interval : 4;
+    if (c.timestep % si == 0) particles_sort(c);
+    record(c, 8);
+    int rc = check_device(c);
+    update_currents(c);
+    c.energy_valid = true;
+    c.timestep += 1;
+    if (c.ev[0]) {
+        FOPIS_CUDA(cudaEventSynchronize(c.ev[8]));
+        float ms = 0.f;
+        const int map[8][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 5}, {3, 5}, {5, 6}, {6, 7}, {7, 8}};
+        for (int q = 0; q < 8; ++q) {
+            cudaEventElapsedTime(&ms, c.ev[map[q][0]], c.ev[map[q][1]]);
+            c.ms_phase[q] = ms;
+        }
+        c.ms_phase[3] = 0.0;   // absorb runs inside the rho phase
+    }
+    if (rc != FOPIS_OK) return rc;
+    if (rc1 != FOPIS_OK) return rc1;
+    return rc2;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fopis_version(void) { return "fopis-b200 0.1 (sm_100a)"; }
+
+const char* fopis_last_error(void* h) {
+    if (!h) return g_create_error.c_str();
+    return static_cast<Ctx*>(h)->err.c_str();
+}
+
+int fopis_create(const fopis_params* p, int device, void** out) {
+    if (!p || !out) return FOPIS_ERR_ARG;
+    *out = nullptr;
+    Ctx* c = new (std::nothrow) Ctx();
+    if (!c) return FOPIS_ERR_NOMEM;
+    int rc = guarded(c, [&](Ctx& x) -> int {
+        x.p = *p;
+        if (p->nx < 3 || p->ny < 3 || p->nz < 3 || p->nx > 1020 || p->ny > 1020 || p->nz > 1020)
+            throw ApiError{FOPIS_ERR_ARG, "nx, ny, nz must lie in [3, 1020]"};
+        if (p->nspecies < 1 || p->nspecies > FOPIS_MAX_SPECIES) throw ApiError{FOPIS_ERR_ARG, "nspecies out of range"};
+        if (!(p->eps0 > 0.0)) throw ApiError{FOPIS_ERR_ARG, "eps0 must be positive"};
+        for (int t = 0; t < 6; ++t) {
+            const char b = p->boundary[t];
+            if (b != 'D' && b != 'N' && b != 'P')
+                throw ApiError{FOPIS_ERR_ARG, "Unknown boundary condition type was used"};  // Field.cpp:25-28
+        }
+        if (p->precision != FOPIS_MIXED) throw ApiError{FOPIS_ERR_ARG, "only the mixed-precision path is built"};
+        for (int s = 0; s < p->nspecies; ++s)
+            if (!(p->species[s].mass > 0.0)) throw ApiError{FOPIS_ERR_ARG, "species mass must be positive"};
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw ApiError{FOPIS_ERR_NO_CUDA, "no CUDA device"};
+        x.device = device >= 0 ? device : 0;
+        if (device < 0) cudaGetDevice(&x.device);
+        FOPIS_CUDA(cudaSetDevice(x.device));
+        FOPIS_CUDA(cudaStreamCreateWithFlags(&x.st, cudaStreamNonBlocking));
+        x.nx = p->nx; x.ny = p->ny; x.nz = p->nz;
+        x.cx = x.nx + 2; x.cy = x.ny + 2; x.cz = x.nz + 2;
+        x.N = (size_t)x.cx * x.cy * x.cz;
+        for (int t = 0; t < 6; ++t) x.per[t] = p->boundary[t] == 'P';
+        x.nsp = p->nspecies;
+        FOPIS_CUDA(cudaMalloc(&x.rho_i64, sizeof(unsigned long long) * x.N * x.nsp));
+        FOPIS_CUDA(cudaMalloc(&x.rho0, sizeof(double) * x.N));
+        FOPIS_CUDA(cudaMalloc(&x.phi, sizeof(double) * x.N));
+        FOPIS_CUDA(cudaMalloc(&x.phi_prev, sizeof(double) * x.N));
+        FOPIS_CUDA(cudaMalloc(&x.phi_prev2, sizeof(double) * x.N));
+        FOPIS_CUDA(cudaMalloc(&x.scratch64, sizeof(double) * x.N));
+        FOPIS_CUDA(cudaMalloc(&x.E, sizeof(float4) * x.N));
+        FOPIS_CUDA(cudaMalloc(&x.cellmap, x.N));
+        FOPIS_CUDA(cudaMalloc(&x.node_cmat, sizeof(int32_t) * x.N));
+        FOPIS_CUDA(cudaMalloc(&x.sort_count, sizeof(int32_t) * (x.N + 1)));
+        FOPIS_CUDA(cudaMalloc(&x.sort_offset, sizeof(int32_t) * (x.N + 1)));
+        const size_t tiles = (x.N + 1 + 8191) / 8192;
+        FOPIS_CUDA(cudaMalloc(&x.scan_partials, sizeof(int32_t) * (tiles + 1)));
+        FOPIS_CUDA(cudaMemset(x.rho_i64, 0, sizeof(unsigned long long) * x.N * x.nsp));
+        FOPIS_CUDA(cudaMemset(x.rho0, 0, sizeof(double) * x.N));
+        FOPIS_CUDA(cudaMemset(x.phi, 0, sizeof(double) * x.N));
+        FOPIS_CUDA(cudaMemset(x.phi_prev, 0, sizeof(double) * x.N));
+        FOPIS_CUDA(cudaMemset(x.phi_prev2, 0, sizeof(double) * x.N));
+        FOPIS_CUDA(cudaMemset(x.E, 0, sizeof(float4) * x.N));
+        FOPIS_CUDA(cudaMemset(x.cellmap, 0, x.N));
+        FOPIS_CUDA(cudaMemset(x.node_cmat, 0xff, sizeof(int32_t) * x.N));
+        // absorbed list: generous for conductor-heavy steps
+        x.ab.cap = std::max<int64_t>(1 << 20, (int64_t)x.N / 2);
+        FOPIS_CUDA(cudaMalloc(&x.ab.cell, sizeof(int32_t) * x.ab.cap));
+        float** fl[6] = {&x.ab.ox, &x.ab.oy, &x.ab.oz, &x.ab.vx, &x.ab.vy, &x.ab.vz};
+        for (auto* q : fl) FOPIS_CUDA(cudaMalloc(q, sizeof(float) * x.ab.cap));
+        FOPIS_CUDA(cudaMalloc(&x.ab.species, x.ab.cap));
+        FOPIS_CUDA(cudaMalloc(&x.ab.object, x.ab.cap));
+        FOPIS_CUDA(cudaMalloc(&x.d_sc, sizeof(DevScalars)));
+        FOPIS_CUDA(cudaMemset(x.d_sc, 0, sizeof(DevScalars)));
+        FOPIS_CUDA(cudaMallocHost(&x.h_sc, sizeof(DevScalars)));
+        std::memset(x.h_sc, 0, sizeof(DevScalars));
+        for (auto& e : x.ev) FOPIS_CUDA(cudaEventCreate(&e));
+        mg_setup(x);
+        FOPIS_CUDA(cudaDeviceSynchronize());
+        return FOPIS_OK;
+    });
+    if (rc != FOPIS_OK) {
+        g_create_error = c->err;
+        fopis_destroy(c);
+        return rc;
+    }
+    *out = c;
+    return FOPIS_OK;
+}
+
+void fopis_destroy(void* h) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return;
+    if (c->st) cudaStreamSynchronize(c->st);
+    unet_free(*c);
+    for (int s = 0; s < FOPIS_MAX_SPECIES; ++s) {
+        Soa* v[2] = {&c->sp[s], &c->sp2[s]};
+        for (Soa* q : v) {
+            cudaFree(q->cell); cudaFree(q->ox); cudaFree(q->oy); cudaFree(q->oz);
+            cudaFree(q->vx); cudaFree(q->vy); cudaFree(q->vz);
+        }
+    }
+    for (auto& o : c->objs) {
+        cudaFree(o.nodes); cudaFree(o.C); cudaFree(o.colsum); cudaFree(o.charge_tmp);
+        cudaFree(o.charge_map); cudaFree(o.phis); cudaFree(o.scal); cudaFree(o.lit);
+    }
+    mg_free(*c);
+    void* ptrs[] = {c->rho_i64, c->rho0, c->phi, c->phi_prev, c->phi_prev2, c->scratch64, c->E, c->cellmap,
+                    c->node_cmat, c->sort_count, c->sort_offset, c->scan_partials, c->ab.cell, c->ab.ox,
+                    c->ab.oy, c->ab.oz, c->ab.vx, c->ab.vy, c->ab.vz, c->ab.species, c->ab.object, c->d_sc};
+    for (void* q : ptrs) if (q) cudaFree(q);
+    if (c->h_sc) cudaFreeHost(c->h_sc);
+    for (auto& e : c->ev) if (e) cudaEventDestroy(e);
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+}
+
+int fopis_add_object(void* h, const fopis_object_desc* d, int* object_id) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (!d || !d->cmat_nodes || (d->n_cells > 0 && !d->cells)) throw ApiError{FOPIS_ERR_ARG, "null object description"};
+        if ((int)c.objs.size() >= FOPIS_MAX_OBJECTS) throw ApiError{FOPIS_ERR_ARG, "too many objects"};
+        if (d->emit_species >= c.nsp) throw ApiError{FOPIS_ERR_ARG, "emit_species out of range"};
+        const int id = (int)c.objs.size();
+        c.objs.emplace_back();
+        try {
+            object_upload(c, c.objs.back(), d, id);
+        } catch (...) {
+            c.objs.pop_back();
+            throw;
+        }
+        if (object_id) *object_id = id;
+        return FOPIS_OK;
+    });
+}
+
+int fopis_build_capacity_matrix(void* h, int id) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (id < 0 || id >= (int)c.objs.size()) throw ApiError{FOPIS_ERR_ARG, "object id"};
+        cmatrix_build(c, id);
+        return FOPIS_OK;
+    });
+}
+
+int fopis_set_capacity_matrix(void* h, int id, const double* C, int n) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (id < 0 || id >= (int)c.objs.size() || !C || n != c.objs[id].n) throw ApiError{FOPIS_ERR_ARG, "object id or size"};
+        cmatrix_set(c, id, C);
+        return FOPIS_OK;
+    });
+}
+
+int fopis_get_capacity_matrix(void* h, int id, double* C, int n) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (id < 0 || id >= (int)c.objs.size() || !C || n != c.objs[id].n) throw ApiError{FOPIS_ERR_ARG, "object id or size"};
+        if (!c.objs[id].has_C) throw ApiError{FOPIS_ERR_STATE, "capacity matrix not built"};
+        FOPIS_CUDA(cudaMemcpy(C, c.objs[id].C, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToHost));
+        return FOPIS_OK;
+    });
+}
+
+int fopis_get_object(void* h, int id, double* V, double* Q, double* I) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (id < 0 || id >= (int)c.objs.size()) throw ApiError{FOPIS_ERR_ARG, "object id"};
+        const ObjectDev& o = c.objs[id];
+        if (V) *V = o.potential;
+        if (Q) *Q = o.total_charge;
+        if (I) for (int s = 0; s < c.nsp; ++s) I[s] = o.current[s];
+        return FOPIS_OK;
+    });
+}
+
+int fopis_get_charge_map(void* h, int id, double* out, int n) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (id < 0 || id >= (int)c.objs.size() || !out || n != c.nsp * c.objs[id].n) throw ApiError{FOPIS_ERR_ARG, "object id or size"};
+        FOPIS_CUDA(cudaMemcpy(out, c.objs[id].charge_map, sizeof(double) * n, cudaMemcpyDeviceToHost));
+        return FOPIS_OK;
+    });
+}
+
+int fopis_load_particles(void* h, int s, const void* p56, int64_t n) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (s < 0 || s >= c.nsp || (n > 0 && !p56) || n < 0) throw ApiError{FOPIS_ERR_ARG, "species or buffer"};
+        if (n) particles_append_aos(c, s, p56, n);
+        c.energy_valid = false;
+        return check_device(c);
+    });
+}
+
+int fopis_get_particles(void* h, int s, void* p56, int64_t cap, int64_t* n_out) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (s < 0 || s >= c.nsp || (cap > 0 && !p56)) throw ApiError{FOPIS_ERR_ARG, "species or buffer"};
+        const int64_t n = c.cap[s] ? particles_export_aos(c, s, p56, cap) : 0;
+        if (n_out) *n_out = n;
+        return FOPIS_OK;
+    });
+}
+
+int fopis_get_particles_raw(void* h, int s, int32_t* cell, float* ox, float* oy, float* oz, float* vx, float* vy,
+                            float* vz, int64_t cap, int64_t* n_out) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (s < 0 || s >= c.nsp) throw ApiError{FOPIS_ERR_ARG, "species"};
+        if (cap > 0 && !(cell && ox && oy && oz && vx && vy && vz)) throw ApiError{FOPIS_ERR_ARG, "buffers"};
+        const int64_t n = c.cap[s] ? particles_export_raw(c, s, cell, ox, oy, oz, vx, vy, vz, cap) : 0;
+        if (n_out) *n_out = n;
+        return FOPIS_OK;
+    });
+}
+
+int fopis_generate_ambient(void* h) {
+    return guarded(h, [&](Ctx& c) -> int {
+        particles_generate_ambient(c);
+        c.energy_valid = false;
+        return check_device(c);
+    });
+}
+
+int fopis_sort_particles(void* h) {
+    return guarded(h, [&](Ctx& c) -> int {
+        particles_sort(c);
+        return check_device(c);
+    });
+}
+
+int fopis_remove_invalid_particles(void* h) { return fopis_sort_particles(h); }
+
+int fopis_initialize(void* h) {
+    return guarded(h, [&](Ctx& c) -> int {
+        particles_sort(c);
+        step_begin(c);
+        FOPIS_CUDA(cudaMemsetAsync(&c.d_sc->absorbed_n, 0, sizeof(unsigned long long), c.st));
+        rho_zero(c);
+        launch_deposit_all(c);
+        int rc1 = FOPIS_OK;
+        rho_tail(c, &rc1);
+        const int rc2 = solve(c, false);
+        efield_update(c);
+        FOPIS_CUDA(cudaMemcpyAsync(c.phi_prev, c.phi, sizeof(double) * c.N, cudaMemcpyDeviceToDevice, c.st));
+        FOPIS_CUDA(cudaMemcpyAsync(c.phi_prev2, c.phi, sizeof(double) * c.N, cudaMemcpyDeviceToDevice, c.st));
+        const int rc = check_device(c);
+        update_currents(c);
+        c.energy_valid = false;
+        if (rc != FOPIS_OK) return rc;
+        return rc1 != FOPIS_OK ? rc1 : rc2;
+    });
+}
+
+int fopis_step(void* h, int n) {
+    return guarded(h, [&](Ctx& c) -> int {
+        int rc = FOPIS_OK;
+        for (int t = 0; t < n; ++t) {
+            rc = one_step(c);
+            if (rc != FOPIS_OK && rc != FOPIS_ERR_NOT_CONVERGED) return rc;
+        }
+        return rc;
+    });
+}
+
+int fopis_update_velocity(void* h) {
+    return guarded(h, [&](Ctx& c) -> int {
+        step_begin(c);   // RootGrid::resetObjects precedes it in mainLoopES
+        launch_push(c, true, false, false);
+        c.energy_valid = false;
+        return check_device(c);
+    });
+}
+
+int fopis_emit_particles(void* h) {
+    return guarded(h, [&](Ctx& c) -> int {
+        launch_emit(c, false);
+        c.energy_valid = false;
+        return check_device(c);
+    });
+}
+
+int fopis_update_position(void* h) {
+    return guarded(h, [&](Ctx& c) -> int {
+        launch_push(c, false, true, false);
+        c.energy_valid = false;
+        return check_device(c);
+    });
+}
+
+int fopis_inject_particles(void* h) {
+    return guarded(h, [&](Ctx& c) -> int {
+        launch_inject(c, false);
+        c.energy_valid = false;
+        return check_device(c);
+    });
+}
+
+int fopis_update_rho(void* h) {
+    return guarded(h, [&](Ctx& c) -> int {
+        FOPIS_CUDA(cudaMemsetAsync(&c.d_sc->absorbed_n, 0, sizeof(unsigned long long), c.st));
+        rho_zero(c);
+        launch_deposit_all(c);
+        int rc1 = FOPIS_OK;
+        rho_tail(c, &rc1);
+        const int rc = check_device(c);
+        update_currents(c);
+        c.energy_valid = false;
+        return rc != FOPIS_OK ? rc : rc1;
+    });
+}
+
+int fopis_solve_poisson(void* h) {
+    return guarded(h, [&](Ctx& c) -> int { return solve(c, false); });
+}
+
+int fopis_update_efield(void* h) {
+    return guarded(h, [&](Ctx& c) -> int {
+        efield_update(c);
+        FOPIS_CUDA(cudaStreamSynchronize(c.st));
+        return FOPIS_OK;
+    });
+}
+
+int fopis_advance_timestep(void* h) {
+    return guarded(h, [&](Ctx& c) -> int {
+        const int si = c.p.sort_interval > 0 ? c.p.sort_interval : 4;
+        if (c.timestep % si == 0) particles_sort(c);
+        c.timestep += 1;
+        return FOPIS_OK;
+    });
+}
+
+int fopis_get_field(void* h, int which, double* out, size_t n) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (!out || n != c.N) throw ApiError{FOPIS_ERR_ARG, "output size must be (nx+2)(ny+2)(nz+2)"};
+        field_export(c, which, out);
+        return FOPIS_OK;
+    });
+}
+
+int fopis_set_field(void* h, int which, const double* in, size_t n) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (!in || n != c.N) throw ApiError{FOPIS_ERR_ARG, "input size must be (nx+2)(ny+2)(nz+2)"};
+        double* dst = which == FOPIS_FIELD_PHI ? c.phi : (which == FOPIS_FIELD_RHO0 ? c.rho0 : nullptr);
+        if (!dst) throw ApiError{FOPIS_ERR_ARG, "only PHI and RHO0 can be set"};
+        FOPIS_CUDA(cudaMemcpy(dst, in, sizeof(double) * c.N, cudaMemcpyHostToDevice));
+        return FOPIS_OK;
+    });
+}
+
+int fopis_get_energy(void* h, double* pe, double* fe) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (!c.energy_valid) { launch_energy(c); sync_scalars(c); c.energy_valid = true; }
+        double e = 0.0;
+        for (int s = 0; s < c.nsp; ++s) e += 0.5 * c.p.species[s].mass * c.h_sc->energy[s] * c.p.species[s].size;
+        if (pe) *pe = e;
+        if (fe) *fe = efield_energy(c);
+        return FOPIS_OK;
+    });
+}
+
+int fopis_get_stats(void* h, fopis_stats* st) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (!st) throw ApiError{FOPIS_ERR_ARG, "null stats"};
+        sync_scalars(c);
+        std::memset(st, 0, sizeof(*st));
+        st->timestep = c.timestep;
+        st->vcycles_last = c.last_vcycles;
+        st->vcycles_step = c.step_vcycles;
+        st->solves_step = c.step_solves;
+        st->converged = c.last_converged;
+        st->residual_last = c.last_res;
+        st->residual_initial = c.first_res;
+        for (int s = 0; s < c.nsp; ++s) { st->num_particles[s] = c.nslots[s]; st->capacity[s] = c.cap[s]; }
+        st->absorbed_step = c.absorbed_step;
+        st->injected_step = c.injected_step;
+        st->emitted_step = c.emitted_step;
+        st->device_status = c.h_sc->status;
+        st->learned_used = c.learned_used;
+        for (int q = 0; q < 8; ++q) st->ms_phase[q] = c.ms_phase[q];
+        st->kernel_launches = c.launches;
+        return FOPIS_OK;
+    });
+}
+
+int fopis_get_stream(void* h, void** stream) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (!stream) throw ApiError{FOPIS_ERR_ARG, "null stream pointer"};
+        *stream = (void*)c.st;
+        return FOPIS_OK;
+    });
+}
+
+int fopis_set_guess_mode(void* h, int mode) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (mode < FOPIS_GUESS_ZERO || mode > FOPIS_GUESS_LEARNED) throw ApiError{FOPIS_ERR_ARG, "guess mode"};
+        c.p.guess_mode = mode;
+        return FOPIS_OK;
+    });
+}
+
+int fopis_unet_set_training(void* h, int enable, double lr) {
+    return guarded(h, [&](Ctx& c) -> int { return unet_set_training(c, enable, lr); });
+}
+
+int fopis_unet_get_state(void* h, double* loss, int64_t* steps) {
+    return guarded(h, [&](Ctx& c) -> int { return unet_get_state(c, loss, steps); });
+}
+
+void fopis_free(void* p) { std::free(p); }
+
+}  // extern "C"

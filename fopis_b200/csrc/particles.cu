@@ -1,0 +1,1152 @@
+// particles.cu — particle kernels of the ES step on sm_100a.
+//
+// Particles are structure-of-arrays, split precision: a packed int32 node cell
+// (i,j,k glue-layout indices, i = floor(x)+1 as include/position.hpp:59-69)
+// plus FP32 in-cell offsets x-(i-1) and FP32 velocities: 28 bytes a particle.
+// Charge is deposited as int64 fixed point (17 fractional bits per axis), so
+// rho is bit-exact and independent of the order of the additions.
+#include "internal.cuh"
+
+#include <algorithm>
+#include <cstring>
+
+namespace fopis {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr unsigned kFull = 0xffffffffu;
+
+struct Grid {
+    int cx, cy, cz;      // nodes with glue
+    int n[3];            // reference node counts
+    int per[6];          // periodic sides
+    long long sj, si;    // linear strides of j and i
+};
+
+__host__ Grid make_grid(const Ctx& c) {
+    Grid g;
+    g.cx = c.cx; g.cy = c.cy; g.cz = c.cz;
+    g.n[0] = c.nx; g.n[1] = c.ny; g.n[2] = c.nz;
+    for (int t = 0; t < 6; ++t) g.per[t] = c.per[t];
+    g.sj = c.cz; g.si = (long long)c.cy * c.cz;
+    return g;
+}
+
+__device__ __forceinline__ long long lin(const Grid& g, int i, int j, int k) {
+    return (long long)i * g.si + (long long)j * g.sj + k;
+}
+
+// Boundary rule of one axis on the split position (cell index ci, offset o):
+// the coordinate is (ci-1)+o. Restates RootGrid::checkX/Y/ZBoundary
+// (include/grid.hpp:309-395) plus the single-rank periodic migration
+// (src/Grid/GridParticleTreatmentES.cpp:115-177). Returns false to invalidate.
+__device__ __forceinline__ bool axis_boundary(const Grid& g, int axis, int& ci, float o) {
+    const int n = g.n[axis];
+    if (ci <= 0) {                                 // x < 0
+        if (g.per[2 * axis]) { if (ci <= -1) ci += n; }   // x < -1 -> x + sl
+        else return false;
+    } else if (ci > n || (ci == n && o > 0.0f)) {  // x > sl - 1
+        if (g.per[2 * axis + 1]) { if (ci >= n + 1) ci -= n; }  // x >= sl -> x - sl
+        else return false;
+    }
+    return true;
+}
+
+// Same rule on an FP64 coordinate (sources created in double).
+__device__ __forceinline__ bool axis_boundary_d(const Grid& g, int axis, double& x) {
+    const double sl = g.n[axis];
+    if (x < 0.0) {
+        if (g.per[2 * axis]) { if (x < -1.0) x += sl; }
+        else return false;
+    } else if (x > sl - 1.0) {
+        if (g.per[2 * axis + 1]) { if (x >= sl) x -= sl; }
+        else return false;
+    }
+    return true;
+}
+
+// Split an FP64 coordinate into node cell index and FP32 offset.
+__device__ __forceinline__ void split(double x, int& ci, float& o) {
+    const double f = floor(x);
+    ci = (int)f + 1;
+    o = (float)(x - f);
+    if (o >= 1.0f) { o = 0.0f; ci += 1; }
+}
+
+__device__ __forceinline__ bool cell_in_range(const Grid& g, int i, int j, int k) {
+    return i >= 0 && j >= 0 && k >= 0 && i <= g.cx - 2 && j <= g.cy - 2 && k <= g.cz - 2;
+}
+
+// Eight integer CIC corner weights (sum 2^51) in the corner order
+// (di,dj,dk) = 000,001,010,011,100,101,110,111.
+__device__ __forceinline__ void corner_weights(float ox, float oy, float oz, unsigned long long w[8]) {
+    const long long a = __float2int_rn(ox * kDepositScale);
+    const long long b = __float2int_rn(oy * kDepositScale);
+    const long long d = __float2int_rn(oz * kDepositScale);
+    const long long wx[2] = {kDepositOne - a, a}, wy[2] = {kDepositOne - b, b}, wz[2] = {kDepositOne - d, d};
+#pragma unroll
+    for (int t = 0; t < 8; ++t) w[t] = (unsigned long long)(wx[t >> 2] * wy[(t >> 1) & 1] * wz[t & 1]);
+}
+
+__device__ __forceinline__ long long corner_offset(const Grid& g, int t) {
+    return ((t >> 2) ? g.si : 0) + (((t >> 1) & 1) ? g.sj : 0) + (t & 1);
+}
+
+// Warp-aggregated int64 deposit. Lanes whose cell is unique in the warp add
+// their eight weights directly; lanes sharing a cell are reduced first with
+// three 17-bit-chunk redux.sync sums per corner (exact), then their leader adds.
+// Every lane of the warp must call this (dep selects the depositing ones).
+__device__ __forceinline__ void warp_deposit(unsigned long long* rho, const Grid& g, bool dep, long long base,
+                                             float ox, float oy, float oz) {
+    const int lane = threadIdx.x & 31;
+    unsigned long long w[8];
+    if (dep) corner_weights(ox, oy, oz, w);
+    else {
+#pragma unroll
+        for (int t = 0; t < 8; ++t) w[t] = 0ull;
+    }
+    const long long key = dep ? base : -1ll - lane;
+    const unsigned grp = __match_any_sync(kFull, key);
+    const bool single = __popc(grp) == 1;
+    if (dep && single) {
+#pragma unroll
+        for (int t = 0; t < 8; ++t)
+            if (w[t]) atomicAdd(rho + base + corner_offset(g, t), w[t]);
+    }
+    unsigned multi = __ballot_sync(kFull, dep && !single);
+    while (multi) {
+        const int leader = __ffs(multi) - 1;
+        const unsigned members = __shfl_sync(kFull, grp, leader);
+        const bool in = (members >> lane) & 1u;
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            const unsigned long long v = in ? w[t] : 0ull;
+            const unsigned s0 = __reduce_add_sync(kFull, (unsigned)(v & 0x1FFFFull));
+            const unsigned s1 = __reduce_add_sync(kFull, (unsigned)((v >> 17) & 0x1FFFFull));
+            const unsigned s2 = __reduce_add_sync(kFull, (unsigned)(v >> 34));
+            if (lane == leader) {
+                const unsigned long long tot = (unsigned long long)s0 + ((unsigned long long)s1 << 17) +
+                                               ((unsigned long long)s2 << 34);
+                if (tot) atomicAdd(rho + base + corner_offset(g, t), tot);
+            }
+        }
+        multi &= ~members;
+    }
+}
+
+// Warp-aggregated slot reservation on a 64-bit counter.
+__device__ __forceinline__ unsigned long long warp_reserve(unsigned long long* counter, bool want) {
+    const int lane = threadIdx.x & 31;
+    const unsigned m = __ballot_sync(kFull, want);
+    unsigned long long base = 0;
+    if (m) {
+        const int leader = __ffs(m) - 1;
+        if (lane == leader) base = atomicAdd(counter, (unsigned long long)__popc(m));
+        base = __shfl_sync(kFull, base, leader);
+    }
+    return base + __popc(m & ((1u << lane) - 1u));
+}
+
+__device__ __forceinline__ double block_sum(double v) {
+    __shared__ double red[32];
+    for (int o = 16; o; o >>= 1) v += __shfl_down_sync(kFull, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) red[w] = v;
+    __syncthreads();
+    v = 0.0;
+    if (w == 0) {
+        v = (l < (int)(blockDim.x >> 5)) ? red[l] : 0.0;
+        for (int o = 16; o; o >>= 1) v += __shfl_down_sync(kFull, v, o);
+    }
+    return v;
+}
+
+struct PushArgs {
+    Soa p;
+    int s;
+    long long cap;
+    const unsigned long long* count;
+    const float4* E;
+    Grid g;
+    float qm;                 // 0.5 q/m
+    float bx, by, bz, boris;  // static B as the reference uses it, 2/(1+|b|^2)
+    const uint8_t* cellmap;   // nullptr without objects
+    unsigned long long* rho;  // species rho (fixed point)
+    AbsorbList ab;
+    DevScalars* sc;
+};
+
+// The fused particle pass. VEL: CIC gather of nodal E and Boris kick/rotate
+// (Grid::updateParticleVelocityES, GridParticleTreatmentES.cpp:13-88). POS:
+// x += v and boundaries (RootGrid::updateParticlePositionES, :90-181). DEP: the
+// per-particle part of RootGrid::updateRho (RootGridField.cpp:1168-1196):
+// particles inside a body go to the absorbed list (Spacecraft::
+// distributeInnerParticleCharge, Spacecraft.cpp:512-592, finished by
+// absorb_kernel); the rest deposit their CIC weights.
+template <bool VEL, bool POS, bool DEP>
+__global__ void __launch_bounds__(kThreads) push_kernel(PushArgs a) {
+    const long long n = (long long)min(*a.count, (unsigned long long)a.cap);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    double e2 = 0.0;
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        const long long idx = base + (threadIdx.x & 31);
+        const bool inb = idx < n;
+        int32_t cell = inb ? a.p.cell[idx] : -1;
+        bool live = cell >= 0;
+        float ox = 0.f, oy = 0.f, oz = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
+        int i = 0, j = 0, k = 0;
+        if (live) {
+            unpack_cell(cell, i, j, k);
+            ox = a.p.ox[idx]; oy = a.p.oy[idx]; oz = a.p.oz[idx];
+            if (VEL || POS || DEP) { vx = a.p.vx[idx]; vy = a.p.vy[idx]; vz = a.p.vz[idx]; }
+        }
+        if (VEL && live) {
+            const long long b = lin(a.g, i, j, k);
+            const float x1 = ox, x2 = 1.0f - ox, y1 = oy, y2 = 1.0f - oy, z1 = oz, z2 = 1.0f - oz;
+            const float4 e000 = __ldg(a.E + b), e001 = __ldg(a.E + b + 1);
+            const float4 e010 = __ldg(a.E + b + a.g.sj), e011 = __ldg(a.E + b + a.g.sj + 1);
+            const float4 e100 = __ldg(a.E + b + a.g.si), e101 = __ldg(a.E + b + a.g.si + 1);
+            const float4 e110 = __ldg(a.E + b + a.g.si + a.g.sj), e111 = __ldg(a.E + b + a.g.si + a.g.sj + 1);
+            const float w000 = x2 * y2 * z2, w100 = x1 * y2 * z2, w010 = x2 * y1 * z2, w110 = x1 * y1 * z2;
+            const float w001 = x2 * y2 * z1, w101 = x1 * y2 * z1, w011 = x2 * y1 * z1, w111 = x1 * y1 * z1;
+            const float ex = a.qm * (w000 * e000.x + w100 * e100.x + w010 * e010.x + w110 * e110.x +
+                                     w001 * e001.x + w101 * e101.x + w011 * e011.x + w111 * e111.x);
+            const float ey = a.qm * (w000 * e000.y + w100 * e100.y + w010 * e010.y + w110 * e110.y +
+                                     w001 * e001.y + w101 * e101.y + w011 * e011.y + w111 * e111.y);
+            const float ez = a.qm * (w000 * e000.z + w100 * e100.z + w010 * e010.z + w110 * e110.z +
+                                     w001 * e001.z + w101 * e101.z + w011 * e011.z + w111 * e111.z);
+            const float vx1 = vx + ex, vy1 = vy + ey, vz1 = vz + ez;
+            const float vxt = vx1 + vy1 * a.bz - vz1 * a.by;
+            const float vyt = vy1 + vz1 * a.bx - vx1 * a.bz;
+            const float vzt = vz1 + vx1 * a.by - vy1 * a.bx;
+            vx = vx1 + (ex + a.boris * (vyt * a.bz - vzt * a.by));
+            vy = vy1 + (ey + a.boris * (vzt * a.bx - vxt * a.bz));
+            vz = vz1 + (ez + a.boris * (vxt * a.by - vyt * a.bx));
+        }
+        if (POS && live) {
+            ox += vx; oy += vy; oz += vz;
+            const float fx = floorf(ox), fy = floorf(oy), fz = floorf(oz);
+            ox -= fx; oy -= fy; oz -= fz;
+            i += __float2int_rd(fx); j += __float2int_rd(fy); k += __float2int_rd(fz);
+            live = axis_boundary(a.g, 0, i, ox) && axis_boundary(a.g, 1, j, oy) && axis_boundary(a.g, 2, k, oz);
+            if (live && !cell_in_range(a.g, i, j, k)) {  // non-finite or runaway velocity
+                live = false;
+                atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_NONFINITE);
+            }
+        }
+        bool absorbed = false;
+        if (DEP && live && a.cellmap) {
+            const uint8_t ob = a.cellmap[lin(a.g, i, j, k)];
+            absorbed = ob != 0;
+        }
+        if (DEP) {
+            const unsigned long long slot = warp_reserve(&a.sc->absorbed_n, absorbed);
+            if (absorbed) {
+                if ((long long)slot < a.ab.cap) {
+                    a.ab.cell[slot] = pack_cell(i, j, k);
+                    a.ab.ox[slot] = ox; a.ab.oy[slot] = oy; a.ab.oz[slot] = oz;
+                    a.ab.vx[slot] = vx; a.ab.vy[slot] = vy; a.ab.vz[slot] = vz;
+                    a.ab.species[slot] = (uint8_t)a.s;
+                    a.ab.object[slot] = (uint8_t)(a.cellmap[lin(a.g, i, j, k)] - 1);
+                } else {
+                    atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_ABSORB_OVERFLOW);
+                }
+                live = false;
+            }
+            const bool dep = live;
+            warp_deposit(a.rho, a.g, dep, dep ? lin(a.g, i, j, k) : 0, ox, oy, oz);
+            if (dep && VEL) e2 += (double)vx * vx + (double)vy * vy + (double)vz * vz;
+        }
+        if (inb && cell >= 0) {
+            if (POS || DEP) a.p.cell[idx] = live ? pack_cell(i, j, k) : -1;
+            if (POS) { a.p.ox[idx] = ox; a.p.oy[idx] = oy; a.p.oz[idx] = oz; }
+            if (VEL) { a.p.vx[idx] = vx; a.p.vy[idx] = vy; a.p.vz[idx] = vz; }
+        }
+    }
+    if (DEP && VEL) {
+        const double t = block_sum(e2);
+        if (threadIdx.x == 0 && t != 0.0) atomicAdd(&a.sc->energy[a.s], t);
+    }
+}
+
+// Writes a particle created in FP64 into a species slot (split precision).
+__device__ __forceinline__ void store_split(Soa p, long long slot, int i, int j, int k, float ox, float oy, float oz,
+                                            double vx, double vy, double vz) {
+    p.cell[slot] = pack_cell(i, j, k);
+    p.ox[slot] = ox; p.oy[slot] = oy; p.oz[slot] = oz;
+    p.vx[slot] = (float)vx; p.vy[slot] = (float)vy; p.vz[slot] = (float)vz;
+}
+
+struct SourceArgs {
+    Soa p[FOPIS_MAX_SPECIES];
+    long long cap[FOPIS_MAX_SPECIES];
+    Grid g;
+    const uint8_t* cellmap;
+    unsigned long long* rho;       // base of [nsp][N]
+    long long N;
+    AbsorbList ab;
+    DevScalars* sc;
+    uint64_t seed;
+    int fused;                     // 1: move, absorb-check and deposit now
+};
+
+// Finishes a newly created particle: in the fused step it is moved (emission
+// only), checked against the bodies and deposited; it is then appended.
+__device__ void finish_source(const SourceArgs& a, int s, double x, double y, double z, double vx, double vy,
+                              double vz, bool move, bool want) {
+    bool live = want;
+    int i = 0, j = 0, k = 0;
+    float ox = 0.f, oy = 0.f, oz = 0.f;
+    if (live && a.fused && move) {
+        x += vx; y += vy; z += vz;
+        live = axis_boundary_d(a.g, 0, x) && axis_boundary_d(a.g, 1, y) && axis_boundary_d(a.g, 2, z);
+    }
+    if (live) {
+        split(x, i, ox); split(y, j, oy); split(z, k, oz);
+        if (!cell_in_range(a.g, i, j, k)) { live = false; atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_NONFINITE); }
+    }
+    bool absorbed = false;
+    if (live && a.fused && a.cellmap) absorbed = a.cellmap[lin(a.g, i, j, k)] != 0;
+    if (absorbed) {
+        const unsigned long long slot = atomicAdd(&a.sc->absorbed_n, 1ull);
+        if ((long long)slot < a.ab.cap) {
+            a.ab.cell[slot] = pack_cell(i, j, k);
+            a.ab.ox[slot] = ox; a.ab.oy[slot] = oy; a.ab.oz[slot] = oz;
+            a.ab.vx[slot] = (float)vx; a.ab.vy[slot] = (float)vy; a.ab.vz[slot] = (float)vz;
+            a.ab.species[slot] = (uint8_t)s;
+            a.ab.object[slot] = (uint8_t)(a.cellmap[lin(a.g, i, j, k)] - 1);
+        } else {
+            atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_ABSORB_OVERFLOW);
+        }
+        live = false;
+    }
+    if (!live) return;
+    if (a.fused) {
+        unsigned long long w[8];
+        corner_weights(ox, oy, oz, w);
+        unsigned long long* rho = a.rho + (long long)s * a.N;
+        const long long b = lin(a.g, i, j, k);
+#pragma unroll
+        for (int t = 0; t < 8; ++t) if (w[t]) atomicAdd(rho + b + corner_offset(a.g, t), w[t]);
+        const float fx = (float)vx, fy = (float)vy, fz = (float)vz;
+        atomicAdd(&a.sc->energy[s], (double)fx * fx + (double)fy * fy + (double)fz * fz);
+    }
+    const unsigned long long slot = atomicAdd(&a.sc->count[s], 1ull);
+    if ((long long)slot < a.cap[s]) store_split(a.p[s], (long long)slot, i, j, k, ox, oy, oz, vx, vy, vz);
+    else atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_PARTICLE_OVERFLOW);
+}
+
+// ------------------------------------------------------------------ injection
+struct InjectTable {
+    int n;                         // batches
+    int species[FOPIS_MAX_SPECIES * 6];
+    int face[FOPIS_MAX_SPECIES * 6];
+    long long start[FOPIS_MAX_SPECIES * 6 + 1];
+    double vth[FOPIS_MAX_SPECIES * 6], dev[FOPIS_MAX_SPECIES * 6];
+    double drift[FOPIS_MAX_SPECIES * 6][3];
+    double maxe[3];                // RootGrid max_x/y/z (RootGridParticle.cpp:196-203)
+    long long step;
+};
+
+// One injected particle: AmbientParticleType::generateNewInjectionVelocity
+// (AmbientParticleType.cpp:101-157, rejection redrawing all three components)
+// and generateNewParticle with the slab ranges of
+// RootGrid::injectParticlesFromBoundary (RootGridParticle.cpp:212-302).
+__global__ void inject_kernel(SourceArgs a, InjectTable tb) {
+    const long long total = tb.start[tb.n];
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        int b = 0;
+        while (b + 1 < tb.n && tb.start[b + 1] <= t) ++b;
+        const uint32_t idx = (uint32_t)(t - tb.start[b]);
+        const int s = tb.species[b], face = tb.face[b], axis = face >> 1;
+        const double sign = (face & 1) ? -1.0 : 1.0;
+        const uint32_t cc = (uint32_t)s | ((uint32_t)face << 8), dtag = TAG_INJECT << 24;
+        double v[3] = {0, 0, 0};
+        int attempt = 0;
+        for (; attempt < 256; ++attempt) {
+            const U2 r0 = draw2(a.seed, idx, (uint32_t)tb.step, cc, dtag | (uint32_t)(2 * attempt));
+            const U2 r1 = draw2(a.seed, idx, (uint32_t)tb.step, cc, dtag | (uint32_t)(2 * attempt + 1));
+            double n0, n1, n2, n3;
+            box_muller(r0.a, r0.b, n0, n1);
+            box_muller(r1.a, r1.b, n2, n3);
+            const double nn[3] = {n0, n1, n2};
+#pragma unroll
+            for (int c = 0; c < 3; ++c) v[c] = tb.drift[b][c] + (c == axis ? tb.vth[b] : tb.dev[b]) * nn[c];
+            if (!((v[axis] * sign) < 0.0)) break;
+        }
+        if (attempt == 256) atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_INJECT_REJECTS);
+        const U2 q0 = draw2(a.seed, idx, (uint32_t)tb.step, cc, dtag | 0xFFF0u);
+        const U2 q1 = draw2(a.seed, idx, (uint32_t)tb.step, cc, dtag | 0xFFF1u);
+        const double u[3] = {q0.a, q0.b, q1.a};
+        double lo[3] = {0, 0, 0}, hi[3] = {tb.maxe[0], tb.maxe[1], tb.maxe[2]};
+        if ((face & 1) == 0) hi[axis] = v[axis];
+        else lo[axis] = tb.maxe[axis] + v[axis];
+        double x[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) x[c] = lo[c] + (hi[c] - lo[c]) * u[c];
+        finish_source(a, s, x[0], x[1], x[2], v[0], v[1], v[2], false, true);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.sc->injected, (unsigned long long)total);
+}
+
+// ------------------------------------------------------------------ emission
+struct EmitArgs {
+    int obj, s, K, eaxis;
+    double ev[3];
+    double vth;
+    int n_lit;
+    const int32_t* lit;          // cmat numbers
+    const int32_t* lit_ijk;      // packed node of each lit cmat
+    const int32_t* node_cmat;
+    long long* charge_tmp;       // this object's [nsp][n_cmat]
+    int n_cmat;
+    long long step;
+};
+
+__device__ __forceinline__ long long qsurf(double d) {
+    long long q = __double2ll_rn(d * kSurfaceScale);
+    return q < 0 ? 0 : (q > kSurfaceOne ? kSurfaceOne : q);
+}
+
+// Looks up the cmat number of node (i,j,k) for object obj; -1 when absent.
+__device__ __forceinline__ int cmat_of(const Grid& g, const int32_t* node_cmat, int obj, int i, int j, int k) {
+    if (i < 0 || j < 0 || k < 0 || i >= g.cx || j >= g.cy || k >= g.cz) return -1;
+    const int32_t v = node_cmat[lin(g, i, j, k)];
+    if (v < 0 || (v >> 24) != obj) return -1;
+    return v & 0xFFFFFF;
+}
+
+// Fixed-point bilinear surface charge of Spacecraft::distributeInnerParticle
+// ChargeTo{X,Y,Z}surface / subtractChargeOfParticleFrom{X,Y,Z}surface
+// (Spacecraft.cpp:594-613, :945-970): in-face coordinates rounded to 20 bits,
+// four weights summing to 2^40, signed by add (+1 absorb, -1 emit).
+__device__ bool surface_charge(const Grid& g, const int32_t* node_cmat, int obj, long long* tmp, int axis, int pi,
+                               int pj, int pk, double d1a, double d1b, long long sign) {
+    const long long qa = qsurf(d1a), qb = qsurf(d1b);
+    const long long wa[2] = {kSurfaceOne - qa, qa}, wb[2] = {kSurfaceOne - qb, qb};
+    int nodes[4];
+    // corner order (a,b) = 00, 10, 01, 11 as the reference lists them
+    const int da[4] = {0, 1, 0, 1}, db[4] = {0, 0, 1, 1};
+    for (int t = 0; t < 4; ++t) {
+        int ii = pi, jj = pj, kk = pk;
+        if (axis == 0) { jj += da[t]; kk += db[t]; }
+        else if (axis == 1) { ii += da[t]; kk += db[t]; }
+        else { ii += da[t]; jj += db[t]; }
+        nodes[t] = cmat_of(g, node_cmat, obj, ii, jj, kk);
+        if (nodes[t] < 0) return false;
+    }
+    for (int t = 0; t < 4; ++t) {
+        const long long w = wa[da[t]] * wb[db[t]] * sign;
+        if (w) atomicAdd((unsigned long long*)(tmp + nodes[t]), (unsigned long long)w);
+    }
+    return true;
+}
+
+// One photoelectron per thread: PhotoElectronParticleType::generateNewParticle
+// (PhotoElectronParticleType.cpp:9-101) at a lit node of the emitting face,
+// its charge taken off the surface at its next crossing point
+// (Spacecraft::emitParticles, Spacecraft.cpp:882-899).
+__global__ void emit_kernel(SourceArgs a, EmitArgs e) {
+    const long long total = (long long)e.n_lit * e.K;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const int node = (int)(t / e.K);
+        const uint32_t m = (uint32_t)(t % e.K);
+        const int cm = e.lit[node];
+        int ni, nj, nk;
+        unpack_cell(e.lit_ijk[node], ni, nj, nk);
+        const double rel[3] = {(double)(ni - 1), (double)(nj - 1), (double)(nk - 1)};
+        const uint32_t cc = (uint32_t)e.s | ((uint32_t)cm << 8), dtag = TAG_EMIT << 24;
+        const U2 r0 = draw2(a.seed, m, (uint32_t)e.step, cc, dtag | 0);
+        const U2 r1 = draw2(a.seed, m, (uint32_t)e.step, cc, dtag | 1);
+        const U2 r2 = draw2(a.seed, m, (uint32_t)e.step, cc, dtag | 2);
+        const double dep = asin(2.0 * r0.a - 1.0);
+        const double az = 2.0 * 3.14159265358979323846 * r0.b;
+        const double cd = cos(dep), sd = sin(dep), ca = cos(az), sa = sin(az);
+        double v[3];
+        if (e.eaxis == 0) { v[0] = e.vth * cd * e.ev[0]; v[1] = e.vth * sd * ca; v[2] = e.vth * sd * sa; }
+        else if (e.eaxis == 1) { v[0] = e.vth * sd * sa; v[1] = e.vth * cd * e.ev[1]; v[2] = e.vth * sd * ca; }
+        else { v[0] = e.vth * sd * ca; v[1] = e.vth * sd * sa; v[2] = e.vth * cd * e.ev[2]; }
+        const double tw = r1.a;
+        double x[3] = {rel[0] + (tw - 1.0) * v[0], rel[1] + (tw - 1.0) * v[1], rel[2] + (tw - 1.0) * v[2]};
+        if (e.eaxis == 0) { x[1] += r1.b; x[2] += r2.a; }
+        else if (e.eaxis == 1) { x[0] += r1.b; x[2] += r2.a; }
+        else { x[0] += r1.b; x[1] += r2.a; }
+        // Particle::getNext{X,Y,Z}CrossPoint (src/Particle/particle.cpp:206-255)
+        double cp[3] = {x[0], x[1], x[2]};
+        const int ax = e.eaxis;
+        const double fl = floor(x[ax]);
+        const double d1 = x[ax] - fl, d2 = 1.0 - d1;
+        if (v[ax] > 0.0) {
+            const double mv = d2 / v[ax];
+            for (int c = 0; c < 3; ++c) cp[c] = (c == ax) ? ceil(x[c]) : x[c] + v[c] * mv;
+        } else if (v[ax] < 0.0) {
+            const double mv = d1 / (-v[ax]);
+            for (int c = 0; c < 3; ++c) cp[c] = (c == ax) ? floor(x[c]) : x[c] + v[c] * mv;
+        }
+        const double f0 = floor(cp[0]), f1 = floor(cp[1]), f2 = floor(cp[2]);
+        const int pi = (int)f0 + 1, pj = (int)f1 + 1, pk = (int)f2 + 1;
+        const double dd[3] = {cp[0] - f0, cp[1] - f1, cp[2] - f2};
+        const int oa = ax == 0 ? 1 : 0, ob = ax == 2 ? 1 : 2;
+        long long* tmp = e.charge_tmp + (long long)e.s * e.n_cmat;
+        if (!surface_charge(a.g, e.node_cmat, e.obj, tmp, ax, pi, pj, pk, dd[oa], dd[ob], -1))
+            atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_BAD_CMAT_NODE);
+        atomicAdd(&a.sc->emitted_by[e.obj][e.s], 1ull);
+        finish_source(a, e.s, x[0], x[1], x[2], v[0], v[1], v[2], true, true);
+    }
+}
+
+// ------------------------------------------------------------------ absorption
+struct AbsorbArgs {
+    AbsorbList ab;
+    Grid g;
+    const uint8_t* cellmap;
+    const int32_t* node_cmat;
+    long long* charge_tmp[FOPIS_MAX_OBJECTS];
+    int n_cmat[FOPIS_MAX_OBJECTS];
+    DevScalars* sc;
+};
+
+struct DPos {  // Position in FP64 (include/position.hpp)
+    int i, j, k;
+    double d1[3];
+    __device__ void set(double x, double y, double z) {
+        const double f0 = floor(x), f1 = floor(y), f2 = floor(z);
+        i = (int)f0 + 1; j = (int)f1 + 1; k = (int)f2 + 1;
+        d1[0] = x - f0; d1[1] = y - f1; d1[2] = z - f2;
+    }
+};
+
+__device__ __forceinline__ bool valid_cell(const Grid& g, int i, int j, int k) {
+    return i >= 0 && i < g.n[0] + 1 && j >= 0 && j < g.n[1] + 1 && k >= 0 && k < g.n[2] + 1;
+}
+__device__ __forceinline__ bool cell_in(const AbsorbArgs& a, int obj, int i, int j, int k) {
+    if (!valid_cell(a.g, i, j, k)) return false;
+    return a.cellmap[lin(a.g, i, j, k)] == obj + 1;
+}
+
+// Spacecraft::is{X,Y,Z}surfacePoint (Spacecraft.cpp:462-506) for axis ax.
+__device__ bool surface_point(const AbsorbArgs& a, int obj, const DPos& p, int ax, int sign) {
+    if (p.d1[ax] >= 1e-10) return false;
+    int di = 0, dj = 0, dk = 0;
+    if (ax == 0) di = 1; else if (ax == 1) dj = 1; else dk = 1;
+    if (valid_cell(a.g, p.i, p.j, p.k) && valid_cell(a.g, p.i - di, p.j - dj, p.k - dk)) {
+        const bool here = cell_in(a, obj, p.i, p.j, p.k), below = cell_in(a, obj, p.i - di, p.j - dj, p.k - dk);
+        return sign > 0 ? (here && !below) : (!here && below);
+    }
+    const int oa[3][3] = {{0, 1, 0}, {1, 0, 0}, {1, 0, 0}};
+    const int ob[3][3] = {{0, 0, 1}, {0, 0, 1}, {0, 1, 0}};
+    for (int t = 0; t < 4; ++t) {
+        const int ii = p.i + ((t & 1) ? oa[ax][0] : 0) + ((t & 2) ? ob[ax][0] : 0);
+        const int jj = p.j + ((t & 1) ? oa[ax][1] : 0) + ((t & 2) ? ob[ax][1] : 0);
+        const int kk = p.k + ((t & 1) ? oa[ax][2] : 0) + ((t & 2) ? ob[ax][2] : 0);
+        if (cmat_of(a.g, a.node_cmat, obj, ii, jj, kk) < 0) return false;
+    }
+    return true;
+}
+
+// Particle::get{X,Y,Z}MoveRatio (src/Particle/particle.cpp:46-80).
+__device__ __forceinline__ double move_ratio(double d1, double v) {
+    if (v == 0.0) return 0.0;
+    return v > 0.0 ? d1 / fabs(v) : (1.0 - d1) / fabs(v);
+}
+
+// Absorbed particle: Particle::computeCrossPoints (particle.cpp:82-204, with the
+// xz-case comparison `mvx <= mvx` that always puts x first) and the first
+// crossing that is a body face (Spacecraft::distributeInnerParticleCharge,
+// Spacecraft.cpp:556-591).
+__global__ void absorb_kernel(AbsorbArgs a) {
+    const long long n = (long long)min(a.sc->absorbed_n, (unsigned long long)a.ab.cap);
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int s = a.ab.species[t], obj = a.ab.object[t];
+        int ci, cj, ck;
+        unpack_cell(a.ab.cell[t], ci, cj, ck);
+        const double x = (ci - 1) + (double)a.ab.ox[t], y = (cj - 1) + (double)a.ab.oy[t], z = (ck - 1) + (double)a.ab.oz[t];
+        const double vx = a.ab.vx[t], vy = a.ab.vy[t], vz = a.ab.vz[t];
+        DPos pos, old;
+        pos.set(x, y, z);
+        old.set(x - vx, y - vy, z - vz);
+        const double ox_[3] = {x - vx, y - vy, z - vz};
+        const double v[3] = {vx, vy, vz};
+        const double mv[3] = {1.0 - move_ratio(pos.d1[0], vx), 1.0 - move_ratio(pos.d1[1], vy), 1.0 - move_ratio(pos.d1[2], vz)};
+        const bool mvd[3] = {pos.i != old.i, pos.j != old.j, pos.k != old.k};
+        DPos cps[3];
+        auto cross = [&](int ax) {
+            double c[3];
+            for (int q = 0; q < 3; ++q)
+                c[q] = (q == ax) ? (v[ax] > 0.0 ? ceil(ox_[q]) : floor(ox_[q])) : ox_[q] + v[q] * mv[ax];
+            DPos r;
+            r.set(c[0], c[1], c[2]);
+            return r;
+        };
+        int order[3], cnt = 0;
+        const int count = (int)mvd[0] + (int)mvd[1] + (int)mvd[2];
+        const double mvx = mv[0], mvy = mv[1], mvz = mv[2];
+        if (count == 3) {
+            if (mvx <= mvy) {
+                if (mvx <= mvz) { order[0] = 0; if (mvy <= mvz) { order[1] = 1; order[2] = 2; } else { order[1] = 2; order[2] = 1; } }
+                else { order[0] = 2; order[1] = 0; order[2] = 1; }
+            } else {
+                if (mvy <= mvz) { order[0] = 1; if (mvx <= mvz) { order[1] = 0; order[2] = 2; } else { order[1] = 2; order[2] = 0; } }
+                else { order[0] = 2; order[1] = 1; order[2] = 0; }
+            }
+            cnt = 3;
+        } else if (count == 2) {
+            if (mvd[0] && mvd[1]) { if (mvx <= mvy) { order[0] = 0; order[1] = 1; } else { order[0] = 1; order[1] = 0; } }
+            else if (mvd[0]) { order[0] = 0; order[1] = 2; }
+            else { if (mvy <= mvz) { order[0] = 1; order[1] = 2; } else { order[0] = 2; order[1] = 1; } }
+            cnt = 2;
+        } else if (count == 1) {
+            order[0] = mvd[0] ? 0 : (mvd[1] ? 1 : 2);
+            cnt = 1;
+        }
+        for (int q = 0; q < cnt; ++q) cps[q] = cross(order[q]);
+        const int sgn[3] = {vx > 0.0 ? 1 : -1, vy > 0.0 ? 1 : -1, vz > 0.0 ? 1 : -1};
+        bool found = false;
+        long long* tmp = a.charge_tmp[obj] + (long long)s * a.n_cmat[obj];
+        for (int q = 0; q < cnt && !found; ++q) {
+            const DPos& cp = cps[q];
+            for (int ax = 0; ax < 3 && !found; ++ax) {
+                if (surface_point(a, obj, cp, ax, sgn[ax])) {
+                    const int oa = ax == 0 ? 1 : 0, ob = ax == 2 ? 1 : 2;
+                    if (!surface_charge(a.g, a.node_cmat, obj, tmp, ax, cp.i, cp.j, cp.k, cp.d1[oa], cp.d1[ob], 1))
+                        atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_BAD_CMAT_NODE);
+                    found = true;
+                }
+            }
+        }
+        if (!found) { atomicAdd(&a.sc->not_found, 1ull); atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_SURFACE_NOT_FOUND); }
+        atomicAdd(&a.sc->absorbed_by[obj][s], 1ull);
+    }
+}
+
+// ------------------------------------------------------------------ loading
+struct AmbientArgs {
+    Soa p;
+    long long cap;
+    int s;
+    long long total;
+    double maxe[3];
+    double drift[3], dev;
+    uint64_t seed;
+    Grid g;
+    const uint8_t* cellmap;
+    DevScalars* sc;
+};
+
+// RootGrid::RootGrid uniform loading (RootGrid.cpp:59-79): positions uniform in
+// [0,max), velocities Maxwellian about the drift, particles inside a body
+// dropped (Spacecraft::removeInnerParticle, Spacecraft.cpp:508-510).
+__global__ void ambient_kernel(AmbientArgs a) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < a.total; base += stride) {
+        const long long t = base + (threadIdx.x & 31);
+        bool keep = t < a.total;
+        int i = 0, j = 0, k = 0;
+        float ox = 0, oy = 0, oz = 0;
+        double vx = 0, vy = 0, vz = 0;
+        if (keep) {
+            const uint32_t c0 = (uint32_t)t, c1 = (uint32_t)(t >> 32), c2 = (uint32_t)a.s, dt = TAG_LOAD << 24;
+            const U2 r0 = draw2(a.seed, c0, c1, c2, dt | 0), r1 = draw2(a.seed, c0, c1, c2, dt | 1);
+            const U2 r2 = draw2(a.seed, c0, c1, c2, dt | 2), r3 = draw2(a.seed, c0, c1, c2, dt | 3);
+            const double x = a.maxe[0] * r0.a, y = a.maxe[1] * r0.b, z = a.maxe[2] * r1.a;
+            double n0, n1, n2, n3;
+            box_muller(r1.b, r2.a, n0, n1);
+            box_muller(r2.b, r3.a, n2, n3);
+            vx = a.drift[0] + a.dev * n0; vy = a.drift[1] + a.dev * n1; vz = a.drift[2] + a.dev * n2;
+            split(x, i, ox); split(y, j, oy); split(z, k, oz);
+            if (a.cellmap && valid_cell(a.g, i, j, k) && a.cellmap[lin(a.g, i, j, k)]) keep = false;
+        }
+        const unsigned long long slot = warp_reserve(&a.sc->count[a.s], keep);
+        if (keep) {
+            if ((long long)slot < a.cap) store_split(a.p, (long long)slot, i, j, k, ox, oy, oz, vx, vy, vz);
+            else atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_PARTICLE_OVERFLOW);
+        }
+    }
+}
+
+struct Rec56 { double x, y, z, vx, vy, vz; int typeId, isValid; };
+
+__global__ void load56_kernel(Soa p, long long cap, unsigned long long* count, const Rec56* in, long long n, Grid g,
+                              DevScalars* sc) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        const long long t = base + (threadIdx.x & 31);
+        bool keep = t < n && in[t].isValid;
+        int i = 0, j = 0, k = 0;
+        float ox = 0, oy = 0, oz = 0;
+        if (keep) {
+            split(in[t].x, i, ox); split(in[t].y, j, oy); split(in[t].z, k, oz);
+            if (!cell_in_range(g, i, j, k)) { keep = false; atomicOr(&sc->status, (unsigned)FOPIS_DEV_NONFINITE); }
+        }
+        const unsigned long long slot = warp_reserve(count, keep);
+        if (keep) {
+            if ((long long)slot < cap) store_split(p, (long long)slot, i, j, k, ox, oy, oz, in[t].vx, in[t].vy, in[t].vz);
+            else atomicOr(&sc->status, (unsigned)FOPIS_DEV_PARTICLE_OVERFLOW);
+        }
+    }
+}
+
+// Compacts the valid particles of [lo, hi) into AoS56 records or raw arrays.
+__global__ void export_kernel(Soa p, long long lo, long long hi, int s, Rec56* out56, Soa raw,
+                              unsigned long long* counter) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = lo + (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < hi; base += stride) {
+        const long long t = base + (threadIdx.x & 31);
+        const int32_t c = t < hi ? p.cell[t] : -1;
+        const bool keep = c >= 0;
+        const unsigned long long slot = warp_reserve(counter, keep);
+        if (!keep) continue;
+        if (out56) {
+            int i, j, k;
+            unpack_cell(c, i, j, k);
+            Rec56 r;
+            r.x = (i - 1) + (double)p.ox[t]; r.y = (j - 1) + (double)p.oy[t]; r.z = (k - 1) + (double)p.oz[t];
+            r.vx = p.vx[t]; r.vy = p.vy[t]; r.vz = p.vz[t];
+            r.typeId = s; r.isValid = 1;
+            out56[slot] = r;
+        } else {
+            raw.cell[slot] = c;
+            raw.ox[slot] = p.ox[t]; raw.oy[slot] = p.oy[t]; raw.oz[slot] = p.oz[t];
+            raw.vx[slot] = p.vx[t]; raw.vy[slot] = p.vy[t]; raw.vz[slot] = p.vz[t];
+        }
+    }
+}
+
+__global__ void energy_kernel(Soa p, long long cap, const unsigned long long* count, double* out) {
+    const long long n = (long long)min(*count, (unsigned long long)cap);
+    double e = 0.0;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        if (p.cell[t] >= 0) e += (double)p.vx[t] * p.vx[t] + (double)p.vy[t] * p.vy[t] + (double)p.vz[t] * p.vz[t];
+    e = block_sum(e);
+    if (threadIdx.x == 0 && e != 0.0) atomicAdd(out, e);
+}
+
+// ------------------------------------------------------------------ counting sort
+__global__ void sort_count_kernel(Soa p, long long cap, const unsigned long long* count, Grid g, int32_t* cnt) {
+    const long long n = (long long)min(*count, (unsigned long long)cap);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        const long long t = base + (threadIdx.x & 31);
+        const int32_t c = t < n ? p.cell[t] : -1;
+        long long key = -1 - (long long)(threadIdx.x & 31);
+        if (c >= 0) { int i, j, k; unpack_cell(c, i, j, k); key = lin(g, i, j, k); }
+        const unsigned grp = __match_any_sync(kFull, key);
+        const int lane = threadIdx.x & 31;
+        if (c >= 0 && (__ffs(grp) - 1) == lane) atomicAdd(cnt + key, __popc(grp));
+    }
+}
+
+// Exclusive scan of n int32 values in three passes (block sums, a single-block
+// scan of the sums, block rescans).
+constexpr int kScanThreads = 1024, kScanItems = 8, kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* total) {
+    __shared__ int ws[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) { const int y = __shfl_up_sync(kFull, x, o); if (lane >= o) x += y; }
+    if (lane == 31) ws[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int s = lane < (int)(blockDim.x >> 5) ? ws[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) { const int y = __shfl_up_sync(kFull, s, o); if (lane >= o) s += y; }
+        ws[lane] = s;
+    }
+    __syncthreads();
+    const int pre = (w ? ws[w - 1] : 0) + x - v;
+    *total = ws[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return pre;
+}
+
+__global__ void scan_tiles_kernel(const int32_t* in, long long n, int32_t* partial) {
+    const long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
+    int s = 0;
+    for (int q = 0; q < kScanItems; ++q) if (base + q < n) s += in[base + q];
+    int tot;
+    block_exclusive_scan(s, &tot);
+    if (threadIdx.x == 0) partial[blockIdx.x] = tot;
+}
+__global__ void scan_partials_kernel(int32_t* partial, int np) {
+    int carry = 0;
+    for (int b0 = 0; b0 < np; b0 += blockDim.x) {
+        const int t = b0 + threadIdx.x;
+        const int v = t < np ? partial[t] : 0;
+        int tot;
+        const int pre = block_exclusive_scan(v, &tot);
+        if (t < np) partial[t] = carry + pre;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) partial[np] = carry;
+}
+__global__ void scan_apply_kernel(const int32_t* in, long long n, const int32_t* partial, int32_t* out) {
+    const long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
+    int v[kScanItems], s = 0;
+    for (int q = 0; q < kScanItems; ++q) { v[q] = (base + q < n) ? in[base + q] : 0; s += v[q]; }
+    int tot;
+    int pre = block_exclusive_scan(s, &tot) + partial[blockIdx.x];
+    for (int q = 0; q < kScanItems; ++q) { if (base + q < n) out[base + q] = pre; pre += v[q]; }
+}
+
+__global__ void sort_scatter_kernel(Soa src, Soa dst, long long cap, const unsigned long long* count, Grid g,
+                                    int32_t* cursor) {
+    const long long n = (long long)min(*count, (unsigned long long)cap);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        const long long t = base + lane;
+        const int32_t c = t < n ? src.cell[t] : -1;
+        long long key = -1 - lane;
+        if (c >= 0) { int i, j, k; unpack_cell(c, i, j, k); key = lin(g, i, j, k); }
+        const unsigned grp = __match_any_sync(kFull, key);
+        const int leader = __ffs(grp) - 1;
+        int b = 0;
+        if (c >= 0 && leader == lane) b = atomicAdd(cursor + key, __popc(grp));
+        b = __shfl_sync(kFull, b, leader);
+        if (c < 0) continue;
+        const long long d = (long long)b + __popc(grp & ((1u << lane) - 1u));
+        dst.cell[d] = c;
+        dst.ox[d] = src.ox[t]; dst.oy[d] = src.oy[t]; dst.oz[d] = src.oz[t];
+        dst.vx[d] = src.vx[t]; dst.vy[d] = src.vy[t]; dst.vz[d] = src.vz[t];
+    }
+}
+
+int grid_for(long long n, int threads = kThreads) {
+    const long long b = (n + threads - 1) / threads;
+    return (int)std::max<long long>(1, std::min<long long>(b, 148LL * 16));
+}
+
+void alloc_soa(Soa& s, int64_t cap) {
+    FOPIS_CUDA(cudaMalloc(&s.cell, sizeof(int32_t) * cap));
+    float** f[6] = {&s.ox, &s.oy, &s.oz, &s.vx, &s.vy, &s.vz};
+    for (auto* q : f) FOPIS_CUDA(cudaMalloc(q, sizeof(float) * cap));
+}
+void free_soa(Soa& s) {
+    cudaFree(s.cell);
+    float* f[6] = {s.ox, s.oy, s.oz, s.vx, s.vy, s.vz};
+    for (auto* q : f) cudaFree(q);
+    s = Soa{};
+}
+void copy_soa(Soa& d, const Soa& s, int64_t n, cudaStream_t st) {
+    if (n <= 0) return;
+    FOPIS_CUDA(cudaMemcpyAsync(d.cell, s.cell, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st));
+    float* df[6] = {d.ox, d.oy, d.oz, d.vx, d.vy, d.vz};
+    float* sf[6] = {s.ox, s.oy, s.oz, s.vx, s.vy, s.vz};
+    for (int t = 0; t < 6; ++t) FOPIS_CUDA(cudaMemcpyAsync(df[t], sf[t], sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+}
+
+}  // namespace
+
+// Makes sure species s can hold at least `need` slots (grows both buffers).
+void particles_alloc(Ctx& c, int s, int64_t need) {
+    if (need <= c.cap[s]) return;
+    int64_t cap = std::max<int64_t>(need, 1024);
+    Soa a{}, b{};
+    alloc_soa(a, cap);
+    alloc_soa(b, cap);
+    FOPIS_CUDA(cudaMemsetAsync(a.cell, 0xff, sizeof(int32_t) * cap, c.st));
+    if (c.cap[s] > 0) {
+        sync_scalars(c);
+        copy_soa(a, c.sp[s], std::min<int64_t>(c.nslots[s], c.cap[s]), c.st);
+        FOPIS_CUDA(cudaStreamSynchronize(c.st));
+        free_soa(c.sp[s]);
+        free_soa(c.sp2[s]);
+    }
+    c.sp[s] = a;
+    c.sp2[s] = b;
+    c.cap[s] = cap;
+}
+
+void sync_scalars(Ctx& c) {
+    FOPIS_CUDA(cudaMemcpyAsync(c.h_sc, c.d_sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, c.st));
+    FOPIS_CUDA(cudaStreamSynchronize(c.st));
+    for (int s = 0; s < c.nsp; ++s) c.nslots[s] = (int64_t)std::min<unsigned long long>(c.h_sc->count[s], (unsigned long long)c.cap[s]);
+}
+
+void particles_append_aos(Ctx& c, int s, const void* host56, int64_t n) {
+    sync_scalars(c);
+    particles_alloc(c, s, (int64_t)((c.nslots[s] + n) * std::max(1.0, c.p.capacity_factor)) + 4096);
+    const int64_t chunk = 1 << 20;
+    Rec56* d = nullptr;
+    FOPIS_CUDA(cudaMalloc(&d, sizeof(Rec56) * chunk));
+    const Grid g = make_grid(c);
+    for (int64_t off = 0; off < n; off += chunk) {
+        const int64_t m = std::min(chunk, n - off);
+        FOPIS_CUDA(cudaMemcpyAsync(d, (const char*)host56 + 56 * off, 56 * m, cudaMemcpyHostToDevice, c.st));
+        ++c.launches;
+        load56_kernel<<<grid_for(m), kThreads, 0, c.st>>>(c.sp[s], c.cap[s], &c.d_sc->count[s], d, m, g, c.d_sc);
+        FOPIS_LAUNCH_CHECK();
+    }
+    FOPIS_CUDA(cudaStreamSynchronize(c.st));
+    cudaFree(d);
+    sync_scalars(c);
+}
+
+static int64_t export_range(Ctx& c, int s, Rec56* d56, Soa* raw, int64_t lo, int64_t hi, unsigned long long* dcount) {
+    FOPIS_CUDA(cudaMemsetAsync(dcount, 0, sizeof(unsigned long long), c.st));
+    ++c.launches;
+    export_kernel<<<grid_for(hi - lo), kThreads, 0, c.st>>>(c.sp[s], lo, hi, s, d56, raw ? *raw : Soa{}, dcount);
+    FOPIS_LAUNCH_CHECK();
+    unsigned long long k = 0;
+    FOPIS_CUDA(cudaMemcpyAsync(&k, dcount, sizeof(k), cudaMemcpyDeviceToHost, c.st));
+    FOPIS_CUDA(cudaStreamSynchronize(c.st));
+    return (int64_t)k;
+}
+
+int64_t particles_export_aos(Ctx& c, int s, void* host56, int64_t cap) {
+    sync_scalars(c);
+    const int64_t n = c.nslots[s];
+    const int64_t chunk = 1 << 20;
+    Rec56* d = nullptr;
+    unsigned long long* dc = nullptr;
+    FOPIS_CUDA(cudaMalloc(&d, sizeof(Rec56) * chunk));
+    FOPIS_CUDA(cudaMalloc(&dc, sizeof(unsigned long long)));
+    int64_t total = 0;
+    for (int64_t lo = 0; lo < n; lo += chunk) {
+        const int64_t hi = std::min(n, lo + chunk);
+        const int64_t k = export_range(c, s, d, nullptr, lo, hi, dc);
+        const int64_t w = std::max<int64_t>(0, std::min(k, cap - total));
+        if (w > 0) FOPIS_CUDA(cudaMemcpy((char*)host56 + 56 * total, d, 56 * w, cudaMemcpyDeviceToHost));
+        total += k;
+    }
+    cudaFree(d);
+    cudaFree(dc);
+    return total;
+}
+
+int64_t particles_export_raw(Ctx& c, int s, int32_t* cell, float* ox, float* oy, float* oz, float* vx, float* vy,
+                             float* vz, int64_t cap) {
+    sync_scalars(c);
+    const int64_t n = c.nslots[s];
+    const int64_t chunk = 1 << 20;
+    Soa raw{};
+    alloc_soa(raw, chunk);
+    unsigned long long* dc = nullptr;
+    FOPIS_CUDA(cudaMalloc(&dc, sizeof(unsigned long long)));
+    int64_t total = 0;
+    for (int64_t lo = 0; lo < n; lo += chunk) {
+        const int64_t hi = std::min(n, lo + chunk);
+        const int64_t k = export_range(c, s, nullptr, &raw, lo, hi, dc);
+        const int64_t w = std::max<int64_t>(0, std::min(k, cap - total));
+        if (w > 0) {
+            FOPIS_CUDA(cudaMemcpy(cell + total, raw.cell, 4 * w, cudaMemcpyDeviceToHost));
+            float* dst[6] = {ox, oy, oz, vx, vy, vz};
+            float* src[6] = {raw.ox, raw.oy, raw.oz, raw.vx, raw.vy, raw.vz};
+            for (int t = 0; t < 6; ++t) FOPIS_CUDA(cudaMemcpy(dst[t] + total, src[t], 4 * w, cudaMemcpyDeviceToHost));
+        }
+        total += k;
+    }
+    free_soa(raw);
+    cudaFree(dc);
+    return total;
+}
+
+static double max_extent(const Ctx& c, int axis) {
+    const int n = axis == 0 ? c.nx : (axis == 1 ? c.ny : c.nz);
+    return c.per[2 * axis + 1] ? (double)n : n - 1.0;
+}
+
+void particles_generate_ambient(Ctx& c) {
+    const Grid g = make_grid(c);
+    for (int s = 0; s < c.nsp; ++s) {
+        const fopis_species& sp = c.p.species[s];
+        if (sp.kind != FOPIS_SPECIES_AMBIENT) continue;
+        // ParticleType::getTotalNumber (ParticleType.cpp:39-47)
+        const int64_t cxn = c.per[1] ? c.nx : c.nx - 1, cyn = c.per[3] ? c.ny : c.ny - 1, czn = c.per[5] ? c.nz : c.nz - 1;
+        const int64_t total = cxn * cyn * czn * (int64_t)sp.particle_per_cell;
+        sync_scalars(c);
+        particles_alloc(c, s, (int64_t)((c.nslots[s] + total) * std::max(1.0, c.p.capacity_factor)) + 4096);
+        AmbientArgs a;
+        a.p = c.sp[s]; a.cap = c.cap[s]; a.s = s; a.total = total;
+        for (int q = 0; q < 3; ++q) { a.maxe[q] = max_extent(c, q); a.drift[q] = sp.drift[q]; }
+        a.dev = sp.deviation; a.seed = c.p.seed; a.g = g;
+        a.cellmap = c.objs.empty() ? nullptr : c.cellmap;
+        a.sc = c.d_sc;
+        ++c.launches;
+        ambient_kernel<<<grid_for(total), kThreads, 0, c.st>>>(a);
+        FOPIS_LAUNCH_CHECK();
+    }
+    sync_scalars(c);
+}
+
+void particles_sort(Ctx& c) {
+    sync_scalars(c);
+    const Grid g = make_grid(c);
+    const long long N = (long long)c.N;
+    const int tiles = (int)((N + kScanTile - 1) / kScanTile);
+    for (int s = 0; s < c.nsp; ++s) {
+        if (c.cap[s] == 0 || c.nslots[s] == 0) continue;
+        FOPIS_CUDA(cudaMemsetAsync(c.sort_count, 0, sizeof(int32_t) * (N + 1), c.st));
+        ++c.launches;
+        sort_count_kernel<<<grid_for(c.nslots[s]), kThreads, 0, c.st>>>(c.sp[s], c.cap[s], &c.d_sc->count[s], g,
+                                                                         c.sort_count);
+        FOPIS_LAUNCH_CHECK();
+        ++c.launches;
+        scan_tiles_kernel<<<tiles, kScanThreads, 0, c.st>>>(c.sort_count, N + 1, c.scan_partials);
+        ++c.launches;
+        scan_partials_kernel<<<1, kScanThreads, 0, c.st>>>(c.scan_partials, tiles);
+        ++c.launches;
+        scan_apply_kernel<<<tiles, kScanThreads, 0, c.st>>>(c.sort_count, N + 1, c.scan_partials, c.sort_offset);
+        FOPIS_LAUNCH_CHECK();
+        ++c.launches;
+        sort_scatter_kernel<<<grid_for(c.nslots[s]), kThreads, 0, c.st>>>(c.sp[s], c.sp2[s], c.cap[s],
+                                                                          &c.d_sc->count[s], g, c.sort_offset);
+        FOPIS_LAUNCH_CHECK();
+        // new count = total of valid particles = sort_offset[N] after the scatter
+        // cursors advanced; the exclusive scan's last entry holds the total.
+        FOPIS_CUDA(cudaMemcpyAsync(&c.d_sc->count[s], c.scan_partials + tiles, sizeof(int32_t), cudaMemcpyDeviceToDevice, c.st));
+        FOPIS_CUDA(cudaMemsetAsync(((char*)&c.d_sc->count[s]) + 4, 0, 4, c.st));
+        std::swap(c.sp[s], c.sp2[s]);
+        // invalidate the tail beyond the new count so stale slots never read as live
+    }
+    sync_scalars(c);
+    for (int s = 0; s < c.nsp; ++s) {
+        if (c.cap[s] == 0) continue;
+        const int64_t n = c.nslots[s];
+        if (n < c.cap[s]) FOPIS_CUDA(cudaMemsetAsync(c.sp[s].cell + n, 0xff, sizeof(int32_t) * (c.cap[s] - n), c.st));
+        // keep head room for the appends of the coming steps
+        const int64_t want = (int64_t)(n * 1.25) + 65536;
+        if (want > c.cap[s]) particles_alloc(c, s, (int64_t)(n * std::max(1.5, c.p.capacity_factor)) + 65536);
+    }
+}
+
+static PushArgs push_args(Ctx& c, int s) {
+    PushArgs a;
+    a.p = c.sp[s]; a.s = s; a.cap = c.cap[s]; a.count = &c.d_sc->count[s];
+    a.E = c.E; a.g = make_grid(c);
+    a.qm = (float)(0.5 * c.p.species[s].charge / c.p.species[s].mass);
+    a.bx = (float)c.p.static_bfield[0]; a.by = (float)c.p.static_bfield[1]; a.bz = (float)c.p.static_bfield[2];
+    const double b2 = c.p.static_bfield[0] * c.p.static_bfield[0] + c.p.static_bfield[1] * c.p.static_bfield[1] +
+                      c.p.static_bfield[2] * c.p.static_bfield[2];
+    a.boris = (float)(2.0 / (1.0 + b2));
+    a.cellmap = c.objs.empty() ? nullptr : c.cellmap;
+    a.rho = c.rho_i64 + (size_t)s * c.N;
+    a.ab = c.ab; a.sc = c.d_sc;
+    return a;
+}
+
+void launch_push(Ctx& c, bool vel, bool pos, bool dep) {
+    for (int s = 0; s < c.nsp; ++s) {
+        if (c.cap[s] == 0) continue;
+        PushArgs a = push_args(c, s);
+        const int grid = grid_for(c.cap[s]);
+        if (vel && pos && dep) { ++c.launches; push_kernel<true, true, true><<<grid, kThreads, 0, c.st>>>(a); }
+        else if (vel && !pos && !dep) { ++c.launches; push_kernel<true, false, false><<<grid, kThreads, 0, c.st>>>(a); }
+        else if (!vel && pos && !dep) { ++c.launches; push_kernel<false, true, false><<<grid, kThreads, 0, c.st>>>(a); }
+        else if (!vel && !pos && dep) { ++c.launches; push_kernel<false, false, true><<<grid, kThreads, 0, c.st>>>(a); }
+        else throw ApiError{FOPIS_ERR_ARG, "unsupported push combination"};
+        FOPIS_LAUNCH_CHECK();
+    }
+}
+
+void launch_deposit_all(Ctx& c) { launch_push(c, false, false, true); }
+
+static SourceArgs source_args(Ctx& c, bool fused) {
+    SourceArgs a;
+    for (int s = 0; s < FOPIS_MAX_SPECIES; ++s) { a.p[s] = c.sp[s]; a.cap[s] = c.cap[s]; }
+    a.g = make_grid(c);
+    a.cellmap = c.objs.empty() ? nullptr : c.cellmap;
+    a.rho = c.rho_i64; a.N = (long long)c.N; a.ab = c.ab; a.sc = c.d_sc; a.seed = c.p.seed;
+    a.fused = fused ? 1 : 0;
+    return a;
+}
+
+void launch_emit(Ctx& c, bool fused) {
+    int eaxis = -1;
+    for (int q = 0; q < 3; ++q) if (std::fabs(c.p.shine_vector[q]) == 1.0) { eaxis = q; break; }
+    for (size_t o = 0; o < c.objs.size(); ++o) {
+        ObjectDev& ob = c.objs[o];
+        const int s = ob.emit_species;
+        if (s < 0 || c.p.species[s].kind != FOPIS_SPECIES_PHOTOELECTRON || ob.n_lit == 0) continue;
+        if (eaxis < 0) throw ApiError{FOPIS_ERR_ARG, "shine_vector must be [+-1,0,0], [0,+-1,0] or [0,0,+-1]"};
+        const int K = (int)std::ceil(c.p.species[s].emission_amount);
+        if (K <= 0) continue;
+        const int64_t add = (int64_t)ob.n_lit * K;
+        sync_scalars(c);
+        if (c.nslots[s] + add > c.cap[s]) particles_alloc(c, s, (int64_t)((c.nslots[s] + add) * 1.5) + 65536);
+        SourceArgs a = source_args(c, fused);
+        EmitArgs e;
+        e.obj = (int)o; e.s = s; e.K = K; e.eaxis = eaxis;
+        for (int q = 0; q < 3; ++q) e.ev[q] = -c.p.shine_vector[q];
+        e.vth = c.p.species[s].thermal_velocity;
+        e.n_lit = ob.n_lit; e.lit = ob.lit; e.lit_ijk = ob.lit + ob.n_lit;
+        e.node_cmat = c.node_cmat; e.charge_tmp = ob.charge_tmp; e.n_cmat = ob.n; e.step = c.timestep;
+        ++c.launches;
+        emit_kernel<<<grid_for(add), kThreads, 0, c.st>>>(a, e);
+        FOPIS_LAUNCH_CHECK();
+    }
+}
+
+static int node_size(const Ctx& c, int axis) {
+    const int n = axis == 0 ? c.nx : (axis == 1 ? c.ny : c.nz);
+    return c.per[2 * axis + 1] ? n + 1 : n;
+}
+
+void launch_inject(Ctx& c, bool fused) {
+    InjectTable tb{};
+    tb.n = 0;
+    tb.start[0] = 0;
+    for (int q = 0; q < 3; ++q) tb.maxe[q] = max_extent(c, q);
+    tb.step = c.timestep;
+    int64_t need[FOPIS_MAX_SPECIES] = {0};
+    for (int s = 0; s < c.nsp; ++s) {
+        const fopis_species& sp = c.p.species[s];
+        if (sp.kind != FOPIS_SPECIES_AMBIENT) continue;
+        for (int face = 0; face < 6; ++face) {
+            const int axis = face / 2, side = face % 2;
+            if (c.per[2 * axis + side]) continue;
+            const int a1 = (axis + 1) % 3, a2 = (axis + 2) % 3;
+            const double area = (double)(node_size(c, a2) - 1) * (node_size(c, a1) - 1);
+            const double flux = sp.injection_axis[face] ? sp.flux[face] : 0.0;
+            const double nd = 1.0 * area * flux;
+            const int num = (int)std::floor(nd + c.inject_residual[s][face]);
+            c.inject_residual[s][face] += nd - num;
+            if (num <= 0) continue;
+            tb.species[tb.n] = s; tb.face[tb.n] = face;
+            tb.vth[tb.n] = sp.thermal_velocity; tb.dev[tb.n] = sp.deviation;
+            for (int q = 0; q < 3; ++q) tb.drift[tb.n][q] = sp.drift[q];
+            tb.start[tb.n + 1] = tb.start[tb.n] + num;
+            need[s] += num;
+            ++tb.n;
+        }
+    }
+    c.injected_step = tb.n ? tb.start[tb.n] : 0;
+    if (tb.n == 0) return;
+    bool grow = false;
+    for (int s = 0; s < c.nsp; ++s) if (need[s] && c.nslots[s] + need[s] > c.cap[s]) grow = true;
+    if (grow) {
+        sync_scalars(c);
+        for (int s = 0; s < c.nsp; ++s)
+            if (need[s] && c.nslots[s] + need[s] > c.cap[s]) particles_alloc(c, s, (int64_t)((c.nslots[s] + need[s]) * 1.5) + 65536);
+    }
+    SourceArgs a = source_args(c, fused);
+    ++c.launches;
+    inject_kernel<<<grid_for(tb.start[tb.n]), kThreads, 0, c.st>>>(a, tb);
+    FOPIS_LAUNCH_CHECK();
+}
+
+void launch_absorb(Ctx& c) {
+    if (c.objs.empty()) return;
+    AbsorbArgs a;
+    a.ab = c.ab; a.g = make_grid(c); a.cellmap = c.cellmap; a.node_cmat = c.node_cmat; a.sc = c.d_sc;
+    for (int o = 0; o < FOPIS_MAX_OBJECTS; ++o) { a.charge_tmp[o] = nullptr; a.n_cmat[o] = 0; }
+    for (size_t o = 0; o < c.objs.size(); ++o) { a.charge_tmp[o] = c.objs[o].charge_tmp; a.n_cmat[o] = c.objs[o].n; }
+    ++c.launches;
+    absorb_kernel<<<148 * 4, kThreads, 0, c.st>>>(a);
+    FOPIS_LAUNCH_CHECK();
+}
+
+void launch_energy(Ctx& c) {
+    FOPIS_CUDA(cudaMemsetAsync(c.d_sc->energy, 0, sizeof(double) * FOPIS_MAX_SPECIES, c.st));
+    for (int s = 0; s < c.nsp; ++s) {
+        if (c.cap[s] == 0) continue;
+        ++c.launches;
+        energy_kernel<<<grid_for(c.cap[s]), kThreads, 0, c.st>>>(c.sp[s], c.cap[s], &c.d_sc->count[s],
+                                                                  &c.d_sc->energy[s]);
+        FOPIS_LAUNCH_CHECK();
+    }
+}
+
+}  // namespace fopis

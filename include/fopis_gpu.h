@@ -1,0 +1,268 @@
+/*
+ * fopis_gpu.h — C ABI of libfopis_gpu.so, the B200 (sm_100a) electrostatic
+ * particle-in-cell timestep of FOPIS ("TDPIC").
+ *
+ * The reference has no plugin or FFI layer: its ES path is the RootGrid phase
+ * methods that RootGrid::mainLoopES calls in order (src/Grid/RootGrid/RootGrid.cpp:82-143)
+ * plus the start-up in Initializer::initTDPIC (src/Misc/Initialize.cpp:16-107).
+ * Each entry point below replaces one of those methods; the citation beside it
+ * names the reference function whose behaviour it keeps.
+ *
+ * Conventions (all inherited from the reference):
+ *   - Normalised units: length = dx, time = dt, mass = m_e, charge = e
+ *     (src/Misc/Initialize.cpp:33-36). Positions are in cells, velocities in
+ *     cells/step.
+ *   - Node arrays carry one glue layer: (nx+2)(ny+2)(nz+2) doubles in C order
+ *     [i][j][k], k fastest (src/Grid/Grid.cpp:148-196). A particle at x sits in
+ *     node cell i = floor(x)+1 (include/position.hpp:59-69).
+ *   - nx, ny, nz are the reference's node counts (Environment::nx). On a
+ *     Dirichlet/Neumann axis nx nodes span nx-1 cells; on a periodic axis nx
+ *     nodes span nx cells.
+ *   - boundary is the 6-letter string "x-x+y-y+z-z+" of D/N/P
+ *     (src/Misc/Environment.cpp:51-60).
+ *
+ * Every function returns 0 (FOPIS_OK) or a negative fopis_status. No C++
+ * exception crosses the ABI. A context is used by one host thread at a time;
+ * all of its work runs on its own CUDA stream. Host pointers are borrowed for
+ * the duration of the call only.
+ */
+#ifndef FOPIS_GPU_H
+#define FOPIS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FOPIS_MAX_SPECIES 8
+#define FOPIS_MAX_OBJECTS 8
+
+typedef enum fopis_status {
+    FOPIS_OK = 0,
+    FOPIS_ERR_ARG = -1,            /* bad argument (std::invalid_argument in the reference) */
+    FOPIS_ERR_CUDA = -2,           /* CUDA runtime error */
+    FOPIS_ERR_NOMEM = -3,          /* device allocation failed */
+    FOPIS_ERR_STATE = -4,          /* call out of order (e.g. step before load) */
+    FOPIS_ERR_NOT_CONVERGED = -5,  /* Poisson solve hit max_vcycles; phi kept */
+    FOPIS_ERR_DEVICE = -6,         /* a kernel latched an error bit in the device status word */
+    FOPIS_ERR_CAPACITY = -7,       /* particle / absorbed-list capacity exceeded */
+    FOPIS_ERR_NO_CUDA = -8         /* no usable CUDA device */
+} fopis_status;
+
+/* Device status bits (fopis_get_stats().device_status). */
+#define FOPIS_DEV_PARTICLE_OVERFLOW   0x1   /* appended particles exceeded capacity */
+#define FOPIS_DEV_ABSORB_OVERFLOW     0x2   /* absorbed list exceeded capacity */
+#define FOPIS_DEV_BAD_CMAT_NODE       0x4   /* absorption/emission hit a node that is not a surface node
+                                               (Spacecraft::getCmatNumber throws, Spacecraft.cpp:233-234) */
+#define FOPIS_DEV_SURFACE_NOT_FOUND   0x8   /* absorbed particle without a crossing face (Spacecraft.cpp:573-582) */
+#define FOPIS_DEV_INJECT_REJECTS      0x10  /* injection rejection sampling hit its attempt cap */
+#define FOPIS_DEV_NONFINITE           0x20  /* NaN/Inf met in a reduction */
+
+typedef enum fopis_species_kind {
+    FOPIS_SPECIES_AMBIENT = 0,        /* AmbientParticleType */
+    FOPIS_SPECIES_PHOTOELECTRON = 1   /* PhotoElectronParticleType */
+} fopis_species_kind;
+
+/* One particle species; fields mirror ParticleType (include/particle_type.hpp:13-120). */
+typedef struct fopis_species {
+    int kind;                   /* fopis_species_kind */
+    int particle_per_cell;      /* ParticleType::particle_per_cell */
+    double charge;              /* ParticleType::charge, in e */
+    double mass;                /* ParticleType::mass, in m_e */
+    double size;                /* ParticleType::size = int(dx^3 n / ppc) (ParticleType.cpp:33-36) */
+    double thermal_velocity;    /* calcThermalVelocity() = sqrt(2T/m), normalised (ParticleType.cpp:49-51) */
+    double deviation;           /* calcDeviation() = sqrt(T/m), normalised (ParticleType.cpp:53-55) */
+    double drift[3];            /* AmbientParticleType::drift_velocity, normalised */
+    int injection_axis[6];      /* AmbientParticleType::injection_axis (-x,+x,-y,+y,-z,+z) */
+    double flux[6];             /* AmbientParticleType::calcFlux() (AmbientParticleType.cpp:8-57) */
+    double emission_amount;     /* photoelectrons per lit surface node per step:
+                                   dx^2 * getEmissionAmount() (Spacecraft.cpp:876-877) */
+} fopis_species;
+
+typedef enum fopis_precision {
+    FOPIS_MIXED = 0,   /* int32 cell + FP32 offset/velocity particles, int64 fixed-point rho,
+                          FP32 smoother inside FP64 iterative refinement */
+    FOPIS_FP64 = 1     /* FP64 particles, FP64 deposit and FP64 smoother */
+} fopis_precision;
+
+typedef enum fopis_guess_mode {
+    FOPIS_GUESS_ZERO = 0,      /* every solve starts from phi = 0 */
+    FOPIS_GUESS_WARM = 1,      /* start from the previous phi (the reference's behaviour) */
+    FOPIS_GUESS_LEARNED = 2    /* previous phi + U-Net predicted increment, with fallback */
+} fopis_guess_mode;
+
+/* Simulation parameters: the normalised content of input.json after
+ * Initializer::loadEnvironment / loadParticleType / loadStaticField. */
+typedef struct fopis_params {
+    int nx, ny, nz;              /* Environment::nx,ny,nz (one rank: cell_x = nx) */
+    char boundary[8];            /* Environment::boundary, e.g. "DDDDDD" */
+    double eps0;                 /* Normalizer::eps0 */
+    double static_bfield[3];     /* StaticField::static_bfield, normalised (Initialize.cpp:312-319) */
+    double shine_vector[3];      /* StaticField::shine_vector */
+    int nspecies;                /* Environment::num_of_particle_types; order ambient -> photo */
+    fopis_species species[FOPIS_MAX_SPECIES];
+    double poisson_tol;          /* ||f - A phi||_2 <= tol ||f||_2 ; 0 -> 1e-8 */
+    int max_vcycles;             /* V-cycle cap per solve; 0 -> 100 */
+    int guess_mode;              /* fopis_guess_mode */
+    int sort_interval;           /* counting-sort period in steps; 0 -> 4 */
+    int remove_interval;         /* removeInvalidParticles period (RootGrid.cpp:136-140); 0 -> 50 */
+    double capacity_factor;      /* particle capacity / initial count; 0 -> 1.5 */
+    int precision;               /* fopis_precision */
+    int reserved0;
+    uint64_t seed;               /* Philox key for loading, injection and emission */
+} fopis_params;
+
+/* A voxel conductor; replaces the ObjectDataFromFile + Spacecraft construction
+ * (src/Spacecraft/ObjectUtils.cpp:9-333, Spacecraft.cpp:16-152). */
+typedef struct fopis_object_desc {
+    int n_cmat;                  /* surface node count = capacity-matrix size */
+    const int32_t* cmat_nodes;   /* [n_cmat][3] glue-layout node indices; row c = cmat number c */
+    int n_cells;                 /* inner (body) cells */
+    const int32_t* cells;        /* [n_cells][3] glue-layout cell indices */
+    int is_potential_fixed;      /* ObjectInfo_t::is_potential_fixed */
+    double fixed_potential;      /* normalised */
+    double initial_potential_offset; /* normalised (Spacecraft::initializeChargeMapOffset) */
+    int emit_species;            /* photoelectron species emitted from the lit face, -1 = none */
+} fopis_object_desc;
+
+/* Field selectors for fopis_get_field / fopis_set_field. */
+typedef enum fopis_field {
+    FOPIS_FIELD_PHI = 0,     /* Field::phi */
+    FOPIS_FIELD_RHO0 = 1,    /* Field::rho[0] (total, after redistribution) */
+    FOPIS_FIELD_EXREF = 2,   /* Field::exref (nodal E) */
+    FOPIS_FIELD_EYREF = 3,
+    FOPIS_FIELD_EZREF = 4,
+    FOPIS_FIELD_RHO_SPECIES = 16 /* + species id: Field::rho[1 + s] */
+} fopis_field;
+
+typedef struct fopis_stats {
+    int64_t timestep;            /* steps taken by this context */
+    int vcycles_last;            /* V-cycles of the last solve */
+    int vcycles_step;            /* V-cycles summed over the solves of the last step */
+    int solves_step;             /* solves in the last step (2 with conductors) */
+    int converged;               /* last solve reached the tolerance */
+    double residual_last;        /* ||r||_2/||f||_2 of the last solve */
+    double residual_initial;     /* same, before the first V-cycle of the last solve */
+    int64_t num_particles[FOPIS_MAX_SPECIES];   /* valid particles per species */
+    int64_t capacity[FOPIS_MAX_SPECIES];
+    int64_t absorbed_step;       /* particles absorbed by conductors in the last step */
+    int64_t injected_step;
+    int64_t emitted_step;
+    uint32_t device_status;      /* FOPIS_DEV_* bits */
+    int learned_used;            /* the learned guess seeded the last step's solves */
+    double ms_phase[8];          /* last step: push, emit, inject, absorb, rho, solve, efield, sort */
+    int64_t kernel_launches;     /* kernels this context has launched since creation */
+} fopis_stats;
+
+/* ---- lifetime ----------------------------------------------------------- */
+
+/* Replaces RootGrid::RootGrid field set-up (RootGrid.cpp:7-40, Grid.cpp:148-196).
+ * device < 0 selects the current device. */
+int fopis_create(const fopis_params* params, int device, void** ctx);
+void fopis_destroy(void* ctx);
+const char* fopis_last_error(void* ctx);
+const char* fopis_version(void);
+
+/* ---- conductors --------------------------------------------------------- */
+
+/* Replaces RootGrid::initializeObjects (RootGridObject.cpp:6-75). */
+int fopis_add_object(void* ctx, const fopis_object_desc* desc, int* object_id);
+/* Replaces RootGrid::initializeObjectsCmatrix (RootGridObject.cpp:77-148): one
+ * Poisson solve per surface node for B, then C = B^-1 (Cmatrix.hpp:31-34),
+ * then Spacecraft::initializeChargeMapOffset (Spacecraft.cpp:160-183). */
+int fopis_build_capacity_matrix(void* ctx, int object_id);
+/* IO::loadCmatrixData / writeCmatrixData (IO.cpp:28-120): C row-major [i][j] = capacity_matrix(i, j). */
+int fopis_set_capacity_matrix(void* ctx, int object_id, const double* C, int n);
+int fopis_get_capacity_matrix(void* ctx, int object_id, double* C, int n);
+/* Spacecraft::getLogEntry values (Spacecraft.cpp:1011-1044), normalised:
+ * potential, total charge, current per species (charge per step). */
+int fopis_get_object(void* ctx, int object_id, double* potential, double* charge,
+                     double* current_per_species);
+/* Spacecraft::charge_map [nspecies][n_cmat], normalised charge. */
+int fopis_get_charge_map(void* ctx, int object_id, double* charge_map, int n);
+
+/* ---- particles ---------------------------------------------------------- */
+
+/* Loads particles of one species from the reference's 56-byte Particle record
+ * {double x,y,z,vx,vy,vz; int typeId,isValid} (include/particle.hpp:14-20).
+ * Invalid records are skipped. Appends to what the species already holds. */
+int fopis_load_particles(void* ctx, int species, const void* particles56, int64_t n);
+/* Copies the valid particles of one species out in the 56-byte record layout.
+ * *n_out receives the count; at most cap records are written. */
+int fopis_get_particles(void* ctx, int species, void* particles56, int64_t cap, int64_t* n_out);
+/* Raw split-precision state of the valid particles (mixed precision only): the
+ * particle's node cell packed as (i << 20) | (j << 10) | k in glue-layout indices
+ * (i = floor(x)+1, include/position.hpp:59-69), the in-cell offsets x-(i-1) and
+ * the velocities. */
+int fopis_get_particles_raw(void* ctx, int species, int32_t* cell, float* ox, float* oy,
+                            float* oz, float* vx, float* vy, float* vz, int64_t cap, int64_t* n_out);
+/* Uniform ambient loading of RootGrid::RootGrid (RootGrid.cpp:45-79) on the device:
+ * Philox-keyed positions and Maxwellian velocities, conductor interiors removed
+ * (Spacecraft::removeInnerParticle, Spacecraft.cpp:508-510). */
+int fopis_generate_ambient(void* ctx);
+/* Counting sort of every species by cell; drops invalid particles
+ * (Grid::removeInvalidParticles, GridParticleTreatment.cpp:93-102, and more). */
+int fopis_sort_particles(void* ctx);
+
+/* ---- the ES step and its phases (RootGrid::mainLoopES order) ------------ */
+
+/* Grid::initialize (Grid.cpp:23-36): updateRho, solvePoisson, updateEfield. */
+int fopis_initialize(void* ctx);
+/* n calls of RootGrid::mainLoopES (RootGrid.cpp:82-143), fused: the push kernel
+ * gathers, pushes, moves, applies boundaries and deposits in one pass. */
+int fopis_step(void* ctx, int n);
+/* Phase entry points, for parity checks between phases. */
+int fopis_update_velocity(void* ctx);        /* Grid::updateParticleVelocityES (GridParticleTreatmentES.cpp:13-88) */
+int fopis_emit_particles(void* ctx);         /* RootGrid::emitParticlesFromObjects (RootGridObject.cpp:175-181) */
+int fopis_update_position(void* ctx);        /* RootGrid::updateParticlePositionES (GridParticleTreatmentES.cpp:90-181) */
+int fopis_inject_particles(void* ctx);       /* RootGrid::injectParticlesFromBoundary (RootGridParticle.cpp:3-130) */
+int fopis_update_rho(void* ctx);             /* RootGrid::updateRho (RootGridField.cpp:1153-1252), incl. the
+                                                first solve and Spacecraft::redistributeCharge when objects exist */
+int fopis_solve_poisson(void* ctx);          /* RootGrid::solvePoisson (RootGridField.cpp:41-63) */
+int fopis_update_efield(void* ctx);          /* RootGrid::updateEfield + updateReferenceEfield (RootGridField.cpp:456-582) */
+int fopis_remove_invalid_particles(void* ctx); /* Grid::removeInvalidParticles */
+/* Ends a step driven through the phase entry points: ++Environment::timestep
+ * (src/main.cpp:33), which keys the Philox draws of injection and emission. */
+int fopis_advance_timestep(void* ctx);
+
+/* ---- fields and diagnostics --------------------------------------------- */
+
+/* Copies a node field out in the reference layout (n = (nx+2)(ny+2)(nz+2)). */
+int fopis_get_field(void* ctx, int which, double* out, size_t n);
+/* Overwrites PHI or RHO0 (for solver-only use and warm starts). */
+int fopis_set_field(void* ctx, int which, const double* in, size_t n);
+/* Grid::getParticleEnergy (GridParticleTreatment.cpp:104-118) and
+ * Field::getEfieldEnergy (Field.cpp:194-213), normalised. */
+int fopis_get_energy(void* ctx, double* particle_energy, double* efield_energy);
+int fopis_get_stats(void* ctx, fopis_stats* stats);
+/* The cudaStream_t all of the context's work runs on (for callers that order
+ * their own work or events against it). */
+int fopis_get_stream(void* ctx, void** stream);
+/* Sets the Poisson start mode (fopis_guess_mode). */
+int fopis_set_guess_mode(void* ctx, int mode);
+
+/* ---- learned initial guess (no reference counterpart) -------------------- */
+
+/* Trains the U-Net online on the (rho^n, phi^{n-1}, phi^{n-2}) -> phi^n - phi^{n-1}
+ * pairs that the plain solver produces during fopis_step. enable = 0 stops. */
+int fopis_unet_set_training(void* ctx, int enable, double learning_rate);
+/* Loss of the last training step and number of steps taken. */
+int fopis_unet_get_state(void* ctx, double* last_loss, int64_t* train_steps);
+
+/* ---- set-up helpers (host side, no device work) ------------------------- */
+
+/* ObjectUtils::getObjectNodesFromObjFile (ObjectUtils.cpp:9-333): parses a
+ * MagicaVoxel .obj into surface nodes (cmat order) and inner cells, both in
+ * glue-layout indices for a single-rank domain of nx,ny,nz nodes. Arrays are
+ * allocated with malloc; release them with fopis_free. */
+int fopis_parse_obj(const char* path, int nx, int ny, int nz,
+                    int32_t** cmat_nodes, int* n_cmat, int32_t** cells, int* n_cells);
+void fopis_free(void* p);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FOPIS_GPU_H */

@@ -1,0 +1,1444 @@
+// fopis_oracle.cpp — TEST INFRASTRUCTURE, NOT PRODUCT CODE.
+//
+// A CPU, FP64, OpenMP restatement of the FOPIS (TDPIC) electrostatic timestep for
+// one MPI rank. It is the correctness oracle for libfopis_gpu.so and the timed
+// CPU baseline ("port" kind). Only tests, the smoke check and the benchmark's CPU
+// leg load it; nothing in the product links it.
+//
+// It keeps the reference's data layout and order of operations:
+//   * the 56-byte array-of-structs Particle (include/particle.hpp:14-20);
+//   * boost::multi_array<double,3> node fields with one glue layer, C order;
+//   * RootGrid::mainLoopES phase order (src/Grid/RootGrid/RootGrid.cpp:82-143);
+//   * the reference PSOR with its partial-sweep order, omega and pointwise
+//     residual check (src/Grid/RootGrid/RootGridField.cpp:65-317);
+//   * the single-rank periodic self-exchange semantics of src/MPI/Communicator.cpp
+//     (node fold :497-574, field copy :265-343, partial phi :193-263).
+// Deviations (each one also noted at its site):
+//   * random numbers come from Philox4x32-10 (Salmon et al., SC'11) keyed by
+//     (seed, species, step, face/node, index) instead of std::mt19937 +
+//     std::normal_distribution, whose output is implementation-defined; the GPU
+//     path uses the same keys, so both sides draw identical particle sets;
+//   * migrated (wrapped) particles stay in place instead of being appended;
+//     order only changes FP64 summation order in the deposit;
+//   * a particle landing exactly on x == nx on a periodic axis wraps to 0 (the
+//     reference keeps it and reads one node past the array);
+//   * Eigen's MatrixXd::inverse (include/Spacecraft/Cmatrix.hpp:31-34) is replaced
+//     by Gauss-Jordan elimination with partial pivoting;
+//   * an extra "exact" Poisson solve (conjugate gradients to a tight tolerance)
+//     serves as the converged FP64 reference for phi.
+// Parity pins: Philox known-answer vectors, the reference's own Position header
+// compiled by oracle/Makefile into oracle/_ref/pin_position, analytic checks
+// (charge conservation, point-charge potential, Langmuir oscillation). The
+// reference ships no golden vectors for this path (its test/ tree pins only AMR
+// ID maps and does not compile).
+
+#include "../include/fopis_gpu.h"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace orc {
+
+// ---------------------------------------------------------------- Philox RNG
+// Philox4x32-10 as published by Salmon, Moraes, Dror, Shaw, "Parallel random
+// numbers: as easy as 1, 2, 3" (SC'11): 10 rounds of a 32x32->64 multiply
+// bijection with a Weyl-sequence key schedule.
+static inline void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+    for (int r = 0; r < 10; ++r) {
+        if (r) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
+        const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0;
+        const uint32_t n1 = (uint32_t)p1;
+        const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1;
+        const uint32_t n3 = (uint32_t)p0;
+        c[0] = n0; c[1] = n1; c[2] = n2; c[3] = n3;
+    }
+}
+
+// Two uniforms in [0,1) with 53 random bits each from one Philox call.
+struct U2 { double a, b; };
+static inline U2 draw2(uint64_t seed, uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3) {
+    uint32_t c[4] = {c0, c1, c2, c3};
+    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const uint64_t x = ((uint64_t)c[0] << 32) | c[1];
+    const uint64_t y = ((uint64_t)c[2] << 32) | c[3];
+    return {(double)(x >> 11) * 0x1p-53, (double)(y >> 11) * 0x1p-53};
+}
+
+// Box-Muller pair; 1-u keeps the logarithm's argument in (0,1].
+static inline void box_muller(double u1, double u2, double& n0, double& n1) {
+    const double r = std::sqrt(-2.0 * std::log(1.0 - u1));
+    const double t = 2.0 * M_PI * u2;
+    n0 = r * std::cos(t);
+    n1 = r * std::sin(t);
+}
+
+enum : uint32_t { TAG_LOAD = 1u, TAG_INJECT = 2u, TAG_EMIT = 3u };
+
+// ---------------------------------------------------------------- containers
+struct Arr3 {
+    int cx = 0, cy = 0, cz = 0;
+    std::vector<double> v;
+    void resize(int a, int b, int c) { cx = a; cy = b; cz = c; v.assign((size_t)a * b * c, 0.0); }
+    inline double& operator()(int i, int j, int k) { return v[((size_t)i * cy + j) * cz + k]; }
+    inline double operator()(int i, int j, int k) const { return v[((size_t)i * cy + j) * cz + k]; }
+    void zero() { std::fill(v.begin(), v.end(), 0.0); }
+};
+
+// include/particle.hpp:14-20 — 56 bytes.
+struct Particle {
+    double x, y, z;
+    double vx, vy, vz;
+    int typeId;
+    int isValid;
+};
+static_assert(sizeof(Particle) == 56, "reference Particle is 56 bytes");
+
+// include/position.hpp:13-69 — Position::setXYZ / setIJK / updateDelta.
+struct Pos {
+    int i, j, k;
+    double x, y, z, dx1, dy1, dz1, dx2, dy2, dz2;
+    void delta() {
+        dx1 = x - (i - 1); dy1 = y - (j - 1); dz1 = z - (k - 1);
+        dx2 = 1.0 - dx1; dy2 = 1.0 - dy1; dz2 = 1.0 - dz1;
+    }
+    void setXYZ(double a, double b, double c) {
+        x = a; y = b; z = c;
+        i = (int)std::floor(x) + 1; j = (int)std::floor(y) + 1; k = (int)std::floor(z) + 1;
+        delta();
+    }
+    void setIJK(int a, int b, int c) {
+        i = a; j = b; k = c;
+        x = (double)(i - 1); y = (double)(j - 1); z = (double)(k - 1);
+        delta();
+    }
+};
+static inline Pos posXYZ(double x, double y, double z) { Pos p; p.setXYZ(x, y, z); return p; }
+
+struct Object {
+    int n_cmat = 0;
+    std::vector<std::array<int, 3>> cmat;      // capacity_matrix_relation (cmat number -> glue node)
+    std::vector<int> node_to_cmat;             // dense replacement of getCmatNumber's map scan
+    std::vector<unsigned char> cell_map;       // object_cell_map [nx+1][ny+1][nz+1]
+    std::vector<double> C;                     // capacity_matrix, row-major C(i,j) = C[i*n+j]
+    double total_cmat_value = 0.0;
+    std::vector<double> charge_map;            // [nsp][n]
+    std::vector<double> tmp_charge_map;        // [nsp][n]
+    std::vector<double> current;               // [nsp]
+    double potential = 0.0, total_charge = 0.0;
+    int is_potential_fixed = 0;
+    double fixed_potential = 0.0, initial_potential_offset = 0.0;
+    int emit_species = -1;
+    bool has_C = false;
+};
+
+struct Ctx {
+    fopis_params p;
+    int nx, ny, nz;              // cell_x.. (single rank: equal to Environment::nx)
+    int cx, cy, cz;              // nx+2 ..
+    bool notb[6];                // Environment::isNotBoundary(axis, side) for x-,x+,y-,y+,z-,z+
+    int nsp;
+    std::vector<std::vector<Particle>> particles;
+    std::vector<Arr3> rho;       // rho[0] total, rho[1+s]
+    Arr3 phi, poisson_error, ex, ey, ez, exref, eyref, ezref;
+    std::vector<Object> objects;
+    std::vector<std::array<double, 6>> inject_residual;
+    int64_t timestep = 1;        // Environment::timestep starts at 1 (Initialize.cpp:161)
+    // solver
+    int solver_mode = 0;         // 0 reference PSOR, 1 exact CG
+    int max_post_loop = 1000;    // Options::maximum_poisson_post_loop
+    double exact_tol = 1e-13;
+    int last_iterations = 0;
+    double last_residual = 0.0;
+    int64_t injected_step = 0, emitted_step = 0, absorbed_step = 0;
+    char err[256] = {0};
+};
+
+static inline bool isBoundary(const Ctx& c, int axis, int side) { return !c.notb[2 * axis + side]; }
+
+// Environment::isValidCellPosition (src/Misc/Environment.cpp:287-293).
+static inline bool validCell(const Ctx& c, int i, int j, int k) {
+    return i >= 0 && i < c.nx + 1 && j >= 0 && j < c.ny + 1 && k >= 0 && k < c.nz + 1;
+}
+static inline size_t cellIndex(const Ctx& c, int i, int j, int k) {
+    return ((size_t)i * (c.ny + 1) + j) * (c.nz + 1) + k;
+}
+static inline size_t nodeIndex(const Ctx& c, int i, int j, int k) {
+    return ((size_t)i * c.cy + j) * c.cz + k;
+}
+
+// ---------------------------------------------------------------- set-up
+static void init_ctx(Ctx& c, const fopis_params* p) {
+    c.p = *p;
+    c.nx = p->nx; c.ny = p->ny; c.nz = p->nz;
+    c.cx = c.nx + 2; c.cy = c.ny + 2; c.cz = c.nz + 2;
+    for (int s = 0; s < 6; ++s) c.notb[s] = (p->boundary[s] == 'P');
+    c.nsp = p->nspecies;
+    c.particles.assign(c.nsp, {});
+    c.rho.resize(c.nsp + 1);
+    for (auto& r : c.rho) r.resize(c.cx, c.cy, c.cz);
+    c.phi.resize(c.cx, c.cy, c.cz);
+    c.poisson_error.resize(c.cx, c.cy, c.cz);
+    c.ex.resize(c.cx - 1, c.cy, c.cz);
+    c.ey.resize(c.cx, c.cy - 1, c.cz);
+    c.ez.resize(c.cx, c.cy, c.cz - 1);
+    c.exref.resize(c.cx, c.cy, c.cz);
+    c.eyref.resize(c.cx, c.cy, c.cz);
+    c.ezref.resize(c.cx, c.cy, c.cz);
+    c.inject_residual.assign(c.nsp, {0, 0, 0, 0, 0, 0});
+}
+
+// ---------------------------------------------------------------- halo semantics
+// Communicator::sendRecvScalarX/Y/Z with prev == next == self and glue size 2
+// (src/MPI/Communicator.cpp:497-574): node 0 and node n become the sum of both,
+// node 1 and node n+1 likewise. Applied only on periodic axes
+// (MPIw::Environment::sendRecvNodeScalar, src/MPI/Environment.cpp:53-72).
+static void fold_node_scalar(const Ctx& c, Arr3& a) {
+    const int X = a.cx, Y = a.cy, Z = a.cz;
+    if (c.notb[0]) {
+        for (int j = 0; j < Y; ++j) for (int k = 0; k < Z; ++k) {
+            double s0 = a(0, j, k) + a(X - 2, j, k), s1 = a(1, j, k) + a(X - 1, j, k);
+            a(0, j, k) = s0; a(X - 2, j, k) = s0; a(1, j, k) = s1; a(X - 1, j, k) = s1;
+        }
+    }
+    if (c.notb[2]) {
+        for (int i = 0; i < X; ++i) for (int k = 0; k < Z; ++k) {
+            double s0 = a(i, 0, k) + a(i, Y - 2, k), s1 = a(i, 1, k) + a(i, Y - 1, k);
+            a(i, 0, k) = s0; a(i, Y - 2, k) = s0; a(i, 1, k) = s1; a(i, Y - 1, k) = s1;
+        }
+    }
+    if (c.notb[4]) {
+        for (int i = 0; i < X; ++i) for (int j = 0; j < Y; ++j) {
+            double s0 = a(i, j, 0) + a(i, j, Z - 2), s1 = a(i, j, 1) + a(i, j, Z - 1);
+            a(i, j, 0) = s0; a(i, j, Z - 2) = s0; a(i, j, 1) = s1; a(i, j, Z - 1) = s1;
+        }
+    }
+}
+
+// Communicator::sendRecvFieldX/Y/Z self branch (src/MPI/Communicator.cpp:290-299):
+// node 0 <- node n, node n+1 <- node 1, per periodic axis, x then y then z.
+static void copy_field_glue(const Ctx& c, Arr3& a) {
+    const int X = a.cx, Y = a.cy, Z = a.cz;
+    if (c.notb[0])
+        for (int j = 0; j < Y; ++j) for (int k = 0; k < Z; ++k) {
+            double lo = a(1, j, k);
+            a(0, j, k) = a(X - 2, j, k); a(X - 1, j, k) = lo;
+        }
+    if (c.notb[2])
+        for (int i = 0; i < X; ++i) for (int k = 0; k < Z; ++k) {
+            double lo = a(i, 1, k);
+            a(i, 0, k) = a(i, Y - 2, k); a(i, Y - 1, k) = lo;
+        }
+    if (c.notb[4])
+        for (int i = 0; i < X; ++i) for (int j = 0; j < Y; ++j) {
+            double lo = a(i, j, 1);
+            a(i, j, 0) = a(i, j, Z - 2); a(i, j, Z - 1) = lo;
+        }
+}
+
+// MPIw::Environment::sendRecvPartialPhi self branch (src/MPI/Environment.cpp:174-208,
+// Communicator.cpp:193-263): a plane segment at index 1 is copied to index n+1,
+// one at index n to index 0, only when that side is periodic.
+static void partial_phi(Ctx& c, int ib, int ie, int jb, int je, int kb, int ke) {
+    Arr3& phi = c.phi;
+    if (ib == ie) {
+        const bool low = (ib == 1);
+        if (low ? c.notb[0] : c.notb[1]) {
+            const int dst = low ? c.cx - 1 : 0;
+            for (int j = jb; j <= je; ++j) for (int k = kb; k <= ke; ++k) phi(dst, j, k) = phi(ib, j, k);
+        }
+    } else if (jb == je) {
+        const bool low = (jb == 1);
+        if (low ? c.notb[2] : c.notb[3]) {
+            const int dst = low ? c.cy - 1 : 0;
+            for (int i = ib; i <= ie; ++i) for (int k = kb; k <= ke; ++k) phi(i, dst, k) = phi(i, jb, k);
+        }
+    } else if (kb == ke) {
+        const bool low = (kb == 1);
+        if (low ? c.notb[4] : c.notb[5]) {
+            const int dst = low ? c.cz - 1 : 0;
+            for (int i = ib; i <= ie; ++i) for (int j = jb; j <= je; ++j) phi(i, j, dst) = phi(i, j, kb);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- particle phases
+// Grid::updateParticleVelocityES (src/Grid/GridParticleTreatmentES.cpp:13-88).
+static void update_velocity(Ctx& c) {
+    const double bx = c.p.static_bfield[0], by = c.p.static_bfield[1], bz = c.p.static_bfield[2];
+    const double time_factor = 1.0;  // 1 / 2^level, level 0
+    for (int pid = 0; pid < c.nsp; ++pid) {
+        const double qm = 0.5 * c.p.species[pid].charge / c.p.species[pid].mass;
+        auto& parray = c.particles[pid];
+        const long n = (long)parray.size();
+        const Arr3& exr = c.exref; const Arr3& eyr = c.eyref; const Arr3& ezr = c.ezref;
+#pragma omp parallel for schedule(static)
+        for (long pn = 0; pn < n; ++pn) {
+            Particle& p = parray[pn];
+            if (!p.isValid) continue;
+            Pos pos = posXYZ(p.x, p.y, p.z);
+            const int i = pos.i, j = pos.j, k = pos.k;
+            const double v1 = qm * pos.dx2 * pos.dy2 * pos.dz2, v2 = qm * pos.dx1 * pos.dy2 * pos.dz2;
+            const double v3 = qm * pos.dx2 * pos.dy1 * pos.dz2, v4 = qm * pos.dx1 * pos.dy1 * pos.dz2;
+            const double v5 = qm * pos.dx2 * pos.dy2 * pos.dz1, v6 = qm * pos.dx1 * pos.dy2 * pos.dz1;
+            const double v7 = qm * pos.dx2 * pos.dy1 * pos.dz1, v8 = qm * pos.dx1 * pos.dy1 * pos.dz1;
+            auto g = [&](const Arr3& e) {
+                return v1 * e(i, j, k) + v2 * e(i + 1, j, k) + v3 * e(i, j + 1, k) + v4 * e(i + 1, j + 1, k) +
+                       v5 * e(i, j, k + 1) + v6 * e(i + 1, j, k + 1) + v7 * e(i, j + 1, k + 1) +
+                       v8 * e(i + 1, j + 1, k + 1);
+            };
+            const double exv = g(exr), eyv = g(eyr), ezv = g(ezr);
+            const double boris = 2.0 / (1.0 + (bx * bx + by * by + bz * bz));
+            const double vx1 = p.vx + exv, vy1 = p.vy + eyv, vz1 = p.vz + ezv;
+            const double vxt = vx1 + vy1 * bz - vz1 * by;
+            const double vyt = vy1 + vz1 * bx - vx1 * bz;
+            const double vzt = vz1 + vx1 * by - vy1 * bx;
+            p.vx = vx1 + (exv + boris * (vyt * bz - vzt * by)) * time_factor;
+            p.vy = vy1 + (eyv + boris * (vzt * bx - vxt * bz)) * time_factor;
+            p.vz = vz1 + (ezv + boris * (vxt * by - vyt * bx)) * time_factor;
+        }
+    }
+}
+
+// RootGrid::checkX/Y/ZBoundary (include/grid.hpp:309-395) followed by the
+// single-rank migration of updateParticlePositionES (:115-177): on a periodic
+// axis a coordinate beyond -1 gains sl, one beyond sl loses sl (here also one
+// exactly at sl, see the header); on a D/N axis x < 0 or x > sl-1 invalidates.
+static inline void boundary_axis(const Ctx& c, double& x, int& valid, int axis, double sl) {
+    if (x < 0.0) {
+        if (c.notb[2 * axis]) { if (x < -1.0) x += sl; }
+        else valid = 0;
+    } else if (x > sl - 1.0) {
+        if (c.notb[2 * axis + 1]) { if (x >= sl) x -= sl; }
+        else valid = 0;
+    }
+}
+
+// RootGrid::updateParticlePositionES (src/Grid/GridParticleTreatmentES.cpp:90-181).
+static void update_position(Ctx& c) {
+    const double slx = c.nx, sly = c.ny, slz = c.nz;
+    for (int pid = 0; pid < c.nsp; ++pid) {
+        auto& parray = c.particles[pid];
+        const long n = (long)parray.size();
+#pragma omp parallel for schedule(static)
+        for (long pn = 0; pn < n; ++pn) {
+            Particle& p = parray[pn];
+            if (!p.isValid) continue;
+            p.x += p.vx; p.y += p.vy; p.z += p.vz;  // Particle::updatePosition
+            boundary_axis(c, p.x, p.isValid, 0, slx);
+            boundary_axis(c, p.y, p.isValid, 1, sly);
+            boundary_axis(c, p.z, p.isValid, 2, slz);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- conductors
+static inline bool cell_in(const Ctx& c, const Object& o, int i, int j, int k) {
+    return o.cell_map[cellIndex(c, i, j, k)] != 0;
+}
+// Spacecraft::isContaining (Spacecraft.cpp:320-332).
+static inline bool isContaining(const Ctx& c, const Object& o, const Pos& pos) {
+    if (!validCell(c, pos.i, pos.j, pos.k)) return false;
+    return cell_in(c, o, pos.i, pos.j, pos.k);
+}
+// Spacecraft::getCmatNumber (Spacecraft.cpp:210-235); -1 where the reference throws.
+static inline int cmatNumber(const Ctx& c, const Object& o, int i, int j, int k) {
+    if (i < 0 || j < 0 || k < 0 || i >= c.cx || j >= c.cy || k >= c.cz) return -1;
+    return o.node_to_cmat[nodeIndex(c, i, j, k)];
+}
+static inline bool isCmatNode(const Ctx& c, const Object& o, int i, int j, int k) {
+    return cmatNumber(c, o, i, j, k) >= 0;
+}
+// Spacecraft::isX/Y/Zsurface{Minus,Plus} (Spacecraft.cpp:334-356).
+static inline bool xMinus(const Ctx& c, const Object& o, int i, int j, int k) { return cell_in(c, o, i, j, k) && !cell_in(c, o, i - 1, j, k); }
+static inline bool xPlus(const Ctx& c, const Object& o, int i, int j, int k) { return !cell_in(c, o, i, j, k) && cell_in(c, o, i - 1, j, k); }
+static inline bool yMinus(const Ctx& c, const Object& o, int i, int j, int k) { return cell_in(c, o, i, j, k) && !cell_in(c, o, i, j - 1, k); }
+static inline bool yPlus(const Ctx& c, const Object& o, int i, int j, int k) { return !cell_in(c, o, i, j, k) && cell_in(c, o, i, j - 1, k); }
+static inline bool zMinus(const Ctx& c, const Object& o, int i, int j, int k) { return cell_in(c, o, i, j, k) && !cell_in(c, o, i, j, k - 1); }
+static inline bool zPlus(const Ctx& c, const Object& o, int i, int j, int k) { return !cell_in(c, o, i, j, k) && cell_in(c, o, i, j, k - 1); }
+
+// Spacecraft::isX/Y/ZsurfacePoint (Spacecraft.cpp:462-506).
+static bool isXsurfacePoint(const Ctx& c, const Object& o, const Pos& pos, int sign) {
+    if (pos.dx1 >= 1e-10) return false;
+    if (validCell(c, pos.i, pos.j, pos.k) && validCell(c, pos.i - 1, pos.j, pos.k))
+        return sign > 0 ? xMinus(c, o, pos.i, pos.j, pos.k) : xPlus(c, o, pos.i, pos.j, pos.k);
+    return isCmatNode(c, o, pos.i, pos.j, pos.k) && isCmatNode(c, o, pos.i, pos.j + 1, pos.k) &&
+           isCmatNode(c, o, pos.i, pos.j, pos.k + 1) && isCmatNode(c, o, pos.i, pos.j + 1, pos.k + 1);
+}
+static bool isYsurfacePoint(const Ctx& c, const Object& o, const Pos& pos, int sign) {
+    if (pos.dy1 >= 1e-10) return false;
+    if (validCell(c, pos.i, pos.j, pos.k) && validCell(c, pos.i, pos.j - 1, pos.k))
+        return sign > 0 ? yMinus(c, o, pos.i, pos.j, pos.k) : yPlus(c, o, pos.i, pos.j, pos.k);
+    return isCmatNode(c, o, pos.i, pos.j, pos.k) && isCmatNode(c, o, pos.i + 1, pos.j, pos.k) &&
+           isCmatNode(c, o, pos.i, pos.j, pos.k + 1) && isCmatNode(c, o, pos.i + 1, pos.j, pos.k + 1);
+}
+static bool isZsurfacePoint(const Ctx& c, const Object& o, const Pos& pos, int sign) {
+    if (pos.dz1 >= 1e-10) return false;
+    if (validCell(c, pos.i, pos.j, pos.k) && validCell(c, pos.i, pos.j, pos.k - 1))
+        return sign > 0 ? zMinus(c, o, pos.i, pos.j, pos.k) : zPlus(c, o, pos.i, pos.j, pos.k);
+    return isCmatNode(c, o, pos.i, pos.j, pos.k) && isCmatNode(c, o, pos.i + 1, pos.j, pos.k) &&
+           isCmatNode(c, o, pos.i, pos.j + 1, pos.k) && isCmatNode(c, o, pos.i + 1, pos.j + 1, pos.k);
+}
+
+// Particle::get{X,Y,Z}MoveRatio (src/Particle/particle.cpp:46-80).
+static inline double moveRatio(double d1, double d2, double v) {
+    if (v == 0.0) return 0.0;
+    return v > 0.0 ? d1 / std::fabs(v) : d2 / std::fabs(v);
+}
+
+// Particle::computeCrossPoints (src/Particle/particle.cpp:82-204), including the
+// `mvx <= mvx` comparison of the xz case (:175), which always puts x first.
+static int computeCrossPoints(const Particle& p, Pos out[3]) {
+    const Pos pos = posXYZ(p.x, p.y, p.z);
+    const Pos old = posXYZ(p.x - p.vx, p.y - p.vy, p.z - p.vz);
+    const double mvx = 1.0 - moveRatio(pos.dx1, pos.dx2, p.vx);
+    const double mvy = 1.0 - moveRatio(pos.dy1, pos.dy2, p.vy);
+    const double mvz = 1.0 - moveRatio(pos.dz1, pos.dz2, p.vz);
+    int count = 0;
+    Pos xc, yc, zc;
+    const bool mx = (pos.i != old.i), my = (pos.j != old.j), mz = (pos.k != old.k);
+    if (mx) { xc.setXYZ(p.vx > 0.0 ? std::ceil(old.x) : std::floor(old.x), old.y + p.vy * mvx, old.z + p.vz * mvx); ++count; }
+    if (my) { yc.setXYZ(old.x + p.vx * mvy, p.vy > 0.0 ? std::ceil(old.y) : std::floor(old.y), old.z + p.vz * mvy); ++count; }
+    if (mz) { zc.setXYZ(old.x + p.vx * mvz, old.y + p.vy * mvz, p.vz > 0.0 ? std::ceil(old.z) : std::floor(old.z)); ++count; }
+    int n = 0;
+    if (count == 3) {
+        if (mvx <= mvy) {
+            if (mvx <= mvz) {
+                out[n++] = xc;
+                if (mvy <= mvz) { out[n++] = yc; out[n++] = zc; } else { out[n++] = zc; out[n++] = yc; }
+            } else { out[n++] = zc; out[n++] = xc; out[n++] = yc; }
+        } else {
+            if (mvy <= mvz) {
+                out[n++] = yc;
+                if (mvx <= mvz) { out[n++] = xc; out[n++] = zc; } else { out[n++] = zc; out[n++] = xc; }
+            } else { out[n++] = zc; out[n++] = yc; out[n++] = xc; }
+        }
+    } else if (count == 2) {
+        if (mx) {
+            if (my) { if (mvx <= mvy) { out[n++] = xc; out[n++] = yc; } else { out[n++] = yc; out[n++] = xc; } }
+            else { out[n++] = xc; out[n++] = zc; }  // reference compares mvx <= mvx here
+        } else {
+            if (mvy <= mvz) { out[n++] = yc; out[n++] = zc; } else { out[n++] = zc; out[n++] = yc; }
+        }
+    } else if (count == 1) {
+        out[n++] = mx ? xc : (my ? yc : zc);
+    }
+    return n;
+}
+
+// Spacecraft::distributeInnerParticleChargeTo{X,Y,Z}surface (Spacecraft.cpp:594-613)
+// and subtractChargeOfParticleFrom{X,Y,Z}surface (:945-970); sign = +1 or -1.
+// Returns false where getCmatNumber would throw.
+static bool surface_charge(const Ctx& c, Object& o, int axis, const Pos& pos, int id, double q) {
+    int n[4]; double w[4];
+    if (axis == 0) {
+        n[0] = cmatNumber(c, o, pos.i, pos.j, pos.k);         w[0] = pos.dy2 * pos.dz2;
+        n[1] = cmatNumber(c, o, pos.i, pos.j + 1, pos.k);     w[1] = pos.dy1 * pos.dz2;
+        n[2] = cmatNumber(c, o, pos.i, pos.j, pos.k + 1);     w[2] = pos.dy2 * pos.dz1;
+        n[3] = cmatNumber(c, o, pos.i, pos.j + 1, pos.k + 1); w[3] = pos.dy1 * pos.dz1;
+    } else if (axis == 1) {
+        n[0] = cmatNumber(c, o, pos.i, pos.j, pos.k);         w[0] = pos.dx2 * pos.dz2;
+        n[1] = cmatNumber(c, o, pos.i + 1, pos.j, pos.k);     w[1] = pos.dx1 * pos.dz2;
+        n[2] = cmatNumber(c, o, pos.i, pos.j, pos.k + 1);     w[2] = pos.dx2 * pos.dz1;
+        n[3] = cmatNumber(c, o, pos.i + 1, pos.j, pos.k + 1); w[3] = pos.dx1 * pos.dz1;
+    } else {
+        n[0] = cmatNumber(c, o, pos.i, pos.j, pos.k);         w[0] = pos.dx2 * pos.dy2;
+        n[1] = cmatNumber(c, o, pos.i + 1, pos.j, pos.k);     w[1] = pos.dx1 * pos.dy2;
+        n[2] = cmatNumber(c, o, pos.i, pos.j + 1, pos.k);     w[2] = pos.dx2 * pos.dy1;
+        n[3] = cmatNumber(c, o, pos.i + 1, pos.j + 1, pos.k); w[3] = pos.dx1 * pos.dy1;
+    }
+    for (int t = 0; t < 4; ++t) if (n[t] < 0) return false;
+    for (int t = 0; t < 4; ++t) o.tmp_charge_map[(size_t)id * o.n_cmat + n[t]] += q * w[t];
+    return true;
+}
+
+// Spacecraft::distributeInnerParticleCharge (Spacecraft.cpp:512-592), non-secondary
+// branch. Returns 1 if absorbed.
+static int absorb(Ctx& c, Object& o, Particle& p, int& bad) {
+    const Pos pos = posXYZ(p.x, p.y, p.z);
+    if (!isContaining(c, o, pos)) return 0;
+    const int id = p.typeId;
+    const double q = c.p.species[id].charge * c.p.species[id].size;
+    const int isign = (p.vx > 0.0) ? 1 : -1, jsign = (p.vy > 0.0) ? 1 : -1, ksign = (p.vz > 0.0) ? 1 : -1;
+    Pos cps[3];
+    const int ncp = computeCrossPoints(p, cps);
+    bool found = false;
+    for (int t = 0; t < ncp && !found; ++t) {
+        const Pos& cp = cps[t];
+        if (isXsurfacePoint(c, o, cp, isign)) { if (!surface_charge(c, o, 0, cp, id, q)) bad = 1; found = true; }
+        else if (isYsurfacePoint(c, o, cp, jsign)) { if (!surface_charge(c, o, 1, cp, id, q)) bad = 1; found = true; }
+        else if (isZsurfacePoint(c, o, cp, ksign)) { if (!surface_charge(c, o, 2, cp, id, q)) bad = 1; found = true; }
+    }
+    o.current[id] += q;
+    p.isValid = 0;
+    return 1;
+}
+
+// Spacecraft::sumWholeCharge (Spacecraft.cpp:615-626).
+static void sum_whole_charge(Ctx& c, Object& o) {
+    for (size_t t = 0; t < o.charge_map.size(); ++t) { o.charge_map[t] += o.tmp_charge_map[t]; o.tmp_charge_map[t] = 0.0; }
+}
+
+// Spacecraft::getTotalCharge (Spacecraft.cpp:248-259).
+static double total_charge(const Ctx& c, const Object& o) {
+    double q = 0.0;
+    for (int m = 0; m < o.n_cmat; ++m)
+        for (int s = 0; s < c.nsp; ++s) q += o.charge_map[(size_t)s * o.n_cmat + m];
+    return q;
+}
+
+// Spacecraft::redistributeChargeForPerfectConductor (Spacecraft.cpp:708-758).
+static void redistribute(Ctx& c, Object& o) {
+    o.total_charge = total_charge(c, o);
+    const int n = o.n_cmat;
+    double ctp = 0.0;
+    for (int j = 0; j < n; ++j) {
+        const auto& nd = o.cmat[j];
+        const double ph = c.phi(nd[0], nd[1], nd[2]);
+        for (int i = 0; i < n; ++i) ctp += o.C[(size_t)i * n + j] * ph;
+    }
+    o.potential = o.is_potential_fixed ? o.fixed_potential : (ctp + o.total_charge) / o.total_cmat_value;
+    std::vector<double> d(n);
+    for (int j = 0; j < n; ++j) { const auto& nd = o.cmat[j]; d[j] = o.potential - c.phi(nd[0], nd[1], nd[2]); }
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        double dr = 0.0;
+        for (int j = 0; j < n; ++j) dr += o.C[(size_t)i * n + j] * d[j];
+        const auto& nd = o.cmat[i];
+        c.rho[0](nd[0], nd[1], nd[2]) += dr;
+    }
+}
+
+// ---------------------------------------------------------------- Poisson
+// RootGrid::doSORPartial (src/Grid/RootGrid/RootGridField.cpp:216-264).
+static void sor_partial(Ctx& c, double omega, double rho_coeff, int ib, int ie, int jb, int je, int kb, int ke,
+                        bool parallel) {
+    Arr3& phi = c.phi; const Arr3& rho = c.rho[0];
+    int ibt = 0, iet = 0, jbt = 0, jet = 0, kbt = 0, ket = 0;
+    if (isBoundary(c, 0, 0) && ib == 1) ibt = 1;
+    if (isBoundary(c, 0, 1) && ie == c.cx - 2) iet = -1;
+    if (isBoundary(c, 1, 0) && jb == 1) jbt = 1;
+    if (isBoundary(c, 1, 1) && je == c.cy - 2) jet = -1;
+    if (isBoundary(c, 2, 0) && kb == 1) kbt = 1;
+    if (isBoundary(c, 2, 1) && ke == c.cz - 2) ket = -1;
+    const int i0 = ib + ibt, i1 = ie + iet, j0 = jb + jbt, j1 = je + jet, k0 = kb + kbt, k1 = ke + ket;
+    const int isize = i1 - i0 + 1;
+    auto upd = [&](int i, int j, int k) {
+        phi(i, j, k) = (1.0 - omega) * phi(i, j, k) +
+                       omega * (phi(i + 1, j, k) + phi(i - 1, j, k) + phi(i, j + 1, k) + phi(i, j - 1, k) +
+                                phi(i, j, k + 1) + phi(i, j, k - 1) + rho_coeff * rho(i, j, k)) / 6.0;
+    };
+    if (isize > 2) {
+        // red-black over i planes: odd offsets then even offsets
+        for (int color = 0; color < 2; ++color) {
+            const int nplanes = (i1 - (i0 + color)) >= 0 ? (i1 - (i0 + color)) / 2 + 1 : 0;
+#pragma omp parallel for schedule(static) if (parallel)
+            for (int t = 0; t < nplanes; ++t) {
+                const int i = i0 + color + 2 * t;
+                for (int j = j0; j <= j1; ++j)
+                    for (int k = k0; k <= k1; ++k) upd(i, j, k);
+            }
+        }
+    } else {
+        for (int i = i0; i <= i1; ++i)
+            for (int j = j0; j <= j1; ++j)
+                for (int k = k0; k <= k1; ++k) upd(i, j, k);
+    }
+}
+
+// RootGrid::doPSOR (src/Grid/RootGrid/RootGridField.cpp:105-214).
+static void do_psor(Ctx& c) {
+    const int minimum_radius = std::min({c.nx, c.ny, c.nz});
+    const double omega = 2.0 / (1.0 + std::sin(M_PI / minimum_radius));
+    const double rho_coeff = 1.0 / c.p.eps0;  // dx^2 / eps0 with dx = 1
+    const int X = c.cx, Y = c.cy, Z = c.cz;
+    int ib = 1, ie = 1, jb = 1, je = 1, kb = 1, ke = 1;
+    sor_partial(c, omega, rho_coeff, ib, ie, jb, je, kb, ke, false);
+    partial_phi(c, ib, ie, jb, je, kb, ke);
+    ib = 2; ie = X - 2;
+    sor_partial(c, omega, rho_coeff, ib, ie, jb, je, kb, ke, false);
+    partial_phi(c, ib - 1, ie + 1, jb, je, kb, ke);
+    ib = 1; ie = 1; jb = 2; je = Y - 2;
+    sor_partial(c, omega, rho_coeff, ib, ie, jb, je, kb, ke, false);
+    partial_phi(c, ib, ie, jb, je + 1, kb, ke);
+    ib = 2; ie = X - 2;
+    sor_partial(c, omega, rho_coeff, ib, ie, jb, je, kb, ke, false);
+    partial_phi(c, ib - 1, ie + 1, jb - 1, je + 1, kb, ke);
+    ib = 1; ie = 1; jb = 1; je = 1; kb = 2; ke = Z - 2;
+    sor_partial(c, omega, rho_coeff, ib, ie, jb, je, kb, ke, false);
+    partial_phi(c, ib, ie, jb, je, kb, ke + 1);
+    ib = 2; ie = X - 2;
+    sor_partial(c, omega, rho_coeff, ib, ie, jb, je, kb, ke, false);
+    partial_phi(c, ib - 1, ie + 1, jb, je, kb, ke + 1);
+    ib = 1; ie = 1; jb = 2; je = Y - 2;
+    sor_partial(c, omega, rho_coeff, ib, ie, jb, je, kb, ke, false);
+    partial_phi(c, ib, ie, jb, je + 1, kb, ke + 1);
+    ib = 2; ie = X - 2;
+    sor_partial(c, omega, rho_coeff, ib, ie, jb, je, kb, ke, true);  // the one #pragma omp parallel region
+    ib = 0; ie = X - 1; jb = 0; je = Y - 1; kb = Z - 2; ke = Z - 2;
+    partial_phi(c, ib, ie, jb, je, kb, ke);
+    jb = Y - 2; je = Y - 2; kb = 0; ke = Z - 1;
+    partial_phi(c, ib, ie, jb, je, kb, ke);
+    ib = X - 2; ie = X - 2; jb = 0; je = Y - 1;
+    partial_phi(c, ib, ie, jb, je, kb, ke);
+}
+
+// RootGrid::checkPhiResidual (src/Grid/RootGrid/RootGridField.cpp:267-317).
+static double check_phi_residual(Ctx& c) {
+    double residual = 0.0;
+    const Arr3& phi = c.phi; const Arr3& rho = c.rho[0];
+    const double eps = c.p.eps0;
+    const int X = c.cx, Y = c.cy, Z = c.cz;
+#pragma omp parallel for reduction(max : residual) schedule(static)
+    for (int i = 1; i < X - 1; ++i) {
+        if (!((i != 1 || c.notb[0]) && (i != X - 2 || c.notb[1]))) continue;
+        for (int j = 1; j < Y - 1; ++j) {
+            if (!((j != 1 || c.notb[2]) && (j != Y - 2 || c.notb[3]))) continue;
+            for (int k = 1; k < Z - 1; ++k) {
+                if (!((k != 1 || c.notb[4]) && (k != Z - 2 || c.notb[5]))) continue;
+                const double src = rho(i, j, k) / eps;
+                if (std::fabs(src) > 0.0) {
+                    const double op = phi(i - 1, j, k) + phi(i + 1, j, k) + phi(i, j - 1, k) + phi(i, j + 1, k) +
+                                      phi(i, j, k - 1) + phi(i, j, k + 1) - 6.0 * phi(i, j, k);
+                    const double r = std::fabs((op + src) / src);
+                    if (r > residual) residual = r;
+                }
+            }
+        }
+    }
+    return residual;
+}
+
+// Field::setBoundaryConditionPhi / setNeumannPhi / setDirichletPhi (src/Grid/Field.cpp:10-96).
+static void set_boundary_phi(Ctx& c) {
+    Arr3& phi = c.phi;
+    const int X = c.cx, Y = c.cy, Z = c.cz;
+    for (int axis = 0; axis < 3; ++axis)
+        for (int side = 0; side < 2; ++side) {
+            const char b = c.p.boundary[2 * axis + side];
+            if (b == 'P') continue;
+            const int maxi = axis == 0 ? X : (axis == 1 ? Y : Z);
+            const int bi = side == 0 ? 1 : maxi - 2;
+            const int ni = side == 0 ? 2 : maxi - 3;
+            if (axis == 0) {
+                for (int k = 1; k < Z - 1; ++k) for (int j = 1; j < Y - 1; ++j) phi(bi, j, k) = (b == 'D') ? 0.0 : phi(ni, j, k);
+            } else if (axis == 1) {
+                for (int k = 1; k < Z - 1; ++k) for (int i = 1; i < X - 1; ++i) phi(i, bi, k) = (b == 'D') ? 0.0 : phi(i, ni, k);
+            } else {
+                for (int j = 1; j < Y - 1; ++j) for (int i = 1; i < X - 1; ++i) phi(i, j, bi) = (b == 'D') ? 0.0 : phi(i, j, ni);
+            }
+        }
+}
+
+// Unknown-node test shared by the exact solver: nodes the PSOR updates.
+static inline bool is_unknown(const Ctx& c, int i, int j, int k) {
+    auto ok = [&](int idx, int n2, int axis) {
+        if (idx < 1 || idx > n2 - 2) return false;
+        if (idx == 1 && isBoundary(c, axis, 0)) return false;
+        if (idx == n2 - 2 && isBoundary(c, axis, 1)) return false;
+        return true;
+    };
+    return ok(i, c.cx, 0) && ok(j, c.cy, 1) && ok(k, c.cz, 2);
+}
+
+// Converged FP64 reference solve: conjugate gradients on A = 6 - sum(neighbours)
+// over the unknown nodes, boundary nodes held at their current values, periodic
+// neighbours wrapped, mean of the right-hand side removed when every axis is
+// periodic; stops at ||r||2 <= tol ||f||2.
+static void exact_solve(Ctx& c) {
+    const int X = c.cx, Y = c.cy, Z = c.cz;
+    const size_t N = (size_t)X * Y * Z;
+    std::vector<unsigned char> unk(N, 0);
+    for (int i = 0; i < X; ++i) for (int j = 0; j < Y; ++j) for (int k = 0; k < Z; ++k)
+        unk[nodeIndex(c, i, j, k)] = is_unknown(c, i, j, k);
+    const bool allp = c.notb[0] && c.notb[2] && c.notb[4];
+    auto wrap = [&](int idx, int n2, int axis) {
+        if (c.notb[2 * axis]) { if (idx == 0) return n2 - 2; if (idx == n2 - 1) return 1; }
+        return idx;
+    };
+    std::vector<double> f(N, 0.0), x(N, 0.0), r(N, 0.0), pp(N, 0.0), Ap(N, 0.0);
+    for (size_t t = 0; t < N; ++t) x[t] = c.phi.v[t];
+    // Ap = A * v restricted to unknowns, using full field v (boundary values included)
+    auto apply = [&](const std::vector<double>& v, std::vector<double>& out, bool with_fixed) {
+#pragma omp parallel for schedule(static)
+        for (int i = 1; i < X - 1; ++i)
+            for (int j = 1; j < Y - 1; ++j)
+                for (int k = 1; k < Z - 1; ++k) {
+                    const size_t id = nodeIndex(c, i, j, k);
+                    if (!unk[id]) { out[id] = 0.0; continue; }
+                    double s = 6.0 * v[id];
+                    const int nb[6][3] = {{i - 1, j, k}, {i + 1, j, k}, {i, j - 1, k}, {i, j + 1, k}, {i, j, k - 1}, {i, j, k + 1}};
+                    for (int t = 0; t < 6; ++t) {
+                        const int a = wrap(nb[t][0], X, 0), b = wrap(nb[t][1], Y, 1), d = wrap(nb[t][2], Z, 2);
+                        const size_t nid = nodeIndex(c, a, b, d);
+                        if (unk[nid] || with_fixed) s -= v[nid];
+                    }
+                    out[id] = s;
+                }
+    };
+    double fsum = 0.0; size_t nunk = 0;
+    for (int i = 1; i < X - 1; ++i) for (int j = 1; j < Y - 1; ++j) for (int k = 1; k < Z - 1; ++k) {
+        const size_t id = nodeIndex(c, i, j, k);
+        if (unk[id]) { f[id] = c.rho[0].v[id] / c.p.eps0; fsum += f[id]; ++nunk; }
+    }
+    if (allp && nunk) { const double m = fsum / nunk; for (size_t t = 0; t < N; ++t) if (unk[t]) f[t] -= m; }
+    apply(x, Ap, true);
+    double fn = 0.0, rr = 0.0;
+    for (size_t t = 0; t < N; ++t) if (unk[t]) { r[t] = f[t] - Ap[t]; fn += f[t] * f[t]; }
+    if (allp) { double m = 0; for (size_t t = 0; t < N; ++t) if (unk[t]) m += r[t]; m /= nunk; for (size_t t = 0; t < N; ++t) if (unk[t]) r[t] -= m; }
+    for (size_t t = 0; t < N; ++t) if (unk[t]) { pp[t] = r[t]; rr += r[t] * r[t]; }
+    fn = std::sqrt(fn);
+    int it = 0;
+    const double stop = c.exact_tol * (fn > 0 ? fn : 1.0);
+    while (std::sqrt(rr) > stop && it < 20000) {
+        apply(pp, Ap, false);
+        double pAp = 0.0;
+        for (size_t t = 0; t < N; ++t) if (unk[t]) pAp += pp[t] * Ap[t];
+        const double alpha = rr / pAp;
+        double rr2 = 0.0;
+        for (size_t t = 0; t < N; ++t) if (unk[t]) { x[t] += alpha * pp[t]; r[t] -= alpha * Ap[t]; rr2 += r[t] * r[t]; }
+        const double beta = rr2 / rr;
+        rr = rr2;
+        for (size_t t = 0; t < N; ++t) if (unk[t]) pp[t] = r[t] + beta * pp[t];
+        ++it;
+    }
+    if (allp) {  // gauge: mean of the unknowns zero
+        double m = 0; for (size_t t = 0; t < N; ++t) if (unk[t]) m += x[t]; m /= nunk;
+        for (size_t t = 0; t < N; ++t) if (unk[t]) x[t] -= m;
+    }
+    for (size_t t = 0; t < N; ++t) if (unk[t]) c.phi.v[t] = x[t];
+    // glue copies of the periodic axes, as doPSOR's trailing exchanges leave them
+    copy_field_glue(c, c.phi);
+    c.last_iterations = it;
+    c.last_residual = fn > 0 ? std::sqrt(rr) / fn : 0.0;
+}
+
+// RootGrid::solvePoissonPSOR (src/Grid/RootGrid/RootGridField.cpp:65-103).
+static void solve_poisson(Ctx& c) {
+    c.poisson_error = c.phi;
+    if (c.solver_mode == 1) {
+        exact_solve(c);
+    } else {
+        constexpr double required_error = 1.0e-7;
+        int loop = 1;
+        for (; loop <= c.max_post_loop; ++loop) {
+            do_psor(c);
+            if ((loop % 10 == 0)) {
+                c.last_residual = check_phi_residual(c);
+                if (c.last_residual < required_error) break;
+            }
+        }
+        c.last_iterations = loop - 1 < c.max_post_loop ? loop : c.max_post_loop;
+    }
+    set_boundary_phi(c);
+    for (int i = 1; i < c.cx - 1; ++i) for (int j = 1; j < c.cy - 1; ++j) for (int k = 1; k < c.cz - 1; ++k)
+        c.poisson_error(i, j, k) = c.phi(i, j, k) - c.poisson_error(i, j, k);
+}
+
+// RootGrid::updateRho (src/Grid/RootGrid/RootGridField.cpp:1153-1252).
+static int update_rho(Ctx& c) {
+    for (auto& r : c.rho) r.zero();
+    int bad = 0;
+    int64_t absorbed = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad) reduction(+ : absorbed)
+    for (int pid = 0; pid < c.nsp; ++pid) {
+        const double q = c.p.species[pid].charge * c.p.species[pid].size;
+        Arr3& r = c.rho[pid + 1];
+        for (auto& p : c.particles[pid]) {
+            if (!p.isValid) continue;
+            for (auto& o : c.objects) { int b = 0; absorbed += absorb(c, o, p, b); bad |= b; }
+            if (p.isValid) {
+                const Pos pos = posXYZ(p.x, p.y, p.z);
+                const int i = pos.i, j = pos.j, k = pos.k;
+                r(i, j, k) += pos.dx2 * pos.dy2 * pos.dz2 * q;
+                r(i + 1, j, k) += pos.dx1 * pos.dy2 * pos.dz2 * q;
+                r(i, j + 1, k) += pos.dx2 * pos.dy1 * pos.dz2 * q;
+                r(i + 1, j + 1, k) += pos.dx1 * pos.dy1 * pos.dz2 * q;
+                r(i, j, k + 1) += pos.dx2 * pos.dy2 * pos.dz1 * q;
+                r(i + 1, j, k + 1) += pos.dx1 * pos.dy2 * pos.dz1 * q;
+                r(i, j + 1, k + 1) += pos.dx2 * pos.dy1 * pos.dz1 * q;
+                r(i + 1, j + 1, k + 1) += pos.dx1 * pos.dy1 * pos.dz1 * q;
+            }
+        }
+    }
+    c.absorbed_step = absorbed;
+    for (auto& o : c.objects) sum_whole_charge(c, o);
+    for (int pid = 1; pid <= c.nsp; ++pid)
+        for (size_t t = 0; t < c.rho[0].v.size(); ++t) c.rho[0].v[t] += c.rho[pid].v[t];
+    for (auto& r : c.rho) fold_node_scalar(c, r);
+    if (!c.objects.empty()) {
+        solve_poisson(c);
+        for (auto& o : c.objects) redistribute(c, o);
+        copy_field_glue(c, c.rho[0]);
+    }
+    return bad;
+}
+
+// RootGrid::updateEfield + updateReferenceEfield (RootGridField.cpp:456-582).
+static void update_efield(Ctx& c) {
+    const int X = c.cx, Y = c.cy, Z = c.cz;
+    Arr3& phi = c.phi;
+    for (int i = 0; i < X; ++i)
+        for (int j = 0; j < Y; ++j)
+            for (int k = 0; k < Z; ++k) {
+                if (i < X - 1) c.ex(i, j, k) = phi(i, j, k) - phi(i + 1, j, k);
+                if (j < Y - 1) c.ey(i, j, k) = phi(i, j, k) - phi(i, j + 1, k);
+                if (k < Z - 1) c.ez(i, j, k) = phi(i, j, k) - phi(i, j, k + 1);
+            }
+#pragma omp parallel for schedule(static)
+    for (int i = 1; i < X - 1; ++i)
+        for (int j = 1; j < Y - 1; ++j)
+            for (int k = 1; k < Z - 1; ++k) {
+                c.exref(i, j, k) = 0.5 * (c.ex(i - 1, j, k) + c.ex(i, j, k));
+                c.eyref(i, j, k) = 0.5 * (c.ey(i, j - 1, k) + c.ey(i, j, k));
+                c.ezref(i, j, k) = 0.5 * (c.ez(i, j, k - 1) + c.ez(i, j, k));
+            }
+    if (isBoundary(c, 0, 0))
+        for (int j = 1; j < Y - 1; ++j) for (int k = 1; k < Z - 1; ++k) {
+            c.exref(0, j, k) = 0.0;
+            c.exref(1, j, k) = 0.5 * (phi(3, j, k) - 4.0 * phi(2, j, k) + 3.0 * phi(1, j, k));
+        }
+    if (isBoundary(c, 0, 1))
+        for (int j = 1; j < Y - 1; ++j) for (int k = 1; k < Z - 1; ++k) {
+            c.exref(X - 1, j, k) = 0.0;
+            c.exref(X - 2, j, k) = 0.5 * (-phi(X - 4, j, k) + 4.0 * phi(X - 3, j, k) - 3.0 * phi(X - 2, j, k));
+        }
+    if (isBoundary(c, 1, 0))
+        for (int i = 1; i < X - 1; ++i) for (int k = 1; k < Z - 1; ++k) {
+            c.eyref(i, 0, k) = 0.0;
+            c.eyref(i, 1, k) = 0.5 * (phi(i, 3, k) - 4.0 * phi(i, 2, k) + 3.0 * phi(i, 1, k));
+        }
+    if (isBoundary(c, 1, 1))
+        for (int i = 1; i < X - 1; ++i) for (int k = 1; k < Z - 1; ++k) {
+            c.eyref(i, Y - 1, k) = 0.0;
+            c.eyref(i, Y - 2, k) = 0.5 * (-phi(i, Y - 4, k) + 4.0 * phi(i, Y - 3, k) - 3.0 * phi(i, Y - 2, k));
+        }
+    if (isBoundary(c, 2, 0))
+        for (int i = 1; i < X - 1; ++i) for (int j = 1; j < Y - 1; ++j) {
+            c.ezref(i, j, 0) = 0.0;
+            c.ezref(i, j, 1) = 0.5 * (phi(i, j, 3) - 4.0 * phi(i, j, 2) + 3.0 * phi(i, j, 1));
+        }
+    if (isBoundary(c, 2, 1))
+        for (int i = 1; i < X - 1; ++i) for (int j = 1; j < Y - 1; ++j) {
+            c.ezref(i, j, Z - 1) = 0.0;
+            c.ezref(i, j, Z - 2) = 0.5 * (-phi(i, j, Z - 4) + 4.0 * phi(i, j, Z - 3) - 3.0 * phi(i, j, Z - 2));
+        }
+    copy_field_glue(c, c.exref);
+    copy_field_glue(c, c.eyref);
+    copy_field_glue(c, c.ezref);
+}
+
+// ---------------------------------------------------------------- sources
+static inline double max_extent(const Ctx& c, int axis) {
+    const int n = axis == 0 ? c.nx : (axis == 1 ? c.ny : c.nz);
+    return isBoundary(c, axis, 1) ? n - 1.0 : (double)n;  // RootGrid.cpp:46-53
+}
+
+// RootGrid::RootGrid ambient loading (RootGrid.cpp:45-79) with
+// ParticleType::getTotalNumber (ParticleType.cpp:39-47),
+// AmbientParticleType::generateNewPosition/Velocity (AmbientParticleType.cpp:76-99).
+static void generate_ambient(Ctx& c) {
+    const double mx = max_extent(c, 0), my = max_extent(c, 1), mz = max_extent(c, 2);
+    for (int s = 0; s < c.nsp; ++s) {
+        const fopis_species& sp = c.p.species[s];
+        if (sp.kind != FOPIS_SPECIES_AMBIENT) continue;
+        const int64_t cxn = isBoundary(c, 0, 1) ? c.nx - 1 : c.nx;
+        const int64_t cyn = isBoundary(c, 1, 1) ? c.ny - 1 : c.ny;
+        const int64_t czn = isBoundary(c, 2, 1) ? c.nz - 1 : c.nz;
+        const int64_t total = cxn * cyn * czn * sp.particle_per_cell;
+        std::vector<Particle> out((size_t)total);
+        std::vector<unsigned char> keep((size_t)total, 1);
+#pragma omp parallel for schedule(static)
+        for (int64_t t = 0; t < total; ++t) {
+            const uint32_t a = (uint32_t)t, b = (uint32_t)(t >> 32), cc = (uint32_t)s, dtag = TAG_LOAD << 24;
+            const U2 r0 = draw2(c.p.seed, a, b, cc, dtag | 0), r1 = draw2(c.p.seed, a, b, cc, dtag | 1);
+            const U2 r2 = draw2(c.p.seed, a, b, cc, dtag | 2), r3 = draw2(c.p.seed, a, b, cc, dtag | 3);
+            Particle p;
+            p.x = 0.0 + (mx - 0.0) * r0.a; p.y = 0.0 + (my - 0.0) * r0.b; p.z = 0.0 + (mz - 0.0) * r1.a;
+            double n0, n1, n2, n3;
+            box_muller(r1.b, r2.a, n0, n1);
+            box_muller(r2.b, r3.a, n2, n3);
+            p.vx = sp.drift[0] + sp.deviation * n0;
+            p.vy = sp.drift[1] + sp.deviation * n1;
+            p.vz = sp.drift[2] + sp.deviation * n2;
+            p.typeId = s; p.isValid = 1;
+            const Pos pos = posXYZ(p.x, p.y, p.z);
+            for (const auto& o : c.objects) if (isContaining(c, o, pos)) keep[(size_t)t] = 0;
+            out[(size_t)t] = p;
+        }
+        for (int64_t t = 0; t < total; ++t) if (keep[(size_t)t]) c.particles[s].push_back(out[(size_t)t]);
+    }
+}
+
+// Injection velocity by rejection (AmbientParticleType::generateNewInjectionVelocity,
+// AmbientParticleType.cpp:101-157): all three components are redrawn until the
+// normal component points inward. Returns the attempts used (cap 256).
+static int injection_particle(const Ctx& c, int s, int face, int64_t step, uint32_t t, Particle& p) {
+    const fopis_species& sp = c.p.species[s];
+    const int axis = face / 2;
+    const double sign = (face % 2 == 0) ? 1.0 : -1.0;
+    const uint32_t cc = (uint32_t)s | ((uint32_t)face << 8), dtag = TAG_INJECT << 24;
+    double v[3];
+    int attempt = 0;
+    for (; attempt < 256; ++attempt) {
+        const U2 r0 = draw2(c.p.seed, t, (uint32_t)step, cc, dtag | (uint32_t)(2 * attempt));
+        const U2 r1 = draw2(c.p.seed, t, (uint32_t)step, cc, dtag | (uint32_t)(2 * attempt + 1));
+        double n0, n1, n2, n3;
+        box_muller(r0.a, r0.b, n0, n1);
+        box_muller(r1.a, r1.b, n2, n3);
+        const double nn[3] = {n0, n1, n2};
+        for (int a = 0; a < 3; ++a) v[a] = sp.drift[a] + (a == axis ? sp.thermal_velocity : sp.deviation) * nn[a];
+        if (!((v[axis] * sign) < 0.0)) break;
+    }
+    const U2 q0 = draw2(c.p.seed, t, (uint32_t)step, cc, dtag | 0xFFF0u);
+    const U2 q1 = draw2(c.p.seed, t, (uint32_t)step, cc, dtag | 0xFFF1u);
+    const double u[3] = {q0.a, q0.b, q1.a};
+    double lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) { lo[a] = 0.0; hi[a] = max_extent(c, a); }
+    if (face % 2 == 0) { hi[axis] = v[axis]; }                       // [0, v dt)
+    else { lo[axis] = max_extent(c, axis) + v[axis]; }               // [max + v dt, max)
+    double x[3];
+    for (int a = 0; a < 3; ++a) x[a] = lo[a] + (hi[a] - lo[a]) * u[a];  // uniform_real_distribution(lo, hi)
+    p.x = x[0]; p.y = x[1]; p.z = x[2];
+    p.vx = v[0]; p.vy = v[1]; p.vz = v[2];
+    p.typeId = s; p.isValid = 1;
+    return attempt;
+}
+
+// Node size along an axis as RootGrid::getXNodeSize (RootGrid.cpp:192-204).
+static inline int node_size(const Ctx& c, int axis) {
+    const int n = axis == 0 ? c.nx : (axis == 1 ? c.ny : c.nz);
+    return c.notb[2 * axis + 1] ? n + 1 : n;
+}
+
+// RootGrid::injectParticlesFromBoundary (src/Grid/RootGrid/RootGridParticle.cpp:3-130).
+static void inject(Ctx& c, int64_t* counts_out) {
+    int64_t injected = 0;
+    for (int s = 0; s < c.nsp; ++s) {
+        const fopis_species& sp = c.p.species[s];
+        if (sp.kind != FOPIS_SPECIES_AMBIENT) continue;
+        for (int face = 0; face < 6; ++face) {
+            const int axis = face / 2, side = face % 2;
+            if (!isBoundary(c, axis, side)) continue;
+            const int a1 = (axis + 1) % 3, a2 = (axis + 2) % 3;
+            const double area = (double)(node_size(c, a2) - 1) * (node_size(c, a1) - 1);
+            const double flux = sp.injection_axis[face] ? sp.flux[face] : 0.0;
+            const double num_double = 1.0 * area * flux;
+            const int num = (int)std::floor(num_double + c.inject_residual[s][face]);
+            c.inject_residual[s][face] += num_double - num;
+            if (counts_out) counts_out[s * 6 + face] = num;
+            std::vector<Particle> batch(num > 0 ? num : 0);
+#pragma omp parallel for schedule(static)
+            for (int t = 0; t < num; ++t) injection_particle(c, s, face, c.timestep, (uint32_t)t, batch[t]);
+            for (auto& p : batch) c.particles[s].push_back(p);
+            injected += num;
+        }
+    }
+    c.injected_step = injected;
+}
+
+// Particle::getNext{X,Y,Z}CrossPoint (src/Particle/particle.cpp:206-255).
+static Pos next_cross(const Particle& p, int axis) {
+    Pos pos = posXYZ(p.x, p.y, p.z);
+    const double v[3] = {p.vx, p.vy, p.vz};
+    const double d1[3] = {pos.dx1, pos.dy1, pos.dz1}, d2[3] = {pos.dx2, pos.dy2, pos.dz2};
+    double xyz[3] = {pos.x, pos.y, pos.z};
+    if (v[axis] > 0.0) {
+        const double m = d2[axis] / v[axis];
+        for (int a = 0; a < 3; ++a) xyz[a] = (a == axis) ? std::ceil(xyz[a]) : xyz[a] + v[a] * m;
+        pos.setXYZ(xyz[0], xyz[1], xyz[2]);
+    } else if (v[axis] < 0.0) {
+        const double m = d1[axis] / (-v[axis]);
+        for (int a = 0; a < 3; ++a) xyz[a] = (a == axis) ? std::floor(xyz[a]) : xyz[a] + v[a] * m;
+        pos.setXYZ(xyz[0], xyz[1], xyz[2]);
+    }
+    return pos;
+}
+
+// One photoelectron (PhotoElectronParticleType::generateNewParticle/Position/Velocity,
+// src/Particle/PhotoElectronParticleType.cpp:9-101, CosineEmission in
+// include/random_distribution.hpp:19-28).
+static void photo_particle(const Ctx& c, int s, int cm, int64_t step, uint32_t t, const Pos& rel,
+                           const double ev[3], int eaxis, Particle& p) {
+    const fopis_species& sp = c.p.species[s];
+    const uint32_t cc = (uint32_t)s | ((uint32_t)cm << 8), dtag = TAG_EMIT << 24;
+    const U2 r0 = draw2(c.p.seed, t, (uint32_t)step, cc, dtag | 0);
+    const U2 r1 = draw2(c.p.seed, t, (uint32_t)step, cc, dtag | 1);
+    const U2 r2 = draw2(c.p.seed, t, (uint32_t)step, cc, dtag | 2);
+    const double vth = sp.thermal_velocity;
+    const double dep = std::asin(2.0 * r0.a - 1.0);
+    const double az = 2.0 * M_PI * r0.b;
+    double v[3];
+    if (eaxis == 0) { v[0] = vth * std::cos(dep) * ev[0]; v[1] = vth * std::sin(dep) * std::cos(az); v[2] = vth * std::sin(dep) * std::sin(az); }
+    else if (eaxis == 1) { v[0] = vth * std::sin(dep) * std::sin(az); v[1] = vth * std::cos(dep) * ev[1]; v[2] = vth * std::sin(dep) * std::cos(az); }
+    else { v[0] = vth * std::sin(dep) * std::cos(az); v[1] = vth * std::sin(dep) * std::sin(az); v[2] = vth * std::cos(dep) * ev[2]; }
+    const double tw = r1.a;
+    const double w1 = r1.b, w2 = r2.a;
+    double x[3] = {rel.x + (tw - 1.0) * v[0], rel.y + (tw - 1.0) * v[1], rel.z + (tw - 1.0) * v[2]};
+    if (eaxis == 0) { x[1] += w1; x[2] += w2; }
+    else if (eaxis == 1) { x[0] += w1; x[2] += w2; }
+    else { x[0] += w1; x[1] += w2; }
+    p.x = x[0]; p.y = x[1]; p.z = x[2]; p.vx = v[0]; p.vy = v[1]; p.vz = v[2];
+    p.typeId = s; p.isValid = 1;
+}
+
+// Spacecraft::emitParticles, photoelectron branch (src/Spacecraft/Spacecraft.cpp:829-900).
+// The loop `for (int i = 0; i < emission_amount_per_area; ++i)` compares an int
+// with a double, so ceil(amount) particles leave each lit node.
+static int emit(Ctx& c) {
+    int bad = 0;
+    int64_t emitted = 0;
+    const double* sv = c.p.shine_vector;
+    int eaxis = -1;
+    for (int a = 0; a < 3; ++a) if (std::fabs(sv[a]) == 1.0) { eaxis = a; break; }
+    for (auto& o : c.objects) {
+        const int s = o.emit_species;
+        if (s < 0 || c.p.species[s].kind != FOPIS_SPECIES_PHOTOELECTRON) continue;
+        if (eaxis < 0) return -1;  // reference throws std::invalid_argument
+        const int surface_sign = (sv[eaxis] > 0.0) ? 1 : -1;
+        const double ev[3] = {-sv[0], -sv[1], -sv[2]};
+        const double q = c.p.species[s].charge * c.p.species[s].size;
+        const double amount = c.p.species[s].emission_amount;
+        for (int cm = 0; cm < o.n_cmat; ++cm) {
+            Pos pos; pos.setIJK(o.cmat[cm][0], o.cmat[cm][1], o.cmat[cm][2]);
+            const bool lit = eaxis == 0 ? isXsurfacePoint(c, o, pos, surface_sign)
+                           : eaxis == 1 ? isYsurfacePoint(c, o, pos, surface_sign)
+                                        : isZsurfacePoint(c, o, pos, surface_sign);
+            if (!lit) continue;
+            for (int t = 0; t < amount; ++t) {
+                Particle p;
+                photo_particle(c, s, cm, c.timestep, (uint32_t)t, pos, ev, eaxis, p);
+                const Pos ep = next_cross(p, eaxis);
+                if (!surface_charge(c, o, eaxis, ep, s, -q)) bad = 1;
+                o.current[s] -= q;
+                c.particles[s].push_back(p);
+                ++emitted;
+            }
+        }
+    }
+    c.emitted_step = emitted;
+    return bad;
+}
+
+// Grid::removeInvalidParticles (src/Grid/GridParticleTreatment.cpp:93-102).
+static void remove_invalid(Ctx& c) {
+    for (auto& v : c.particles)
+        v.erase(std::remove_if(v.begin(), v.end(), [](const Particle& p) { return p.isValid == 0; }), v.end());
+}
+
+// RootGrid::resetObjects (RootGridObject.cpp:162-173).
+static void reset_objects(Ctx& c) {
+    for (auto& o : c.objects) std::fill(o.current.begin(), o.current.end(), 0.0);
+}
+
+// RootGrid::mainLoopES (src/Grid/RootGrid/RootGrid.cpp:82-143).
+static int main_loop(Ctx& c) {
+    reset_objects(c);
+    update_velocity(c);
+    int bad = emit(c);
+    update_position(c);
+    inject(c, nullptr);
+    bad |= update_rho(c);
+    solve_poisson(c);
+    update_efield(c);
+    if (c.timestep % 50 == 0) remove_invalid(c);
+    ++c.timestep;
+    return bad;
+}
+
+// Gauss-Jordan inverse with partial pivoting (stands in for Eigen's inverse).
+static bool invert(std::vector<double>& A, int n) {
+    std::vector<double> I((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i) I[(size_t)i * n + i] = 1.0;
+    for (int k = 0; k < n; ++k) {
+        int piv = k; double best = std::fabs(A[(size_t)k * n + k]);
+        for (int r = k + 1; r < n; ++r) { double v = std::fabs(A[(size_t)r * n + k]); if (v > best) { best = v; piv = r; } }
+        if (best == 0.0) return false;
+        if (piv != k) for (int col = 0; col < n; ++col) { std::swap(A[(size_t)k * n + col], A[(size_t)piv * n + col]); std::swap(I[(size_t)k * n + col], I[(size_t)piv * n + col]); }
+        const double d = 1.0 / A[(size_t)k * n + k];
+        for (int col = 0; col < n; ++col) { A[(size_t)k * n + col] *= d; I[(size_t)k * n + col] *= d; }
+#pragma omp parallel for schedule(static)
+        for (int r = 0; r < n; ++r) {
+            if (r == k) continue;
+            const double f = A[(size_t)r * n + k];
+            if (f == 0.0) continue;
+            for (int col = 0; col < n; ++col) { A[(size_t)r * n + col] -= f * A[(size_t)k * n + col]; I[(size_t)r * n + col] -= f * I[(size_t)k * n + col]; }
+        }
+    }
+    A.swap(I);
+    return true;
+}
+
+// Cmatrix::total (include/Spacecraft/Cmatrix.hpp:36-44).
+static double cmat_total(const std::vector<double>& C) { double s = 0; for (double v : C) s += v; return s; }
+
+// Spacecraft::initializeChargeMapOffset (Spacecraft.cpp:160-183).
+static void charge_map_offset(Ctx& c, Object& o) {
+    if (o.initial_potential_offset == 0.0) return;
+    o.potential = o.initial_potential_offset;
+    for (int i = 0; i < o.n_cmat; ++i) {
+        double d = 0.0;
+        for (int j = 0; j < o.n_cmat; ++j) d += o.C[(size_t)i * o.n_cmat + j] * o.potential;
+        o.charge_map[i] += d;  // species row 0
+    }
+}
+
+// RootGrid::initializeObjectsCmatrix (RootGridObject.cpp:77-148): column c holds
+// phi at every surface node for rho = 1 at node c; the matrix stored is
+// capacity_matrix(col = c, row = r) and is then inverted.
+static bool build_cmatrix(Ctx& c, Object& o) {
+    const int n = o.n_cmat;
+    std::vector<double> M((size_t)n * n);
+    for (auto& r : c.rho) r.zero();
+    for (int col = 0; col < n; ++col) {
+        c.phi.zero();
+        const auto& nd = o.cmat[col];
+        c.rho[0](nd[0], nd[1], nd[2]) = 1.0;
+        solve_poisson(c);
+        for (int row = 0; row < n; ++row) {
+            const auto& t = o.cmat[row];
+            M[(size_t)col * n + row] = c.phi(t[0], t[1], t[2]);
+        }
+        c.rho[0](nd[0], nd[1], nd[2]) = 0.0;
+    }
+    c.phi.zero();
+    if (!invert(M, n)) return false;
+    o.C.swap(M);
+    o.total_cmat_value = cmat_total(o.C);
+    o.has_C = true;
+    charge_map_offset(c, o);
+    return true;
+}
+
+// ---------------------------------------------------------------- .obj loader
+// ObjectUtils::getObjectNodesFromObjFile (src/Spacecraft/ObjectUtils.cpp:9-333),
+// without textures and the connectivity list (not used on the ES path).
+// Outputs glue-layout indices (getRelativePositionOnRootWithGlue adds 1).
+static int parse_obj(const char* path, int nx, int ny, int nz, std::vector<std::array<int, 3>>& nodes,
+                     std::vector<std::array<int, 3>>& cells) {
+    std::ifstream in(path);
+    if (!in) return -1;
+    std::vector<int> node_map((size_t)nx * ny * nz, -1);
+    auto nm = [&](int i, int j, int k) -> int& { return node_map[((size_t)i * ny + j) * nz + k]; };
+    std::vector<unsigned char> xf((size_t)nx * ny * nz, 0), yf(xf.size(), 0), zf(xf.size(), 0);
+    auto fi = [&](int i, int j, int k) { return ((size_t)i * ny + j) * nz + k; };
+    std::vector<std::array<int, 3>> verts;
+    std::vector<std::array<int, 4>> faces;
+    std::string line;
+    while (std::getline(in, line)) {
+        if (line.size() > 2 && line[0] == 'v' && line[1] == ' ') {
+            std::istringstream ss(line.substr(2));
+            int a, b, d; ss >> a >> b >> d;
+            verts.push_back({a + nx / 2, b + ny / 2, d + nz / 2});
+        } else if (line.size() > 2 && line[0] == 'f' && line[1] == ' ') {
+            std::istringstream ss(line.substr(2));
+            std::array<int, 4> f{};
+            for (int t = 0; t < 4; ++t) { std::string tok; ss >> tok; f[t] = std::atoi(tok.substr(0, tok.find('/')).c_str()); }
+            faces.push_back(f);
+        }
+    }
+    for (const auto& f : faces) {
+        const auto& v1 = verts[f[0] - 1]; const auto& v2 = verts[f[1] - 1];
+        const auto& v3 = verts[f[2] - 1]; const auto& v4 = verts[f[3] - 1];
+        int ax = -1;
+        for (int a = 0; a < 3; ++a) if (v1[a] == v2[a] && v1[a] == v3[a] && v1[a] == v4[a]) { ax = a; break; }
+        if (ax < 0) return -2;
+        const int b1 = (ax == 0) ? 1 : 0, b2 = (ax == 2) ? 1 : 2;
+        const int mn1 = std::min({v1[b1], v2[b1], v3[b1], v4[b1]}), mx1 = std::max({v1[b1], v2[b1], v3[b1], v4[b1]});
+        const int mn2 = std::min({v1[b2], v2[b2], v3[b2], v4[b2]}), mx2 = std::max({v1[b2], v2[b2], v3[b2], v4[b2]});
+        for (int u = mn1; u <= mx1; ++u)
+            for (int w = mn2; w <= mx2; ++w) {
+                int ijk[3]; ijk[ax] = v1[ax]; ijk[b1] = u; ijk[b2] = w;
+                if (nm(ijk[0], ijk[1], ijk[2]) < 0) { nm(ijk[0], ijk[1], ijk[2]) = (int)nodes.size(); nodes.push_back({ijk[0], ijk[1], ijk[2]}); }
+                if (u != mx1 && w != mx2) { auto& fm = (ax == 0 ? xf : (ax == 1 ? yf : zf)); fm[fi(ijk[0], ijk[1], ijk[2])] = 1; }
+            }
+    }
+    std::vector<int> cnt((size_t)nx * ny * nz, 0);
+    auto scan = [&](int axis) {
+        const int na = axis == 0 ? nx : (axis == 1 ? ny : nz);
+        const int o1 = axis == 0 ? ny : nx, o2 = axis == 2 ? ny : nz;
+        const auto& fm = (axis == 0 ? xf : (axis == 1 ? yf : zf));
+        for (int p = 0; p < o1 - 1; ++p)
+            for (int q = 0; q < o2 - 1; ++q)
+                for (int lo = 0; lo < na - 1; ++lo) {
+                    auto at = [&](int s) { int ijk[3]; ijk[axis] = s; ijk[axis == 0 ? 1 : 0] = p; ijk[axis == 2 ? 1 : 2] = q; return fi(ijk[0], ijk[1], ijk[2]); };
+                    if (!fm[at(lo)]) continue;
+                    for (int up = lo + 1; up < na - 1; ++up) {
+                        if (fm[at(up)]) { for (int s = lo; s < up; ++s) cnt[at(s)] += 1; lo = up; break; }
+                    }
+                }
+    };
+    scan(0); scan(1); scan(2);
+    for (int i = 0; i < nx - 1; ++i) for (int j = 0; j < ny - 1; ++j) for (int k = 0; k < nz - 1; ++k)
+        if (cnt[fi(i, j, k)] == 3) cells.push_back({i + 1, j + 1, k + 1});
+    for (auto& n : nodes) { n[0] += 1; n[1] += 1; n[2] += 1; }
+    return 0;
+}
+
+// ---------------------------------------------------------------- fixed-point replay
+// Integer CIC weights of the split-precision deposit: each in-cell offset is
+// rounded to 17 fractional bits (round half to even) and the eight corner
+// weights are products of (2^17 - a) or a per axis, so they sum to 2^51.
+static inline int64_t qoff(float o) { return (int64_t)std::nearbyintf(o * 131072.0f); }
+
+}  // namespace orc
+
+using namespace orc;
+
+extern "C" {
+
+void* orc_create(const fopis_params* p) {
+    Ctx* c = new Ctx();
+    init_ctx(*c, p);
+    return c;
+}
+void orc_destroy(void* h) { delete (Ctx*)h; }
+int orc_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#endif
+}
+
+// Philox known-answer access for tests.
+void orc_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    uint32_t c[4] = {ctr[0], ctr[1], ctr[2], ctr[3]};
+    philox4x32_10(c, key[0], key[1]);
+    for (int t = 0; t < 4; ++t) out[t] = c[t];
+}
+
+// The oracle's Position::setXYZ on n points: ijk[3n], d[6n] = dx1,dy1,dz1,dx2,dy2,dz2.
+void orc_position(const double* xyz, int64_t n, int32_t* ijk, double* d) {
+    for (int64_t t = 0; t < n; ++t) {
+        const Pos p = posXYZ(xyz[3 * t], xyz[3 * t + 1], xyz[3 * t + 2]);
+        ijk[3 * t] = p.i; ijk[3 * t + 1] = p.j; ijk[3 * t + 2] = p.k;
+        d[6 * t] = p.dx1; d[6 * t + 1] = p.dy1; d[6 * t + 2] = p.dz1;
+        d[6 * t + 3] = p.dx2; d[6 * t + 4] = p.dy2; d[6 * t + 5] = p.dz2;
+    }
+}
+
+void orc_set_solver(void* h, int mode, int max_post_loop, double exact_tol) {
+    Ctx* c = (Ctx*)h;
+    c->solver_mode = mode;
+    if (max_post_loop > 0) c->max_post_loop = max_post_loop;
+    if (exact_tol > 0) c->exact_tol = exact_tol;
+}
+void orc_solver_stats(void* h, int* iterations, double* residual) {
+    Ctx* c = (Ctx*)h; *iterations = c->last_iterations; *residual = c->last_residual;
+}
+
+int orc_add_object(void* h, const fopis_object_desc* d) {
+    Ctx* c = (Ctx*)h;
+    Object o;
+    o.n_cmat = d->n_cmat;
+    o.cmat.resize(d->n_cmat);
+    o.node_to_cmat.assign((size_t)c->cx * c->cy * c->cz, -1);
+    for (int m = 0; m < d->n_cmat; ++m) {
+        o.cmat[m] = {d->cmat_nodes[3 * m], d->cmat_nodes[3 * m + 1], d->cmat_nodes[3 * m + 2]};
+        o.node_to_cmat[nodeIndex(*c, o.cmat[m][0], o.cmat[m][1], o.cmat[m][2])] = m;
+    }
+    o.cell_map.assign((size_t)(c->nx + 1) * (c->ny + 1) * (c->nz + 1), 0);
+    for (int m = 0; m < d->n_cells; ++m)
+        o.cell_map[cellIndex(*c, d->cells[3 * m], d->cells[3 * m + 1], d->cells[3 * m + 2])] = 1;
+    o.charge_map.assign((size_t)c->nsp * o.n_cmat, 0.0);
+    o.tmp_charge_map.assign((size_t)c->nsp * o.n_cmat, 0.0);
+    o.current.assign(c->nsp, 0.0);
+    o.is_potential_fixed = d->is_potential_fixed;
+    o.fixed_potential = d->fixed_potential;
+    o.initial_potential_offset = d->initial_potential_offset;
+    o.emit_species = d->emit_species;
+    c->objects.push_back(std::move(o));
+    return (int)c->objects.size() - 1;
+}
+int orc_build_cmatrix(void* h, int obj) {
+    Ctx* c = (Ctx*)h;
+    return build_cmatrix(*c, c->objects[obj]) ? 0 : -1;
+}
+int orc_set_cmatrix(void* h, int obj, const double* C, int n) {
+    Ctx* c = (Ctx*)h; Object& o = c->objects[obj];
+    if (n != o.n_cmat) return -1;
+    o.C.assign(C, C + (size_t)n * n);
+    o.total_cmat_value = cmat_total(o.C);
+    o.has_C = true;
+    charge_map_offset(*c, o);
+    return 0;
+}
+int orc_get_cmatrix(void* h, int obj, double* C, int n) {
+    Ctx* c = (Ctx*)h; Object& o = c->objects[obj];
+    if (n != o.n_cmat || !o.has_C) return -1;
+    std::memcpy(C, o.C.data(), sizeof(double) * (size_t)n * n);
+    return 0;
+}
+void orc_get_object(void* h, int obj, double* V, double* Q, double* current) {
+    Ctx* c = (Ctx*)h; Object& o = c->objects[obj];
+    *V = o.potential; *Q = o.total_charge;
+    for (int s = 0; s < c->nsp; ++s) current[s] = o.current[s];
+}
+void orc_get_charge_map(void* h, int obj, double* out) {
+    Ctx* c = (Ctx*)h; Object& o = c->objects[obj];
+    std::memcpy(out, o.charge_map.data(), sizeof(double) * o.charge_map.size());
+}
+
+int64_t orc_load_particles(void* h, int s, const void* aos, int64_t n) {
+    Ctx* c = (Ctx*)h;
+    const Particle* p = (const Particle*)aos;
+    int64_t k = 0;
+    for (int64_t t = 0; t < n; ++t) if (p[t].isValid) { Particle q = p[t]; q.typeId = s; c->particles[s].push_back(q); ++k; }
+    return k;
+}
+int64_t orc_num_particles(void* h, int s) {
+    Ctx* c = (Ctx*)h; int64_t k = 0;
+    for (const auto& p : c->particles[s]) k += p.isValid;
+    return k;
+}
+int64_t orc_get_particles(void* h, int s, void* aos, int64_t cap) {
+    Ctx* c = (Ctx*)h; Particle* out = (Particle*)aos; int64_t k = 0;
+    for (const auto& p : c->particles[s]) if (p.isValid) { if (k < cap) out[k] = p; ++k; }
+    return k;
+}
+void orc_generate_ambient(void* h) { generate_ambient(*(Ctx*)h); }
+
+void orc_reset_objects(void* h) { reset_objects(*(Ctx*)h); }
+void orc_update_velocity(void* h) { update_velocity(*(Ctx*)h); }
+int orc_emit(void* h) { return emit(*(Ctx*)h); }
+void orc_update_position(void* h) { update_position(*(Ctx*)h); }
+void orc_inject(void* h, int64_t* counts) { inject(*(Ctx*)h, counts); }
+int orc_update_rho(void* h) { return update_rho(*(Ctx*)h); }
+void orc_solve_poisson(void* h) { solve_poisson(*(Ctx*)h); }
+void orc_update_efield(void* h) { update_efield(*(Ctx*)h); }
+void orc_remove_invalid(void* h) { remove_invalid(*(Ctx*)h); }
+int orc_main_loop(void* h, int n) { int bad = 0; for (int t = 0; t < n; ++t) bad |= main_loop(*(Ctx*)h); return bad; }
+// Grid::initialize (src/Grid/Grid.cpp:23-36).
+int orc_initialize(void* h) {
+    Ctx* c = (Ctx*)h;
+    int bad = update_rho(*c);
+    solve_poisson(*c);
+    update_efield(*c);
+    return bad;
+}
+void orc_set_timestep(void* h, int64_t t) { ((Ctx*)h)->timestep = t; }
+int64_t orc_get_timestep(void* h) { return ((Ctx*)h)->timestep; }
+void orc_step_counts(void* h, int64_t* injected, int64_t* emitted, int64_t* absorbed) {
+    Ctx* c = (Ctx*)h; *injected = c->injected_step; *emitted = c->emitted_step; *absorbed = c->absorbed_step;
+}
+
+// which: 0 phi, 1 rho0, 2..4 E ref, 16+s rho species, 32..34 edge E (their own shapes)
+int orc_get_field(void* h, int which, double* out) {
+    Ctx* c = (Ctx*)h;
+    const Arr3* a = nullptr;
+    switch (which) {
+        case 0: a = &c->phi; break;
+        case 1: a = &c->rho[0]; break;
+        case 2: a = &c->exref; break;
+        case 3: a = &c->eyref; break;
+        case 4: a = &c->ezref; break;
+        case 32: a = &c->ex; break;
+        case 33: a = &c->ey; break;
+        case 34: a = &c->ez; break;
+        default:
+            if (which >= 16 && which < 16 + c->nsp) a = &c->rho[which - 15];
+    }
+    if (!a) return -1;
+    std::memcpy(out, a->v.data(), sizeof(double) * a->v.size());
+    return 0;
+}
+int orc_set_field(void* h, int which, const double* in) {
+    Ctx* c = (Ctx*)h;
+    Arr3* a = which == 0 ? &c->phi : (which == 1 ? &c->rho[0] : nullptr);
+    if (!a) return -1;
+    std::memcpy(a->v.data(), in, sizeof(double) * a->v.size());
+    return 0;
+}
+
+// Grid::getParticleEnergy (GridParticleTreatment.cpp:104-118) and
+// Field::getEfieldEnergy (Field.cpp:194-213).
+void orc_energy(void* h, double* pe, double* fe) {
+    Ctx* c = (Ctx*)h;
+    double res = 0.0;
+    for (int s = 0; s < c->nsp; ++s) {
+        double e = 0.0;
+        for (const auto& p : c->particles[s]) if (p.isValid) e += p.vx * p.vx + p.vy * p.vy + p.vz * p.vz;
+        res += 0.5 * c->p.species[s].mass * e * c->p.species[s].size;
+    }
+    *pe = res;
+    double en = 0.0;
+    const int X = c->cx, Y = c->cy, Z = c->cz;
+    for (int i = 1; i < X - 1; ++i) for (int j = 1; j < Y - 1; ++j) for (int k = 1; k < Z - 1; ++k) {
+        if (i < X - 2) en += c->ex(i, j, k) * c->ex(i, j, k);
+        if (j < Y - 2) en += c->ey(i, j, k) * c->ey(i, j, k);
+        if (k < Z - 2) en += c->ez(i, j, k) * c->ez(i, j, k);
+    }
+    *fe = 0.5 * c->p.eps0 * en;
+}
+
+int orc_parse_obj(const char* path, int nx, int ny, int nz, int32_t* nodes, int cap_nodes, int* n_nodes,
+                  int32_t* cells, int cap_cells, int* n_cells) {
+    std::vector<std::array<int, 3>> nd, cl;
+    const int rc = parse_obj(path, nx, ny, nz, nd, cl);
+    if (rc) return rc;
+    *n_nodes = (int)nd.size(); *n_cells = (int)cl.size();
+    for (int t = 0; t < (int)nd.size() && t < cap_nodes; ++t) for (int a = 0; a < 3; ++a) nodes[3 * t + a] = nd[t][a];
+    for (int t = 0; t < (int)cl.size() && t < cap_cells; ++t) for (int a = 0; a < 3; ++a) cells[3 * t + a] = cl[t][a];
+    return 0;
+}
+
+// Fixed-point replay of the split-precision CIC deposit for one species:
+// out[node] += integer corner weight (sum 2^51 per particle). cell is the
+// particle's glue-layout node cell packed as (i << 20) | (j << 10) | k.
+void orc_fixed_deposit(const fopis_params* p, const int32_t* cell, const float* ox, const float* oy,
+                       const float* oz, int64_t n, int64_t* out) {
+    const int cy = p->ny + 2, cz = p->nz + 2;
+    const int64_t A = 131072;
+    const int64_t sj = cz, si = (int64_t)cy * cz;
+    for (int64_t t = 0; t < n; ++t) {
+        if (cell[t] < 0) continue;
+        const int64_t a = qoff(ox[t]), b = qoff(oy[t]), d = qoff(oz[t]);
+        const int64_t wx[2] = {A - a, a}, wy[2] = {A - b, b}, wz[2] = {A - d, d};
+        const int ci = (cell[t] >> 20) & 1023, cj = (cell[t] >> 10) & 1023, ck = cell[t] & 1023;
+        const int64_t base = ((int64_t)ci * cy + cj) * cz + ck;
+        for (int di = 0; di < 2; ++di) for (int dj = 0; dj < 2; ++dj) for (int dk = 0; dk < 2; ++dk)
+            out[base + di * si + dj * sj + dk] += wx[di] * wy[dj] * wz[dk];
+    }
+}
+// Periodic fold of an integer node array (same semantics as fold_node_scalar).
+void orc_fixed_fold(const fopis_params* p, int64_t* a) {
+    const int X = p->nx + 2, Y = p->ny + 2, Z = p->nz + 2;
+    auto at = [&](int i, int j, int k) -> int64_t& { return a[((size_t)i * Y + j) * Z + k]; };
+    if (p->boundary[0] == 'P')
+        for (int j = 0; j < Y; ++j) for (int k = 0; k < Z; ++k) {
+            int64_t s0 = at(0, j, k) + at(X - 2, j, k), s1 = at(1, j, k) + at(X - 1, j, k);
+            at(0, j, k) = s0; at(X - 2, j, k) = s0; at(1, j, k) = s1; at(X - 1, j, k) = s1;
+        }
+    if (p->boundary[2] == 'P')
+        for (int i = 0; i < X; ++i) for (int k = 0; k < Z; ++k) {
+            int64_t s0 = at(i, 0, k) + at(i, Y - 2, k), s1 = at(i, 1, k) + at(i, Y - 1, k);
+            at(i, 0, k) = s0; at(i, Y - 2, k) = s0; at(i, 1, k) = s1; at(i, Y - 1, k) = s1;
+        }
+    if (p->boundary[4] == 'P')
+        for (int i = 0; i < X; ++i) for (int j = 0; j < Y; ++j) {
+            int64_t s0 = at(i, j, 0) + at(i, j, Z - 2), s1 = at(i, j, 1) + at(i, j, Z - 1);
+            at(i, j, 0) = s0; at(i, j, Z - 2) = s0; at(i, j, 1) = s1; at(i, j, Z - 1) = s1;
+        }
+}
+
+}  // extern "C"
