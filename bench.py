@@ -156,6 +156,8 @@ def run_gpu(args, world, rank, local):
     push_ms, vcyc, pushed = [], [], []
     barrier(world)
     torch.cuda.synchronize(local)
+    if args.profile:
+        torch.cuda.profiler.start()
     with ClockSampler(local) as clk:
         ev0.record(stream)
         for _ in range(args.steps):
@@ -168,6 +170,8 @@ def run_gpu(args, world, rank, local):
             vcyc.append(st.vcycles_step)
         ev1.record(stream)
         torch.cuda.synchronize(local)
+    if args.profile:
+        torch.cuda.profiler.stop()
     barrier(world)
     ms = ev0.elapsed_time(ev1)
     launches = g.stats().kernel_launches - launches0
@@ -268,6 +272,7 @@ def main():
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu", dest="cpu", action="store_false")
     ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--profile", action="store_true", help="cudaProfilerStart/Stop around the timed steps")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
