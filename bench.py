@@ -153,20 +153,23 @@ def run_gpu(args, world, rank, local):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     launches0 = g.stats().kernel_launches
     psteps = 0
-    push_ms, vcyc, pushed = [], [], []
+    push_ms, vcyc, pushed, phases_all = [], [], [], []
     barrier(world)
     torch.cuda.synchronize(local)
     if args.profile:
         torch.cuda.profiler.start()
+    step_ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     with ClockSampler(local) as clk:
         ev0.record(stream)
-        for _ in range(args.steps):
+        for t in range(args.steps):
             n_before = total_particles(g.stats(), nsp)
             g.mainLoopES(1)
+            step_ev[t].record(stream)
             st = g.stats()
             psteps += n_before
             pushed.append(n_before)
             push_ms.append(st.ms_phase[0])
+            phases_all.append([round(x, 3) for x in st.ms_phase])
             vcyc.append(st.vcycles_step)
         ev1.record(stream)
         torch.cuda.synchronize(local)
@@ -174,6 +177,7 @@ def run_gpu(args, world, rank, local):
         torch.cuda.profiler.stop()
     barrier(world)
     ms = ev0.elapsed_time(ev1)
+    step_ms = [ev0.elapsed_time(step_ev[0])] + [step_ev[t - 1].elapsed_time(step_ev[t]) for t in range(1, args.steps)]
     launches = g.stats().kernel_launches - launches0
     ms_max = allreduce(ms, "max", world)
     psteps_all = allreduce(float(psteps), "sum", world)
@@ -184,6 +188,7 @@ def run_gpu(args, world, rank, local):
         "push_ms": float(np.mean(push_ms)), "pushed": float(np.mean(pushed)),
         "vcycles_per_step": float(np.mean(vcyc)), "phases_last": phases, "t_cmat": t_cmat,
         "particles": total_particles(st, nsp), "n_cmat": [len(o.nodes) for o in cfg.objects],
+        "step_ms": [round(x, 3) for x in step_ms], "phases_all": phases_all,
     }
     Cm = g.get_cmatrix(0) if cfg.objects else None
     V, Q, cur = g.getObject(0) if cfg.objects else (0.0, 0.0, None)
@@ -268,11 +273,12 @@ def main():
     ap.add_argument("--impl", default="fopis", choices=["fopis", "reference"])
     ap.add_argument("--workload", default="cube128")
     ap.add_argument("--ppc", type=int, default=32)
-    ap.add_argument("--sort-interval", type=int, default=4)
+    ap.add_argument("--sort-interval", type=int, default=8)
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu", dest="cpu", action="store_false")
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--profile", action="store_true", help="cudaProfilerStart/Stop around the timed steps")
+    ap.add_argument("--phases", action="store_true", help="report the phase times of every timed step")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
@@ -329,6 +335,10 @@ def main():
     line["phases_ms_last_step"] = dict(zip(["push", "emit", "inject", "absorb", "rho+solve1", "solve2", "efield",
                                             "sort"], [round(x, 4) for x in res["phases_last"]]))
     line["spacecraft_potential_V"] = res["potential_V"]
+    line["step_ms"] = res["step_ms"]
+    if args.phases:
+        line["phases_all"] = res["phases_all"]
+    line["setup_cmatrix_s"] = round(res["t_cmat"], 2)
     if "e2e" in res:
         line["e2e"] = res["e2e"]
     if rank == 0 and res["cmatrix"] is not None:

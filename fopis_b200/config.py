@@ -158,7 +158,7 @@ def _species_struct(sp: SpeciesInfo, norm: Normalizer, dx: float) -> _abi.Specie
 
 def make_params(nxyz: Tuple[int, int, int], boundary: str, dx: float, dt: float, species: List[SpeciesInfo],
                 bfield_nT=(0.0, 0.0, 0.0), shine=(0.0, 0.0, 0.0), seed: int = 12345, tol: float = 1e-8,
-                max_vcycles: int = 100, sort_interval: int = 4, guess: int = _abi.GUESS_WARM,
+                max_vcycles: int = 100, sort_interval: int = 8, guess: int = _abi.GUESS_WARM,
                 capacity_factor: float = 1.5) -> Tuple[_abi.Params, Normalizer]:
     norm = Normalizer(dx, dt)
     p = _abi.Params()

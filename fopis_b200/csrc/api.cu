@@ -150,7 +150,7 @@ int one_step(Ctx& c) {
     efield_update(c);
     record(c, 7);
     if (c.unet) unet_observe(c);
-    const int si = c.p.sort_interval > 0 ? c.p.sort_interval : 4;
+    const int si = c.p.sort_interval > 0 ? c.p.sort_interval : 8;
     if (c.timestep % si == 0) particles_sort(c);
     record(c, 8);
     int rc = check_device(c);
@@ -208,6 +208,12 @@ int fopis_create(const fopis_params* p, int device, void** out) {
         if (device < 0) cudaGetDevice(&x.device);
         FOPIS_CUDA(cudaSetDevice(x.device));
         FOPIS_CUDA(cudaStreamCreateWithFlags(&x.st, cudaStreamNonBlocking));
+        {   // the particle arrays grow through this process's default pool: keep freed blocks cached
+            cudaMemPool_t pool;
+            FOPIS_CUDA(cudaDeviceGetDefaultMemPool(&pool, x.device));
+            uint64_t keep = UINT64_MAX;
+            FOPIS_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        }
         x.nx = p->nx; x.ny = p->ny; x.nz = p->nz;
         x.cx = x.nx + 2; x.cy = x.ny + 2; x.cz = x.nz + 2;
         x.N = (size_t)x.cx * x.cy * x.cz;
@@ -222,9 +228,10 @@ int fopis_create(const fopis_params* p, int device, void** out) {
         FOPIS_CUDA(cudaMalloc(&x.E, sizeof(float4) * x.N));
         FOPIS_CUDA(cudaMalloc(&x.cellmap, x.N));
         FOPIS_CUDA(cudaMalloc(&x.node_cmat, sizeof(int32_t) * x.N));
-        FOPIS_CUDA(cudaMalloc(&x.sort_count, sizeof(int32_t) * (x.N + 1)));
-        FOPIS_CUDA(cudaMalloc(&x.sort_offset, sizeof(int32_t) * (x.N + 1)));
-        const size_t tiles = (x.N + 1 + 8191) / 8192;
+        const size_t keys = std::max<size_t>(x.N, (size_t)brick_keys(x));
+        FOPIS_CUDA(cudaMalloc(&x.sort_count, sizeof(int32_t) * (keys + 1)));
+        FOPIS_CUDA(cudaMalloc(&x.sort_offset, sizeof(int32_t) * (keys + 1)));
+        const size_t tiles = (keys + 1 + 8191) / 8192;
         FOPIS_CUDA(cudaMalloc(&x.scan_partials, sizeof(int32_t) * (tiles + 1)));
         FOPIS_CUDA(cudaMemset(x.rho_i64, 0, sizeof(unsigned long long) * x.N * x.nsp));
         FOPIS_CUDA(cudaMemset(x.rho0, 0, sizeof(double) * x.N));
@@ -267,10 +274,12 @@ void fopis_destroy(void* h) {
     for (int s = 0; s < FOPIS_MAX_SPECIES; ++s) {
         Soa* v[2] = {&c->sp[s], &c->sp2[s]};
         for (Soa* q : v) {
-            cudaFree(q->cell); cudaFree(q->ox); cudaFree(q->oy); cudaFree(q->oz);
-            cudaFree(q->vx); cudaFree(q->vy); cudaFree(q->vz);
+            void* arr[7] = {q->cell, q->ox, q->oy, q->oz, q->vx, q->vy, q->vz};
+            for (void* a : arr) if (a) cudaFreeAsync(a, c->st);
         }
     }
+    if (c->st) cudaStreamSynchronize(c->st);
+    for (int s = 0; s < FOPIS_MAX_SPECIES; ++s) if (c->brick_start[s]) cudaFree(c->brick_start[s]);
     for (auto& o : c->objs) {
         cudaFree(o.nodes); cudaFree(o.C); cudaFree(o.colsum); cudaFree(o.charge_tmp);
         cudaFree(o.charge_map); cudaFree(o.phis); cudaFree(o.scal); cudaFree(o.lit);
@@ -487,7 +496,7 @@ int fopis_update_efield(void* h) {
 
 int fopis_advance_timestep(void* h) {
     return guarded(h, [&](Ctx& c) -> int {
-        const int si = c.p.sort_interval > 0 ? c.p.sort_interval : 4;
+        const int si = c.p.sort_interval > 0 ? c.p.sort_interval : 8;
         if (c.timestep % si == 0) particles_sort(c);
         c.timestep += 1;
         return FOPIS_OK;

@@ -163,6 +163,8 @@ struct Ctx {
     Soa sp2[FOPIS_MAX_SPECIES];   // sort targets
     int64_t cap[FOPIS_MAX_SPECIES] = {0};
     int64_t nslots[FOPIS_MAX_SPECIES] = {0};   // host mirror of DevScalars::count
+    int64_t sorted_n[FOPIS_MAX_SPECIES] = {0}; // slots [0, sorted_n) are brick-sorted
+    int32_t* brick_start[FOPIS_MAX_SPECIES] = {nullptr};  // first slot of each brick
     // fields
     unsigned long long* rho_i64 = nullptr;  // [nsp][N] two's complement fixed point
     double* rho0 = nullptr;
@@ -182,6 +184,10 @@ struct Ctx {
     // multigrid
     std::vector<MGLevel> mg;
     double* coarse64 = nullptr;
+    cudaGraph_t mg_graph = nullptr;  // one refinement iteration, recorded once
+    cudaGraphExec_t mg_exec = nullptr;
+    int64_t cycle_launches = 0;      // kernels in that graph
+    int mg_cta_start = -1;           // first level whose V-cycle runs inside one CTA
     double* red_partials = nullptr;  // block partial sums
     int red_blocks = 0;
     // objects
@@ -216,6 +222,7 @@ int64_t particles_export_raw(Ctx& c, int s, int32_t* cell, float* ox, float* oy,
                              float* vx, float* vy, float* vz, int64_t cap);
 void particles_generate_ambient(Ctx& c);
 void particles_sort(Ctx& c);
+int64_t brick_keys(const Ctx& c);
 void launch_push(Ctx& c, bool vel, bool pos, bool dep);
 void launch_deposit_all(Ctx& c);
 void launch_emit(Ctx& c, bool fused);

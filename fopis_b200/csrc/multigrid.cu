@@ -24,7 +24,7 @@ namespace fopis {
 namespace {
 
 constexpr int kT = 256;
-constexpr int kRedBlocks = 148 * 2;
+constexpr int kRedBlocks = 148 * 8;
 constexpr int kCoarseMax = 8192;    // unknowns the single-CTA coarsest solve holds (3 FP64 arrays, 192 KB)
 
 struct Lv {
@@ -39,60 +39,80 @@ Lv lv(const MGLevel& m) {
     return Lv{m.n[0], m.n[1], m.n[2], m.per[0], m.per[1], m.per[2], m.u, m.f, m.r, (float)(1.0 / m.scale)};
 }
 
-int nblocks(long long n) {
-    long long b = (n + kT - 1) / kT;
-    return (int)std::max<long long>(1, std::min<long long>(b, 148LL * 32));
+// Kernels walk rows: block b takes rows (a, b) of the level in a grid-stride
+// loop (one 32-bit division per row), threads run along the contiguous axis.
+constexpr int kRowThreads = 128;
+int row_blocks(long long rows) { return (int)std::max<long long>(1, std::min<long long>(rows, 1LL << 30)); }
+
+__device__ __forceinline__ int wrap_or_out(int q, int n, int per) {
+    if (q < 0) return per ? q + n : -1;
+    if (q >= n) return per ? q - n : -1;
+    return q;
 }
 
-__device__ __forceinline__ float nb(const float* u, int n, int per, long long base, long long stride, int idx, int d) {
-    int q = idx + d;
-    if (q < 0) { if (!per) return 0.0f; q += n; }
-    else if (q >= n) { if (!per) return 0.0f; q -= n; }
-    return u[base + (long long)(q - idx) * stride];
+// The four neighbour rows (a-1, a+1, b-1, b+1) of row (a, b); null where the
+// homogeneous Dirichlet closure gives zero.
+struct NRows { const float* r[4]; };
+__device__ __forceinline__ NRows neighbour_rows(const Lv& L, const float* u, int a, int b) {
+    NRows n;
+    const int am = wrap_or_out(a - 1, L.n0, L.p0), ap = wrap_or_out(a + 1, L.n0, L.p0);
+    const int bm = wrap_or_out(b - 1, L.n1, L.p1), bp = wrap_or_out(b + 1, L.n1, L.p1);
+    n.r[0] = am >= 0 ? u + ((long long)am * L.n1 + b) * L.n2 : nullptr;
+    n.r[1] = ap >= 0 ? u + ((long long)ap * L.n1 + b) * L.n2 : nullptr;
+    n.r[2] = bm >= 0 ? u + ((long long)a * L.n1 + bm) * L.n2 : nullptr;
+    n.r[3] = bp >= 0 ? u + ((long long)a * L.n1 + bp) * L.n2 : nullptr;
+    return n;
 }
 
-// Six-neighbour sum at (a,b,c) with homogeneous Dirichlet or periodic closure.
-__device__ __forceinline__ float nsum(const Lv& L, const float* u, int a, int b, int c) {
-    const long long s1 = L.n2, s0 = (long long)L.n1 * L.n2;
-    const long long id = a * s0 + b * s1 + c;
-    return nb(u, L.n0, L.p0, id, s0, a, -1) + nb(u, L.n0, L.p0, id, s0, a, 1) +
-           nb(u, L.n1, L.p1, id, s1, b, -1) + nb(u, L.n1, L.p1, id, s1, b, 1) +
-           nb(u, L.n2, L.p2, id, 1, c, -1) + nb(u, L.n2, L.p2, id, 1, c, 1);
+// Six-neighbour sum at column c of a row, in the order -a, +a, -b, +b, -c, +c.
+__device__ __forceinline__ float nsum_row(const Lv& L, const float* row, const NRows& n, int c) {
+    float s = (n.r[0] ? n.r[0][c] : 0.0f) + (n.r[1] ? n.r[1][c] : 0.0f) + (n.r[2] ? n.r[2][c] : 0.0f) +
+              (n.r[3] ? n.r[3][c] : 0.0f);
+    const float cm = c > 0 ? row[c - 1] : (L.p2 ? row[L.n2 - 1] : 0.0f);
+    const float cp = c < L.n2 - 1 ? row[c + 1] : (L.p2 ? row[0] : 0.0f);
+    return s + cm + cp;
 }
 
-// One red-black half sweep: u <- (1-w) u + w (sum(nb) + f/scale) / 6 on the
-// nodes with (a+b+c) % 2 == color; thread t owns every other node of a row.
-__global__ void rb_smooth_kernel(Lv L, int color, float omega) {
-    const int hn = (L.n2 + 1) / 2;
-    const long long M = (long long)L.n0 * L.n1 * hn;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < M; t += (long long)gridDim.x * blockDim.x) {
-        const int h = (int)(t % hn);
-        const long long row = t / hn;
-        const int b = (int)(row % L.n1), a = (int)(row / L.n1);
-        const int c = 2 * h + ((a + b + color) & 1);
-        if (c >= L.n2) continue;
-        const long long id = ((long long)a * L.n1 + b) * L.n2 + c;
-        const float s = nsum(L, L.u, a, b, c);
-        const float v = (s + L.f[id] * L.inv_scale) * (1.0f / 6.0f);
-        L.u[id] = (1.0f - omega) * L.u[id] + omega * v;
+// One red-black Gauss-Seidel half sweep (omega = 1) on the nodes with
+// (a+b+c) % 2 == color: u <- (sum(nb) + f/scale) / 6.
+__global__ void __launch_bounds__(kRowThreads) rb_smooth_kernel(Lv L, int color) {
+    const int rows = L.n0 * L.n1;
+    for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int a = row / L.n1, b = row - a * L.n1;
+        const NRows n = neighbour_rows(L, L.u, a, b);
+        float* u = L.u + (long long)row * L.n2;
+        const float* f = L.f + (long long)row * L.n2;
+        for (int c = 2 * threadIdx.x + ((a + b + color) & 1); c < L.n2; c += 2 * blockDim.x)
+            u[c] = (nsum_row(L, u, n, c) + f[c] * L.inv_scale) * (1.0f / 6.0f);
     }
 }
 
 // Weighted Jacobi sweep into r, for levels whose periodic axes are odd.
-__global__ void jacobi_kernel(Lv L, float omega) {
-    const long long M = (long long)L.n0 * L.n1 * L.n2;
-    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < M; id += (long long)gridDim.x * blockDim.x) {
-        const int a = (int)(id / ((long long)L.n1 * L.n2)), b = (int)((id / L.n2) % L.n1), c = (int)(id % L.n2);
-        const float v = (nsum(L, L.u, a, b, c) + L.f[id] * L.inv_scale) * (1.0f / 6.0f);
-        L.r[id] = (1.0f - omega) * L.u[id] + omega * v;
+__global__ void __launch_bounds__(kRowThreads) jacobi_kernel(Lv L, float omega) {
+    const int rows = L.n0 * L.n1;
+    for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int a = row / L.n1, b = row - a * L.n1;
+        const NRows n = neighbour_rows(L, L.u, a, b);
+        const float* u = L.u + (long long)row * L.n2;
+        const float* f = L.f + (long long)row * L.n2;
+        float* r = L.r + (long long)row * L.n2;
+        for (int c = threadIdx.x; c < L.n2; c += blockDim.x) {
+            const float v = (nsum_row(L, u, n, c) + f[c] * L.inv_scale) * (1.0f / 6.0f);
+            r[c] = (1.0f - omega) * u[c] + omega * v;
+        }
     }
 }
 
-__global__ void residual_kernel(Lv L) {
-    const long long M = (long long)L.n0 * L.n1 * L.n2;
-    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < M; id += (long long)gridDim.x * blockDim.x) {
-        const int a = (int)(id / ((long long)L.n1 * L.n2)), b = (int)((id / L.n2) % L.n1), c = (int)(id % L.n2);
-        L.r[id] = L.f[id] - (6.0f * L.u[id] - nsum(L, L.u, a, b, c)) / L.inv_scale;
+__global__ void __launch_bounds__(kRowThreads) residual_kernel(Lv L) {
+    const int rows = L.n0 * L.n1;
+    for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int a = row / L.n1, b = row - a * L.n1;
+        const NRows n = neighbour_rows(L, L.u, a, b);
+        const float* u = L.u + (long long)row * L.n2;
+        const float* f = L.f + (long long)row * L.n2;
+        float* r = L.r + (long long)row * L.n2;
+        for (int c = threadIdx.x; c < L.n2; c += blockDim.x)
+            r[c] = f[c] - (6.0f * u[c] - nsum_row(L, u, n, c)) / L.inv_scale;
     }
 }
 
@@ -100,29 +120,32 @@ __global__ void residual_kernel(Lv L) {
 __device__ __forceinline__ int fine_of(int I, int per) { return per ? 2 * I : 2 * I + 1; }
 
 // Full weighting (1/4, 1/2, 1/4 per axis) of the fine residual.
-__global__ void restrict_kernel(Lv F, Lv C) {
-    const long long M = (long long)C.n0 * C.n1 * C.n2;
+__global__ void __launch_bounds__(kRowThreads) restrict_kernel(Lv F, Lv C) {
+    const int rows = C.n0 * C.n1;
     const float w[3] = {0.25f, 0.5f, 0.25f};
-    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < M; id += (long long)gridDim.x * blockDim.x) {
-        const int A = (int)(id / ((long long)C.n1 * C.n2)), B = (int)((id / C.n2) % C.n1), Cc = (int)(id % C.n2);
-        const int fa = fine_of(A, F.p0), fb = fine_of(B, F.p1), fc = fine_of(Cc, F.p2);
-        float s = 0.0f;
-        for (int da = -1; da <= 1; ++da) {
-            int a = fa + da;
-            if (a < 0) { if (!F.p0) continue; a += F.n0; } else if (a >= F.n0) { if (!F.p0) continue; a -= F.n0; }
-            for (int db = -1; db <= 1; ++db) {
-                int b = fb + db;
-                if (b < 0) { if (!F.p1) continue; b += F.n1; } else if (b >= F.n1) { if (!F.p1) continue; b -= F.n1; }
-                const float wab = w[da + 1] * w[db + 1];
-                const long long rowb = ((long long)a * F.n1 + b) * F.n2;
-                for (int dc = -1; dc <= 1; ++dc) {
-                    int c = fc + dc;
-                    if (c < 0) { if (!F.p2) continue; c += F.n2; } else if (c >= F.n2) { if (!F.p2) continue; c -= F.n2; }
-                    s += wab * w[dc + 1] * F.r[rowb + c];
+    for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int A = row / C.n1, B = row - A * C.n1;
+        const int fa = fine_of(A, F.p0), fb = fine_of(B, F.p1);
+        for (int Cc = threadIdx.x; Cc < C.n2; Cc += blockDim.x) {
+            const int fc = fine_of(Cc, F.p2);
+            float s = 0.0f;
+            for (int da = -1; da <= 1; ++da) {
+                const int a = wrap_or_out(fa + da, F.n0, F.p0);
+                if (a < 0) continue;
+                for (int db = -1; db <= 1; ++db) {
+                    const int b = wrap_or_out(fb + db, F.n1, F.p1);
+                    if (b < 0) continue;
+                    const float wab = w[da + 1] * w[db + 1];
+                    const float* fr = F.r + ((long long)a * F.n1 + b) * F.n2;
+                    for (int dc = -1; dc <= 1; ++dc) {
+                        const int c = wrap_or_out(fc + dc, F.n2, F.p2);
+                        if (c < 0) continue;
+                        s += wab * w[dc + 1] * fr[c];
+                    }
                 }
             }
+            C.f[(long long)row * C.n2 + Cc] = s;
         }
-        C.f[id] = s;
     }
 }
 
@@ -141,21 +164,25 @@ __device__ __forceinline__ int coarse_src(int f, int per, int nc, int* I, float*
 }
 
 // Trilinear prolongation added into the fine correction.
-__global__ void prolong_kernel(Lv C, Lv F) {
-    const long long M = (long long)F.n0 * F.n1 * F.n2;
-    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < M; id += (long long)gridDim.x * blockDim.x) {
-        const int a = (int)(id / ((long long)F.n1 * F.n2)), b = (int)((id / F.n2) % F.n1), c = (int)(id % F.n2);
-        int Ia[2], Ib[2], Ic[2];
-        float wa[2], wb[2], wc[2];
-        const int na = coarse_src(a, F.p0, C.n0, Ia, wa), nbv = coarse_src(b, F.p1, C.n1, Ib, wb),
-                  nc = coarse_src(c, F.p2, C.n2, Ic, wc);
-        float s = 0.0f;
-        for (int x = 0; x < na; ++x)
-            for (int y = 0; y < nbv; ++y) {
-                const long long row = ((long long)Ia[x] * C.n1 + Ib[y]) * C.n2;
-                for (int z = 0; z < nc; ++z) s += wa[x] * wb[y] * wc[z] * C.u[row + Ic[z]];
-            }
-        F.u[id] += s;
+__global__ void __launch_bounds__(kRowThreads) prolong_kernel(Lv C, Lv F) {
+    const int rows = F.n0 * F.n1;
+    for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int a = row / F.n1, b = row - a * F.n1;
+        int Ia[2], Ib[2];
+        float wa[2], wb[2];
+        const int na = coarse_src(a, F.p0, C.n0, Ia, wa), nbv = coarse_src(b, F.p1, C.n1, Ib, wb);
+        for (int c = threadIdx.x; c < F.n2; c += blockDim.x) {
+            int Ic[2];
+            float wc[2];
+            const int nc = coarse_src(c, F.p2, C.n2, Ic, wc);
+            float s = 0.0f;
+            for (int x = 0; x < na; ++x)
+                for (int y = 0; y < nbv; ++y) {
+                    const float* cr = C.u + ((long long)Ia[x] * C.n1 + Ib[y]) * C.n2;
+                    for (int z = 0; z < nc; ++z) s += wa[x] * wb[y] * wc[z] * cr[Ic[z]];
+                }
+            F.u[(long long)row * F.n2 + c] += s;
+        }
     }
 }
 
@@ -201,14 +228,14 @@ __global__ void coarse_kernel(Lv L, int sweeps, int allper, int rb) {
                 for (int t = threadIdx.x; t < M; t += blockDim.x) {
                     const int a = t / (L.n1 * L.n2), b = (t / L.n2) % L.n1, c = t % L.n2;
                     if (((a + b + c) & 1) != color) continue;
-                    u[t] = (nsum_d(u, a, b, c) + f[t]) / 6.0;
+                    u[t] = (nsum_d(u, a, b, c) + f[t]) * (1.0 / 6.0);
                 }
                 __syncthreads();
             }
         } else {
             for (int t = threadIdx.x; t < M; t += blockDim.x) {
                 const int a = t / (L.n1 * L.n2), b = (t / L.n2) % L.n1, c = t % L.n2;
-                tmp[t] = 0.2 * u[t] + 0.8 * (nsum_d(u, a, b, c) + f[t]) / 6.0;
+                tmp[t] = 0.2 * u[t] + 0.8 * (nsum_d(u, a, b, c) + f[t]) * (1.0 / 6.0);
             }
             __syncthreads();
             for (int t = threadIdx.x; t < M; t += blockDim.x) u[t] = tmp[t];
@@ -230,6 +257,168 @@ __global__ void coarse_kernel(Lv L, int sweeps, int allper, int rb) {
     for (int t = threadIdx.x; t < M; t += blockDim.x) L.u[t] = (float)u[t];
 }
 
+// ---- the coarse end of the V-cycle inside one CTA ----
+// From the first level with at most kInCta unknowns down to the coarsest, the
+// V-cycle (2 pre-sweeps, residual, restriction, FP64 coarsest solve,
+// prolongation, 2 post-sweeps per level) runs in one CTA on shared memory,
+// replacing about a dozen dependent launches per level.
+constexpr int kInCta = 4096;
+constexpr int kMaxSmLevels = 12;
+struct SmLv {
+    int n0, n1, n2, p0, p1, p2;
+    float inv_scale;
+    int off;      // float offset of u; f and r follow
+    int rb;       // red-black ordering valid
+};
+struct CoarseCycle {
+    int nl;
+    SmLv lv[kMaxSmLevels];
+    const float* f_in;
+    float* u_out;
+    int coarse_sweeps;
+    int allper;
+    int dbl_off;  // byte offset of the FP64 coarsest arrays
+};
+
+__device__ __forceinline__ int sm_size(const SmLv& L) { return L.n0 * L.n1 * L.n2; }
+
+template <typename T>
+__device__ __forceinline__ T sm_nsum(const SmLv& L, const T* u, int a, int b, int c) {
+    T s = 0;
+    int q;
+    if ((q = wrap_or_out(a - 1, L.n0, L.p0)) >= 0) s += u[(q * L.n1 + b) * L.n2 + c];
+    if ((q = wrap_or_out(a + 1, L.n0, L.p0)) >= 0) s += u[(q * L.n1 + b) * L.n2 + c];
+    if ((q = wrap_or_out(b - 1, L.n1, L.p1)) >= 0) s += u[(a * L.n1 + q) * L.n2 + c];
+    if ((q = wrap_or_out(b + 1, L.n1, L.p1)) >= 0) s += u[(a * L.n1 + q) * L.n2 + c];
+    if ((q = wrap_or_out(c - 1, L.n2, L.p2)) >= 0) s += u[(a * L.n1 + b) * L.n2 + q];
+    if ((q = wrap_or_out(c + 1, L.n2, L.p2)) >= 0) s += u[(a * L.n1 + b) * L.n2 + q];
+    return s;
+}
+
+// `sweeps` red-black (or weighted Jacobi) sweeps: u <- (sum(nb) + f/scale) / 6.
+template <typename T>
+__device__ void sm_smooth(const SmLv& L, T* u, const T* f, T* tmp, int sweeps, T inv_scale) {
+    const int M = sm_size(L);
+    for (int sw = 0; sw < sweeps; ++sw) {
+        if (L.rb) {
+            for (int color = 0; color < 2; ++color) {
+                for (int t = threadIdx.x; t < M; t += blockDim.x) {
+                    const int a = t / (L.n1 * L.n2), b = (t / L.n2) % L.n1, c = t % L.n2;
+                    if (((a + b + c) & 1) != color) continue;
+                    u[t] = (sm_nsum(L, u, a, b, c) + f[t] * inv_scale) * (T)(1.0 / 6.0);
+                }
+                __syncthreads();
+            }
+        } else {
+            for (int t = threadIdx.x; t < M; t += blockDim.x) {
+                const int a = t / (L.n1 * L.n2), b = (t / L.n2) % L.n1, c = t % L.n2;
+                tmp[t] = (T)0.2 * u[t] + (T)0.8 * (sm_nsum(L, u, a, b, c) + f[t] * inv_scale) * (T)(1.0 / 6.0);
+            }
+            __syncthreads();
+            for (int t = threadIdx.x; t < M; t += blockDim.x) u[t] = tmp[t];
+            __syncthreads();
+        }
+    }
+}
+
+__device__ void sm_remove_mean(double* v, int M) {
+    __shared__ double red[32];
+    __shared__ double mean;
+    double s = 0.0;
+    for (int t = threadIdx.x; t < M; t += blockDim.x) s += v[t];
+    for (int o = 16; o; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) { double q = 0; for (int w = 0; w < (int)(blockDim.x >> 5); ++w) q += red[w]; mean = q / M; }
+    __syncthreads();
+    for (int t = threadIdx.x; t < M; t += blockDim.x) v[t] -= mean;
+    __syncthreads();
+}
+
+__global__ void coarse_cycle_kernel(CoarseCycle d) {
+    extern __shared__ float pool[];
+    auto U = [&](int l) { return pool + d.lv[l].off; };
+    auto F = [&](int l) { return pool + d.lv[l].off + sm_size(d.lv[l]); };
+    auto R = [&](int l) { return pool + d.lv[l].off + 2 * sm_size(d.lv[l]); };
+    {
+        const int M = sm_size(d.lv[0]);
+        for (int t = threadIdx.x; t < M; t += blockDim.x) F(0)[t] = d.f_in[t];
+        __syncthreads();
+    }
+    for (int l = 0; l + 1 < d.nl; ++l) {
+        const SmLv& L = d.lv[l];
+        const SmLv& C = d.lv[l + 1];
+        const int M = sm_size(L);
+        for (int t = threadIdx.x; t < M; t += blockDim.x) U(l)[t] = 0.0f;
+        __syncthreads();
+        sm_smooth<float>(L, U(l), F(l), R(l), 2, L.inv_scale);
+        for (int t = threadIdx.x; t < M; t += blockDim.x) {
+            const int a = t / (L.n1 * L.n2), b = (t / L.n2) % L.n1, c = t % L.n2;
+            R(l)[t] = F(l)[t] - (6.0f * U(l)[t] - sm_nsum(L, U(l), a, b, c)) / L.inv_scale;
+        }
+        __syncthreads();
+        const int MC = sm_size(C);
+        const float w[3] = {0.25f, 0.5f, 0.25f};
+        for (int t = threadIdx.x; t < MC; t += blockDim.x) {
+            const int A = t / (C.n1 * C.n2), B = (t / C.n2) % C.n1, Cc = t % C.n2;
+            const int fa = fine_of(A, L.p0), fb = fine_of(B, L.p1), fc = fine_of(Cc, L.p2);
+            float s = 0.0f;
+            for (int da = -1; da <= 1; ++da) {
+                const int a = wrap_or_out(fa + da, L.n0, L.p0);
+                if (a < 0) continue;
+                for (int db = -1; db <= 1; ++db) {
+                    const int b = wrap_or_out(fb + db, L.n1, L.p1);
+                    if (b < 0) continue;
+                    for (int dc = -1; dc <= 1; ++dc) {
+                        const int c = wrap_or_out(fc + dc, L.n2, L.p2);
+                        if (c < 0) continue;
+                        s += w[da + 1] * w[db + 1] * w[dc + 1] * R(l)[(a * L.n1 + b) * L.n2 + c];
+                    }
+                }
+            }
+            F(l + 1)[t] = s;
+        }
+        __syncthreads();
+    }
+    {   // coarsest level in FP64
+        const int l = d.nl - 1;
+        const SmLv& L = d.lv[l];
+        const int M = sm_size(L);
+        double* du = reinterpret_cast<double*>(reinterpret_cast<char*>(pool) + d.dbl_off);
+        double* df = du + M;
+        double* dt = df + M;
+        for (int t = threadIdx.x; t < M; t += blockDim.x) { du[t] = 0.0; df[t] = (double)F(l)[t]; }
+        __syncthreads();
+        if (d.allper) sm_remove_mean(df, M);
+        sm_smooth<double>(L, du, df, dt, d.coarse_sweeps, (double)L.inv_scale);
+        if (d.allper) sm_remove_mean(du, M);
+        for (int t = threadIdx.x; t < M; t += blockDim.x) U(l)[t] = (float)du[t];
+        __syncthreads();
+    }
+    for (int l = d.nl - 2; l >= 0; --l) {
+        const SmLv& Fl = d.lv[l];
+        const SmLv& C = d.lv[l + 1];
+        const int M = sm_size(Fl);
+        for (int t = threadIdx.x; t < M; t += blockDim.x) {
+            const int a = t / (Fl.n1 * Fl.n2), b = (t / Fl.n2) % Fl.n1, c = t % Fl.n2;
+            int Ia[2], Ib[2], Ic[2];
+            float wa[2], wb[2], wc[2];
+            const int na = coarse_src(a, Fl.p0, C.n0, Ia, wa), nbv = coarse_src(b, Fl.p1, C.n1, Ib, wb),
+                      nc = coarse_src(c, Fl.p2, C.n2, Ic, wc);
+            float s = 0.0f;
+            for (int x = 0; x < na; ++x)
+                for (int y = 0; y < nbv; ++y)
+                    for (int z = 0; z < nc; ++z) s += wa[x] * wb[y] * wc[z] * U(l + 1)[(Ia[x] * C.n1 + Ib[y]) * C.n2 + Ic[z]];
+            U(l)[t] += s;
+        }
+        __syncthreads();
+        sm_smooth<float>(Fl, U(l), F(l), R(l), 2, Fl.inv_scale);
+    }
+    const int M0 = sm_size(d.lv[0]);
+    for (int t = threadIdx.x; t < M0; t += blockDim.x) d.u_out[t] = U(0)[t];
+}
+
 // ---- FP64 outer loop on the glue-layout arrays ----
 struct Outer {
     int cx, cy, cz;
@@ -238,7 +427,7 @@ struct Outer {
     int p0, p1, p2;       // periodic axes
     int nref0, nref1, nref2;
     double inv_eps0;
-    double fmean;         // removed from f when every axis is periodic
+    const double* fmean;  // device scalar removed from f when every axis is periodic
 };
 
 __device__ __forceinline__ long long gl(const Outer& O, int i, int j, int k) {
@@ -263,15 +452,19 @@ __device__ __forceinline__ double bsum(double v, double* red) {
     return v;
 }
 
-// Per-block partial sums of f and f^2 over the unknown nodes.
-__global__ void fstats_kernel(Outer O, const double* rho0, double* partial) {
+// Per-block partial sums of f and f^2 over the unknown nodes (rows of the
+// unknown grid, block-strided).
+__global__ void __launch_bounds__(kT) fstats_kernel(Outer O, const double* rho0, double* partial) {
     __shared__ double red[32];
-    const long long M = (long long)O.n0 * O.n1 * O.n2;
+    const int rows = O.n0 * O.n1;
     double s = 0.0, s2 = 0.0;
-    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < M; id += (long long)gridDim.x * blockDim.x) {
-        const int a = (int)(id / ((long long)O.n1 * O.n2)), b = (int)((id / O.n2) % O.n1), c = (int)(id % O.n2);
-        const double f = rho0[gl(O, a + O.o0, b + O.o1, c + O.o2)] * O.inv_eps0;
-        s += f; s2 += f * f;
+    for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int a = row / O.n1, b = row - a * O.n1;
+        const double* rr = rho0 + gl(O, a + O.o0, b + O.o1, O.o2);
+        for (int c = threadIdx.x; c < O.n2; c += blockDim.x) {
+            const double f = rr[c] * O.inv_eps0;
+            s += f; s2 += f * f;
+        }
     }
     s = bsum(s, red);
     s2 = bsum(s2, red);
@@ -280,51 +473,65 @@ __global__ void fstats_kernel(Outer O, const double* rho0, double* partial) {
 
 // r = f - A phi in FP64; stores r to the level-0 right-hand side (FP32) and
 // per-block partial sums of r^2.
-__global__ void outer_residual_kernel(Outer O, const double* rho0, const double* phi, float* f0, double* partial) {
+__global__ void __launch_bounds__(kT) outer_residual_kernel(Outer O, const double* rho0, const double* phi, float* f0,
+                                                           double* partial) {
     __shared__ double red[32];
-    const long long M = (long long)O.n0 * O.n1 * O.n2;
+    const int rows = O.n0 * O.n1;
+    const double fm = *O.fmean;
     double s2 = 0.0;
-    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < M; id += (long long)gridDim.x * blockDim.x) {
-        const int a = (int)(id / ((long long)O.n1 * O.n2)), b = (int)((id / O.n2) % O.n1), c = (int)(id % O.n2);
-        const int i = a + O.o0, j = b + O.o1, k = c + O.o2;
-        const double p = phi[gl(O, i, j, k)];
-        const double s = phi[gl(O, wrapn(i - 1, O.p0, O.nref0), j, k)] + phi[gl(O, wrapn(i + 1, O.p0, O.nref0), j, k)] +
-                         phi[gl(O, i, wrapn(j - 1, O.p1, O.nref1), k)] + phi[gl(O, i, wrapn(j + 1, O.p1, O.nref1), k)] +
-                         phi[gl(O, i, j, wrapn(k - 1, O.p2, O.nref2))] + phi[gl(O, i, j, wrapn(k + 1, O.p2, O.nref2))];
-        const double r = (rho0[gl(O, i, j, k)] * O.inv_eps0 - O.fmean) - (6.0 * p - s);
-        f0[id] = (float)r;
-        s2 += r * r;
+    for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int a = row / O.n1, b = row - a * O.n1;
+        const int i = a + O.o0, j = b + O.o1;
+        const double* p0 = phi + gl(O, i, j, 0);
+        const double* pim = phi + gl(O, wrapn(i - 1, O.p0, O.nref0), j, 0);
+        const double* pip = phi + gl(O, wrapn(i + 1, O.p0, O.nref0), j, 0);
+        const double* pjm = phi + gl(O, i, wrapn(j - 1, O.p1, O.nref1), 0);
+        const double* pjp = phi + gl(O, i, wrapn(j + 1, O.p1, O.nref1), 0);
+        const double* rr = rho0 + gl(O, i, j, 0);
+        float* fr = f0 + (long long)row * O.n2;
+        for (int c = threadIdx.x; c < O.n2; c += blockDim.x) {
+            const int k = c + O.o2;
+            const double s = pim[k] + pip[k] + pjm[k] + pjp[k] + p0[wrapn(k - 1, O.p2, O.nref2)] +
+                             p0[wrapn(k + 1, O.p2, O.nref2)];
+            const double r = (rr[k] * O.inv_eps0 - fm) - (6.0 * p0[k] - s);
+            fr[c] = (float)r;
+            s2 += r * r;
+        }
     }
     s2 = bsum(s2, red);
     if (threadIdx.x == 0) partial[blockIdx.x] = s2;
 }
 
-__global__ void correct_kernel(Outer O, double* phi, const float* e) {
-    const long long M = (long long)O.n0 * O.n1 * O.n2;
-    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < M; id += (long long)gridDim.x * blockDim.x) {
-        const int a = (int)(id / ((long long)O.n1 * O.n2)), b = (int)((id / O.n2) % O.n1), c = (int)(id % O.n2);
-        phi[gl(O, a + O.o0, b + O.o1, c + O.o2)] += (double)e[id];
+__global__ void __launch_bounds__(kT) correct_kernel(Outer O, double* phi, const float* e) {
+    const int rows = O.n0 * O.n1;
+    for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int a = row / O.n1, b = row - a * O.n1;
+        double* pr = phi + gl(O, a + O.o0, b + O.o1, O.o2);
+        const float* er = e + (long long)row * O.n2;
+        for (int c = threadIdx.x; c < O.n2; c += blockDim.x) pr[c] += (double)er[c];
     }
 }
 
-__global__ void phi_mean_kernel(Outer O, const double* phi, double* partial) {
+__global__ void __launch_bounds__(kT) phi_mean_kernel(Outer O, const double* phi, double* partial) {
     __shared__ double red[32];
-    const long long M = (long long)O.n0 * O.n1 * O.n2;
+    const int rows = O.n0 * O.n1;
     double s = 0.0;
-    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < M; id += (long long)gridDim.x * blockDim.x) {
-        const int a = (int)(id / ((long long)O.n1 * O.n2)), b = (int)((id / O.n2) % O.n1), c = (int)(id % O.n2);
-        s += phi[gl(O, a + O.o0, b + O.o1, c + O.o2)];
+    for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int a = row / O.n1, b = row - a * O.n1;
+        const double* pr = phi + gl(O, a + O.o0, b + O.o1, O.o2);
+        for (int c = threadIdx.x; c < O.n2; c += blockDim.x) s += pr[c];
     }
     s = bsum(s, red);
     if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 
-__global__ void phi_shift_kernel(Outer O, double* phi, const double* sum) {
-    const long long M = (long long)O.n0 * O.n1 * O.n2;
-    const double m = *sum / (double)M;
-    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < M; id += (long long)gridDim.x * blockDim.x) {
-        const int a = (int)(id / ((long long)O.n1 * O.n2)), b = (int)((id / O.n2) % O.n1), c = (int)(id % O.n2);
-        phi[gl(O, a + O.o0, b + O.o1, c + O.o2)] -= m;
+__global__ void __launch_bounds__(kT) phi_shift_kernel(Outer O, double* phi, const double* sum) {
+    const int rows = O.n0 * O.n1;
+    const double m = *sum / ((double)rows * O.n2);
+    for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int a = row / O.n1, b = row - a * O.n1;
+        double* pr = phi + gl(O, a + O.o0, b + O.o1, O.o2);
+        for (int c = threadIdx.x; c < O.n2; c += blockDim.x) pr[c] -= m;
     }
 }
 
@@ -346,7 +553,7 @@ Outer make_outer(const Ctx& c) {
     O.o0 = O.p0 ? 1 : 2; O.o1 = O.p1 ? 1 : 2; O.o2 = O.p2 ? 1 : 2;
     O.nref0 = c.nx; O.nref1 = c.ny; O.nref2 = c.nz;
     O.inv_eps0 = 1.0 / c.p.eps0;
-    O.fmean = 0.0;
+    O.fmean = &c.d_sc->red[4];
     return O;
 }
 
@@ -358,17 +565,19 @@ bool level_rb(const MGLevel& m) {
 void smooth(Ctx& c, int l, int sweeps) {
     MGLevel& m = c.mg[l];
     const Lv L = lv(m);
+    const int rb = row_blocks((long long)m.n[0] * m.n[1]);
+    const int th = std::min(kRowThreads, ((m.n[2] + 31) / 32) * 32);
     if (level_rb(m)) {
-        const long long half = (long long)m.n[0] * m.n[1] * ((m.n[2] + 1) / 2);
+        const int th2 = std::min(kRowThreads, ((m.n[2] / 2 + 32) / 32) * 32);
         for (int s = 0; s < sweeps; ++s)
             for (int color = 0; color < 2; ++color) {
                 ++c.launches;
-                rb_smooth_kernel<<<nblocks(half), kT, 0, c.st>>>(L, color, 1.0f);
+                rb_smooth_kernel<<<rb, th2, 0, c.st>>>(L, color);
             }
     } else {
         for (int s = 0; s < sweeps; ++s) {
             ++c.launches;
-            jacobi_kernel<<<nblocks((long long)m.size()), kT, 0, c.st>>>(L, 0.8f);
+            jacobi_kernel<<<rb, th, 0, c.st>>>(L, 0.8f);
             FOPIS_CUDA(cudaMemcpyAsync(m.u, m.r, sizeof(float) * m.size(), cudaMemcpyDeviceToDevice, c.st));
         }
     }
@@ -380,11 +589,12 @@ void coarse_solve(Ctx& c, int l) {
     const int M = (int)m.size();
     const bool allper = m.per[0] && m.per[1] && m.per[2];
     const int nmax = std::max({m.n[0], m.n[1], m.n[2]});
-    const int sweeps = std::min(4000, std::max(30, 2 * nmax * nmax));
+    const int sweeps = std::min(4000, 4 + 4 * nmax * nmax);
     if (M <= kCoarseMax) {
         const size_t smem = sizeof(double) * 3 * M;
+        const int threads = std::min(1024, ((M + 31) / 32) * 32);
         ++c.launches;
-        coarse_kernel<<<1, 1024, smem, c.st>>>(lv(m), sweeps, allper ? 1 : 0, level_rb(m) ? 1 : 0);
+        coarse_kernel<<<1, threads, smem, c.st>>>(lv(m), sweeps, allper ? 1 : 0, level_rb(m) ? 1 : 0);
         FOPIS_LAUNCH_CHECK();
     } else {
         FOPIS_CUDA(cudaMemsetAsync(m.u, 0, sizeof(float) * M, c.st));
@@ -392,23 +602,62 @@ void coarse_solve(Ctx& c, int l) {
     }
 }
 
+void coarse_cycle(Ctx& c);
+
 void vcycle(Ctx& c, int l) {
     const int L = (int)c.mg.size();
+    if (l == c.mg_cta_start) { coarse_cycle(c); return; }
     if (l == L - 1) { coarse_solve(c, l); return; }
     MGLevel& m = c.mg[l];
     MGLevel& n = c.mg[l + 1];
     FOPIS_CUDA(cudaMemsetAsync(m.u, 0, sizeof(float) * m.size(), c.st));
     smooth(c, l, 2);
     ++c.launches;
-    residual_kernel<<<nblocks((long long)m.size()), kT, 0, c.st>>>(lv(m));
+    residual_kernel<<<row_blocks((long long)m.n[0] * m.n[1]), std::min(kRowThreads, ((m.n[2] + 31) / 32) * 32), 0,
+                      c.st>>>(lv(m));
     ++c.launches;
-    restrict_kernel<<<nblocks((long long)n.size()), kT, 0, c.st>>>(lv(m), lv(n));
+    restrict_kernel<<<row_blocks((long long)n.n[0] * n.n[1]), std::min(kRowThreads, ((n.n[2] + 31) / 32) * 32), 0,
+                      c.st>>>(lv(m), lv(n));
     FOPIS_LAUNCH_CHECK();
     vcycle(c, l + 1);
     ++c.launches;
-    prolong_kernel<<<nblocks((long long)m.size()), kT, 0, c.st>>>(lv(n), lv(m));
+    prolong_kernel<<<row_blocks((long long)m.n[0] * m.n[1]), std::min(kRowThreads, ((m.n[2] + 31) / 32) * 32), 0,
+                     c.st>>>(lv(n), lv(m));
     FOPIS_LAUNCH_CHECK();
     smooth(c, l, 2);
+}
+
+
+size_t coarse_cycle_smem(const Ctx& c, int start) {
+    size_t floats = 0;
+    for (int l = start; l < (int)c.mg.size(); ++l) floats += 3 * c.mg[l].size();
+    const size_t dbl = ((floats * 4 + 15) / 16) * 16;
+    return dbl + 3 * sizeof(double) * c.mg.back().size();
+}
+
+void coarse_cycle(Ctx& c) {
+    const int start = c.mg_cta_start;
+    CoarseCycle d{};
+    d.nl = (int)c.mg.size() - start;
+    int off = 0;
+    for (int l = 0; l < d.nl; ++l) {
+        const MGLevel& m = c.mg[start + l];
+        d.lv[l] = SmLv{m.n[0], m.n[1], m.n[2], m.per[0], m.per[1], m.per[2], (float)(1.0 / m.scale), off,
+                       level_rb(m) ? 1 : 0};
+        off += 3 * (int)m.size();
+    }
+    d.dbl_off = ((off * 4 + 15) / 16) * 16;
+    d.f_in = c.mg[start].f;
+    d.u_out = c.mg[start].u;
+    const MGLevel& last = c.mg.back();
+    const int nmax = std::max({last.n[0], last.n[1], last.n[2]});
+    d.coarse_sweeps = std::min(4000, 4 + 4 * nmax * nmax);
+    d.allper = (last.per[0] && last.per[1] && last.per[2]) ? 1 : 0;
+    const size_t smem = coarse_cycle_smem(c, start);
+    const int threads = std::min(1024, std::max(64, ((int)c.mg[start].size() + 31) / 32 * 32));
+    ++c.launches;
+    coarse_cycle_kernel<<<1, threads, smem, c.st>>>(d);
+    FOPIS_LAUNCH_CHECK();
 }
 
 double read_red(Ctx& c, int slot) {
@@ -435,7 +684,7 @@ void mg_setup(Ctx& c) {
     c.mg.push_back(m);
     for (;;) {
         const MGLevel& f = c.mg.back();
-        bool ok = f.size() > 64;
+        bool ok = f.size() > 1;
         for (int a = 0; a < 3; ++a) {
             if (f.per[a]) ok = ok && (f.n[a] % 2 == 0) && f.n[a] >= 4;
             else ok = ok && f.n[a] >= 3;
@@ -452,6 +701,18 @@ void mg_setup(Ctx& c) {
         FOPIS_CUDA(cudaMalloc(&l.r, sizeof(float) * l.size()));
         FOPIS_CUDA(cudaMemset(l.u, 0, sizeof(float) * l.size()));
     }
+    c.mg_cta_start = -1;
+    if ((int)c.mg.size() <= kMaxSmLevels + 64) {
+        for (int l = 0; l < (int)c.mg.size(); ++l) {
+            if ((int)c.mg.size() - l > kMaxSmLevels) continue;
+            if (c.mg[l].size() <= (size_t)kInCta && coarse_cycle_smem(c, l) <= 200 * 1024) { c.mg_cta_start = l; break; }
+        }
+    }
+    if (c.mg_cta_start >= 0) {
+        const size_t smem = coarse_cycle_smem(c, c.mg_cta_start);
+        if (smem > 48 * 1024)
+            FOPIS_CUDA(cudaFuncSetAttribute(coarse_cycle_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
     const MGLevel& last = c.mg.back();
     if ((int)last.size() <= kCoarseMax) {
         const size_t smem = sizeof(double) * 3 * last.size();
@@ -463,12 +724,46 @@ void mg_setup(Ctx& c) {
 }
 
 void mg_free(Ctx& c) {
+    if (c.mg_exec) { cudaGraphExecDestroy(c.mg_exec); c.mg_exec = nullptr; }
+    if (c.mg_graph) { cudaGraphDestroy(c.mg_graph); c.mg_graph = nullptr; }
     for (auto& l : c.mg) { cudaFree(l.u); cudaFree(l.f); cudaFree(l.r); }
     c.mg.clear();
     if (c.red_partials) { cudaFree(c.red_partials); c.red_partials = nullptr; }
 }
 
+// Records one refinement iteration — V-cycle, FP64 correction, FP64 residual
+// and its squared norm copied to pinned host memory — as a CUDA graph, once per
+// context; every later iteration is one graph launch.
+static void ensure_cycle_graph(Ctx& c) {
+    if (c.mg_exec) return;
+    Outer O = make_outer(c);
+    const long long M = (long long)O.n0 * O.n1 * O.n2;
+    const int64_t before = c.launches;
+    FOPIS_CUDA(cudaStreamBeginCapture(c.st, cudaStreamCaptureModeThreadLocal));
+    try {
+        vcycle(c, 0);
+        ++c.launches;
+        correct_kernel<<<row_blocks((long long)O.n0 * O.n1), kT, 0, c.st>>>(O, c.phi, c.mg[0].u);
+        ++c.launches;
+        outer_residual_kernel<<<kRedBlocks, kT, 0, c.st>>>(O, c.rho0, c.phi, c.mg[0].f, c.red_partials);
+        ++c.launches;
+        reduce_partials_kernel<<<1, 1024, 0, c.st>>>(c.red_partials, kRedBlocks, 1, 0, &c.d_sc->red[2]);
+        FOPIS_LAUNCH_CHECK();
+        FOPIS_CUDA(cudaMemcpyAsync(&c.h_sc->red[2], &c.d_sc->red[2], sizeof(double), cudaMemcpyDeviceToHost, c.st));
+    } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(c.st, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    FOPIS_CUDA(cudaStreamEndCapture(c.st, &c.mg_graph));
+    FOPIS_CUDA(cudaGraphInstantiate(&c.mg_exec, c.mg_graph, 0));
+    c.cycle_launches = c.launches - before;
+    c.launches = before;
+}
+
 int mg_solve(Ctx& c, double tol, int max_cycles) {
+    ensure_cycle_graph(c);
     Outer O = make_outer(c);
     const bool allper = O.p0 && O.p1 && O.p2;
     const long long M = (long long)O.n0 * O.n1 * O.n2;
@@ -482,26 +777,23 @@ int mg_solve(Ctx& c, double tol, int max_cycles) {
     FOPIS_CUDA(cudaMemcpyAsync(c.h_sc->red, c.d_sc->red, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.st));
     FOPIS_CUDA(cudaStreamSynchronize(c.st));
     const double fsum = c.h_sc->red[0], fsq = c.h_sc->red[1];
-    if (allper) O.fmean = fsum / (double)M;
+    c.h_sc->red[4] = allper ? fsum / (double)M : 0.0;
+    FOPIS_CUDA(cudaMemcpyAsync(&c.d_sc->red[4], &c.h_sc->red[4], sizeof(double), cudaMemcpyHostToDevice, c.st));
     double fnorm = std::sqrt(std::max(0.0, fsq - (allper ? fsum * fsum / (double)M : 0.0)));
     if (!(fnorm > 0.0)) fnorm = 1.0;
-    auto residual = [&]() {
-        ++c.launches;
-        outer_residual_kernel<<<kRedBlocks, kT, 0, c.st>>>(O, c.rho0, c.phi, c.mg[0].f, c.red_partials);
-        ++c.launches;
-        reduce_partials_kernel<<<1, 1024, 0, c.st>>>(c.red_partials, kRedBlocks, 1, 0, &c.d_sc->red[2]);
-        FOPIS_LAUNCH_CHECK();
-        return std::sqrt(read_red(c, 2));
-    };
-    double res = residual();
+    ++c.launches;
+    outer_residual_kernel<<<kRedBlocks, kT, 0, c.st>>>(O, c.rho0, c.phi, c.mg[0].f, c.red_partials);
+    ++c.launches;
+    reduce_partials_kernel<<<1, 1024, 0, c.st>>>(c.red_partials, kRedBlocks, 1, 0, &c.d_sc->red[2]);
+    FOPIS_LAUNCH_CHECK();
+    double res = std::sqrt(read_red(c, 2));
     c.first_res = res / fnorm;
     int cycles = 0;
     while (res > tol * fnorm && cycles < max_cycles) {
-        vcycle(c, 0);
-        ++c.launches;
-        correct_kernel<<<nblocks(M), kT, 0, c.st>>>(O, c.phi, c.mg[0].u);
-        FOPIS_LAUNCH_CHECK();
-        res = residual();
+        FOPIS_CUDA(cudaGraphLaunch(c.mg_exec, c.st));
+        c.launches += c.cycle_launches;
+        FOPIS_CUDA(cudaStreamSynchronize(c.st));
+        res = std::sqrt(c.h_sc->red[2]);
         ++cycles;
         if (!std::isfinite(res)) break;
     }
@@ -511,7 +803,7 @@ int mg_solve(Ctx& c, double tol, int max_cycles) {
         ++c.launches;
         reduce_partials_kernel<<<1, 1024, 0, c.st>>>(c.red_partials, kRedBlocks, 1, 0, &c.d_sc->red[3]);
         ++c.launches;
-        phi_shift_kernel<<<nblocks(M), kT, 0, c.st>>>(O, c.phi, &c.d_sc->red[3]);
+        phi_shift_kernel<<<row_blocks((long long)O.n0 * O.n1), kT, 0, c.st>>>(O, c.phi, &c.d_sc->red[3]);
         FOPIS_LAUNCH_CHECK();
     }
     phi_boundary(c);

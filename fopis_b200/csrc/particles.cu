@@ -22,7 +22,12 @@ struct Grid {
     int n[3];            // reference node counts
     int per[6];          // periodic sides
     long long sj, si;    // linear strides of j and i
+    int nb[3];           // bricks per axis over the node cells 0..c-2
 };
+
+// Particles are counting-sorted by brick: 4 x 4 x 8 node cells (k fastest),
+// then by cell inside the brick. One CTA of the fused push owns one brick.
+constexpr int kBX = 4, kBY = 4, kBZ = 8, kBrickCells = kBX * kBY * kBZ;
 
 __host__ Grid make_grid(const Ctx& c) {
     Grid g;
@@ -30,7 +35,15 @@ __host__ Grid make_grid(const Ctx& c) {
     g.n[0] = c.nx; g.n[1] = c.ny; g.n[2] = c.nz;
     for (int t = 0; t < 6; ++t) g.per[t] = c.per[t];
     g.sj = c.cz; g.si = (long long)c.cy * c.cz;
+    g.nb[0] = (c.cx - 1 + kBX - 1) / kBX;
+    g.nb[1] = (c.cy - 1 + kBY - 1) / kBY;
+    g.nb[2] = (c.cz - 1 + kBZ - 1) / kBZ;
     return g;
+}
+
+__device__ __forceinline__ long long brick_key(const Grid& g, int i, int j, int k) {
+    const long long b = ((long long)(i / kBX) * g.nb[1] + (j / kBY)) * g.nb[2] + (k / kBZ);
+    return b * kBrickCells + ((i % kBX) * kBY + (j % kBY)) * kBZ + (k % kBZ);
 }
 
 __device__ __forceinline__ long long lin(const Grid& g, int i, int j, int k) {
@@ -167,6 +180,7 @@ struct PushArgs {
     Soa p;
     int s;
     long long cap;
+    long long lo;             // first slot of the pass (the unsorted tail in the fused step)
     const unsigned long long* count;
     const float4* E;
     Grid g;
@@ -178,97 +192,262 @@ struct PushArgs {
     DevScalars* sc;
 };
 
-// The fused particle pass. VEL: CIC gather of nodal E and Boris kick/rotate
-// (Grid::updateParticleVelocityES, GridParticleTreatmentES.cpp:13-88). POS:
-// x += v and boundaries (RootGrid::updateParticlePositionES, :90-181). DEP: the
-// per-particle part of RootGrid::updateRho (RootGridField.cpp:1168-1196):
-// particles inside a body go to the absorbed list (Spacecraft::
-// distributeInnerParticleCharge, Spacecraft.cpp:512-592, finished by
-// absorb_kernel); the rest deposit their CIC weights.
+struct PState {
+    int i, j, k;
+    float ox, oy, oz, vx, vy, vz;
+};
+
+// CIC gather of nodal E and the Boris kick/rotate/kick of
+// Grid::updateParticleVelocityES (GridParticleTreatmentES.cpp:13-88): weights
+// qm dx2 dy2 dz2 ... on the eight nodes, B used as given.
+__device__ __forceinline__ void gather_boris(const PushArgs& a, PState& s) {
+    const long long b = lin(a.g, s.i, s.j, s.k);
+    const float x1 = s.ox, x2 = 1.0f - s.ox, y1 = s.oy, y2 = 1.0f - s.oy, z1 = s.oz, z2 = 1.0f - s.oz;
+    const float4 e000 = __ldg(a.E + b), e001 = __ldg(a.E + b + 1);
+    const float4 e010 = __ldg(a.E + b + a.g.sj), e011 = __ldg(a.E + b + a.g.sj + 1);
+    const float4 e100 = __ldg(a.E + b + a.g.si), e101 = __ldg(a.E + b + a.g.si + 1);
+    const float4 e110 = __ldg(a.E + b + a.g.si + a.g.sj), e111 = __ldg(a.E + b + a.g.si + a.g.sj + 1);
+    const float w000 = x2 * y2 * z2, w100 = x1 * y2 * z2, w010 = x2 * y1 * z2, w110 = x1 * y1 * z2;
+    const float w001 = x2 * y2 * z1, w101 = x1 * y2 * z1, w011 = x2 * y1 * z1, w111 = x1 * y1 * z1;
+    const float ex = a.qm * (w000 * e000.x + w100 * e100.x + w010 * e010.x + w110 * e110.x +
+                             w001 * e001.x + w101 * e101.x + w011 * e011.x + w111 * e111.x);
+    const float ey = a.qm * (w000 * e000.y + w100 * e100.y + w010 * e010.y + w110 * e110.y +
+                             w001 * e001.y + w101 * e101.y + w011 * e011.y + w111 * e111.y);
+    const float ez = a.qm * (w000 * e000.z + w100 * e100.z + w010 * e010.z + w110 * e110.z +
+                             w001 * e001.z + w101 * e101.z + w011 * e011.z + w111 * e111.z);
+    const float vx1 = s.vx + ex, vy1 = s.vy + ey, vz1 = s.vz + ez;
+    const float vxt = vx1 + vy1 * a.bz - vz1 * a.by;
+    const float vyt = vy1 + vz1 * a.bx - vx1 * a.bz;
+    const float vzt = vz1 + vx1 * a.by - vy1 * a.bx;
+    s.vx = vx1 + (ex + a.boris * (vyt * a.bz - vzt * a.by));
+    s.vy = vy1 + (ey + a.boris * (vzt * a.bx - vxt * a.bz));
+    s.vz = vz1 + (ez + a.boris * (vxt * a.by - vyt * a.bx));
+}
+
+// x += v with the cell carry, then the boundary rules; false invalidates.
+// Cells 1..n-1 of every axis are away from both faces (the rules only act on
+// cells <= 0 and >= n), so most particles skip them.
+__device__ __forceinline__ bool move_boundary(const PushArgs& a, PState& s) {
+    s.ox += s.vx; s.oy += s.vy; s.oz += s.vz;
+    const float fx = floorf(s.ox), fy = floorf(s.oy), fz = floorf(s.oz);
+    s.ox -= fx; s.oy -= fy; s.oz -= fz;
+    s.i += __float2int_rd(fx); s.j += __float2int_rd(fy); s.k += __float2int_rd(fz);
+    if ((unsigned)(s.i - 1) < (unsigned)(a.g.n[0] - 1) && (unsigned)(s.j - 1) < (unsigned)(a.g.n[1] - 1) &&
+        (unsigned)(s.k - 1) < (unsigned)(a.g.n[2] - 1))
+        return true;
+    bool live = axis_boundary(a.g, 0, s.i, s.ox) && axis_boundary(a.g, 1, s.j, s.oy) &&
+                axis_boundary(a.g, 2, s.k, s.oz);
+    if (live && !cell_in_range(a.g, s.i, s.j, s.k)) {  // non-finite or runaway velocity
+        live = false;
+        atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_NONFINITE);
+    }
+    return live;
+}
+
+// Body test and absorbed-list append of RootGrid::updateRho's per-particle
+// part (RootGridField.cpp:1173-1178); every lane of the warp calls it.
+__device__ __forceinline__ bool absorb_check(const PushArgs& a, const PState& s, bool live) {
+    uint8_t ob = 0;
+    if (live && a.cellmap) ob = a.cellmap[lin(a.g, s.i, s.j, s.k)];
+    const bool absorbed = ob != 0;
+    const unsigned long long slot = warp_reserve(&a.sc->absorbed_n, absorbed);
+    if (absorbed) {
+        if ((long long)slot < a.ab.cap) {
+            a.ab.cell[slot] = pack_cell(s.i, s.j, s.k);
+            a.ab.ox[slot] = s.ox; a.ab.oy[slot] = s.oy; a.ab.oz[slot] = s.oz;
+            a.ab.vx[slot] = s.vx; a.ab.vy[slot] = s.vy; a.ab.vz[slot] = s.vz;
+            a.ab.species[slot] = (uint8_t)a.s;
+            a.ab.object[slot] = (uint8_t)(ob - 1);
+        } else {
+            atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_ABSORB_OVERFLOW);
+        }
+    }
+    return absorbed;
+}
+
+// The fused particle pass over slots [lo, count). VEL: CIC gather of nodal E
+// and Boris kick/rotate (Grid::updateParticleVelocityES,
+// GridParticleTreatmentES.cpp:13-88). POS: x += v and boundaries
+// (RootGrid::updateParticlePositionES, :90-181). DEP: the per-particle part of
+// RootGrid::updateRho (RootGridField.cpp:1168-1196): particles inside a body go
+// to the absorbed list (Spacecraft::distributeInnerParticleCharge,
+// Spacecraft.cpp:512-592, finished by absorb_kernel); the rest deposit their CIC
+// weights with warp-aggregated atomics. The fused step runs it only on the
+// unsorted tail; push_tile_kernel takes the sorted bricks.
 template <bool VEL, bool POS, bool DEP>
 __global__ void __launch_bounds__(kThreads) push_kernel(PushArgs a) {
     const long long n = (long long)min(*a.count, (unsigned long long)a.cap);
     const long long stride = (long long)gridDim.x * blockDim.x;
     double e2 = 0.0;
-    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+    for (long long base = a.lo + (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
         const long long idx = base + (threadIdx.x & 31);
         const bool inb = idx < n;
-        int32_t cell = inb ? a.p.cell[idx] : -1;
+        const int32_t cell = inb ? a.p.cell[idx] : -1;
         bool live = cell >= 0;
-        float ox = 0.f, oy = 0.f, oz = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
-        int i = 0, j = 0, k = 0;
+        PState st{0, 0, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         if (live) {
-            unpack_cell(cell, i, j, k);
-            ox = a.p.ox[idx]; oy = a.p.oy[idx]; oz = a.p.oz[idx];
-            if (VEL || POS || DEP) { vx = a.p.vx[idx]; vy = a.p.vy[idx]; vz = a.p.vz[idx]; }
+            unpack_cell(cell, st.i, st.j, st.k);
+            st.ox = a.p.ox[idx]; st.oy = a.p.oy[idx]; st.oz = a.p.oz[idx];
+            st.vx = a.p.vx[idx]; st.vy = a.p.vy[idx]; st.vz = a.p.vz[idx];
         }
-        if (VEL && live) {
-            const long long b = lin(a.g, i, j, k);
-            const float x1 = ox, x2 = 1.0f - ox, y1 = oy, y2 = 1.0f - oy, z1 = oz, z2 = 1.0f - oz;
-            const float4 e000 = __ldg(a.E + b), e001 = __ldg(a.E + b + 1);
-            const float4 e010 = __ldg(a.E + b + a.g.sj), e011 = __ldg(a.E + b + a.g.sj + 1);
-            const float4 e100 = __ldg(a.E + b + a.g.si), e101 = __ldg(a.E + b + a.g.si + 1);
-            const float4 e110 = __ldg(a.E + b + a.g.si + a.g.sj), e111 = __ldg(a.E + b + a.g.si + a.g.sj + 1);
-            const float w000 = x2 * y2 * z2, w100 = x1 * y2 * z2, w010 = x2 * y1 * z2, w110 = x1 * y1 * z2;
-            const float w001 = x2 * y2 * z1, w101 = x1 * y2 * z1, w011 = x2 * y1 * z1, w111 = x1 * y1 * z1;
-            const float ex = a.qm * (w000 * e000.x + w100 * e100.x + w010 * e010.x + w110 * e110.x +
-                                     w001 * e001.x + w101 * e101.x + w011 * e011.x + w111 * e111.x);
-            const float ey = a.qm * (w000 * e000.y + w100 * e100.y + w010 * e010.y + w110 * e110.y +
-                                     w001 * e001.y + w101 * e101.y + w011 * e011.y + w111 * e111.y);
-            const float ez = a.qm * (w000 * e000.z + w100 * e100.z + w010 * e010.z + w110 * e110.z +
-                                     w001 * e001.z + w101 * e101.z + w011 * e011.z + w111 * e111.z);
-            const float vx1 = vx + ex, vy1 = vy + ey, vz1 = vz + ez;
-            const float vxt = vx1 + vy1 * a.bz - vz1 * a.by;
-            const float vyt = vy1 + vz1 * a.bx - vx1 * a.bz;
-            const float vzt = vz1 + vx1 * a.by - vy1 * a.bx;
-            vx = vx1 + (ex + a.boris * (vyt * a.bz - vzt * a.by));
-            vy = vy1 + (ey + a.boris * (vzt * a.bx - vxt * a.bz));
-            vz = vz1 + (ez + a.boris * (vxt * a.by - vyt * a.bx));
-        }
-        if (POS && live) {
-            ox += vx; oy += vy; oz += vz;
-            const float fx = floorf(ox), fy = floorf(oy), fz = floorf(oz);
-            ox -= fx; oy -= fy; oz -= fz;
-            i += __float2int_rd(fx); j += __float2int_rd(fy); k += __float2int_rd(fz);
-            live = axis_boundary(a.g, 0, i, ox) && axis_boundary(a.g, 1, j, oy) && axis_boundary(a.g, 2, k, oz);
-            if (live && !cell_in_range(a.g, i, j, k)) {  // non-finite or runaway velocity
-                live = false;
-                atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_NONFINITE);
-            }
-        }
-        bool absorbed = false;
-        if (DEP && live && a.cellmap) {
-            const uint8_t ob = a.cellmap[lin(a.g, i, j, k)];
-            absorbed = ob != 0;
-        }
+        if (VEL && live) gather_boris(a, st);
+        if (POS && live) live = move_boundary(a, st);
         if (DEP) {
-            const unsigned long long slot = warp_reserve(&a.sc->absorbed_n, absorbed);
-            if (absorbed) {
-                if ((long long)slot < a.ab.cap) {
-                    a.ab.cell[slot] = pack_cell(i, j, k);
-                    a.ab.ox[slot] = ox; a.ab.oy[slot] = oy; a.ab.oz[slot] = oz;
-                    a.ab.vx[slot] = vx; a.ab.vy[slot] = vy; a.ab.vz[slot] = vz;
-                    a.ab.species[slot] = (uint8_t)a.s;
-                    a.ab.object[slot] = (uint8_t)(a.cellmap[lin(a.g, i, j, k)] - 1);
-                } else {
-                    atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_ABSORB_OVERFLOW);
-                }
-                live = false;
-            }
-            const bool dep = live;
-            warp_deposit(a.rho, a.g, dep, dep ? lin(a.g, i, j, k) : 0, ox, oy, oz);
-            if (dep && VEL) e2 += (double)vx * vx + (double)vy * vy + (double)vz * vz;
+            if (absorb_check(a, st, live)) live = false;
+            warp_deposit(a.rho, a.g, live, live ? lin(a.g, st.i, st.j, st.k) : 0, st.ox, st.oy, st.oz);
+            if (live && VEL) e2 += (double)st.vx * st.vx + (double)st.vy * st.vy + (double)st.vz * st.vz;
         }
         if (inb && cell >= 0) {
-            if (POS || DEP) a.p.cell[idx] = live ? pack_cell(i, j, k) : -1;
-            if (POS) { a.p.ox[idx] = ox; a.p.oy[idx] = oy; a.p.oz[idx] = oz; }
-            if (VEL) { a.p.vx[idx] = vx; a.p.vy[idx] = vy; a.p.vz[idx] = vz; }
+            if (POS || DEP) a.p.cell[idx] = live ? pack_cell(st.i, st.j, st.k) : -1;
+            if (POS) { a.p.ox[idx] = st.ox; a.p.oy[idx] = st.oy; a.p.oz[idx] = st.oz; }
+            if (VEL) { a.p.vx[idx] = st.vx; a.p.vy[idx] = st.vy; a.p.vz[idx] = st.vz; }
         }
     }
     if (DEP && VEL) {
         const double t = block_sum(e2);
         if (threadIdx.x == 0 && t != 0.0) atomicAdd(&a.sc->energy[a.s], t);
     }
+}
+
+// ------------------------------------------------------------------ brick-tiled fused push
+constexpr int kTileThreads = 256;
+constexpr int kHalo = 2;                           // cells a particle may drift out of its brick
+constexpr int kWX = kBX + 1 + 2 * kHalo, kWY = kBY + 1 + 2 * kHalo, kWZ = kBZ + 1 + 2 * kHalo;
+constexpr int kTile = kWX * kWY * kWZ;             // 9 x 9 x 13 nodes
+
+// Adds one integer corner weight (< 2^52) to the shared tile, held as three
+// 32-bit planes of 17-bit chunks so the additions are native 32-bit shared
+// atomics; a plane overflows only after 2^15 full-weight additions to a node.
+__device__ __forceinline__ void tile_add(unsigned* t0, unsigned* t1, unsigned* t2, int idx, unsigned long long w) {
+    atomicAdd(t0 + idx, (unsigned)(w & 0x1FFFFull));
+    atomicAdd(t1 + idx, (unsigned)((w >> 17) & 0x1FFFFull));
+    const unsigned c2 = (unsigned)(w >> 34);
+    if (c2) atomicAdd(t2 + idx, c2);
+}
+
+constexpr int kRun = 4;                               // consecutive particles per thread
+constexpr int kChunk = kTileThreads * kRun;           // particles staged per pass
+constexpr int kChunkPad = kChunk + kChunk / 32;       // one pad word per 32 entries
+__device__ __forceinline__ int padi(int q) { return q + (q >> 5); }
+
+__device__ __forceinline__ void tile_flush(unsigned* t0, unsigned* t1, unsigned* t2, int tb,
+                                           const unsigned long long acc[8]) {
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        const int off = ((t >> 2) ? kWY * kWZ : 0) + (((t >> 1) & 1) ? kWZ : 0) + (t & 1);
+        if (acc[t]) tile_add(t0, t1, t2, tb + off, acc[t]);
+    }
+}
+
+// The fused push (gather + Boris + move + boundaries + absorption flag +
+// deposit + kinetic energy) over the brick-sorted particles, one brick per CTA.
+// A chunk of kChunk particles is staged through shared memory with coalesced
+// loads; thread (warp w, lane l) then owns the kRun consecutive entries starting
+// at l*32 + w*kRun, so the lanes of a warp sit ~32 particles (about one cell)
+// apart while each thread walks a run of particles that mostly share a cell. A
+// thread sums its run's corner weights in registers and adds them to the shared
+// tile (brick + 2-cell halo, three 32-bit planes of 17-bit chunks) when the
+// cell changes; particles that drifted beyond the halo add straight to HBM. The
+// tile is flushed with one 64-bit atomic per nonzero node.
+__global__ void __launch_bounds__(kTileThreads, 4) push_tile_kernel(PushArgs a, const int32_t* brick_start) {
+    __shared__ unsigned t0[kTile], t1[kTile], t2[kTile];
+    __shared__ int32_t s_cell[kChunkPad];
+    __shared__ float s_f[6][kChunkPad];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int b = blockIdx.x;
+    const int bi = b / (a.g.nb[1] * a.g.nb[2]), bj = (b / a.g.nb[2]) % a.g.nb[1], bk = b % a.g.nb[2];
+    const int wx0 = bi * kBX - kHalo, wy0 = bj * kBY - kHalo, wz0 = bk * kBZ - kHalo;
+    for (int t = tid; t < kTile; t += kTileThreads) { t0[t] = 0u; t1[t] = 0u; t2[t] = 0u; }
+    const long long p0 = brick_start[b], p1 = brick_start[b + 1];
+    // every particle adds at most once to a node, so fewer than 2^15 particles
+    // cannot overflow a 32-bit chunk plane; denser bricks deposit to HBM
+    const bool tile_ok = (p1 - p0) < 32768;
+    double e2 = 0.0;
+    __syncthreads();
+    for (long long c0 = p0; c0 < p1; c0 += kChunk) {
+        const int m = (int)min((long long)kChunk, p1 - c0);
+        for (int q = tid; q < kChunk; q += kTileThreads) {
+            const int d = padi(q);
+            if (q < m) {
+                s_cell[d] = a.p.cell[c0 + q];
+                s_f[0][d] = a.p.ox[c0 + q]; s_f[1][d] = a.p.oy[c0 + q]; s_f[2][d] = a.p.oz[c0 + q];
+                s_f[3][d] = a.p.vx[c0 + q]; s_f[4][d] = a.p.vy[c0 + q]; s_f[5][d] = a.p.vz[c0 + q];
+            } else {
+                s_cell[d] = -1;
+            }
+        }
+        __syncthreads();
+        int cur = -1;
+        unsigned long long acc[8];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) acc[t] = 0ull;
+#pragma unroll 1
+        for (int r = 0; r < kRun; ++r) {
+            const int d = padi(lane * 32 + warp * kRun + r);
+            const int32_t cell = s_cell[d];
+            bool live = cell >= 0;
+            PState st{0, 0, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            if (live) {
+                unpack_cell(cell, st.i, st.j, st.k);
+                st.ox = s_f[0][d]; st.oy = s_f[1][d]; st.oz = s_f[2][d];
+                st.vx = s_f[3][d]; st.vy = s_f[4][d]; st.vz = s_f[5][d];
+                gather_boris(a, st);
+                live = move_boundary(a, st);
+            }
+            if (absorb_check(a, st, live)) live = false;
+            if (live) {
+                const unsigned qa = (unsigned)__float2int_rn(st.ox * kDepositScale);
+                const unsigned qb = (unsigned)__float2int_rn(st.oy * kDepositScale);
+                const unsigned qd = (unsigned)__float2int_rn(st.oz * kDepositScale);
+                const unsigned wx[2] = {(unsigned)kDepositOne - qa, qa}, wy[2] = {(unsigned)kDepositOne - qb, qb};
+                const unsigned wz[2] = {(unsigned)kDepositOne - qd, qd};
+                const int li = st.i - wx0, lj = st.j - wy0, lk = st.k - wz0;
+                if (tile_ok && li >= 0 && lj >= 0 && lk >= 0 && li < kWX - 1 && lj < kWY - 1 && lk < kWZ - 1) {
+                    const int tb = (li * kWY + lj) * kWZ + lk;
+                    if (tb != cur) {
+                        if (cur >= 0) tile_flush(t0, t1, t2, cur, acc);
+                        cur = tb;
+#pragma unroll
+                        for (int t = 0; t < 8; ++t) acc[t] = 0ull;
+                    }
+#pragma unroll
+                    for (int t = 0; t < 8; ++t)
+                        acc[t] += (unsigned long long)wx[t >> 2] * wy[(t >> 1) & 1] * wz[t & 1];
+                } else {
+                    const long long gb = lin(a.g, st.i, st.j, st.k);
+#pragma unroll
+                    for (int t = 0; t < 8; ++t) {
+                        const unsigned long long w = (unsigned long long)wx[t >> 2] * wy[(t >> 1) & 1] * wz[t & 1];
+                        if (w) atomicAdd(a.rho + gb + corner_offset(a.g, t), w);
+                    }
+                }
+                e2 += (double)st.vx * st.vx + (double)st.vy * st.vy + (double)st.vz * st.vz;
+            }
+            if (cell >= 0) {
+                s_cell[d] = live ? pack_cell(st.i, st.j, st.k) : -1;
+                s_f[0][d] = st.ox; s_f[1][d] = st.oy; s_f[2][d] = st.oz;
+                s_f[3][d] = st.vx; s_f[4][d] = st.vy; s_f[5][d] = st.vz;
+            }
+        }
+        if (cur >= 0) tile_flush(t0, t1, t2, cur, acc);
+        __syncthreads();
+        for (int q = tid; q < m; q += kTileThreads) {
+            const int d = padi(q);
+            a.p.cell[c0 + q] = s_cell[d];
+            a.p.ox[c0 + q] = s_f[0][d]; a.p.oy[c0 + q] = s_f[1][d]; a.p.oz[c0 + q] = s_f[2][d];
+            a.p.vx[c0 + q] = s_f[3][d]; a.p.vy[c0 + q] = s_f[4][d]; a.p.vz[c0 + q] = s_f[5][d];
+        }
+        __syncthreads();
+    }
+    for (int t = tid; t < kTile; t += kTileThreads) {
+        const unsigned long long v = (unsigned long long)t0[t] + ((unsigned long long)t1[t] << 17) +
+                                     ((unsigned long long)t2[t] << 34);
+        if (!v) continue;
+        const int x = wx0 + t / (kWY * kWZ), y = wy0 + (t / kWZ) % kWY, z = wz0 + t % kWZ;
+        atomicAdd(a.rho + lin(a.g, x, y, z), v);
+    }
+    const double tot = block_sum(e2);
+    if (tid == 0 && tot != 0.0) atomicAdd(&a.sc->energy[a.s], tot);
 }
 
 // Writes a particle created in FP64 into a species slot (split precision).
@@ -731,7 +910,7 @@ __global__ void sort_count_kernel(Soa p, long long cap, const unsigned long long
         const long long t = base + (threadIdx.x & 31);
         const int32_t c = t < n ? p.cell[t] : -1;
         long long key = -1 - (long long)(threadIdx.x & 31);
-        if (c >= 0) { int i, j, k; unpack_cell(c, i, j, k); key = lin(g, i, j, k); }
+        if (c >= 0) { int i, j, k; unpack_cell(c, i, j, k); key = brick_key(g, i, j, k); }
         const unsigned grp = __match_any_sync(kFull, key);
         const int lane = threadIdx.x & 31;
         if (c >= 0 && (__ffs(grp) - 1) == lane) atomicAdd(cnt + key, __popc(grp));
@@ -790,6 +969,12 @@ __global__ void scan_apply_kernel(const int32_t* in, long long n, const int32_t*
     for (int q = 0; q < kScanItems; ++q) { if (base + q < n) out[base + q] = pre; pre += v[q]; }
 }
 
+// brick_start[b] = first sorted slot of brick b (exclusive offsets every kBrickCells keys).
+__global__ void brick_start_kernel(const int32_t* offset, int nbricks, int32_t* brick_start) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= nbricks; b += gridDim.x * blockDim.x)
+        brick_start[b] = offset[(long long)b * kBrickCells];
+}
+
 __global__ void sort_scatter_kernel(Soa src, Soa dst, long long cap, const unsigned long long* count, Grid g,
                                     int32_t* cursor) {
     const long long n = (long long)min(*count, (unsigned long long)cap);
@@ -799,7 +984,7 @@ __global__ void sort_scatter_kernel(Soa src, Soa dst, long long cap, const unsig
         const long long t = base + lane;
         const int32_t c = t < n ? src.cell[t] : -1;
         long long key = -1 - lane;
-        if (c >= 0) { int i, j, k; unpack_cell(c, i, j, k); key = lin(g, i, j, k); }
+        if (c >= 0) { int i, j, k; unpack_cell(c, i, j, k); key = brick_key(g, i, j, k); }
         const unsigned grp = __match_any_sync(kFull, key);
         const int leader = __ffs(grp) - 1;
         int b = 0;
@@ -818,15 +1003,17 @@ int grid_for(long long n, int threads = kThreads) {
     return (int)std::max<long long>(1, std::min<long long>(b, 148LL * 16));
 }
 
-void alloc_soa(Soa& s, int64_t cap) {
-    FOPIS_CUDA(cudaMalloc(&s.cell, sizeof(int32_t) * cap));
+// Particle arrays come from the device's stream-ordered pool, so growing them
+// mid-run neither synchronises the device nor returns memory to the driver.
+void alloc_soa(Soa& s, int64_t cap, cudaStream_t st) {
+    FOPIS_CUDA(cudaMallocAsync((void**)&s.cell, sizeof(int32_t) * cap, st));
     float** f[6] = {&s.ox, &s.oy, &s.oz, &s.vx, &s.vy, &s.vz};
-    for (auto* q : f) FOPIS_CUDA(cudaMalloc(q, sizeof(float) * cap));
+    for (auto* q : f) FOPIS_CUDA(cudaMallocAsync((void**)q, sizeof(float) * cap, st));
 }
-void free_soa(Soa& s) {
-    cudaFree(s.cell);
+void free_soa(Soa& s, cudaStream_t st) {
+    if (s.cell) cudaFreeAsync(s.cell, st);
     float* f[6] = {s.ox, s.oy, s.oz, s.vx, s.vy, s.vz};
-    for (auto* q : f) cudaFree(q);
+    for (auto* q : f) if (q) cudaFreeAsync(q, st);
     s = Soa{};
 }
 void copy_soa(Soa& d, const Soa& s, int64_t n, cudaStream_t st) {
@@ -844,15 +1031,14 @@ void particles_alloc(Ctx& c, int s, int64_t need) {
     if (need <= c.cap[s]) return;
     int64_t cap = std::max<int64_t>(need, 1024);
     Soa a{}, b{};
-    alloc_soa(a, cap);
-    alloc_soa(b, cap);
+    alloc_soa(a, cap, c.st);
+    alloc_soa(b, cap, c.st);
     FOPIS_CUDA(cudaMemsetAsync(a.cell, 0xff, sizeof(int32_t) * cap, c.st));
     if (c.cap[s] > 0) {
         sync_scalars(c);
         copy_soa(a, c.sp[s], std::min<int64_t>(c.nslots[s], c.cap[s]), c.st);
-        FOPIS_CUDA(cudaStreamSynchronize(c.st));
-        free_soa(c.sp[s]);
-        free_soa(c.sp2[s]);
+        free_soa(c.sp[s], c.st);
+        free_soa(c.sp2[s], c.st);
     }
     c.sp[s] = a;
     c.sp2[s] = b;
@@ -922,7 +1108,7 @@ int64_t particles_export_raw(Ctx& c, int s, int32_t* cell, float* ox, float* oy,
     const int64_t n = c.nslots[s];
     const int64_t chunk = 1 << 20;
     Soa raw{};
-    alloc_soa(raw, chunk);
+    alloc_soa(raw, chunk, c.st);
     unsigned long long* dc = nullptr;
     FOPIS_CUDA(cudaMalloc(&dc, sizeof(unsigned long long)));
     int64_t total = 0;
@@ -938,7 +1124,7 @@ int64_t particles_export_raw(Ctx& c, int s, int32_t* cell, float* ox, float* oy,
         }
         total += k;
     }
-    free_soa(raw);
+    free_soa(raw, c.st);
     cudaFree(dc);
     return total;
 }
@@ -971,40 +1157,56 @@ void particles_generate_ambient(Ctx& c) {
     sync_scalars(c);
 }
 
+int64_t brick_keys(const Ctx& c) {
+    const Grid g = make_grid(c);
+    return (int64_t)g.nb[0] * g.nb[1] * g.nb[2] * kBrickCells;
+}
+
+int brick_count(const Ctx& c) {
+    const Grid g = make_grid(c);
+    return g.nb[0] * g.nb[1] * g.nb[2];
+}
+
+// Counting sort of every species by brick, then by cell inside the brick
+// (key = brick_key); invalid slots are dropped. Records each brick's first
+// slot for push_tile_kernel.
 void particles_sort(Ctx& c) {
     sync_scalars(c);
     const Grid g = make_grid(c);
-    const long long N = (long long)c.N;
-    const int tiles = (int)((N + kScanTile - 1) / kScanTile);
+    const long long K = brick_keys(c);
+    const int nbricks = brick_count(c);
+    const int tiles = (int)((K + 1 + kScanTile - 1) / kScanTile);
     for (int s = 0; s < c.nsp; ++s) {
-        if (c.cap[s] == 0 || c.nslots[s] == 0) continue;
-        FOPIS_CUDA(cudaMemsetAsync(c.sort_count, 0, sizeof(int32_t) * (N + 1), c.st));
+        if (c.cap[s] == 0) continue;
+        if (!c.brick_start[s]) FOPIS_CUDA(cudaMalloc(&c.brick_start[s], sizeof(int32_t) * (nbricks + 1)));
+        FOPIS_CUDA(cudaMemsetAsync(c.sort_count, 0, sizeof(int32_t) * (K + 1), c.st));
         ++c.launches;
-        sort_count_kernel<<<grid_for(c.nslots[s]), kThreads, 0, c.st>>>(c.sp[s], c.cap[s], &c.d_sc->count[s], g,
-                                                                         c.sort_count);
+        sort_count_kernel<<<grid_for(std::max<int64_t>(c.nslots[s], 1)), kThreads, 0, c.st>>>(
+            c.sp[s], c.cap[s], &c.d_sc->count[s], g, c.sort_count);
         FOPIS_LAUNCH_CHECK();
         ++c.launches;
-        scan_tiles_kernel<<<tiles, kScanThreads, 0, c.st>>>(c.sort_count, N + 1, c.scan_partials);
+        scan_tiles_kernel<<<tiles, kScanThreads, 0, c.st>>>(c.sort_count, K + 1, c.scan_partials);
         ++c.launches;
         scan_partials_kernel<<<1, kScanThreads, 0, c.st>>>(c.scan_partials, tiles);
         ++c.launches;
-        scan_apply_kernel<<<tiles, kScanThreads, 0, c.st>>>(c.sort_count, N + 1, c.scan_partials, c.sort_offset);
+        scan_apply_kernel<<<tiles, kScanThreads, 0, c.st>>>(c.sort_count, K + 1, c.scan_partials, c.sort_offset);
+        ++c.launches;
+        brick_start_kernel<<<(nbricks + 256) / 256, 256, 0, c.st>>>(c.sort_offset, nbricks, c.brick_start[s]);
         FOPIS_LAUNCH_CHECK();
         ++c.launches;
-        sort_scatter_kernel<<<grid_for(c.nslots[s]), kThreads, 0, c.st>>>(c.sp[s], c.sp2[s], c.cap[s],
-                                                                          &c.d_sc->count[s], g, c.sort_offset);
+        sort_scatter_kernel<<<grid_for(std::max<int64_t>(c.nslots[s], 1)), kThreads, 0, c.st>>>(
+            c.sp[s], c.sp2[s], c.cap[s], &c.d_sc->count[s], g, c.sort_offset);
         FOPIS_LAUNCH_CHECK();
-        // new count = total of valid particles = sort_offset[N] after the scatter
-        // cursors advanced; the exclusive scan's last entry holds the total.
+        // the new count is the total of valid particles: the scan's grand total
         FOPIS_CUDA(cudaMemcpyAsync(&c.d_sc->count[s], c.scan_partials + tiles, sizeof(int32_t), cudaMemcpyDeviceToDevice, c.st));
         FOPIS_CUDA(cudaMemsetAsync(((char*)&c.d_sc->count[s]) + 4, 0, 4, c.st));
         std::swap(c.sp[s], c.sp2[s]);
-        // invalidate the tail beyond the new count so stale slots never read as live
     }
     sync_scalars(c);
     for (int s = 0; s < c.nsp; ++s) {
         if (c.cap[s] == 0) continue;
         const int64_t n = c.nslots[s];
+        c.sorted_n[s] = n;
         if (n < c.cap[s]) FOPIS_CUDA(cudaMemsetAsync(c.sp[s].cell + n, 0xff, sizeof(int32_t) * (c.cap[s] - n), c.st));
         // keep head room for the appends of the coming steps
         const int64_t want = (int64_t)(n * 1.25) + 65536;
@@ -1014,7 +1216,7 @@ void particles_sort(Ctx& c) {
 
 static PushArgs push_args(Ctx& c, int s) {
     PushArgs a;
-    a.p = c.sp[s]; a.s = s; a.cap = c.cap[s]; a.count = &c.d_sc->count[s];
+    a.p = c.sp[s]; a.s = s; a.cap = c.cap[s]; a.lo = 0; a.count = &c.d_sc->count[s];
     a.E = c.E; a.g = make_grid(c);
     a.qm = (float)(0.5 * c.p.species[s].charge / c.p.species[s].mass);
     a.bx = (float)c.p.static_bfield[0]; a.by = (float)c.p.static_bfield[1]; a.bz = (float)c.p.static_bfield[2];
@@ -1032,7 +1234,14 @@ void launch_push(Ctx& c, bool vel, bool pos, bool dep) {
         if (c.cap[s] == 0) continue;
         PushArgs a = push_args(c, s);
         const int grid = grid_for(c.cap[s]);
-        if (vel && pos && dep) { ++c.launches; push_kernel<true, true, true><<<grid, kThreads, 0, c.st>>>(a); }
+        if (vel && pos && dep && c.sorted_n[s] > 0 && c.brick_start[s]) {
+            ++c.launches;
+            push_tile_kernel<<<brick_count(c), kTileThreads, 0, c.st>>>(a, c.brick_start[s]);
+            a.lo = c.sorted_n[s];
+            ++c.launches;
+            push_kernel<true, true, true><<<grid_for(std::max<int64_t>(c.cap[s] - a.lo, 1)), kThreads, 0, c.st>>>(a);
+        }
+        else if (vel && pos && dep) { ++c.launches; push_kernel<true, true, true><<<grid, kThreads, 0, c.st>>>(a); }
         else if (vel && !pos && !dep) { ++c.launches; push_kernel<true, false, false><<<grid, kThreads, 0, c.st>>>(a); }
         else if (!vel && pos && !dep) { ++c.launches; push_kernel<false, true, false><<<grid, kThreads, 0, c.st>>>(a); }
         else if (!vel && !pos && dep) { ++c.launches; push_kernel<false, false, true><<<grid, kThreads, 0, c.st>>>(a); }
@@ -1065,7 +1274,8 @@ void launch_emit(Ctx& c, bool fused) {
         if (K <= 0) continue;
         const int64_t add = (int64_t)ob.n_lit * K;
         sync_scalars(c);
-        if (c.nslots[s] + add > c.cap[s]) particles_alloc(c, s, (int64_t)((c.nslots[s] + add) * 1.5) + 65536);
+        if (c.nslots[s] + add > c.cap[s])
+            particles_alloc(c, s, std::max<int64_t>((int64_t)((c.nslots[s] + add) * 1.5), add * 2048) + 65536);
         SourceArgs a = source_args(c, fused);
         EmitArgs e;
         e.obj = (int)o; e.s = s; e.K = K; e.eaxis = eaxis;

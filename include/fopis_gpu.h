@@ -106,7 +106,7 @@ typedef struct fopis_params {
     double poisson_tol;          /* ||f - A phi||_2 <= tol ||f||_2 ; 0 -> 1e-8 */
     int max_vcycles;             /* V-cycle cap per solve; 0 -> 100 */
     int guess_mode;              /* fopis_guess_mode */
-    int sort_interval;           /* counting-sort period in steps; 0 -> 4 */
+    int sort_interval;           /* counting-sort period in steps; 0 -> 8 */
     int remove_interval;         /* removeInvalidParticles period (RootGrid.cpp:136-140); 0 -> 50 */
     double capacity_factor;      /* particle capacity / initial count; 0 -> 1.5 */
     int precision;               /* fopis_precision */
