@@ -110,13 +110,38 @@ def dist_setup():
 
 
 def allreduce(v: float, op: str, world: int) -> float:
+    """Max or sum of a scalar over the ranks (replicas only: timing and totals)."""
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def aggregate(ms: float, psteps: float, world: int):
+    """Whole-job throughput of N replicas: particle-steps summed, time = max over ranks."""
+    ms_max = allreduce(ms, "max", world)
+    ps = allreduce(psteps, "sum", world)
+    return ms_max, ps, ps / (ms_max * 1e-3)
+
+
+WORKLOADS = {
+    "periodic32": ("32^3 nodes fully periodic, e+i mass ratio 100, Te = Ti, no object", 16),
+    "cube64": ("64^3 cells Dirichlet + 6-face injection, e+i mass ratio 100, 8^3 conductor cube", 32),
+    "cube128": ("128^3 cells Dirichlet + 6-face injection, e+i mass ratio 100, 16^3 conductor cube with "
+                "+x photoemission (10x electron flux, 0.2 Te)", 32),
+    "cube128_plain": ("128^3 cells Dirichlet + 6-face injection, e+i mass ratio 100, 16^3 conductor cube", 32),
+    "craft256": ("256^3 cells Dirichlet + 6-face injection, e+i mass ratio 100, 32x16x16 body + 48x4x16 panel "
+                 "with +x photoemission", 32),
+}
+
+
+def workload_desc(name: str, ppc) -> str:
+    text, default_ppc = WORKLOADS[name]
+    return f"{name}: {text}, {ppc or default_ppc} ppc/species, MG to ||r||/||f|| <= 1e-8, 2 solves/step"
 
 
 def barrier(world: int):
@@ -179,8 +204,7 @@ def run_gpu(args, world, rank, local):
     ms = ev0.elapsed_time(ev1)
     step_ms = [ev0.elapsed_time(step_ev[0])] + [step_ev[t - 1].elapsed_time(step_ev[t]) for t in range(1, args.steps)]
     launches = g.stats().kernel_launches - launches0
-    ms_max = allreduce(ms, "max", world)
-    psteps_all = allreduce(float(psteps), "sum", world)
+    ms_max, psteps_all, _ = aggregate(ms, float(psteps), world)
     st = g.stats()
     phases = list(st.ms_phase)
     result = {
@@ -229,9 +253,8 @@ def run_gpu(args, world, rank, local):
         e1.record(stream2)
         torch.cuda.synchronize(local)
         barrier(world)
-        ms2 = allreduce(e0.elapsed_time(e1), "max", world)
-        ps2 = allreduce(float(ps2), "sum", world)
-        result["e2e"] = {"value": ps2 / (ms2 * 1e-3), "unit": "particle-steps/s",
+        ms2, ps2, v2 = aggregate(e0.elapsed_time(e1), float(ps2), world)
+        result["e2e"] = {"value": v2, "unit": "particle-steps/s",
                          "h2d_bytes_per_step": int(nbytes // max(1, args.steps)),
                          "d2h_bytes_per_step": int(d2h // max(1, args.steps)),
                          "ms_total": ms2, "note": "one upload of the particle set (56-byte records) from pinned "
@@ -243,10 +266,19 @@ def run_gpu(args, world, rank, local):
     return result, cfg
 
 
+def reference_cmatrix(cfg):
+    """Capacity matrix for the CPU arms, as the reference's use_existing_capacity_matrix
+    would load it: the exact sine-basis build of the oracle (host only, untimed)."""
+    if not cfg.objects:
+        return None
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+    return orc.dirichlet_capacity_matrix(cfg.params, cfg.objects[0].nodes)
+
+
 def run_oracle(cfg, Cm, threads: int, steps: int):
     """The oracle (FP64 CPU restatement of the reference path, reference PSOR with
-    its 1000-sweep cap) on the same workload; capacity matrix taken from the GPU
-    build as the reference's use_existing_capacity_matrix would load it."""
+    its 1000-sweep cap) on the same workload, capacity matrix preloaded."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as orc
     orc.lib().orc_set_threads(threads)
@@ -272,7 +304,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fopis", choices=["fopis", "reference"])
     ap.add_argument("--workload", default="cube128")
-    ap.add_argument("--ppc", type=int, default=32)
+    ap.add_argument("--ppc", type=int, default=None, help="particles per cell per species (workload default)")
     ap.add_argument("--sort-interval", type=int, default=8)
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu", dest="cpu", action="store_false")
@@ -287,9 +319,7 @@ def main():
     base = {"metric": "particle-steps/s", "unit": "particle-steps/s", "n_gpus": world, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "data": "synthetic (Philox-seeded Maxwellian plasma)",
             "dtype": "fp32 particles, int64 fixed-point rho, fp32 smoother in fp64 refinement",
-            "config": {"workload": f"{args.workload}: 128^3 cells Dirichlet + 6-face injection, e+i mass ratio 100, "
-                                   f"{args.ppc} ppc/species, 16^3 conductor cube with +x photoemission, "
-                                   "MG to ||r||/||f|| <= 1e-8, 2 solves/step",
+            "config": {"workload": workload_desc(args.workload, args.ppc),
                        "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (particle state ~3.8 GB)",
                        "sort_interval": args.sort_interval}}
     if args.impl == "reference":
@@ -297,15 +327,9 @@ def main():
             return
         from fopis_b200 import config
         cfg = config.workload(args.workload, ppc=args.ppc, seed=20251203)
-        # the reference arm has no GPU: the capacity matrix is built by the same
-        # oracle's exact solves only on small cases, so use the reference's own
-        # load path when a cached matrix exists, else the oracle's build
-        cache = ROOT / "gpurun_out" / f"cmatrix_{args.workload}.npy"
-        Cm = np.load(cache) if cache.exists() else None
-        if Cm is None and cfg.objects:
-            print(json.dumps({"impl": "reference", "unavailable": "capacity matrix cache missing (run the fopis arm "
-                                                                  "first; the CPU build takes n_cmat full solves)"}))
-            return
+        # untimed setup: the capacity matrix the reference would load from its
+        # cache, computed exactly on the host (six Dirichlet faces)
+        Cm = reference_cmatrix(cfg)
         v, dt, n, it = run_oracle(cfg, Cm, threads, args.cpu_steps)
         line = dict(base, impl="reference", value=v, steps=args.cpu_steps, warmup=0, ms_per_step=dt * 1e3 / args.cpu_steps,
                     n_gpus=1)
@@ -342,11 +366,10 @@ def main():
     if "e2e" in res:
         line["e2e"] = res["e2e"]
     if rank == 0 and res["cmatrix"] is not None:
-        out = ROOT / "gpurun_out"
-        out.mkdir(exist_ok=True)
-        np.save(out / f"cmatrix_{args.workload}.npy", res["cmatrix"])
+        Cx = reference_cmatrix(cfg)
+        line["cmatrix_rel_err_vs_exact"] = float(np.abs(res["cmatrix"] - Cx).max() / np.abs(Cx).max())
     if rank == 0 and world == 1 and args.cpu:
-        v, dt, n, it = run_oracle(cfg, res["cmatrix"], os.cpu_count() or 1, args.cpu_steps)
+        v, dt, n, it = run_oracle(cfg, reference_cmatrix(cfg), os.cpu_count() or 1, args.cpu_steps)
         line["cpu_baseline"] = {"value": v, "unit": "particle-steps/s", "cores": os.cpu_count() or 1, "kind": "port",
                                 "sample": f"{args.cpu_steps} full step(s) of the same workload ({n} particles) on the "
                                           f"oracle: FP64 AoS, OpenMP, reference PSOR ({it} sweeps last solve)",

@@ -247,7 +247,7 @@ def plasma_units(n0: float = 1e7, te_ev: float = 1.0, dt_omega: float = 0.1):
     return lam * (1.0 - 1e-6), dt_omega / wpe
 
 
-def workload(name: str, ppc: int = 32, seed: int = 20251203, **kw) -> SimConfig:
+def workload(name: str, ppc: Optional[int] = None, seed: int = 20251203, **kw) -> SimConfig:
     """Synthetic configurations:
     periodic32   32^3 cells periodic, 16 ppc/species, no object (CPU-runnable case);
     cube64       64^3 cells Dirichlet + injection, 8^3 cube conductor, 32 ppc;
@@ -257,6 +257,8 @@ def workload(name: str, ppc: int = 32, seed: int = 20251203, **kw) -> SimConfig:
     Electrons + ions (mass ratio 100), Te = Ti = 1 eV, n = 1e7 m^-3."""
     dx, dt = plasma_units()
     n0, te = 1e7, 1.0
+    if ppc is None:
+        ppc = 16 if name == "periodic32" else 32
     e_sp = SpeciesInfo("Electron", "ambient", 1.0, -1.0, n0, te, ppc)
     i_sp = SpeciesInfo("Ion", "ambient", 100.0, 1.0, n0, te, ppc)
     species = [e_sp, i_sp]
@@ -265,8 +267,6 @@ def workload(name: str, ppc: int = 32, seed: int = 20251203, **kw) -> SimConfig:
     photo = False
     if name == "periodic32":
         nxyz, boundary = (32, 32, 32), "PPPPPP"
-        if "ppc" not in kw:
-            e_sp.ppc = i_sp.ppc = 16
     elif name == "cube64":
         nxyz, boundary = (65, 65, 65), "DDDDDD"
         boxes = [((-4, -4, -4), (4, 4, 4))]

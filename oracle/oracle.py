@@ -123,6 +123,53 @@ def ref_position(xyz: np.ndarray):
     return ijk, d
 
 
+def dirichlet_capacity_matrix(params, nodes, max_table: float = 6e7) -> np.ndarray:
+    """Capacity matrix of one conductor in a box whose six faces are Dirichlet
+    (phi = 0), built exactly instead of by one Poisson solve per surface node.
+
+    RootGrid::initializeObjectsCmatrix (src/Grid/RootGrid/RootGridObject.cpp:77-148)
+    fills M[c][r] = phi at surface node r for rho = 1 at surface node c (the
+    Poisson solve ignores the body) and inverts M. With Dirichlet faces the
+    unknowns of axis d are glue indices 2..n_d-1 (u = 1..m_d, m_d = n_d - 2) and
+    the 7-point operator diagonalises in the sine basis
+        s_k(u) = sqrt(2/(m+1)) sin(pi k u/(m+1)),  lambda_k = 2 - 2 cos(pi k/(m+1)),
+    so M[c][r] = (1/eps0) sum_k prod_d s_{k_d}(r_d) s_{k_d}(c_d) / sum_d lambda_{k_d}.
+    The sum is taken over pairs of the distinct surface coordinates per axis
+    (three BLAS contractions), which is the converged solve the reference's
+    PSOR approximates. Returns C = M^-1 (numpy's LU inverse in place of Eigen's).
+    """
+    b = bytes(params.boundary).split(b"\0")[0].decode()
+    if b != "DDDDDD":
+        raise NotImplementedError("exact capacity matrix needs six Dirichlet faces, got " + b)
+    nodes = np.asarray(nodes, np.int64)
+    dims = (params.nx, params.ny, params.nz)
+    S, W, idx = [], None, []
+    lam = []
+    for d in range(3):
+        m = dims[d] - 2
+        u = nodes[:, d] - 1
+        if u.min() < 1 or u.max() > m:
+            raise ValueError("a surface node sits on a Dirichlet face")
+        U, inv = np.unique(u, return_inverse=True)
+        k = np.arange(1, m + 1)
+        S.append(np.sqrt(2.0 / (m + 1)) * np.sin(np.pi * np.outer(k, U) / (m + 1)))   # (m, |U|)
+        lam.append(2.0 - 2.0 * np.cos(np.pi * k / (m + 1)))
+        idx.append(inv)
+    mx, my, mz = (s.shape[1] for s in S)
+    if float(mx * my * mz) ** 2 > max_table:
+        raise NotImplementedError("surface spans too many distinct coordinates for the pair table")
+    W = 1.0 / (lam[0][:, None, None] + lam[1][None, :, None] + lam[2][None, None, :])
+    P = [np.einsum("ka,kb->kab", s, s).reshape(s.shape[0], -1) for s in S]     # (m, |U|^2)
+    nx_, ny_, nz_ = W.shape
+    Q1 = W.reshape(nx_ * ny_, nz_) @ P[2]                                        # (kx*ky, C)
+    Q1 = Q1.reshape(nx_, ny_, -1)
+    Q2 = np.einsum("yb,xyc->xbc", P[1], Q1, optimize=True)                       # (kx, B, C)
+    T = (P[0].T @ Q2.reshape(nx_, -1)).reshape(mx, mx, my, my, mz, mz)
+    ix, iy, iz = idx
+    M = T[ix[:, None], ix[None, :], iy[:, None], iy[None, :], iz[:, None], iz[None, :]] / params.eps0
+    return np.linalg.inv(M)
+
+
 class Oracle:
     """One CPU simulation with the reference's semantics (FP64)."""
 

@@ -195,3 +195,19 @@ def test_oracle_injection_counts_follow_flux_with_carry():
         for face in range(6):
             expect = 5 * area * sp.flux[face]
             assert abs(total[s, face] - expect) <= 1.0
+
+
+def test_exact_capacity_matrix_matches_solved_one():
+    """The sine-basis capacity matrix equals the one built by a converged solve
+    per surface node (the reference's procedure) on a 25^3 Dirichlet box."""
+    from fopis_b200.config import SpeciesInfo, make_params, plasma_units, objects_from_boxes
+    dx, dt = plasma_units()
+    sp = [SpeciesInfo("Electron", "ambient", 1.0, -1.0, 1e7, 1.0, 2)]
+    p, _ = make_params((25, 25, 25), "DDDDDD", dx, dt, sp, tol=1e-10)
+    obj = objects_from_boxes([((-2, -3, -1), (2, 3, 2))], (25, 25, 25))
+    o = orc.Oracle(p, [obj])
+    o.set_solver(1, exact_tol=1e-13)
+    o.build_cmatrix(0)
+    Cs = o.get_cmatrix(0)
+    Cx = orc.dirichlet_capacity_matrix(p, obj.nodes)
+    assert np.abs(Cx - Cs).max() < 1e-11 * np.abs(Cs).max()
