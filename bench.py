@@ -150,10 +150,16 @@ def barrier(world: int):
         dist.barrier()
 
 
+def guess_mode(args):
+    from fopis_b200 import _abi
+    return _abi.GUESS_HISTORY if args.guess == "history" else _abi.GUESS_WARM
+
+
 def build_sim(args, rank, local):
     from fopis_b200 import RootGrid, config
     cfg = config.workload(args.workload, ppc=args.ppc, seed=20251203 + 7919 * rank, sort_interval=args.sort_interval)
     g = RootGrid(cfg, device=local)
+    g.set_guess_mode(guess_mode(args))
     t0 = time.time()
     for o in range(len(cfg.objects)):
         g.initializeObjectsCmatrix(o)
@@ -226,6 +232,7 @@ def run_gpu(args, world, rank, local):
         host = [torch.from_numpy(r.view(np.uint8)).pin_memory() for r in recs]
         from fopis_b200 import RootGrid
         g2 = RootGrid(cfg, device=local)
+        g2.set_guess_mode(guess_mode(args))
         if Cm is not None:
             g2.set_cmatrix(0, Cm)
         nbytes = sum(h.numel() for h in host)
@@ -264,6 +271,79 @@ def run_gpu(args, world, rank, local):
         g.close()
     result["cmatrix"] = Cm
     return result, cfg
+
+
+def learned_comparison(args, rank, local, Cm):
+    """V-cycles and step time of three Poisson starts at the same tolerance, on
+    contexts with the same seed: `warm` continues from the current phi (the
+    reference), `history` starts each solve from the per-solve history, `learned`
+    adds the network's increment to the history start of the first solve. The
+    learned context trains online on its own first solves for `learned_train`
+    steps (all three step together), then each runs `steps` timed steps with
+    training off."""
+    import torch
+    from fopis_b200 import RootGrid, _abi, config
+
+    def mk():
+        return config.workload(args.workload, ppc=args.ppc, seed=20251203 + 7919 * rank,
+                               sort_interval=args.sort_interval)
+    cfg = mk()
+    names = ("warm", "history", "learned")
+    gs = [RootGrid(mk(), device=local) for _ in names]
+    for g in gs:
+        if Cm is not None:
+            g.set_cmatrix(0, Cm)
+        g.generate_ambient()
+        g.initialize()
+    gs[1].set_guess_mode(_abi.GUESS_HISTORY)
+    gs[2].set_guess_mode(_abi.GUESS_HISTORY)
+    gs[2].unet_training(True, args.learned_lr)
+    loss = []
+    for _ in range(args.learned_train):
+        for g in gs:
+            g.mainLoopES(1)
+        loss.append(gs[2].unet_state()[0])
+    train_ms = gs[2].unet_last()[3]
+    gs[2].unet_training(False)
+    gs[2].set_guess_mode(_abi.GUESS_LEARNED)
+    out = {}
+    for name, g in zip(names, gs):
+        stream = torch.cuda.ExternalStream(g.stream_ptr(), device=torch.device("cuda", local))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        cyc, first, used, ratio, fwd = [], [], [], [], []
+        torch.cuda.synchronize(local)
+        e0.record(stream)
+        for _ in range(args.steps):
+            g.mainLoopES(1)
+            st = g.stats()
+            cyc.append(st.vcycles_step)
+            first.append(st.vcycles_step - (st.vcycles_last if cfg.objects else 0))
+            used.append(st.learned_used)
+            if name == "learned":
+                warm, guess, msf, _ = g.unet_last()
+                fwd.append(msf)
+                if st.learned_used and warm > 0:
+                    ratio.append(guess / warm)
+        e1.record(stream)
+        torch.cuda.synchronize(local)
+        out[name] = dict(ms=e0.elapsed_time(e1) / args.steps, vcycles=float(np.mean(cyc)),
+                         first=float(np.mean(first)), used=int(np.sum(used)), ratio=ratio, fwd=fwd,
+                         V=cfg.norm.unpotential(g.getObject(0)[0]) if cfg.objects else None)
+    pol = gs[2].unet_policy()
+    for g in gs:
+        g.close()
+    w, l = out["warm"], out["learned"]
+    return {"train_steps": args.learned_train, "steps": args.steps, "tolerance": 1e-8,
+            "vcycles_per_step": {k: out[k]["vcycles"] for k in names},
+            "first_solve_vcycles": {k: out[k]["first"] for k in names},
+            "ms_per_step": {k: out[k]["ms"] for k in names},
+            "vcycle_reduction_vs_warm": {k: w["vcycles"] / out[k]["vcycles"] for k in names[1:] if out[k]["vcycles"]},
+            "learned_used_steps": l["used"],
+            "guess_over_history_residual_median": float(np.median(l["ratio"])) if l["ratio"] else None,
+            "ms_network_forward": float(np.mean(l["fwd"])) if l["fwd"] else None, "ms_network_train_step": train_ms,
+            "loss_first_last": [loss[2] if len(loss) > 2 else None, loss[-1] if loss else None],
+            "spacecraft_potential_V": {k: out[k]["V"] for k in names},
+            "policy_history_learned_enabled": list(pol)}
 
 
 def reference_cmatrix(cfg):
@@ -311,6 +391,11 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--profile", action="store_true", help="cudaProfilerStart/Stop around the timed steps")
     ap.add_argument("--phases", action="store_true", help="report the phase times of every timed step")
+    ap.add_argument("--learned-train", type=int, default=200,
+                    help="online training steps before the learned-guess comparison (0: skip it)")
+    ap.add_argument("--learned-lr", type=float, default=1e-3)
+    ap.add_argument("--guess", default="history", choices=["warm", "history"],
+                    help="Poisson start of the timed run: the reference's warm start or the per-solve history")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
@@ -321,7 +406,10 @@ def main():
             "dtype": "fp32 particles, int64 fixed-point rho, fp32 smoother in fp64 refinement",
             "config": {"workload": workload_desc(args.workload, args.ppc),
                        "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (particle state ~3.8 GB)",
-                       "sort_interval": args.sort_interval}}
+                       "sort_interval": args.sort_interval,
+                       "poisson_start": {"warm": "previous phi (the reference's)",
+                                         "history": "per-solve history (first solve from the previous first "
+                                                    "solve, second from it + previous conductor response)"}[args.guess]}}
     if args.impl == "reference":
         if rank != 0:
             return
@@ -365,6 +453,8 @@ def main():
     line["setup_cmatrix_s"] = round(res["t_cmat"], 2)
     if "e2e" in res:
         line["e2e"] = res["e2e"]
+    if args.learned_train > 0 and world == 1:
+        line["learned_guess"] = learned_comparison(args, rank, local, res["cmatrix"])
     if rank == 0 and res["cmatrix"] is not None:
         Cx = reference_cmatrix(cfg)
         line["cmatrix_rel_err_vs_exact"] = float(np.abs(res["cmatrix"] - Cx).max() / np.abs(Cx).max())

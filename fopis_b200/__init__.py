@@ -228,3 +228,53 @@ class RootGrid:
         loss, steps = C.c_double(), C.c_int64()
         self._check(self.lib.fopis_unet_get_state(self.h, C.byref(loss), C.byref(steps)))
         return loss.value, steps.value
+
+    def unet_policy(self):
+        """(history-start V-cycles average, learned V-cycles average, learned guess enabled)."""
+        a, b, on = C.c_double(), C.c_double(), C.c_int()
+        self._check(self.lib.fopis_unet_get_policy(self.h, C.byref(a), C.byref(b), C.byref(on)))
+        return a.value, b.value, bool(on.value)
+
+    def unet_last(self):
+        """(history-start residual, guess residual, forward ms, training ms) of the last first solve."""
+        v = [C.c_double() for _ in range(4)]
+        self._check(self.lib.fopis_unet_get_last(self.h, *[C.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
+    def unet_params(self, new=None):
+        """The FP32 parameter vector; replaced by `new` when given."""
+        n = C.c_int64()
+        self._check(self.lib.fopis_unet_params(self.h, None, None, C.byref(n)))
+        out = np.zeros(n.value, np.float32)
+        src = None
+        if new is not None:
+            src = np.ascontiguousarray(new, np.float32)
+            assert src.size == n.value
+        self._check(self.lib.fopis_unet_params(self.h, out.ctypes.data_as(C.POINTER(C.c_float)),
+                                               None if src is None else src.ctypes.data_as(C.POINTER(C.c_float)),
+                                               C.byref(n)))
+        return out
+
+    def unet_eval(self, rho0, phi1, phi2, phi_target=None, grads=True):
+        """Prediction (glue layout), loss and parameter gradients on caller fields."""
+        f = [np.ascontiguousarray(a, np.float64).ravel() for a in (rho0, phi1, phi2)]
+        tgt = None if phi_target is None else np.ascontiguousarray(phi_target, np.float64).ravel()
+        pred = np.zeros(f[0].size)
+        n = C.c_int64()
+        self._check(self.lib.fopis_unet_params(self.h, None, None, C.byref(n)))
+        g = np.zeros(n.value, np.float32) if (grads and tgt is not None) else None
+        loss = C.c_double()
+        dp = lambda a: None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+        self._check(self.lib.fopis_unet_eval(self.h, dp(f[0]), dp(f[1]), dp(f[2]), dp(tgt), dp(pred),
+                                             None if g is None else g.ctypes.data_as(C.POINTER(C.c_float)),
+                                             C.byref(loss)))
+        return pred.reshape(self.shape), loss.value, g
+
+    def unet_tensor(self, which: int):
+        """An activation / gradient buffer of the last evaluation (unknowns x channels)."""
+        n = C.c_int64()
+        self._check(self.lib.fopis_unet_tensor(self.h, which, None, 0, C.byref(n)))
+        out = np.zeros(n.value, np.float32)
+        self._check(self.lib.fopis_unet_tensor(self.h, which, out.ctypes.data_as(C.POINTER(C.c_float)), n.value,
+                                               C.byref(n)))
+        return out

@@ -37,6 +37,7 @@ FP64 = 1
 GUESS_ZERO = 0
 GUESS_WARM = 1
 GUESS_LEARNED = 2
+GUESS_HISTORY = 3
 
 FIELD_PHI = 0
 FIELD_RHO0 = 1
@@ -158,6 +159,11 @@ SIGNATURES = {
     "fopis_get_stream": (C.c_int, [_VP, C.POINTER(C.c_void_p)]),
     "fopis_unet_set_training": (C.c_int, [_VP, C.c_int, C.c_double]),
     "fopis_unet_get_state": (C.c_int, [_VP, _DP, C.POINTER(C.c_int64)]),
+    "fopis_unet_get_policy": (C.c_int, [_VP, _DP, _DP, C.POINTER(C.c_int)]),
+    "fopis_unet_get_last": (C.c_int, [_VP, _DP, _DP, _DP, _DP]),
+    "fopis_unet_eval": (C.c_int, [_VP, _DP, _DP, _DP, _DP, _DP, C.POINTER(C.c_float), _DP]),
+    "fopis_unet_params": (C.c_int, [_VP, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_int64)]),
+    "fopis_unet_tensor": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_float), C.c_int64, C.POINTER(C.c_int64)]),
     "fopis_parse_obj": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.POINTER(C.c_int32)),
                                   C.POINTER(C.c_int), C.POINTER(C.POINTER(C.c_int32)), C.POINTER(C.c_int)]),
     "fopis_free": (None, [_VP]),

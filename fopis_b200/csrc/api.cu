@@ -10,14 +10,6 @@
 #include <cstring>
 #include <new>
 
-namespace fopis {
-void unet_free(Ctx& c);
-int unet_set_training(Ctx& c, int enable, double lr);
-int unet_get_state(Ctx& c, double* loss, int64_t* steps);
-int unet_predict(Ctx& c);            // writes the guess into phi, 0 when unavailable
-void unet_observe(Ctx& c);           // records a (rho, phi^{n-1}, phi^{n-2}) -> phi^n pair and trains
-}
-
 using namespace fopis;
 
 namespace {
@@ -87,27 +79,68 @@ void step_begin(Ctx& c) {
 double solve_tol(const Ctx& c) { return c.p.poisson_tol > 0 ? c.p.poisson_tol : 1e-8; }
 int solve_cap(const Ctx& c) { return c.p.max_vcycles > 0 ? c.p.max_vcycles : 100; }
 
-// One Poisson solve with the start guess of the context's mode; a solve that
-// fails to converge from the learned guess is redone from the previous phi,
-// and one from the previous phi is redone from zero.
-int solve(Ctx& c, bool first_of_step) {
-    int mode = c.p.guess_mode;
-    if (mode == FOPIS_GUESS_ZERO) FOPIS_CUDA(cudaMemsetAsync(c.phi, 0, sizeof(double) * c.N, c.st));
+// One Poisson solve with the start guess of the context's mode.
+//  WARM     the current phi (the reference's PSOR continues from it).
+//  HISTORY  the first solve of a step (plasma charge only) starts from the
+//           previous step's first solve, the second solve (after the
+//           capacity-matrix redistribution) from the first plus the previous
+//           step's conductor response phi_final - phi_first.
+//  LEARNED  HISTORY with the first solve seeded by the U-Net's increment.
+// Every start converges to the same tolerance. A solve that fails to converge
+// from the learned guess is redone from the history start, and one from a
+// warm start is redone from zero.
+
+// The history becomes usable; on its first valid step phi^{n-2} = phi^{n-1}.
+void history_valid(Ctx& c) {
+    if (!c.hist_ok)
+        FOPIS_CUDA(cudaMemcpyAsync(c.phi_prev2, c.phi_prev, sizeof(double) * c.N, cudaMemcpyDeviceToDevice, c.st));
+    c.hist_ok = true;
+}
+
+int solve(Ctx& c, int kind) {
+    const int mode = c.p.guess_mode;
+    const bool hist = mode == FOPIS_GUESS_HISTORY || mode == FOPIS_GUESS_LEARNED;
+    const bool track = hist || unet_training(c);
+    const bool first = kind != SOLVE_SECOND;
     bool learned = false;
-    if (mode == FOPIS_GUESS_LEARNED && first_of_step) learned = unet_predict(c) != 0;
-    c.learned_used = learned ? 1 : 0;
+    if (first) {
+        if (hist && c.hist_ok)
+            FOPIS_CUDA(cudaMemcpyAsync(c.phi, c.phi_prev, sizeof(double) * c.N, cudaMemcpyDeviceToDevice, c.st));
+        learned = unet_before_solve(c) != 0;
+        c.learned_used = learned ? 1 : 0;
+    } else if (hist && c.hist_ok) {
+        phi_axpy(c, c.phi, c.phi, c.phi_obj, 1.0);
+    }
+    if (mode == FOPIS_GUESS_ZERO) FOPIS_CUDA(cudaMemsetAsync(c.phi, 0, sizeof(double) * c.N, c.st));
     int rc = mg_solve(c, solve_tol(c), solve_cap(c));
+    int cycles = c.last_vcycles;
     if (rc == FOPIS_ERR_NOT_CONVERGED && learned) {
         FOPIS_CUDA(cudaMemcpyAsync(c.phi, c.phi_prev, sizeof(double) * c.N, cudaMemcpyDeviceToDevice, c.st));
         rc = mg_solve(c, solve_tol(c), solve_cap(c));
+        cycles += c.last_vcycles;
         c.learned_used = 0;
     }
     if (rc == FOPIS_ERR_NOT_CONVERGED && mode != FOPIS_GUESS_ZERO) {
         FOPIS_CUDA(cudaMemsetAsync(c.phi, 0, sizeof(double) * c.N, c.st));
         rc = mg_solve(c, solve_tol(c), solve_cap(c));
+        cycles += c.last_vcycles;
     }
+    if (first) {
+        unet_after_solve(c, learned, cycles, rc == FOPIS_OK);
+        if (track) {
+            std::swap(c.phi_prev, c.phi_prev2);
+            FOPIS_CUDA(cudaMemcpyAsync(c.phi_prev, c.phi, sizeof(double) * c.N, cudaMemcpyDeviceToDevice, c.st));
+            if (kind == SOLVE_ONLY) history_valid(c);
+        }
+    } else if (track) {
+        phi_axpy(c, c.phi_obj, c.phi, c.phi_prev, -1.0);
+        history_valid(c);
+    }
+    if (!track) c.hist_ok = false;
     return rc;
 }
+
+int solve_kind_after_rho(const Ctx& c) { return c.objs.empty() ? SOLVE_ONLY : SOLVE_SECOND; }
 
 // RootGrid::updateRho after the per-particle pass: fold and convert, the
 // object charge sums, and with objects the first solve plus the
@@ -118,7 +151,7 @@ int rho_tail(Ctx& c, int* solve_rc) {
     int rc = FOPIS_OK;
     if (!c.objs.empty()) {
         objects_step_end(c);
-        rc = solve(c, true);
+        rc = solve(c, SOLVE_FIRST);
         redistribute(c);
     }
     *solve_rc = rc;
@@ -144,12 +177,10 @@ int one_step(Ctx& c) {
     int rc1 = FOPIS_OK;
     rho_tail(c, &rc1);
     record(c, 5);
-    const bool learned_first = c.objs.empty();
-    int rc2 = solve(c, learned_first);
+    int rc2 = solve(c, solve_kind_after_rho(c));
     record(c, 6);
     efield_update(c);
     record(c, 7);
-    if (c.unet) unet_observe(c);
     const int si = c.p.sort_interval > 0 ? c.p.sort_interval : 8;
     if (c.timestep % si == 0) particles_sort(c);
     record(c, 8);
@@ -224,6 +255,7 @@ int fopis_create(const fopis_params* p, int device, void** out) {
         FOPIS_CUDA(cudaMalloc(&x.phi, sizeof(double) * x.N));
         FOPIS_CUDA(cudaMalloc(&x.phi_prev, sizeof(double) * x.N));
         FOPIS_CUDA(cudaMalloc(&x.phi_prev2, sizeof(double) * x.N));
+        FOPIS_CUDA(cudaMalloc(&x.phi_obj, sizeof(double) * x.N));
         FOPIS_CUDA(cudaMalloc(&x.scratch64, sizeof(double) * x.N));
         FOPIS_CUDA(cudaMalloc(&x.E, sizeof(float4) * x.N));
         FOPIS_CUDA(cudaMalloc(&x.cellmap, x.N));
@@ -238,6 +270,7 @@ int fopis_create(const fopis_params* p, int device, void** out) {
         FOPIS_CUDA(cudaMemset(x.phi, 0, sizeof(double) * x.N));
         FOPIS_CUDA(cudaMemset(x.phi_prev, 0, sizeof(double) * x.N));
         FOPIS_CUDA(cudaMemset(x.phi_prev2, 0, sizeof(double) * x.N));
+        FOPIS_CUDA(cudaMemset(x.phi_obj, 0, sizeof(double) * x.N));
         FOPIS_CUDA(cudaMemset(x.E, 0, sizeof(float4) * x.N));
         FOPIS_CUDA(cudaMemset(x.cellmap, 0, x.N));
         FOPIS_CUDA(cudaMemset(x.node_cmat, 0xff, sizeof(int32_t) * x.N));
@@ -285,7 +318,7 @@ void fopis_destroy(void* h) {
         cudaFree(o.charge_map); cudaFree(o.phis); cudaFree(o.scal); cudaFree(o.lit);
     }
     mg_free(*c);
-    void* ptrs[] = {c->rho_i64, c->rho0, c->phi, c->phi_prev, c->phi_prev2, c->scratch64, c->E, c->cellmap,
+    void* ptrs[] = {c->rho_i64, c->rho0, c->phi, c->phi_prev, c->phi_prev2, c->phi_obj, c->scratch64, c->E, c->cellmap,
                     c->node_cmat, c->sort_count, c->sort_offset, c->scan_partials, c->ab.cell, c->ab.ox,
                     c->ab.oy, c->ab.oz, c->ab.vx, c->ab.vy, c->ab.vz, c->ab.species, c->ab.object, c->d_sc};
     for (void* q : ptrs) if (q) cudaFree(q);
@@ -410,12 +443,11 @@ int fopis_initialize(void* h) {
         FOPIS_CUDA(cudaMemsetAsync(&c.d_sc->absorbed_n, 0, sizeof(unsigned long long), c.st));
         rho_zero(c);
         launch_deposit_all(c);
+        c.hist_ok = false;
         int rc1 = FOPIS_OK;
         rho_tail(c, &rc1);
-        const int rc2 = solve(c, false);
+        const int rc2 = solve(c, solve_kind_after_rho(c));
         efield_update(c);
-        FOPIS_CUDA(cudaMemcpyAsync(c.phi_prev, c.phi, sizeof(double) * c.N, cudaMemcpyDeviceToDevice, c.st));
-        FOPIS_CUDA(cudaMemcpyAsync(c.phi_prev2, c.phi, sizeof(double) * c.N, cudaMemcpyDeviceToDevice, c.st));
         const int rc = check_device(c);
         update_currents(c);
         c.energy_valid = false;
@@ -483,7 +515,7 @@ int fopis_update_rho(void* h) {
 }
 
 int fopis_solve_poisson(void* h) {
-    return guarded(h, [&](Ctx& c) -> int { return solve(c, false); });
+    return guarded(h, [&](Ctx& c) -> int { return solve(c, solve_kind_after_rho(c)); });
 }
 
 int fopis_update_efield(void* h) {
@@ -566,7 +598,7 @@ int fopis_get_stream(void* h, void** stream) {
 
 int fopis_set_guess_mode(void* h, int mode) {
     return guarded(h, [&](Ctx& c) -> int {
-        if (mode < FOPIS_GUESS_ZERO || mode > FOPIS_GUESS_LEARNED) throw ApiError{FOPIS_ERR_ARG, "guess mode"};
+        if (mode < FOPIS_GUESS_ZERO || mode > FOPIS_GUESS_HISTORY) throw ApiError{FOPIS_ERR_ARG, "guess mode"};
         c.p.guess_mode = mode;
         return FOPIS_OK;
     });
@@ -578,6 +610,31 @@ int fopis_unet_set_training(void* h, int enable, double lr) {
 
 int fopis_unet_get_state(void* h, double* loss, int64_t* steps) {
     return guarded(h, [&](Ctx& c) -> int { return unet_get_state(c, loss, steps); });
+}
+
+int fopis_unet_get_policy(void* h, double* plain_vcycles, double* learned_vcycles, int* learned_enabled) {
+    return guarded(h, [&](Ctx& c) -> int { return unet_get_policy(c, plain_vcycles, learned_vcycles, learned_enabled); });
+}
+
+int fopis_unet_get_last(void* h, double* warm_residual, double* guess_residual, double* ms_forward,
+                        double* ms_train) {
+    return guarded(h, [&](Ctx& c) -> int { return unet_get_last(c, warm_residual, guess_residual, ms_forward, ms_train); });
+}
+
+int fopis_unet_eval(void* h, const double* rho0, const double* phi1, const double* phi2, const double* phi_target,
+                    double* pred, float* grads, double* loss) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (!rho0 || !phi1 || !phi2) throw ApiError{FOPIS_ERR_ARG, "null field"};
+        return unet_eval(c, rho0, phi1, phi2, phi_target, pred, grads, loss);
+    });
+}
+
+int fopis_unet_params(void* h, float* get, const float* set, int64_t* count) {
+    return guarded(h, [&](Ctx& c) -> int { return unet_params(c, get, set, count); });
+}
+
+int fopis_unet_tensor(void* h, int which, float* host, int64_t cap, int64_t* count) {
+    return guarded(h, [&](Ctx& c) -> int { return unet_tensor(c, which, host, cap, count); });
 }
 
 void fopis_free(void* p) { std::free(p); }

@@ -2,6 +2,8 @@
 // conditions of phi, nodal electric field, field energy and exports.
 #include "internal.cuh"
 
+#include <algorithm>
+
 namespace fopis {
 
 namespace {
@@ -294,6 +296,20 @@ double efield_energy(Ctx& c) {
     FOPIS_CUDA(cudaMemcpyAsync(&v, &c.d_sc->red[15], sizeof(double), cudaMemcpyDeviceToHost, c.st));
     FOPIS_CUDA(cudaStreamSynchronize(c.st));
     return 0.5 * c.p.eps0 * v;
+}
+
+namespace {
+__global__ void __launch_bounds__(256) axpy_kernel(double* dst, const double* a, const double* b, double sb, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = a[i] + sb * b[i];
+}
+}  // namespace
+
+void phi_axpy(Ctx& c, double* dst, const double* a, const double* b, double sb) {
+    const long long n = (long long)c.N;
+    ++c.launches;
+    axpy_kernel<<<(int)std::min<long long>((n + 255) / 256, 148 * 16), 256, 0, c.st>>>(dst, a, b, sb, n);
+    FOPIS_LAUNCH_CHECK();
 }
 
 }  // namespace fopis

@@ -169,8 +169,9 @@ struct Ctx {
     unsigned long long* rho_i64 = nullptr;  // [nsp][N] two's complement fixed point
     double* rho0 = nullptr;
     double* phi = nullptr;
-    double* phi_prev = nullptr;      // phi^{n-1}
-    double* phi_prev2 = nullptr;     // phi^{n-2}
+    double* phi_prev = nullptr;      // first-solve phi of the previous step
+    double* phi_prev2 = nullptr;     // first-solve phi two steps back
+    double* phi_obj = nullptr;       // previous step's conductor response
     double* scratch64 = nullptr;     // [N] residual / field export
     float4* E = nullptr;             // nodal E (FP32) for the gather
     uint8_t* cellmap = nullptr;      // [N] object id + 1 of the node cell, 0 outside
@@ -209,6 +210,8 @@ struct Ctx {
     cudaEvent_t ev[9] = {nullptr};
     std::string err;
     int64_t launches = 0;            // kernels launched by this context
+    // solve history valid (phi_prev, phi_prev2, phi_obj)
+    bool hist_ok = false;
     // learned guess (allocated on demand)
     void* unet = nullptr;
 };
@@ -237,6 +240,7 @@ void efield_update(Ctx& c);
 void field_export(Ctx& c, int which, double* host);
 double efield_energy(Ctx& c);
 void phi_boundary(Ctx& c);
+void phi_axpy(Ctx& c, double* dst, const double* a, const double* b, double sb);   // dst = a + sb * b over all nodes
 void glue_copy(Ctx& c, double* a);
 // multigrid.cu
 void mg_setup(Ctx& c);
@@ -249,5 +253,19 @@ void cmatrix_set(Ctx& c, int id, const double* hostC);
 void redistribute(Ctx& c);
 void objects_step_begin(Ctx& c);
 void objects_step_end(Ctx& c);
+// unet.cu (learned initial guess)
+enum SolveKind { SOLVE_ONLY = 0, SOLVE_FIRST = 1, SOLVE_SECOND = 2 };
+void unet_free(Ctx& c);
+int unet_set_training(Ctx& c, int enable, double lr);
+int unet_get_state(Ctx& c, double* loss, int64_t* steps);
+int unet_get_policy(Ctx& c, double* plain, double* learned, int* active);
+int unet_get_last(Ctx& c, double* warm_res, double* guess_res, double* ms_forward, double* ms_train);
+bool unet_training(const Ctx& c);
+int unet_before_solve(Ctx& c);       // 1 when phi keeps the learned guess
+void unet_after_solve(Ctx& c, bool used, int cycles, bool converged);
+int unet_eval(Ctx& c, const double* rho0, const double* phi1, const double* phi2, const double* phi_target,
+              double* pred, float* grads, double* loss);
+int unet_params(Ctx& c, float* get, const float* set, int64_t* count);
+int unet_tensor(Ctx& c, int which, float* host, int64_t cap, int64_t* count);
 
 }  // namespace fopis

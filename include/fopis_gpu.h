@@ -90,7 +90,11 @@ typedef enum fopis_precision {
 typedef enum fopis_guess_mode {
     FOPIS_GUESS_ZERO = 0,      /* every solve starts from phi = 0 */
     FOPIS_GUESS_WARM = 1,      /* start from the previous phi (the reference's behaviour) */
-    FOPIS_GUESS_LEARNED = 2    /* previous phi + U-Net predicted increment, with fallback */
+    FOPIS_GUESS_LEARNED = 2,   /* FOPIS_GUESS_HISTORY with the first solve seeded by the U-Net's
+                                  predicted increment, with fallback */
+    FOPIS_GUESS_HISTORY = 3    /* per-solve history: the first solve of a step starts from the
+                                  previous step's first solve, the second from the first plus
+                                  the previous step's conductor response */
 } fopis_guess_mode;
 
 /* Simulation parameters: the normalised content of input.json after
@@ -250,6 +254,36 @@ int fopis_set_guess_mode(void* ctx, int mode);
 int fopis_unet_set_training(void* ctx, int enable, double learning_rate);
 /* Loss of the last training step and number of steps taken. */
 int fopis_unet_get_state(void* ctx, double* last_loss, int64_t* train_steps);
+/* The fallback policy of FOPIS_GUESS_LEARNED: running averages of the first
+ * solve's V-cycles from the history start and from the learned guess, and
+ * whether the learned guess is currently enabled (0 while falling back). */
+int fopis_unet_get_policy(void* ctx, double* plain_vcycles, double* learned_vcycles, int* learned_enabled);
+/* The last first solve: initial residual ||f - A phi||/||f|| from the history
+ * start and from the learned guess (equal when the guess was not used), and
+ * the device time of the network's forward pass (with the guess check) and of
+ * its training step, in milliseconds. A guess that does not lower the initial
+ * residual is discarded for that solve. */
+int fopis_unet_get_last(void* ctx, double* warm_residual, double* guess_residual, double* ms_forward,
+                        double* ms_train);
+/* The network on caller fields (host arrays of N glue-layout nodes): features
+ * of rho0, phi^{n-1}, phi^{n-2}; pred (optional) receives the predicted
+ * increment phi^n - phi^{n-1} on the solver's unknowns (0 elsewhere). With
+ * phi_target the loss mean((out - (phi_target - phi1)/sigma)^2) goes to loss
+ * and, when grads is given, its gradient for every parameter
+ * (fopis_unet_params order); no optimiser step is taken. */
+int fopis_unet_eval(void* ctx, const double* rho0, const double* phi1, const double* phi2,
+                    const double* phi_target, double* pred, float* grads, double* loss);
+/* FP32 master parameters: copied to get and/or replaced from set (either may be
+ * null); *count receives their number. Order per convolution l = 0..5:
+ * W[27][cout][cin] (tap = (di+1)*9 + (dj+1)*3 + (dk+1)), b[cout]; then the
+ * head w[16], b. Convolutions (cin, cout, level): (16,16,0) (16,32,1) (32,64,2)
+ * (64,64,2) (64,32,1) (32,16,0). */
+int fopis_unet_params(void* ctx, float* get, const float* set, int64_t* count);
+/* One activation or gradient buffer of the last evaluation as FP32, solver
+ * unknown order with channels last (index: x0 e0 d1 e1 d2 e2 e3 u1 a4 u0 a5
+ * g5 du0 da1 g4 du1 de3 g3 g2 dd2 g1 dd1 g0 ge0, then 24 = prediction).
+ * With host null only *count (values) is set. */
+int fopis_unet_tensor(void* ctx, int which, float* host, int64_t cap, int64_t* count);
 
 /* ---- allocation-free variant (no reference counterpart) ------------------ */
 
