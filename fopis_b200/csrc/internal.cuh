@@ -187,6 +187,13 @@ struct Ctx {
     double* coarse64 = nullptr;
     cudaGraph_t mg_graph = nullptr;  // one refinement iteration, recorded once
     cudaGraphExec_t mg_exec = nullptr;
+    // the whole solve as one graph with a device-side while loop over refinement
+    // iterations (state: 0 not built, 1 built, -1 unavailable -> host loop)
+    cudaGraph_t solve_graph = nullptr;
+    cudaGraphExec_t solve_exec = nullptr;
+    cudaStream_t body_st = nullptr;
+    int solve_state = 0;
+    int64_t solve_pre_launches = 0, solve_post_launches = 0;
     int64_t cycle_launches = 0;      // kernels in that graph
     int mg_cta_start = -1;           // first level whose V-cycle runs inside one CTA
     double* red_partials = nullptr;  // block partial sums

@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 namespace fopis {
 
@@ -295,26 +296,46 @@ __device__ __forceinline__ T sm_nsum(const SmLv& L, const T* u, int a, int b, in
     return s;
 }
 
+// Runs body(t, a, b, c) for every element t = (a*n1 + b)*n2 + c of level L.
+// Each thread keeps one (b, c) column and walks a, so the index arithmetic
+// costs two divisions per thread per pass instead of three per element.
+template <typename Body>
+__device__ __forceinline__ void sm_for_each(const SmLv& L, Body body) {
+    const int n12 = L.n1 * L.n2;
+    const int bd = blockDim.x, t = threadIdx.x;
+    if (n12 >= bd) {
+        for (int q = t; q < n12; q += bd) {
+            const int b = q / L.n2, c = q - b * L.n2;
+            for (int a = 0; a < L.n0; ++a) body(a * n12 + q, a, b, c);
+        }
+    } else {
+        const int astep = bd / n12;
+        if (t < astep * n12) {
+            const int a0 = t / n12, q = t - a0 * n12;
+            const int b = q / L.n2, c = q - b * L.n2;
+            for (int a = a0; a < L.n0; a += astep) body(a * n12 + q, a, b, c);
+        }
+    }
+}
+
 // `sweeps` red-black (or weighted Jacobi) sweeps: u <- (sum(nb) + f/scale) / 6.
 template <typename T>
 __device__ void sm_smooth(const SmLv& L, T* u, const T* f, T* tmp, int sweeps, T inv_scale) {
-    const int M = sm_size(L);
     for (int sw = 0; sw < sweeps; ++sw) {
         if (L.rb) {
             for (int color = 0; color < 2; ++color) {
-                for (int t = threadIdx.x; t < M; t += blockDim.x) {
-                    const int a = t / (L.n1 * L.n2), b = (t / L.n2) % L.n1, c = t % L.n2;
-                    if (((a + b + c) & 1) != color) continue;
+                sm_for_each(L, [&](int t, int a, int b, int c) {
+                    if (((a + b + c) & 1) != color) return;
                     u[t] = (sm_nsum(L, u, a, b, c) + f[t] * inv_scale) * (T)(1.0 / 6.0);
-                }
+                });
                 __syncthreads();
             }
         } else {
-            for (int t = threadIdx.x; t < M; t += blockDim.x) {
-                const int a = t / (L.n1 * L.n2), b = (t / L.n2) % L.n1, c = t % L.n2;
+            sm_for_each(L, [&](int t, int a, int b, int c) {
                 tmp[t] = (T)0.2 * u[t] + (T)0.8 * (sm_nsum(L, u, a, b, c) + f[t] * inv_scale) * (T)(1.0 / 6.0);
-            }
+            });
             __syncthreads();
+            const int M = sm_size(L);
             for (int t = threadIdx.x; t < M; t += blockDim.x) u[t] = tmp[t];
             __syncthreads();
         }
@@ -353,15 +374,15 @@ __global__ void coarse_cycle_kernel(CoarseCycle d) {
         for (int t = threadIdx.x; t < M; t += blockDim.x) U(l)[t] = 0.0f;
         __syncthreads();
         sm_smooth<float>(L, U(l), F(l), R(l), 2, L.inv_scale);
-        for (int t = threadIdx.x; t < M; t += blockDim.x) {
-            const int a = t / (L.n1 * L.n2), b = (t / L.n2) % L.n1, c = t % L.n2;
-            R(l)[t] = F(l)[t] - (6.0f * U(l)[t] - sm_nsum(L, U(l), a, b, c)) / L.inv_scale;
-        }
+        float* ul = U(l);
+        float* fl = F(l);
+        float* rl = R(l);
+        float* fc_ = F(l + 1);
+        const float scale = 1.0f / L.inv_scale;
+        sm_for_each(L, [&](int t, int a, int b, int c) { rl[t] = fl[t] - (6.0f * ul[t] - sm_nsum(L, ul, a, b, c)) * scale; });
         __syncthreads();
-        const int MC = sm_size(C);
         const float w[3] = {0.25f, 0.5f, 0.25f};
-        for (int t = threadIdx.x; t < MC; t += blockDim.x) {
-            const int A = t / (C.n1 * C.n2), B = (t / C.n2) % C.n1, Cc = t % C.n2;
+        sm_for_each(C, [&](int t, int A, int B, int Cc) {
             const int fa = fine_of(A, L.p0), fb = fine_of(B, L.p1), fc = fine_of(Cc, L.p2);
             float s = 0.0f;
             for (int da = -1; da <= 1; ++da) {
@@ -373,12 +394,12 @@ __global__ void coarse_cycle_kernel(CoarseCycle d) {
                     for (int dc = -1; dc <= 1; ++dc) {
                         const int c = wrap_or_out(fc + dc, L.n2, L.p2);
                         if (c < 0) continue;
-                        s += w[da + 1] * w[db + 1] * w[dc + 1] * R(l)[(a * L.n1 + b) * L.n2 + c];
+                        s += w[da + 1] * w[db + 1] * w[dc + 1] * rl[(a * L.n1 + b) * L.n2 + c];
                     }
                 }
             }
-            F(l + 1)[t] = s;
-        }
+            fc_[t] = s;
+        });
         __syncthreads();
     }
     {   // coarsest level in FP64
@@ -399,9 +420,9 @@ __global__ void coarse_cycle_kernel(CoarseCycle d) {
     for (int l = d.nl - 2; l >= 0; --l) {
         const SmLv& Fl = d.lv[l];
         const SmLv& C = d.lv[l + 1];
-        const int M = sm_size(Fl);
-        for (int t = threadIdx.x; t < M; t += blockDim.x) {
-            const int a = t / (Fl.n1 * Fl.n2), b = (t / Fl.n2) % Fl.n1, c = t % Fl.n2;
+        float* uf = U(l);
+        const float* uc = U(l + 1);
+        sm_for_each(Fl, [&](int t, int a, int b, int c) {
             int Ia[2], Ib[2], Ic[2];
             float wa[2], wb[2], wc[2];
             const int na = coarse_src(a, Fl.p0, C.n0, Ia, wa), nbv = coarse_src(b, Fl.p1, C.n1, Ib, wb),
@@ -409,9 +430,9 @@ __global__ void coarse_cycle_kernel(CoarseCycle d) {
             float s = 0.0f;
             for (int x = 0; x < na; ++x)
                 for (int y = 0; y < nbv; ++y)
-                    for (int z = 0; z < nc; ++z) s += wa[x] * wb[y] * wc[z] * U(l + 1)[(Ia[x] * C.n1 + Ib[y]) * C.n2 + Ic[z]];
-            U(l)[t] += s;
-        }
+                    for (int z = 0; z < nc; ++z) s += wa[x] * wb[y] * wc[z] * uc[(Ia[x] * C.n1 + Ib[y]) * C.n2 + Ic[z]];
+            uf[t] += s;
+        });
         __syncthreads();
         sm_smooth<float>(Fl, U(l), F(l), R(l), 2, Fl.inv_scale);
     }
@@ -726,6 +747,10 @@ void mg_setup(Ctx& c) {
 void mg_free(Ctx& c) {
     if (c.mg_exec) { cudaGraphExecDestroy(c.mg_exec); c.mg_exec = nullptr; }
     if (c.mg_graph) { cudaGraphDestroy(c.mg_graph); c.mg_graph = nullptr; }
+    if (c.solve_exec) { cudaGraphExecDestroy(c.solve_exec); c.solve_exec = nullptr; }
+    if (c.solve_graph) { cudaGraphDestroy(c.solve_graph); c.solve_graph = nullptr; }
+    if (c.body_st) { cudaStreamDestroy(c.body_st); c.body_st = nullptr; }
+    c.solve_state = 0;
     for (auto& l : c.mg) { cudaFree(l.u); cudaFree(l.f); cudaFree(l.r); }
     c.mg.clear();
     if (c.red_partials) { cudaFree(c.red_partials); c.red_partials = nullptr; }
@@ -762,7 +787,138 @@ static void ensure_cycle_graph(Ctx& c) {
     c.launches = before;
 }
 
-int mg_solve(Ctx& c, double tol, int max_cycles) {
+namespace {
+
+// Scalar slots of DevScalars::red used by the solve: [0] sum f, [1] sum f^2,
+// [2] ||r||^2, [3] sum phi, [4] mean f (all-periodic), [5] ||f||, [6] tolerance,
+// [7] V-cycle cap, [8] V-cycles done, [9] initial ||r||.
+__global__ void solve_prep_kernel(DevScalars* sc, double M, int allper) {
+    const double fsum = sc->red[0], fsq = sc->red[1];
+    sc->red[4] = allper ? fsum / M : 0.0;
+    const double fn = sqrt(fmax(0.0, fsq - (allper ? fsum * fsum / M : 0.0)));
+    sc->red[5] = fn > 0.0 ? fn : 1.0;
+}
+// Loop condition: residual above tolerance, cap not reached, residual finite.
+__global__ void solve_init_kernel(DevScalars* sc, cudaGraphConditionalHandle h) {
+    const double res = sqrt(sc->red[2]);
+    sc->red[9] = res;
+    sc->red[8] = 0.0;
+    const bool go = isfinite(res) && res > sc->red[6] * sc->red[5] && sc->red[7] > 0.0;
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+__global__ void solve_decide_kernel(DevScalars* sc, cudaGraphConditionalHandle h) {
+    const double n = sc->red[8] + 1.0;
+    sc->red[8] = n;
+    const double res = sqrt(sc->red[2]);
+    const bool go = isfinite(res) && res > sc->red[6] * sc->red[5] && n < sc->red[7];
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+// Records the whole solve once per context: norms of f, initial residual, a
+// device-side while loop whose body is one refinement iteration (V-cycle,
+// FP64 correction, FP64 residual) plus the convergence test, the mean shift
+// of an all-periodic problem and one copy of the scalars to pinned memory.
+// The host then waits once per solve instead of once per V-cycle.
+void build_solve_graph(Ctx& c) {
+    Outer O = make_outer(c);
+    const bool allper = O.p0 && O.p1 && O.p2;
+    const long long M = (long long)O.n0 * O.n1 * O.n2;
+    if (!c.body_st) FOPIS_CUDA(cudaStreamCreateWithFlags(&c.body_st, cudaStreamNonBlocking));
+    cudaStream_t main_st = c.st;
+    const int64_t before = c.launches;
+    int64_t pre = 0, body = 0;
+    bool capturing = false, body_capturing = false;
+    try {
+        FOPIS_CUDA(cudaStreamBeginCapture(main_st, cudaStreamCaptureModeThreadLocal));
+        capturing = true;
+        FOPIS_CUDA(cudaMemcpyAsync(&c.d_sc->red[6], &c.h_sc->red[6], 2 * sizeof(double), cudaMemcpyHostToDevice,
+                                   main_st));
+        ++c.launches;
+        fstats_kernel<<<kRedBlocks, kT, 0, main_st>>>(O, c.rho0, c.red_partials);
+        ++c.launches;
+        reduce_partials_kernel<<<1, 1024, 0, main_st>>>(c.red_partials, kRedBlocks, 2, 0, &c.d_sc->red[0]);
+        ++c.launches;
+        reduce_partials_kernel<<<1, 1024, 0, main_st>>>(c.red_partials, kRedBlocks, 2, 1, &c.d_sc->red[1]);
+        ++c.launches;
+        solve_prep_kernel<<<1, 1, 0, main_st>>>(c.d_sc, (double)M, allper ? 1 : 0);
+        ++c.launches;
+        outer_residual_kernel<<<kRedBlocks, kT, 0, main_st>>>(O, c.rho0, c.phi, c.mg[0].f, c.red_partials);
+        ++c.launches;
+        reduce_partials_kernel<<<1, 1024, 0, main_st>>>(c.red_partials, kRedBlocks, 1, 0, &c.d_sc->red[2]);
+        FOPIS_LAUNCH_CHECK();
+        cudaStreamCaptureStatus status;
+        cudaGraph_t graph = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        FOPIS_CUDA(cudaStreamGetCaptureInfo(main_st, &status, nullptr, &graph, &deps, &ndeps));
+        cudaGraphConditionalHandle handle;
+        FOPIS_CUDA(cudaGraphConditionalHandleCreate(&handle, graph, 0, 0));
+        ++c.launches;
+        solve_init_kernel<<<1, 1, 0, main_st>>>(c.d_sc, handle);
+        FOPIS_LAUNCH_CHECK();
+        FOPIS_CUDA(cudaStreamGetCaptureInfo(main_st, &status, nullptr, &graph, &deps, &ndeps));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t loop;
+        FOPIS_CUDA(cudaGraphAddNode(&loop, graph, deps, ndeps, &cp));
+        FOPIS_CUDA(cudaStreamUpdateCaptureDependencies(main_st, &loop, 1, cudaStreamSetCaptureDependencies));
+        pre = c.launches - before;
+        // loop body, recorded through the second stream into the node's graph
+        FOPIS_CUDA(cudaStreamBeginCaptureToGraph(c.body_st, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                 cudaStreamCaptureModeThreadLocal));
+        body_capturing = true;
+        c.st = c.body_st;
+        const int64_t b0 = c.launches;
+        vcycle(c, 0);
+        ++c.launches;
+        correct_kernel<<<row_blocks((long long)O.n0 * O.n1), kT, 0, c.st>>>(O, c.phi, c.mg[0].u);
+        ++c.launches;
+        outer_residual_kernel<<<kRedBlocks, kT, 0, c.st>>>(O, c.rho0, c.phi, c.mg[0].f, c.red_partials);
+        ++c.launches;
+        reduce_partials_kernel<<<1, 1024, 0, c.st>>>(c.red_partials, kRedBlocks, 1, 0, &c.d_sc->red[2]);
+        ++c.launches;
+        solve_decide_kernel<<<1, 1, 0, c.st>>>(c.d_sc, handle);
+        FOPIS_LAUNCH_CHECK();
+        body = c.launches - b0;
+        c.st = main_st;
+        cudaGraph_t body_graph = nullptr;
+        body_capturing = false;
+        FOPIS_CUDA(cudaStreamEndCapture(c.body_st, &body_graph));
+        const int64_t p0 = c.launches;
+        if (allper) {
+            ++c.launches;
+            phi_mean_kernel<<<kRedBlocks, kT, 0, main_st>>>(O, c.phi, c.red_partials);
+            ++c.launches;
+            reduce_partials_kernel<<<1, 1024, 0, main_st>>>(c.red_partials, kRedBlocks, 1, 0, &c.d_sc->red[3]);
+            ++c.launches;
+            phi_shift_kernel<<<row_blocks((long long)O.n0 * O.n1), kT, 0, main_st>>>(O, c.phi, &c.d_sc->red[3]);
+            FOPIS_LAUNCH_CHECK();
+        }
+        FOPIS_CUDA(cudaMemcpyAsync(c.h_sc->red, c.d_sc->red, 16 * sizeof(double), cudaMemcpyDeviceToHost, main_st));
+        c.solve_post_launches = c.launches - p0;
+        capturing = false;
+        FOPIS_CUDA(cudaStreamEndCapture(main_st, &c.solve_graph));
+        FOPIS_CUDA(cudaGraphInstantiate(&c.solve_exec, c.solve_graph, 0));
+    } catch (...) {
+        c.st = main_st;
+        if (body_capturing) { cudaGraph_t g = nullptr; cudaStreamEndCapture(c.body_st, &g); }
+        if (capturing) { cudaGraph_t g = nullptr; cudaStreamEndCapture(main_st, &g); if (g) cudaGraphDestroy(g); }
+        if (c.solve_graph) { cudaGraphDestroy(c.solve_graph); c.solve_graph = nullptr; }
+        cudaGetLastError();
+        c.launches = before;
+        throw;
+    }
+    c.solve_pre_launches = pre;
+    c.cycle_launches = body;
+    c.launches = before;
+}
+
+// The solve with the host waiting once per V-cycle (used when the device-side
+// loop cannot be built).
+void mg_solve_host_loop(Ctx& c, double tol, int max_cycles, double* res_out, double* fnorm_out, int* cycles_out) {
     ensure_cycle_graph(c);
     Outer O = make_outer(c);
     const bool allper = O.p0 && O.p1 && O.p2;
@@ -805,6 +961,43 @@ int mg_solve(Ctx& c, double tol, int max_cycles) {
         ++c.launches;
         phi_shift_kernel<<<row_blocks((long long)O.n0 * O.n1), kT, 0, c.st>>>(O, c.phi, &c.d_sc->red[3]);
         FOPIS_LAUNCH_CHECK();
+    }
+    *res_out = res;
+    *fnorm_out = fnorm;
+    *cycles_out = cycles;
+}
+
+}  // namespace
+
+int mg_solve(Ctx& c, double tol, int max_cycles) {
+    if (c.solve_state == 0) {
+        // FOPIS_SOLVE_HOST_LOOP=1 keeps the host-driven loop (same kernels and
+        // results) for profilers that do not trace conditional graph bodies
+        const char* env = std::getenv("FOPIS_SOLVE_HOST_LOOP");
+        if (env && env[0] == '1') c.solve_state = -1;
+    }
+    if (c.solve_state == 0) {
+        try {
+            build_solve_graph(c);
+            c.solve_state = 1;
+        } catch (const CudaError&) {
+            c.solve_state = -1;
+        }
+    }
+    double res = 0.0, fnorm = 1.0;
+    int cycles = 0;
+    if (c.solve_state == 1) {
+        c.h_sc->red[6] = tol;
+        c.h_sc->red[7] = (double)max_cycles;
+        FOPIS_CUDA(cudaGraphLaunch(c.solve_exec, c.st));
+        FOPIS_CUDA(cudaStreamSynchronize(c.st));
+        fnorm = c.h_sc->red[5];
+        res = std::sqrt(c.h_sc->red[2]);
+        cycles = (int)c.h_sc->red[8];
+        c.first_res = c.h_sc->red[9] / fnorm;
+        c.launches += c.solve_pre_launches + (int64_t)cycles * c.cycle_launches + c.solve_post_launches;
+    } else {
+        mg_solve_host_loop(c, tol, max_cycles, &res, &fnorm, &cycles);
     }
     phi_boundary(c);
     c.last_vcycles = cycles;
