@@ -975,26 +975,79 @@ __global__ void brick_start_kernel(const int32_t* offset, int nbricks, int32_t* 
         brick_start[b] = offset[(long long)b * kBrickCells];
 }
 
-__global__ void sort_scatter_kernel(Soa src, Soa dst, long long cap, const unsigned long long* count, Grid g,
-                                    int32_t* cursor) {
+// Scatter of a nearly sorted particle set: a CTA takes a contiguous chunk,
+// finds the runs of equal keys in it (the previous sort leaves them long),
+// reserves each run's slots with one atomic on its key's cursor and copies
+// the run to consecutive slots, so loads and stores stay coalesced and the
+// atomics of a chunk are issued together.
+constexpr int kSortThreads = 256, kSortItems = 8, kSortChunk = kSortThreads * kSortItems;
+
+__global__ void __launch_bounds__(kSortThreads) sort_scatter_chunk_kernel(Soa src, Soa dst, long long cap,
+                                                                          const unsigned long long* count, Grid g,
+                                                                          int32_t* cursor) {
+    __shared__ int32_t s_key[kSortChunk];
+    __shared__ int32_t s_start[kSortChunk];   // first index of the run an entry belongs to
+    __shared__ int32_t s_base[kSortChunk];    // destination of a run's first entry (at its start index)
+    __shared__ int32_t s_wmax[kSortThreads / 32];
     const long long n = (long long)min(*count, (unsigned long long)cap);
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    const int lane = threadIdx.x & 31;
-    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
-        const long long t = base + lane;
-        const int32_t c = t < n ? src.cell[t] : -1;
-        long long key = -1 - lane;
-        if (c >= 0) { int i, j, k; unpack_cell(c, i, j, k); key = brick_key(g, i, j, k); }
-        const unsigned grp = __match_any_sync(kFull, key);
-        const int leader = __ffs(grp) - 1;
-        int b = 0;
-        if (c >= 0 && leader == lane) b = atomicAdd(cursor + key, __popc(grp));
-        b = __shfl_sync(kFull, b, leader);
-        if (c < 0) continue;
-        const long long d = (long long)b + __popc(grp & ((1u << lane) - 1u));
-        dst.cell[d] = c;
-        dst.ox[d] = src.ox[t]; dst.oy[d] = src.oy[t]; dst.oz[d] = src.oz[t];
-        dst.vx[d] = src.vx[t]; dst.vy[d] = src.vy[t]; dst.vz[d] = src.vz[t];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (long long c0 = (long long)blockIdx.x * kSortChunk; c0 < n; c0 += (long long)gridDim.x * kSortChunk) {
+        for (int q = tid; q < kSortChunk; q += kSortThreads) {
+            const long long t = c0 + q;
+            int key = -1;
+            if (t < n) {
+                const int32_t c = src.cell[t];
+                if (c >= 0) { int i, j, k; unpack_cell(c, i, j, k); key = (int)brick_key(g, i, j, k); }
+            }
+            s_key[q] = key;
+        }
+        __syncthreads();
+        // start index of each entry's run: inclusive max-scan of (run start ? q : -1);
+        // thread tid owns entries tid*kSortItems .. +kSortItems-1
+        int m = -1;
+        int loc[kSortItems];
+#pragma unroll
+        for (int e = 0; e < kSortItems; ++e) {
+            const int q = tid * kSortItems + e;
+            const int key = s_key[q];
+            const bool start = key >= 0 && (q == 0 || s_key[q - 1] != key);
+            if (start) m = q;
+            loc[e] = m;
+        }
+        int x = m;
+        for (int o = 1; o < 32; o <<= 1) { const int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x = max(x, y); }
+        if (lane == 31) s_wmax[warp] = x;
+        const int up = __shfl_up_sync(0xffffffffu, x, 1);
+        __syncthreads();
+        int carry = lane > 0 ? up : -1;                  // latest start among earlier lanes of the warp
+        for (int w = 0; w < warp; ++w) carry = max(carry, s_wmax[w]);
+#pragma unroll
+        for (int e = 0; e < kSortItems; ++e) {
+            const int q = tid * kSortItems + e;
+            s_start[q] = max(carry, loc[e]);
+        }
+        __syncthreads();
+        // the last entry of each run reserves the run's slots
+#pragma unroll
+        for (int e = 0; e < kSortItems; ++e) {
+            const int q = tid * kSortItems + e;
+            const int key = s_key[q];
+            if (key < 0) continue;
+            if (q + 1 < kSortChunk && s_key[q + 1] == key) continue;
+            const int st = s_start[q];
+            s_base[st] = atomicAdd(cursor + key, q - st + 1);
+        }
+        __syncthreads();
+        for (int q = tid; q < kSortChunk; q += kSortThreads) {
+            if (s_key[q] < 0) continue;
+            const int st = s_start[q];
+            const long long d = (long long)s_base[st] + (q - st);
+            const long long t = c0 + q;
+            dst.cell[d] = src.cell[t];
+            dst.ox[d] = src.ox[t]; dst.oy[d] = src.oy[t]; dst.oz[d] = src.oz[t];
+            dst.vx[d] = src.vx[t]; dst.vy[d] = src.vy[t]; dst.vz[d] = src.vz[t];
+        }
+        __syncthreads();
     }
 }
 
@@ -1194,8 +1247,12 @@ void particles_sort(Ctx& c) {
         brick_start_kernel<<<(nbricks + 256) / 256, 256, 0, c.st>>>(c.sort_offset, nbricks, c.brick_start[s]);
         FOPIS_LAUNCH_CHECK();
         ++c.launches;
-        sort_scatter_kernel<<<grid_for(std::max<int64_t>(c.nslots[s], 1)), kThreads, 0, c.st>>>(
-            c.sp[s], c.sp2[s], c.cap[s], &c.d_sc->count[s], g, c.sort_offset);
+        {
+            const long long chunks = (std::max<int64_t>(c.nslots[s], 1) + kSortChunk - 1) / kSortChunk;
+            const int grid = (int)std::max<long long>(1, std::min<long long>(chunks, 148LL * 8));
+            sort_scatter_chunk_kernel<<<grid, kSortThreads, 0, c.st>>>(c.sp[s], c.sp2[s], c.cap[s], &c.d_sc->count[s], g,
+                                                                      c.sort_offset);
+        }
         FOPIS_LAUNCH_CHECK();
         // the new count is the total of valid particles: the scan's grand total
         FOPIS_CUDA(cudaMemcpyAsync(&c.d_sc->count[s], c.scan_partials + tiles, sizeof(int32_t), cudaMemcpyDeviceToDevice, c.st));
