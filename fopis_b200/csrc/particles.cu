@@ -472,9 +472,12 @@ struct SourceArgs {
 };
 
 // Finishes a newly created particle: in the fused step it is moved (emission
-// only), checked against the bodies and deposited; it is then appended.
+// only), checked against the bodies and deposited; it is then appended. Every
+// active lane of the warp calls it: slots are reserved with one atomic per
+// species per warp, and the kinetic energy goes to the block's accumulator
+// s_energy (flushed once per block by the caller).
 __device__ void finish_source(const SourceArgs& a, int s, double x, double y, double z, double vx, double vy,
-                              double vz, bool move, bool want) {
+                              double vz, bool move, bool want, double* s_energy) {
     bool live = want;
     int i = 0, j = 0, k = 0;
     float ox = 0.f, oy = 0.f, oz = 0.f;
@@ -501,8 +504,7 @@ __device__ void finish_source(const SourceArgs& a, int s, double x, double y, do
         }
         live = false;
     }
-    if (!live) return;
-    if (a.fused) {
+    if (live && a.fused) {
         unsigned long long w[8];
         corner_weights(ox, oy, oz, w);
         unsigned long long* rho = a.rho + (long long)s * a.N;
@@ -510,11 +512,28 @@ __device__ void finish_source(const SourceArgs& a, int s, double x, double y, do
 #pragma unroll
         for (int t = 0; t < 8; ++t) if (w[t]) atomicAdd(rho + b + corner_offset(a.g, t), w[t]);
         const float fx = (float)vx, fy = (float)vy, fz = (float)vz;
-        atomicAdd(&a.sc->energy[s], (double)fx * fx + (double)fy * fy + (double)fz * fz);
+        atomicAdd(&s_energy[s], (double)fx * fx + (double)fy * fy + (double)fz * fz);
     }
-    const unsigned long long slot = atomicAdd(&a.sc->count[s], 1ull);
+    const unsigned act = __activemask();
+    const unsigned grp = __match_any_sync(act, live ? s : -1);
+    if (!live) return;
+    const int lane = threadIdx.x & 31, leader = __ffs(grp) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(&a.sc->count[s], (unsigned long long)__popc(grp));
+    base = __shfl_sync(grp, base, leader);
+    const unsigned long long slot = base + __popc(grp & ((1u << lane) - 1u));
     if ((long long)slot < a.cap[s]) store_split(a.p[s], (long long)slot, i, j, k, ox, oy, oz, vx, vy, vz);
     else atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_PARTICLE_OVERFLOW);
+}
+
+__device__ __forceinline__ void energy_init(double* s_energy) {
+    for (int t = threadIdx.x; t < FOPIS_MAX_SPECIES; t += blockDim.x) s_energy[t] = 0.0;
+    __syncthreads();
+}
+__device__ __forceinline__ void energy_flush(const SourceArgs& a, const double* s_energy) {
+    __syncthreads();
+    for (int t = threadIdx.x; t < FOPIS_MAX_SPECIES; t += blockDim.x)
+        if (s_energy[t] != 0.0) atomicAdd(&a.sc->energy[t], s_energy[t]);
 }
 
 // ------------------------------------------------------------------ injection
@@ -534,6 +553,8 @@ struct InjectTable {
 // and generateNewParticle with the slab ranges of
 // RootGrid::injectParticlesFromBoundary (RootGridParticle.cpp:212-302).
 __global__ void inject_kernel(SourceArgs a, InjectTable tb) {
+    __shared__ double s_energy[FOPIS_MAX_SPECIES];
+    energy_init(s_energy);
     const long long total = tb.start[tb.n];
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
         int b = 0;
@@ -565,8 +586,9 @@ __global__ void inject_kernel(SourceArgs a, InjectTable tb) {
         double x[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) x[c] = lo[c] + (hi[c] - lo[c]) * u[c];
-        finish_source(a, s, x[0], x[1], x[2], v[0], v[1], v[2], false, true);
+        finish_source(a, s, x[0], x[1], x[2], v[0], v[1], v[2], false, true, s_energy);
     }
+    energy_flush(a, s_energy);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.sc->injected, (unsigned long long)total);
 }
 
@@ -628,6 +650,8 @@ __device__ bool surface_charge(const Grid& g, const int32_t* node_cmat, int obj,
 // its charge taken off the surface at its next crossing point
 // (Spacecraft::emitParticles, Spacecraft.cpp:882-899).
 __global__ void emit_kernel(SourceArgs a, EmitArgs e) {
+    __shared__ double s_energy[FOPIS_MAX_SPECIES];
+    energy_init(s_energy);
     const long long total = (long long)e.n_lit * e.K;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
         const int node = (int)(t / e.K);
@@ -671,9 +695,10 @@ __global__ void emit_kernel(SourceArgs a, EmitArgs e) {
         long long* tmp = e.charge_tmp + (long long)e.s * e.n_cmat;
         if (!surface_charge(a.g, e.node_cmat, e.obj, tmp, ax, pi, pj, pk, dd[oa], dd[ob], -1))
             atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_BAD_CMAT_NODE);
-        atomicAdd(&a.sc->emitted_by[e.obj][e.s], 1ull);
-        finish_source(a, e.s, x[0], x[1], x[2], v[0], v[1], v[2], true, true);
+        finish_source(a, e.s, x[0], x[1], x[2], v[0], v[1], v[2], true, true, s_energy);
     }
+    energy_flush(a, s_energy);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.sc->emitted_by[e.obj][e.s], (unsigned long long)total);
 }
 
 // ------------------------------------------------------------------ absorption
