@@ -287,6 +287,7 @@ int fopis_create(const fopis_params* p, int device, void** out) {
         std::memset(x.h_sc, 0, sizeof(DevScalars));
         for (auto& e : x.ev) FOPIS_CUDA(cudaEventCreate(&e));
         mg_setup(x);
+        mg_prepare(x);
         FOPIS_CUDA(cudaDeviceSynchronize());
         return FOPIS_OK;
     });

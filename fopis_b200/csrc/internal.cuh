@@ -253,6 +253,7 @@ void glue_copy(Ctx& c, double* a);
 void mg_setup(Ctx& c);
 void mg_free(Ctx& c);
 int mg_solve(Ctx& c, double tol, int max_cycles);
+void mg_prepare(Ctx& c);   // records the solve graph (once the context's arrays exist)
 // cmatrix.cu
 void object_upload(Ctx& c, ObjectDev& o, const fopis_object_desc* d, int id);
 void cmatrix_build(Ctx& c, int id);

@@ -1178,7 +1178,7 @@ void mg_solve_host_loop(Ctx& c, double tol, int max_cycles, double* res_out, dou
 
 }  // namespace
 
-int mg_solve(Ctx& c, double tol, int max_cycles) {
+void mg_prepare(Ctx& c) {
     if (c.solve_state == 0) {
         // FOPIS_SOLVE_HOST_LOOP=1 keeps the host-driven loop (same kernels and
         // results) for profilers that do not trace conditional graph bodies
@@ -1193,6 +1193,10 @@ int mg_solve(Ctx& c, double tol, int max_cycles) {
             c.solve_state = -1;
         }
     }
+}
+
+int mg_solve(Ctx& c, double tol, int max_cycles) {
+    mg_prepare(c);
     double res = 0.0, fnorm = 1.0;
     int cycles = 0;
     if (c.solve_state == 1) {
