@@ -357,7 +357,17 @@ __global__ void __launch_bounds__(kTileThreads, 4) push_tile_kernel(PushArgs a, 
     const int b = blockIdx.x;
     const int bi = b / (a.g.nb[1] * a.g.nb[2]), bj = (b / a.g.nb[2]) % a.g.nb[1], bk = b % a.g.nb[2];
     const int wx0 = bi * kBX - kHalo, wy0 = bj * kBY - kHalo, wz0 = bk * kBZ - kHalo;
-    for (int t = tid; t < kTile; t += kTileThreads) { t0[t] = 0u; t1[t] = 0u; t2[t] = 0u; }
+    int body = 0;
+    for (int t = tid; t < kTile; t += kTileThreads) {
+        t0[t] = 0u; t1[t] = 0u; t2[t] = 0u;
+        // a body cell anywhere in the window (cells wx0 .. wx0 + kWX - 2 per axis)?
+        const int x = wx0 + t / (kWY * kWZ), y = wy0 + (t / kWZ) % kWY, z = wz0 + t % kWZ;
+        if (a.cellmap && x >= wx0 && x - wx0 < kWX - 1 && y - wy0 < kWY - 1 && z - wz0 < kWZ - 1 && x >= 0 && y >= 0 &&
+            z >= 0 && x < a.g.cx - 1 && y < a.g.cy - 1 && z < a.g.cz - 1 && a.cellmap[lin(a.g, x, y, z)] != 0)
+            body = 1;
+    }
+    // particles that stay inside a body-free window need no body test
+    const bool window_body = __syncthreads_or(body) != 0;
     const long long p0 = brick_start[b], p1 = brick_start[b + 1];
     // every particle adds at most once to a node, so fewer than 2^15 particles
     // cannot overflow a 32-bit chunk plane; denser bricks deposit to HBM
@@ -394,15 +404,17 @@ __global__ void __launch_bounds__(kTileThreads, 4) push_tile_kernel(PushArgs a, 
                 gather_boris(a, st);
                 live = move_boundary(a, st);
             }
-            if (absorb_check(a, st, live)) live = false;
+            const int li = st.i - wx0, lj = st.j - wy0, lk = st.k - wz0;
+            const bool inwin = li >= 0 && lj >= 0 && lk >= 0 && li < kWX - 1 && lj < kWY - 1 && lk < kWZ - 1;
+            const bool test = live && (window_body || !inwin);
+            if (__any_sync(kFull, test) && absorb_check(a, st, test)) live = false;
             if (live) {
                 const unsigned qa = (unsigned)__float2int_rn(st.ox * kDepositScale);
                 const unsigned qb = (unsigned)__float2int_rn(st.oy * kDepositScale);
                 const unsigned qd = (unsigned)__float2int_rn(st.oz * kDepositScale);
                 const unsigned wx[2] = {(unsigned)kDepositOne - qa, qa}, wy[2] = {(unsigned)kDepositOne - qb, qb};
                 const unsigned wz[2] = {(unsigned)kDepositOne - qd, qd};
-                const int li = st.i - wx0, lj = st.j - wy0, lk = st.k - wz0;
-                if (tile_ok && li >= 0 && lj >= 0 && lk >= 0 && li < kWX - 1 && lj < kWY - 1 && lk < kWZ - 1) {
+                if (tile_ok && inwin) {
                     const int tb = (li * kWY + lj) * kWZ + lk;
                     if (tb != cur) {
                         if (cur >= 0) tile_flush(t0, t1, t2, cur, acc);
