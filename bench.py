@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import re
 import os
 import statistics
 import subprocess
@@ -426,6 +427,7 @@ def main():
         v, dt, n, it = run_oracle(cfg, Cm, threads, args.cpu_steps)
         line = dict(base, impl="reference", value=v, steps=args.cpu_steps, warmup=0, ms_per_step=dt * 1e3 / args.cpu_steps,
                     n_gpus=1)
+        line["config"] = dict(base["config"], poisson_start="the reference's PSOR continues from the previous phi")
         line["cpu_baseline"] = {"value": v, "unit": "particle-steps/s", "cores": threads, "kind": "port",
                                 "sample": f"{args.cpu_steps} full step(s) of the workload ({n} particles), "
                                           f"reference PSOR ({it} sweeps last solve)"}
@@ -436,13 +438,15 @@ def main():
     value = res["psteps"] / (res["ms"] * 1e-3)
     achieved = PUSH_BYTES_PER_PARTICLE * res["pushed"] / (res["push_ms"] * 1e-3) / 1e9
     traffic = None
-    prof = ROOT / "profiles" / "push_kernel_cube128.json"
+    prof = ROOT / "profiles" / "push_kernel_cube64.md"
     if prof.exists():
-        d = json.loads(prof.read_text())
-        traffic = d["dram_bytes_per_particle"] * res["pushed"]
+        # DRAM bytes per particle of one push_tile_kernel launch, from the committed ncu summary
+        m = re.search(r"\| dram_bytes_per_particle \| ([0-9.]+) \|", prof.read_text())
+        if m:
+            traffic = float(m.group(1)) * res["pushed"]
     line = dict(base, value=value, steps=args.steps, warmup=args.warmup, ms_per_step=res["ms"] / args.steps)
     line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                        "traffic": traffic, "kernel": "push_kernel<vel,pos,dep> (all species)",
+                        "traffic": traffic, "kernel": "push_tile_kernel + tail push_kernel (all species)",
                         "peak_kind": peak_kind,
                         "bytes_per_particle": PUSH_BYTES_PER_PARTICLE}
     line["clocks"] = res["clocks"]
