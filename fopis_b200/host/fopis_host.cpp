@@ -1,0 +1,382 @@
+// fopis_host.cpp — the host classes of fopis_host.hpp over the C ABI.
+#include "fopis_host.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sys/stat.h>
+
+#include "json.hpp"
+
+namespace fopis {
+namespace host {
+
+// ---------------------------------------------------------------- units
+Normalizer::Normalizer(double dx, double dt) : x(dx), t(dt) {
+    V_unit = dx * dx * kMe / (kE * dt * dt);
+    A_unit = kE / dt;
+    eps0 = kEps0 * (std::pow(dx, 3.0) * kMe) / (kE * kE * dt * dt);   // Normalizer::normalizeEpsilon
+}
+
+void calc_flux(double vth, double density_norm, double size, const double drift[3], const int injection_axis[6],
+               double flux[6]) {
+    // numerical integral of v f(v) over [-6, 6] thermal units, step 1e-3, split by the sign of v
+    const double ddv = 1e-3;
+    const double nvx = 12.0 / ddv;
+    for (int axis = 0; axis < 3; ++axis) {
+        const double d = drift[axis] / vth;
+        double lo = 0.0, hi = 0.0;
+        for (int i = 0; i < nvx - 1; ++i) {
+            const double arg1 = i * ddv + (d - 6.0);
+            const double argx1 = std::pow(arg1 - d, 2.0);
+            if (arg1 > 0.0) lo += arg1 * std::exp(-argx1) * ddv;
+            else hi += arg1 * std::exp(-argx1) * ddv;
+        }
+        flux[2 * axis] = lo * (vth / std::sqrt(M_PI)) * density_norm / size;
+        flux[2 * axis + 1] = -hi * (vth / std::sqrt(M_PI)) * density_norm / size;
+    }
+    for (int k = 0; k < 6; ++k) if (!injection_axis[k]) flux[k] = 0.0;
+}
+
+fopis_species ParticleType::to_abi(const Normalizer& norm, double dx) const {
+    fopis_species s{};
+    s.kind = type == "ambient" ? FOPIS_SPECIES_AMBIENT : FOPIS_SPECIES_PHOTOELECTRON;
+    s.particle_per_cell = particle_per_cell;
+    s.charge = charge;
+    s.mass = mass;
+    s.size = (double)(long long)(std::pow(dx, 3.0) * density / particle_per_cell);   // ParticleType::updateSize
+    const double T = kE * temperature;                                               // setTemperature: e * T[eV]
+    s.thermal_velocity = norm.velocity(std::sqrt(2.0 * T / (mass * kMe)));
+    s.deviation = norm.velocity(std::sqrt(T / (mass * kMe)));
+    for (int a = 0; a < 3; ++a) s.drift[a] = drift_kms[a] * 1e3 * norm.velocity(1.0);
+    for (int a = 0; a < 6; ++a) s.injection_axis[a] = injection_axis[a];
+    if (type == "ambient") {
+        const double dens_norm = density * std::pow(dx, 3.0);                         // normalizeDensity
+        calc_flux(s.thermal_velocity, dens_norm, s.size, s.drift, s.injection_axis, s.flux);
+    } else {
+        const double j = norm.current_density(current_density);
+        s.emission_amount = 1.0 * j / (std::fabs(charge) * s.size);                   // dx^2 = 1 (Spacecraft.cpp:876-877)
+    }
+    return s;
+}
+
+// ---------------------------------------------------------------- input.json
+namespace {
+
+std::string dir_of(const std::string& path) {
+    const size_t s = path.find_last_of('/');
+    return s == std::string::npos ? std::string(".") : path.substr(0, s);
+}
+
+void parse_obj(const std::string& path, int nx, int ny, int nz, ObjectSpec& o) {
+    int32_t *nodes = nullptr, *cells = nullptr;
+    int nn = 0, nc = 0;
+    const int rc = fopis_parse_obj(path.c_str(), nx, ny, nz, &nodes, &nn, &cells, &nc);
+    if (rc != FOPIS_OK) throw Error(rc, "cannot parse " + path);
+    o.nodes.assign(nodes, nodes + 3 * (size_t)nn);
+    o.cells.assign(cells, cells + 3 * (size_t)nc);
+    fopis_free(nodes);
+    fopis_free(cells);
+}
+
+}  // namespace
+
+Input load_input(const std::string& path) {
+    const Value js = Value::parse_file(path);
+    Input in;
+    const Value& env = js["Environment"];
+    in.dx = env["dx"].number();
+    in.dt = env["dt"].number();
+    const int nxyz[3] = {env["nx"].integer(), env["ny"].integer(), env["nz"].integer()};
+    if (env.integer_or("proc_x", 1) * env.integer_or("proc_y", 1) * env.integer_or("proc_z", 1) != 1)
+        throw Error(FOPIS_ERR_ARG, "the whole domain lives on one GPU: proc_x = proc_y = proc_z = 1");
+    in.max_timestep = env.integer_or("max_timestep", 0);
+    in.norm = Normalizer(in.dx, in.dt);
+    const Normalizer& norm = in.norm;
+
+    std::vector<ParticleType> species;
+    for (const auto& kv : js["Plasma"].items()) {        // std::map order, as picojson's
+        const Value& pl = kv.second;
+        ParticleType p;
+        p.name = kv.first;
+        p.type = pl["type"].str();
+        if (p.type != "ambient" && p.type != "photoelectron")
+            throw Error(FOPIS_ERR_ARG, "species type " + p.type + " is outside the ES hot path");
+        p.mass = pl["mass"].number();
+        p.charge = pl["charge"].number();
+        p.density = pl["density"].number();
+        p.temperature = pl["temperature"].number();
+        p.particle_per_cell = pl["particle_per_cell"].integer();
+        if (pl.has("drift_velocity"))
+            for (int a = 0; a < 3; ++a) p.drift_kms[a] = pl["drift_velocity"][a].number();
+        if (pl.has("injection_axis"))
+            for (int a = 0; a < 6; ++a) p.injection_axis[a] = pl["injection_axis"][a].boolean() ? 1 : 0;
+        p.current_density = pl.number_or("current_density", 0.0);
+        species.push_back(p);
+    }
+    // Environment::resetParticleTypeOrder: ambient first, then photoelectrons
+    std::stable_partition(species.begin(), species.end(), [](const ParticleType& p) { return p.type == "ambient"; });
+    in.species = species;
+
+    double bfield[3] = {0.0, 0.0, 0.0}, shine[3] = {0.0, 0.0, 0.0};
+    if (js.has("Field")) {
+        const Value& f = js["Field"];
+        if (f.has("static_bfield")) for (int a = 0; a < 3; ++a) bfield[a] = f["static_bfield"][a].number();
+        if (f.has("shine_vector")) for (int a = 0; a < 3; ++a) shine[a] = f["shine_vector"][a].number();
+    }
+    if (js.has("Options")) in.use_existing_capacity_matrix = js["Options"].boolean_or("use_existing_capacity_matrix", false);
+
+    fopis_params& p = in.params;
+    p.nx = nxyz[0]; p.ny = nxyz[1]; p.nz = nxyz[2];
+    std::snprintf(p.boundary, sizeof p.boundary, "%s", env["boundary"].str().c_str());
+    p.eps0 = norm.eps0;
+    for (int a = 0; a < 3; ++a) {
+        p.static_bfield[a] = bfield[a] * norm.bfield(1.0) * 1e-9;   // nT
+        p.shine_vector[a] = shine[a];
+    }
+    if ((int)species.size() > FOPIS_MAX_SPECIES) throw Error(FOPIS_ERR_ARG, "too many species");
+    p.nspecies = (int)species.size();
+    for (size_t i = 0; i < species.size(); ++i) p.species[i] = species[i].to_abi(norm, in.dx);
+    p.poisson_tol = 1e-8;
+    p.max_vcycles = 100;
+    p.guess_mode = FOPIS_GUESS_WARM;
+    p.sort_interval = 8;
+    p.remove_interval = 50;
+    p.capacity_factor = 1.5;
+    p.precision = FOPIS_MIXED;
+    p.seed = 12345;
+
+    if (js.has("Object")) {
+        const std::string base = dir_of(path);
+        for (const auto& kv : js["Object"].items()) {
+            const Value& o = kv.second;
+            if (o.str_or("surface_type", "perfect") != "perfect")
+                throw Error(FOPIS_ERR_ARG, "only perfect conductors are on the ES hot path");
+            ObjectSpec spec;
+            spec.name = kv.first;
+            std::string file = o["file_name"].str();
+            if (!file.empty() && file[0] != '/') file = base + "/" + file;
+            parse_obj(file, nxyz[0], nxyz[1], nxyz[2], spec);
+            spec.is_potential_fixed = o.boolean_or("is_potential_fixed", false) ? 1 : 0;
+            spec.fixed_potential = norm.potential(o.number_or("fixed_potential", 0.0));
+            spec.initial_potential_offset = norm.potential(o.number_or("initial_potential_offset", 0.0));
+            if (o.has("emit_particles"))
+                for (const auto& e : o["emit_particles"].items())
+                    for (size_t s = 0; s < species.size(); ++s)
+                        if (species[s].name == e.first && species[s].type == "photoelectron") spec.emit_species = (int)s;
+            in.objects.push_back(spec);
+        }
+    }
+    return in;
+}
+
+// ---------------------------------------------------------------- Spacecraft
+namespace {
+std::string fmt(const char* f, double v) {
+    char b[64];
+    std::snprintf(b, sizeof b, f, v);
+    return b;
+}
+std::string fmts(const char* f, const std::string& v) {
+    char b[256];
+    std::snprintf(b, sizeof b, f, v.c_str());
+    return b;
+}
+}  // namespace
+
+std::string Spacecraft::getLogHeader(const std::vector<ParticleType>& species) const {
+    std::string h = fmts("%16s", "Potential [V]") + " " + fmts("%16s", "Charge [C]");
+    for (const auto& s : species) h += " " + fmts("%16s", s.name + " [A]");
+    return h;
+}
+std::string Spacecraft::getLogEntry(const Normalizer& norm) const {
+    std::string e = fmt("%16.7e", norm.unpotential(potential)) + " " + fmt("%16.7e", norm.uncharge(total_charge));
+    for (double c : current) e += " " + fmt("%16.7e", norm.uncurrent(c));
+    return e;
+}
+
+// ---------------------------------------------------------------- RootGrid
+RootGrid::RootGrid(const Input& in, int device) : in_(in) {
+    const int rc = fopis_create(&in_.params, device, &ctx_);
+    if (rc != FOPIS_OK) throw Error(rc, fopis_last_error(nullptr));
+    for (const auto& o : in_.objects) {
+        fopis_object_desc d{};
+        d.n_cmat = o.n_cmat();
+        d.cmat_nodes = o.nodes.data();
+        d.n_cells = (int)(o.cells.size() / 3);
+        d.cells = o.cells.data();
+        d.is_potential_fixed = o.is_potential_fixed;
+        d.fixed_potential = o.fixed_potential;
+        d.initial_potential_offset = o.initial_potential_offset;
+        d.emit_species = o.emit_species;
+        int id = -1;
+        check(fopis_add_object(ctx_, &d, &id));
+        object_ids_.push_back(id);
+    }
+}
+
+RootGrid::~RootGrid() {
+    if (ctx_) fopis_destroy(ctx_);
+}
+
+void RootGrid::check(int rc, bool allow_not_converged) const {
+    if (rc == FOPIS_OK || (allow_not_converged && rc == FOPIS_ERR_NOT_CONVERGED)) return;
+    throw Error(rc, fopis_last_error(ctx_));
+}
+
+void RootGrid::initializeObjectsCmatrix(const std::string& cache_dir) {
+    for (size_t k = 0; k < in_.objects.size(); ++k) {
+        const int id = object_ids_[k];
+        const int n = in_.objects[k].n_cmat();
+        const std::string file = cache_dir.empty() ? "" : cache_dir + "/cmatrix_" + in_.objects[k].name + ".bin";
+        if (!file.empty() && in_.use_existing_capacity_matrix) {
+            std::ifstream f(file, std::ios::binary);
+            int64_t m = 0;
+            if (f && f.read(reinterpret_cast<char*>(&m), sizeof m) && m == n) {
+                std::vector<double> C((size_t)n * n);
+                if (f.read(reinterpret_cast<char*>(C.data()), sizeof(double) * C.size())) {
+                    check(fopis_set_capacity_matrix(ctx_, id, C.data(), n));
+                    continue;
+                }
+            }
+        }
+        check(fopis_build_capacity_matrix(ctx_, id));
+        if (!file.empty()) {
+            std::vector<double> C((size_t)n * n);
+            check(fopis_get_capacity_matrix(ctx_, id, C.data(), n));
+            std::ofstream f(file, std::ios::binary);
+            const int64_t m = n;
+            f.write(reinterpret_cast<const char*>(&m), sizeof m);
+            f.write(reinterpret_cast<const char*>(C.data()), sizeof(double) * C.size());
+        }
+    }
+}
+
+void RootGrid::generateAmbientParticles() { check(fopis_generate_ambient(ctx_)); }
+void RootGrid::loadParticles(int species, const std::vector<Particle>& p) {
+    check(fopis_load_particles(ctx_, species, p.data(), (int64_t)p.size()));
+}
+void RootGrid::initialize() { check(fopis_initialize(ctx_), true); }
+void RootGrid::mainLoop() { check(fopis_step(ctx_, 1), true); }
+void RootGrid::setGuessMode(int mode) { check(fopis_set_guess_mode(ctx_, mode)); }
+void RootGrid::updateParticleVelocity() { check(fopis_update_velocity(ctx_)); }
+void RootGrid::emitParticlesFromObjects() { check(fopis_emit_particles(ctx_)); }
+void RootGrid::updateParticlePosition() { check(fopis_update_position(ctx_)); }
+void RootGrid::injectParticlesFromBoundary() { check(fopis_inject_particles(ctx_)); }
+void RootGrid::updateRho() { check(fopis_update_rho(ctx_), true); }
+void RootGrid::solvePoisson() { check(fopis_solve_poisson(ctx_), true); }
+void RootGrid::updateEfield() { check(fopis_update_efield(ctx_)); }
+void RootGrid::advanceTimestep() { check(fopis_advance_timestep(ctx_)); }
+
+double RootGrid::getParticleEnergy() const {
+    double pe = 0.0, fe = 0.0;
+    check(fopis_get_energy(ctx_, &pe, &fe));
+    return pe;
+}
+double RootGrid::getEFieldEnergy() const {
+    double pe = 0.0, fe = 0.0;
+    check(fopis_get_energy(ctx_, &pe, &fe));
+    return fe;
+}
+fopis_stats RootGrid::stats() const {
+    fopis_stats st{};
+    check(fopis_get_stats(ctx_, &st));
+    return st;
+}
+std::vector<int64_t> RootGrid::getValidParticleNumbers() const {
+    const fopis_stats st = stats();
+    return std::vector<int64_t>(st.num_particles, st.num_particles + in_.params.nspecies);
+}
+std::vector<Particle> RootGrid::getParticles(int species) const {
+    const int64_t cap = stats().num_particles[species];
+    std::vector<Particle> out((size_t)std::max<int64_t>(cap, 1));
+    int64_t n = 0;
+    check(fopis_get_particles(ctx_, species, out.data(), cap, &n));
+    out.resize((size_t)n);
+    return out;
+}
+std::vector<double> RootGrid::getField(int which) const {
+    const size_t n = (size_t)(in_.params.nx + 2) * (in_.params.ny + 2) * (in_.params.nz + 2);
+    std::vector<double> out(n);
+    check(fopis_get_field(ctx_, which, out.data(), n));
+    return out;
+}
+std::vector<Spacecraft> RootGrid::getObjects() const {
+    std::vector<Spacecraft> out;
+    for (size_t k = 0; k < in_.objects.size(); ++k) {
+        Spacecraft s;
+        s.name = in_.objects[k].name;
+        s.id = object_ids_[k];
+        s.current.assign((size_t)in_.params.nspecies, 0.0);
+        check(fopis_get_object(ctx_, s.id, &s.potential, &s.total_charge, s.current.data()));
+        out.push_back(std::move(s));
+    }
+    return out;
+}
+
+// ---------------------------------------------------------------- IO
+namespace io {
+namespace {
+void ensure_dir(const std::string& dir) { ::mkdir(dir.c_str(), 0755); }
+// IO::putHeader / putLog: "%10s %16s %s" and "%10d %16.7e %s"
+void put_header(const std::string& file, const std::string& header) {
+    std::ofstream f(file, std::ios::out);
+    char b[64];
+    std::snprintf(b, sizeof b, "%10s %16s ", "Timestep", "Datatime");
+    f << b << header << "\n";
+}
+void put_log(const std::string& file, int timestep, double datatime, const std::string& entry) {
+    std::ofstream f(file, std::ios::app);
+    char b[64];
+    std::snprintf(b, sizeof b, "%10d %16.7e ", timestep, datatime);
+    f << b << entry << "\n";
+}
+}  // namespace
+
+void plot_energy(const RootGrid& g, int timestep, const std::string& dir) {
+    ensure_dir(dir);
+    const std::string file = dir + "/energy.txt";
+    const Normalizer& n = g.input().norm;
+    if (timestep == 1) {
+        char h[128];
+        std::snprintf(h, sizeof h, "%16s %16s %16s %16s", "Energy [J]", "Particle [J]", "EField [J]", "BField [J]");
+        put_header(file, h);
+    }
+    const double pe = g.getParticleEnergy(), fe = g.getEFieldEnergy();
+    char e[128];
+    std::snprintf(e, sizeof e, "%16.7e %16.7e %16.7e %16.7e", n.unenergy(pe + fe), n.unenergy(pe), n.unenergy(fe), 0.0);
+    put_log(file, timestep, timestep * g.input().dt, e);
+}
+
+void plot_objects(const RootGrid& g, int timestep, const std::string& dir) {
+    ensure_dir(dir);
+    for (const auto& s : g.getObjects()) {
+        const std::string file = dir + "/object_" + s.name + ".txt";
+        if (timestep == 1) put_header(file, s.getLogHeader(g.input().species));
+        put_log(file, timestep, timestep * g.input().dt, s.getLogEntry(g.input().norm));
+    }
+}
+
+void plot_particle_numbers(const RootGrid& g, int timestep, const std::string& dir) {
+    ensure_dir(dir);
+    const std::string file = dir + "/total_particle_number.txt";
+    const auto counts = g.getValidParticleNumbers();
+    if (timestep == 1) {
+        std::string h = fmts("%16s", "Total");
+        for (const auto& s : g.input().species) h += " " + fmts("%16s", s.name);
+        put_header(file, h);
+    }
+    int64_t total = 0;
+    for (int64_t c : counts) total += c;
+    char b[32];
+    std::snprintf(b, sizeof b, "%16lld", (long long)total);
+    std::string e = b;
+    for (int64_t c : counts) { std::snprintf(b, sizeof b, " %16lld", (long long)c); e += b; }
+    put_log(file, timestep, timestep * g.input().dt, e);
+}
+}  // namespace io
+
+}  // namespace host
+}  // namespace fopis

@@ -1,0 +1,84 @@
+// fopis_run — the reference's main loop (src/main.cpp:16-72) on the GPU
+// library: read input.json, set up the conductors (capacity matrix built or
+// read from the cache), load the ambient plasma, initialize, then per step
+// RootGrid::mainLoop and the energy / object / particle-number logs.
+//
+//   fopis_run [input.json] [--steps N] [--out DIR] [--device D]
+//             [--guess warm|history] [--dump-params FILE]
+//
+// --dump-params writes the normalised parameters and object node lists that
+// input.json produces (no GPU work) and exits.
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <string>
+
+#include "fopis_host.hpp"
+
+using namespace fopis::host;
+
+namespace {
+void dump_params(const Input& in, const std::string& file) {
+    std::ofstream f(file, std::ios::binary);
+    f.write(reinterpret_cast<const char*>(&in.params), sizeof in.params);
+    const int32_t nobj = (int32_t)in.objects.size();
+    f.write(reinterpret_cast<const char*>(&nobj), sizeof nobj);
+    for (const auto& o : in.objects) {
+        const int32_t meta[4] = {(int32_t)(o.nodes.size() / 3), (int32_t)(o.cells.size() / 3), o.is_potential_fixed,
+                                 o.emit_species};
+        f.write(reinterpret_cast<const char*>(meta), sizeof meta);
+        const double pot[2] = {o.fixed_potential, o.initial_potential_offset};
+        f.write(reinterpret_cast<const char*>(pot), sizeof pot);
+        f.write(reinterpret_cast<const char*>(o.nodes.data()), sizeof(int32_t) * o.nodes.size());
+        f.write(reinterpret_cast<const char*>(o.cells.data()), sizeof(int32_t) * o.cells.size());
+    }
+}
+}  // namespace
+
+int main(int argc, char** argv) {
+    std::string input = "input.json", out = "data", dump;
+    int steps = -1, device = 0, guess = FOPIS_GUESS_WARM;
+    for (int i = 1; i < argc; ++i) {
+        const std::string a = argv[i];
+        auto next = [&]() -> std::string {
+            if (i + 1 >= argc) { std::fprintf(stderr, "%s needs a value\n", a.c_str()); std::exit(2); }
+            return argv[++i];
+        };
+        if (a == "--steps") steps = std::stoi(next());
+        else if (a == "--out") out = next();
+        else if (a == "--device") device = std::stoi(next());
+        else if (a == "--dump-params") dump = next();
+        else if (a == "--guess") {
+            const std::string g = next();
+            guess = g == "history" ? FOPIS_GUESS_HISTORY : FOPIS_GUESS_WARM;
+        } else input = a;
+    }
+    try {
+        const Input in = load_input(input);
+        if (!dump.empty()) {
+            dump_params(in, dump);
+            return 0;
+        }
+        if (steps < 0) steps = in.max_timestep;
+        RootGrid grid(in, device);
+        grid.setGuessMode(guess);
+        grid.initializeObjectsCmatrix(out);
+        grid.generateAmbientParticles();
+        grid.initialize();
+        std::cout << "===== Begin Main Loop =====" << std::endl;
+        for (int t = 1; t <= steps; ++t) {
+            grid.mainLoop();
+            io::plot_energy(grid, t, out);
+            io::plot_objects(grid, t, out);
+            io::plot_particle_numbers(grid, t, out);
+        }
+        const fopis_stats st = grid.stats();
+        std::cout << "===== End Main Loop ===== steps " << steps << ", V-cycles in the last step " << st.vcycles_step
+                  << std::endl;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "fopis_run: %s\n", e.what());
+        return 1;
+    }
+    return 0;
+}

@@ -1,0 +1,42 @@
+"""input.json files for the C++ host tests: a Dirichlet box with a voxel cube,
+electrons, ions and (optionally) photoelectrons, in the reference's schema."""
+import json
+import math
+from pathlib import Path
+
+from fopis_b200 import config
+
+
+def write_input(dirpath, n=25, ppc=4, photo=True, steps=5, drift=(0.0, 0.0, 0.0)):
+    d = Path(dirpath)
+    d.mkdir(parents=True, exist_ok=True)
+    (d / "objects").mkdir(exist_ok=True)
+    (d / "objects" / "cube.obj").write_text(config.box_obj_text([((-2, -2, -2), (2, 2, 2))]))
+    dx, dt = config.plasma_units()
+    plasma = {
+        "Electron": {"type": "ambient", "mass": 1.0, "charge": -1.0, "density": 1.0e7, "temperature": 1.0,
+                     "drift_velocity": list(drift), "particle_per_cell": ppc},
+        "Ion": {"type": "ambient", "mass": 100.0, "charge": 1.0, "density": 1.0e7, "temperature": 1.0,
+                "drift_velocity": [0.0, 0.0, 0.0], "particle_per_cell": ppc,
+                "injection_axis": [True, True, False, True, True, True]},
+    }
+    emit = {}
+    if photo:
+        vbar = math.sqrt(8.0 * config.E / (math.pi * config.ME))
+        plasma["Photo"] = {"type": "photoelectron", "mass": 1.0, "charge": -1.0, "density": 1.0e7, "temperature": 0.2,
+                           "particle_per_cell": ppc, "current_density": 10.0 * config.E * 1.0e7 * vbar / 4.0}
+        emit = {"Photo": {}}
+    js = {
+        "Environment": {"max_timestep": steps, "job_type": "new", "solver_type": "ES", "boundary": "DDDDDD",
+                        "dimension": "3D", "nx": n, "ny": n, "nz": n, "proc_x": 1, "proc_y": 1, "proc_z": 1,
+                        "dx": dx, "dt": dt},
+        "Plasma": plasma,
+        "Field": {"static_bfield": [0.0, 0.0, 0.0], "shine_vector": [-1.0, 0.0, 0.0]},
+        "Object": {"Spacecraft": {"file_name": "objects/cube.obj", "surface_type": "perfect", "emit_particles": emit,
+                                  "is_potential_fixed": False, "fixed_potential": 0.0,
+                                  "initial_potential_offset": 0.0}},
+        "Options": {"use_existing_capacity_matrix": False},
+    }
+    path = d / "input.json"
+    path.write_text(json.dumps(js, indent=2))
+    return path

@@ -1,0 +1,71 @@
+"""The C++ host side (fopis_b200/host): its input.json loader gives the same
+normalised parameters and object node lists as the Python loader, for a
+generated input and for the reference's own sample input."""
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from fopis_b200 import _abi, config
+
+from host_input import write_input
+
+ROOT = Path(__file__).resolve().parent.parent
+RUN = ROOT / "fopis_b200" / "fopis_run"
+SAMPLE = Path("/root/reference/input_samples/input.json")
+
+
+def dump(path, tmp_path):
+    out = tmp_path / "params.bin"
+    subprocess.run([str(RUN), str(path), "--dump-params", str(out)], check=True, capture_output=True, timeout=120)
+    raw = out.read_bytes()
+    size = C.sizeof(_abi.Params)
+    p = _abi.Params.from_buffer_copy(raw[:size])
+    off = size
+    nobj = int(np.frombuffer(raw, np.int32, 1, off)[0])
+    off += 4
+    objs = []
+    for _ in range(nobj):
+        nn, nc, fixed, emit = np.frombuffer(raw, np.int32, 4, off)
+        off += 16
+        pot = np.frombuffer(raw, np.float64, 2, off)
+        off += 16
+        nodes = np.frombuffer(raw, np.int32, 3 * nn, off).reshape(-1, 3)
+        off += 12 * nn
+        cells = np.frombuffer(raw, np.int32, 3 * nc, off).reshape(-1, 3)
+        off += 12 * nc
+        objs.append((nodes, cells, int(fixed), int(emit), pot))
+    return p, objs
+
+
+def compare(cpp, py):
+    p, objs = cpp
+    q = py.params
+    assert bytes(p) == bytes(q), [(f, getattr(p, f), getattr(q, f)) for f, _ in q._fields_ if
+                                  not isinstance(getattr(q, f), (int, float)) or getattr(p, f) != getattr(q, f)]
+    assert len(objs) == len(py.objects)
+    for (nodes, cells, fixed, emit, pot), o in zip(objs, py.objects):
+        assert np.array_equal(nodes, o.nodes) and np.array_equal(cells, o.cells)
+        assert fixed == o.is_potential_fixed and emit == o.emit_species
+        assert pot[0] == o.fixed_potential and pot[1] == o.initial_potential_offset
+
+
+@pytest.fixture(scope="module")
+def built():
+    if not RUN.exists():
+        subprocess.run(["make", "-C", str(ROOT / "fopis_b200")], check=True, capture_output=True)
+    return RUN
+
+
+@pytest.mark.parametrize("photo", [True, False])
+def test_cpp_loader_matches_python(built, tmp_path, photo):
+    path = write_input(tmp_path, photo=photo, drift=(50.0, 0.0, -20.0))
+    compare(dump(path, tmp_path), config.load_input(str(path)))
+
+
+def test_cpp_loader_on_reference_sample(built, tmp_path):
+    if not SAMPLE.exists():
+        pytest.skip("reference sample input not available")
+    compare(dump(SAMPLE, tmp_path), config.load_input(str(SAMPLE)))
