@@ -423,7 +423,11 @@ def main():
         cfg = config.workload(args.workload, ppc=args.ppc, seed=20251203)
         # untimed setup: the capacity matrix the reference would load from its
         # cache, computed exactly on the host (six Dirichlet faces)
-        Cm = reference_cmatrix(cfg)
+        try:
+            Cm = reference_cmatrix(cfg)
+        except NotImplementedError as e:
+            print(json.dumps({"impl": "reference", "unavailable": f"capacity matrix of this body: {e}"}))
+            return
         v, dt, n, it = run_oracle(cfg, Cm, threads, args.cpu_steps)
         line = dict(base, impl="reference", value=v, steps=args.cpu_steps, warmup=0, ms_per_step=dt * 1e3 / args.cpu_steps,
                     n_gpus=1)
@@ -465,10 +469,18 @@ def main():
     if args.learned_train > 0 and world == 1:
         line["learned_guess"] = learned_comparison(args, rank, local, res["cmatrix"])
     if rank == 0 and res["cmatrix"] is not None:
-        Cx = reference_cmatrix(cfg)
-        line["cmatrix_rel_err_vs_exact"] = float(np.abs(res["cmatrix"] - Cx).max() / np.abs(Cx).max())
+        try:
+            Cx = reference_cmatrix(cfg)
+            line["cmatrix_rel_err_vs_exact"] = float(np.abs(res["cmatrix"] - Cx).max() / np.abs(Cx).max())
+        except NotImplementedError as e:      # surface too irregular for the exact pair table
+            line["cmatrix_rel_err_vs_exact"] = None
+            line["cmatrix_exact_unavailable"] = str(e)
     if rank == 0 and world == 1 and args.cpu:
-        v, dt, n, it = run_oracle(cfg, reference_cmatrix(cfg), os.cpu_count() or 1, args.cpu_steps)
+        try:
+            Cref = reference_cmatrix(cfg)
+        except NotImplementedError:
+            Cref = res["cmatrix"]       # irregular body: the GPU-built matrix, checked against solves in the tests
+        v, dt, n, it = run_oracle(cfg, Cref, os.cpu_count() or 1, args.cpu_steps)
         line["cpu_baseline"] = {"value": v, "unit": "particle-steps/s", "cores": os.cpu_count() or 1, "kind": "port",
                                 "sample": f"{args.cpu_steps} full step(s) of the same workload ({n} particles) on the "
                                           f"oracle: FP64 AoS, OpenMP, reference PSOR ({it} sweeps last solve)",

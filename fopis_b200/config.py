@@ -203,24 +203,47 @@ def parse_obj(path: str, nx: int, ny: int, nz: int) -> Tuple[np.ndarray, np.ndar
 
 
 def box_obj_text(boxes: Sequence[Tuple[Tuple[int, int, int], Tuple[int, int, int]]]) -> str:
-    """A MagicaVoxel-style .obj of axis-aligned boxes [lo, hi) in vertex units
-    (relative to the domain centre), one quad per box face."""
+    """A MagicaVoxel-style .obj of the union of axis-aligned boxes [lo, hi) in
+    vertex units (relative to the domain centre). Like a MagicaVoxel export it
+    lists only the exposed faces of the voxel union, merged per plane into
+    rectangles, in the order axis, side (low then high), plane; a face two boxes
+    share is not written (ObjectUtils' pair scan would read it as a closing
+    face). A single box gives its six faces."""
+    lo = np.min([b[0] for b in boxes], axis=0)
+    hi = np.max([b[1] for b in boxes], axis=0)
+    occ = np.zeros(tuple(int(h - l) + 2 for l, h in zip(lo, hi)), dtype=bool)   # one empty layer each side
+    for (bl, bh) in boxes:
+        occ[tuple(slice(int(bl[a] - lo[a]) + 1, int(bh[a] - lo[a]) + 1) for a in range(3))] = True
     verts: List[Tuple[int, int, int]] = []
     faces: List[Tuple[int, int, int, int, int]] = []
-    for (lo, hi) in boxes:
-        for axis in range(3):
-            for side in (0, 1):
-                c = hi[axis] if side else lo[axis]
-                u, w = [a for a in range(3) if a != axis]
-                quad = []
-                for (a, b) in ((lo[u], lo[w]), (hi[u], lo[w]), (hi[u], hi[w]), (lo[u], hi[w])):
-                    p = [0, 0, 0]
-                    p[axis] = c
-                    p[u] = a
-                    p[w] = b
-                    verts.append(tuple(p))
-                    quad.append(len(verts))
-                faces.append((*quad, 2 * axis + side + 1))
+    for axis in range(3):
+        u, w = [a for a in range(3) if a != axis]
+        for side in (0, 1):
+            nb = np.roll(occ, 1 if side == 0 else -1, axis=axis)
+            exposed = occ & ~nb                           # cells whose low (high) face is on the surface
+            for c in range(occ.shape[axis]):
+                m = np.take(exposed, c, axis=axis).copy()   # indexed [u, w]
+                for a0 in range(m.shape[0]):
+                    for b0 in range(m.shape[1]):
+                        if not m[a0, b0]:
+                            continue
+                        b1 = b0
+                        while b1 + 1 < m.shape[1] and m[a0, b1 + 1]:
+                            b1 += 1
+                        a1 = a0
+                        while a1 + 1 < m.shape[0] and m[a1 + 1, b0:b1 + 1].all():
+                            a1 += 1
+                        m[a0:a1 + 1, b0:b1 + 1] = False
+                        plane = int(lo[axis]) + c - 1 + side
+                        quad = []
+                        for (a, b) in ((a0, b0), (a1 + 1, b0), (a1 + 1, b1 + 1), (a0, b1 + 1)):
+                            p = [0, 0, 0]
+                            p[axis] = plane
+                            p[u] = int(lo[u]) + a - 1
+                            p[w] = int(lo[w]) + b - 1
+                            verts.append(tuple(p))
+                            quad.append(len(verts))
+                        faces.append((*quad, 2 * axis + side + 1))
     out = ["# voxel bodies", "vt 0.5 0.5"]
     out += [f"v {x} {y} {z}" for (x, y, z) in verts]
     out += [f"f {a}/1/{n} {b}/1/{n} {c}/1/{n} {d}/1/{n}" for (a, b, c, d, n) in faces]

@@ -76,10 +76,27 @@ def test_obj_parser_matches_oracle(tmp_path, boxes, nxyz, n_cmat):
     assert np.array_equal(a_cells, b_cells)
     if n_cmat:
         assert len(a_nodes) == n_cmat
-    # the inner cells of a single box are exactly its volume
-    if len(boxes) == 1:
-        lo, hi = boxes[0]
-        assert len(a_cells) == np.prod([h - l for l, h in zip(lo, hi)])
+    # the inner cells are exactly the union's volume, and every exposed face of
+    # that volume has its four nodes among the surface nodes (absorption and
+    # emission put charge only there)
+    union = np.zeros(tuple(n + 1 for n in nxyz), dtype=bool)
+    for lo, hi in boxes:
+        union[tuple(slice(l + n // 2 + 1, h + n // 2 + 1) for l, h, n in zip(lo, hi, nxyz))] = True
+    cells = np.zeros_like(union)
+    cells[tuple(a_cells.reshape(-1, 3).T)] = True
+    assert np.array_equal(cells, union)
+    surface = {tuple(v) for v in a_nodes.reshape(-1, 3)}
+    for ax in range(3):
+        u, w = [a for a in range(3) if a != ax]
+        for shift, high in ((1, 0), (-1, 1)):
+            for c in np.argwhere(cells & ~np.roll(cells, shift, axis=ax)):
+                c[ax] += high
+                for du in (0, 1):
+                    for dw in (0, 1):
+                        q = c.copy()
+                        q[u] += du
+                        q[w] += dw
+                        assert tuple(q) in surface
 
 
 @pytest.mark.skipif(not (REFERENCE / "input_samples/objects").exists(), reason="reference samples absent")
