@@ -41,9 +41,12 @@ __host__ Grid make_grid(const Ctx& c) {
     return g;
 }
 
-__device__ __forceinline__ long long brick_key(const Grid& g, int i, int j, int k) {
-    const long long b = ((long long)(i / kBX) * g.nb[1] + (j / kBY)) * g.nb[2] + (k / kBZ);
-    return b * kBrickCells + ((i % kBX) * kBY + (j % kBY)) * kBZ + (k % kBZ);
+// Brick of a node cell (i slowest, k fastest) and the cell's place inside it.
+__device__ __forceinline__ int brick_index(const Grid& g, int i, int j, int k) {
+    return ((i / kBX) * g.nb[1] + (j / kBY)) * g.nb[2] + (k / kBZ);
+}
+__device__ __forceinline__ int local_cell(int i, int j, int k) {
+    return ((i % kBX) * kBY + (j % kBY)) * kBZ + (k % kBZ);
 }
 
 __device__ __forceinline__ long long lin(const Grid& g, int i, int j, int k) {
@@ -905,31 +908,6 @@ __global__ void load56_kernel(Soa p, long long cap, unsigned long long* count, c
 }
 
 // Compacts the valid particles of [lo, hi) into AoS56 records or raw arrays.
-__global__ void export_kernel(Soa p, long long lo, long long hi, int s, Rec56* out56, Soa raw,
-                              unsigned long long* counter) {
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long base = lo + (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < hi; base += stride) {
-        const long long t = base + (threadIdx.x & 31);
-        const int32_t c = t < hi ? p.cell[t] : -1;
-        const bool keep = c >= 0;
-        const unsigned long long slot = warp_reserve(counter, keep);
-        if (!keep) continue;
-        if (out56) {
-            int i, j, k;
-            unpack_cell(c, i, j, k);
-            Rec56 r;
-            r.x = (i - 1) + (double)p.ox[t]; r.y = (j - 1) + (double)p.oy[t]; r.z = (k - 1) + (double)p.oz[t];
-            r.vx = p.vx[t]; r.vy = p.vy[t]; r.vz = p.vz[t];
-            r.typeId = s; r.isValid = 1;
-            out56[slot] = r;
-        } else {
-            raw.cell[slot] = c;
-            raw.ox[slot] = p.ox[t]; raw.oy[slot] = p.oy[t]; raw.oz[slot] = p.oz[t];
-            raw.vx[slot] = p.vx[t]; raw.vy[slot] = p.vy[t]; raw.vz[slot] = p.vz[t];
-        }
-    }
-}
-
 __global__ void energy_kernel(Soa p, long long cap, const unsigned long long* count, double* out) {
     const long long n = (long long)min(*count, (unsigned long long)cap);
     double e = 0.0;
@@ -939,15 +917,23 @@ __global__ void energy_kernel(Soa p, long long cap, const unsigned long long* co
     if (threadIdx.x == 0 && e != 0.0) atomicAdd(out, e);
 }
 
-// ------------------------------------------------------------------ counting sort
+// ------------------------------------------------------------------ sort
+// Two passes per species. Pass 1 moves every particle into its brick's slot
+// range; pass 2 orders each brick's range by cell. Both write whole runs of
+// consecutive slots (pass 1 groups a chunk by brick before it writes, pass 2
+// gathers inside one brick), so every 32-byte sector of the destination is
+// filled by one CTA within one chunk or brick: scattered 4-byte stores that
+// leave sectors partial cost a DRAM fill and a write-back each.
+
+// cnt[b] += particles of brick b (valid slots only), one atomic per warp and brick.
 __global__ void sort_count_kernel(Soa p, long long cap, const unsigned long long* count, Grid g, int32_t* cnt) {
     const long long n = (long long)min(*count, (unsigned long long)cap);
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
         const long long t = base + (threadIdx.x & 31);
         const int32_t c = t < n ? p.cell[t] : -1;
-        long long key = -1 - (long long)(threadIdx.x & 31);
-        if (c >= 0) { int i, j, k; unpack_cell(c, i, j, k); key = brick_key(g, i, j, k); }
+        int key = -1 - (int)(threadIdx.x & 31);
+        if (c >= 0) { int i, j, k; unpack_cell(c, i, j, k); key = brick_index(g, i, j, k); }
         const unsigned grp = __match_any_sync(kFull, key);
         const int lane = threadIdx.x & 31;
         if (c >= 0 && (__ffs(grp) - 1) == lane) atomicAdd(cnt + key, __popc(grp));
@@ -1006,83 +992,232 @@ __global__ void scan_apply_kernel(const int32_t* in, long long n, const int32_t*
     for (int q = 0; q < kScanItems; ++q) { if (base + q < n) out[base + q] = pre; pre += v[q]; }
 }
 
-// brick_start[b] = first sorted slot of brick b (exclusive offsets every kBrickCells keys).
-__global__ void brick_start_kernel(const int32_t* offset, int nbricks, int32_t* brick_start) {
-    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= nbricks; b += gridDim.x * blockDim.x)
-        brick_start[b] = offset[(long long)b * kBrickCells];
+// Order-preserving export of slots [lo, hi): each tile of kScanTile slots
+// counts its valid particles, the tile totals are scanned, and each tile
+// writes its particles at its offset plus their rank inside the tile, so the
+// records come out in slot order.
+__global__ void export_count_kernel(Soa p, long long lo, long long hi, int32_t* partial) {
+    const long long base = lo + (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
+    int n = 0;
+    for (int q = 0; q < kScanItems; ++q) if (base + q < hi && p.cell[base + q] >= 0) ++n;
+    int tot;
+    block_exclusive_scan(n, &tot);
+    if (threadIdx.x == 0) partial[blockIdx.x] = tot;
 }
 
-// Scatter of a nearly sorted particle set: a CTA takes a contiguous chunk,
-// finds the runs of equal keys in it (the previous sort leaves them long),
-// reserves each run's slots with one atomic on its key's cursor and copies
-// the run to consecutive slots, so loads and stores stay coalesced and the
-// atomics of a chunk are issued together.
-constexpr int kSortThreads = 256, kSortItems = 8, kSortChunk = kSortThreads * kSortItems;
+__global__ void export_kernel(Soa p, long long lo, long long hi, int s, Rec56* out56, Soa raw,
+                              const int32_t* partial) {
+    const long long base = lo + (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
+    int32_t cell[kScanItems];
+    int n = 0;
+    for (int q = 0; q < kScanItems; ++q) {
+        cell[q] = base + q < hi ? p.cell[base + q] : -1;
+        n += cell[q] >= 0;
+    }
+    int tot;
+    long long slot = (long long)block_exclusive_scan(n, &tot) + partial[blockIdx.x];
+    for (int q = 0; q < kScanItems; ++q) {
+        if (cell[q] < 0) continue;
+        const long long t = base + q;
+        if (out56) {
+            int i, j, k;
+            unpack_cell(cell[q], i, j, k);
+            Rec56 r;
+            r.x = (i - 1) + (double)p.ox[t]; r.y = (j - 1) + (double)p.oy[t]; r.z = (k - 1) + (double)p.oz[t];
+            r.vx = p.vx[t]; r.vy = p.vy[t]; r.vz = p.vz[t];
+            r.typeId = s; r.isValid = 1;
+            out56[slot] = r;
+        } else {
+            raw.cell[slot] = cell[q];
+            raw.ox[slot] = p.ox[t]; raw.oy[slot] = p.oy[t]; raw.oz[slot] = p.oz[t];
+            raw.vx[slot] = p.vx[t]; raw.vy[slot] = p.vy[t]; raw.vz[slot] = p.vz[t];
+        }
+        ++slot;
+    }
+}
 
-__global__ void __launch_bounds__(kSortThreads) sort_scatter_chunk_kernel(Soa src, Soa dst, long long cap,
+// Pass 1. A CTA takes chunks of kSortChunk slots; a shared hash table maps
+// each brick met in the chunk to a slot that counts its particles (ranks in
+// lane order, so equal-brick lanes of a warp get consecutive places); one
+// atomic per brick and chunk then reserves the brick's run in the cursor.
+constexpr int kSortThreads = 256, kSortItems = 4, kSortChunk = kSortThreads * kSortItems;
+constexpr int kSortSlots = 2 * kSortChunk;   // more slots than distinct bricks a chunk can hold
+
+__device__ __forceinline__ int sort_slot(int* keys, int b) {
+    const unsigned h = ((unsigned)b * 2654435761u) >> 21;   // 11 bits: kSortSlots = 2048
+    for (int q = 0; q < kSortSlots; ++q) {
+        const int s = (int)((h + q) & (kSortSlots - 1));
+        const int k = keys[s];
+        if (k == b) return s;
+        if (k == -1) {
+            const int old = atomicCAS(&keys[s], -1, b);
+            if (old == -1 || old == b) return s;
+        }
+    }
+    return -1;   // unreachable: at most kSortChunk distinct bricks in kSortSlots slots
+}
+
+__global__ void __launch_bounds__(kSortThreads) sort_brick_scatter_kernel(Soa src, Soa dst, long long cap,
                                                                           const unsigned long long* count, Grid g,
                                                                           int32_t* cursor) {
-    __shared__ int32_t s_key[kSortChunk];
-    __shared__ int32_t s_start[kSortChunk];   // first index of the run an entry belongs to
-    __shared__ int32_t s_base[kSortChunk];    // destination of a run's first entry (at its start index)
-    __shared__ int32_t s_wmax[kSortThreads / 32];
+    static_assert(kSortSlots == 2048, "sort_slot hashes to 11 bits");
+    __shared__ int s_key[kSortSlots];   // brick of a slot, -1 while free
+    __shared__ int s_cnt[kSortSlots];
+    __shared__ int s_base[kSortSlots];
     const long long n = (long long)min(*count, (unsigned long long)cap);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31;
+    for (int q = tid; q < kSortSlots; q += kSortThreads) { s_key[q] = -1; s_cnt[q] = 0; }
+    __syncthreads();
     for (long long c0 = (long long)blockIdx.x * kSortChunk; c0 < n; c0 += (long long)gridDim.x * kSortChunk) {
-        for (int q = tid; q < kSortChunk; q += kSortThreads) {
-            const long long t = c0 + q;
-            int key = -1;
-            if (t < n) {
-                const int32_t c = src.cell[t];
-                if (c >= 0) { int i, j, k; unpack_cell(c, i, j, k); key = (int)brick_key(g, i, j, k); }
+        int32_t cell[kSortItems];
+        float f[kSortItems][6];
+        int slot[kSortItems], rank[kSortItems];
+#pragma unroll
+        for (int e = 0; e < kSortItems; ++e) {
+            const long long t = c0 + e * kSortThreads + tid;
+            cell[e] = t < n ? src.cell[t] : -1;
+            if (cell[e] >= 0) {
+                f[e][0] = src.ox[t]; f[e][1] = src.oy[t]; f[e][2] = src.oz[t];
+                f[e][3] = src.vx[t]; f[e][4] = src.vy[t]; f[e][5] = src.vz[t];
             }
-            s_key[q] = key;
         }
-        __syncthreads();
-        // start index of each entry's run: inclusive max-scan of (run start ? q : -1);
-        // thread tid owns entries tid*kSortItems .. +kSortItems-1
-        int m = -1;
-        int loc[kSortItems];
 #pragma unroll
         for (int e = 0; e < kSortItems; ++e) {
-            const int q = tid * kSortItems + e;
-            const int key = s_key[q];
-            const bool start = key >= 0 && (q == 0 || s_key[q - 1] != key);
-            if (start) m = q;
-            loc[e] = m;
+            int b = -1 - lane;   // distinct per lane for empty slots
+            if (cell[e] >= 0) { int i, j, k; unpack_cell(cell[e], i, j, k); b = brick_index(g, i, j, k); }
+            const unsigned grp = __match_any_sync(kFull, b);
+            const int leader = __ffs(grp) - 1;
+            int sl = -1, r0 = 0;
+            if (cell[e] >= 0 && lane == leader) {
+                sl = sort_slot(s_key, b);
+                if (sl >= 0) r0 = atomicAdd(&s_cnt[sl], __popc(grp));
+            }
+            slot[e] = __shfl_sync(kFull, sl, leader);
+            rank[e] = __shfl_sync(kFull, r0, leader) + __popc(grp & ((1u << lane) - 1u));
         }
-        int x = m;
-        for (int o = 1; o < 32; o <<= 1) { const int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x = max(x, y); }
-        if (lane == 31) s_wmax[warp] = x;
-        const int up = __shfl_up_sync(0xffffffffu, x, 1);
         __syncthreads();
-        int carry = lane > 0 ? up : -1;                  // latest start among earlier lanes of the warp
-        for (int w = 0; w < warp; ++w) carry = max(carry, s_wmax[w]);
+        for (int q = tid; q < kSortSlots; q += kSortThreads)
+            if (s_key[q] >= 0) s_base[q] = atomicAdd(cursor + s_key[q], s_cnt[q]);
+        __syncthreads();
 #pragma unroll
         for (int e = 0; e < kSortItems; ++e) {
-            const int q = tid * kSortItems + e;
-            s_start[q] = max(carry, loc[e]);
+            if (cell[e] < 0 || slot[e] < 0) continue;
+            const long long d = (long long)s_base[slot[e]] + rank[e];
+            dst.cell[d] = cell[e];
+            dst.ox[d] = f[e][0]; dst.oy[d] = f[e][1]; dst.oz[d] = f[e][2];
+            dst.vx[d] = f[e][3]; dst.vy[d] = f[e][4]; dst.vz[d] = f[e][5];
         }
+        for (int q = tid; q < kSortSlots; q += kSortThreads) { s_key[q] = -1; s_cnt[q] = 0; }
         __syncthreads();
-        // the last entry of each run reserves the run's slots
+    }
+}
+
+// Pass 2. One CTA per brick (grid-stride): a shared histogram of the brick's
+// 128 cells, its exclusive scan, then the inverse permutation and a gather
+// inside the brick's range, so the stores run over consecutive slots. Bricks
+// above kCellCap particles place each particle straight at its cell cursor.
+// Loads are issued kCellBatch particles per thread at a time so their
+// latencies overlap; shared counters take one atomic per warp and cell.
+constexpr int kCellThreads = 256, kCellCap = 8192, kCellBatch = 4;
+
+__device__ __forceinline__ int cell_rank(int* counter, int lc, bool valid) {
+    const unsigned grp = __match_any_sync(kFull, valid ? lc : -1 - (int)(threadIdx.x & 31));
+    const int lane = threadIdx.x & 31, leader = __ffs(grp) - 1;
+    int r0 = 0;
+    if (valid && lane == leader) r0 = atomicAdd(counter + lc, __popc(grp));
+    return __shfl_sync(kFull, r0, leader) + __popc(grp & ((1u << lane) - 1u));
+}
+
+__global__ void __launch_bounds__(kCellThreads) sort_cell_kernel(Soa src, Soa dst, const int32_t* brick_start,
+                                                                 int nbricks) {
+    __shared__ uint8_t s_lc[kCellCap];
+    __shared__ uint16_t s_perm[kCellCap];
+    __shared__ int s_off[kBrickCells];
+    const int tid = threadIdx.x, lane = tid & 31;
+    constexpr int kStep = kCellThreads * kCellBatch;
+    for (int b = blockIdx.x; b < nbricks; b += gridDim.x) {
+        const long long base = brick_start[b];
+        const int n = brick_start[b + 1] - (int)base;
+        if (n <= 0) continue;
+        const bool fits = n <= kCellCap;
+        if (tid < kBrickCells) s_off[tid] = 0;
+        __syncthreads();
+        for (int q0 = 0; q0 < n; q0 += kStep) {
+            int lc[kCellBatch];
 #pragma unroll
-        for (int e = 0; e < kSortItems; ++e) {
-            const int q = tid * kSortItems + e;
-            const int key = s_key[q];
-            if (key < 0) continue;
-            if (q + 1 < kSortChunk && s_key[q + 1] == key) continue;
-            const int st = s_start[q];
-            s_base[st] = atomicAdd(cursor + key, q - st + 1);
+            for (int e = 0; e < kCellBatch; ++e) {
+                const int q = q0 + e * kCellThreads + tid;
+                lc[e] = -1;
+                if (q < n) { int i, j, k; unpack_cell(src.cell[base + q], i, j, k); lc[e] = local_cell(i, j, k); }
+            }
+#pragma unroll
+            for (int e = 0; e < kCellBatch; ++e) {
+                const int q = q0 + e * kCellThreads + tid;
+                if (fits && q < n) s_lc[q] = (uint8_t)lc[e];
+                cell_rank(s_off, lc[e], q < n);
+            }
         }
         __syncthreads();
-        for (int q = tid; q < kSortChunk; q += kSortThreads) {
-            if (s_key[q] < 0) continue;
-            const int st = s_start[q];
-            const long long d = (long long)s_base[st] + (q - st);
-            const long long t = c0 + q;
-            dst.cell[d] = src.cell[t];
-            dst.ox[d] = src.ox[t]; dst.oy[d] = src.oy[t]; dst.oz[d] = src.oz[t];
-            dst.vx[d] = src.vx[t]; dst.vy[d] = src.vy[t]; dst.vz[d] = src.vz[t];
+        if (tid < 32) {   // exclusive scan of 128 counts, 4 per lane
+            static_assert(kBrickCells == 128, "one warp scans 4 counts per lane");
+            int v[4], sum = 0;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) { v[e] = s_off[lane * 4 + e]; sum += v[e]; }
+            int x = sum;
+            for (int o = 1; o < 32; o <<= 1) { const int y = __shfl_up_sync(kFull, x, o); if (lane >= o) x += y; }
+            int pre = x - sum;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) { s_off[lane * 4 + e] = pre; pre += v[e]; }
+        }
+        __syncthreads();
+        if (fits) {
+            for (int q0 = 0; q0 < n; q0 += kCellThreads) {
+                const int q = q0 + tid;
+                const bool ok = q < n;
+                const int lc = ok ? s_lc[q] : 0;
+                const int r = cell_rank(s_off, lc, ok);
+                if (ok) s_perm[r] = (uint16_t)q;
+            }
+            __syncthreads();
+            for (int r0 = 0; r0 < n; r0 += kStep) {
+                int32_t c[kCellBatch];
+                float v[kCellBatch][6];
+#pragma unroll
+                for (int e = 0; e < kCellBatch; ++e) {
+                    const int r = r0 + e * kCellThreads + tid;
+                    if (r < n) {
+                        const long long sidx = base + s_perm[r];
+                        c[e] = src.cell[sidx];
+                        v[e][0] = src.ox[sidx]; v[e][1] = src.oy[sidx]; v[e][2] = src.oz[sidx];
+                        v[e][3] = src.vx[sidx]; v[e][4] = src.vy[sidx]; v[e][5] = src.vz[sidx];
+                    }
+                }
+#pragma unroll
+                for (int e = 0; e < kCellBatch; ++e) {
+                    const int r = r0 + e * kCellThreads + tid;
+                    if (r < n) {
+                        const long long d = base + r;
+                        dst.cell[d] = c[e];
+                        dst.ox[d] = v[e][0]; dst.oy[d] = v[e][1]; dst.oz[d] = v[e][2];
+                        dst.vx[d] = v[e][3]; dst.vy[d] = v[e][4]; dst.vz[d] = v[e][5];
+                    }
+                }
+            }
+        } else {
+            for (int q0 = 0; q0 < n; q0 += kCellThreads) {
+                const int q = q0 + tid;
+                const bool ok = q < n;
+                const long long sidx = base + (ok ? q : 0);
+                const int32_t c = src.cell[sidx];
+                int i, j, k;
+                unpack_cell(c, i, j, k);
+                const int r = cell_rank(s_off, local_cell(i, j, k), ok);
+                if (!ok) continue;
+                const long long d = base + r;
+                dst.cell[d] = c;
+                dst.ox[d] = src.ox[sidx]; dst.oy[d] = src.oy[sidx]; dst.oz[d] = src.oz[sidx];
+                dst.vx[d] = src.vx[sidx]; dst.vy[d] = src.vy[sidx]; dst.vz[d] = src.vz[sidx];
+            }
         }
         __syncthreads();
     }
@@ -1160,13 +1295,21 @@ void particles_append_aos(Ctx& c, int s, const void* host56, int64_t n) {
     sync_scalars(c);
 }
 
-static int64_t export_range(Ctx& c, int s, Rec56* d56, Soa* raw, int64_t lo, int64_t hi, unsigned long long* dcount) {
-    FOPIS_CUDA(cudaMemsetAsync(dcount, 0, sizeof(unsigned long long), c.st));
+// Export chunks hold kExportChunk slots; `partial` has kExportTiles + 1 entries.
+constexpr int64_t kExportChunk = 1 << 20;
+constexpr int kExportTiles = (int)((kExportChunk + kScanTile - 1) / kScanTile);
+
+static int64_t export_range(Ctx& c, int s, Rec56* d56, Soa* raw, int64_t lo, int64_t hi, int32_t* partial) {
+    const int tiles = (int)((hi - lo + kScanTile - 1) / kScanTile);
     ++c.launches;
-    export_kernel<<<grid_for(hi - lo), kThreads, 0, c.st>>>(c.sp[s], lo, hi, s, d56, raw ? *raw : Soa{}, dcount);
+    export_count_kernel<<<tiles, kScanThreads, 0, c.st>>>(c.sp[s], lo, hi, partial);
+    ++c.launches;
+    scan_partials_kernel<<<1, kScanThreads, 0, c.st>>>(partial, tiles);
+    ++c.launches;
+    export_kernel<<<tiles, kScanThreads, 0, c.st>>>(c.sp[s], lo, hi, s, d56, raw ? *raw : Soa{}, partial);
     FOPIS_LAUNCH_CHECK();
-    unsigned long long k = 0;
-    FOPIS_CUDA(cudaMemcpyAsync(&k, dcount, sizeof(k), cudaMemcpyDeviceToHost, c.st));
+    int32_t k = 0;
+    FOPIS_CUDA(cudaMemcpyAsync(&k, partial + tiles, sizeof(k), cudaMemcpyDeviceToHost, c.st));
     FOPIS_CUDA(cudaStreamSynchronize(c.st));
     return (int64_t)k;
 }
@@ -1174,11 +1317,11 @@ static int64_t export_range(Ctx& c, int s, Rec56* d56, Soa* raw, int64_t lo, int
 int64_t particles_export_aos(Ctx& c, int s, void* host56, int64_t cap) {
     sync_scalars(c);
     const int64_t n = c.nslots[s];
-    const int64_t chunk = 1 << 20;
+    const int64_t chunk = kExportChunk;
     Rec56* d = nullptr;
-    unsigned long long* dc = nullptr;
+    int32_t* dc = nullptr;
     FOPIS_CUDA(cudaMalloc(&d, sizeof(Rec56) * chunk));
-    FOPIS_CUDA(cudaMalloc(&dc, sizeof(unsigned long long)));
+    FOPIS_CUDA(cudaMalloc(&dc, sizeof(int32_t) * (kExportTiles + 1)));
     int64_t total = 0;
     for (int64_t lo = 0; lo < n; lo += chunk) {
         const int64_t hi = std::min(n, lo + chunk);
@@ -1196,11 +1339,11 @@ int64_t particles_export_raw(Ctx& c, int s, int32_t* cell, float* ox, float* oy,
                              float* vz, int64_t cap) {
     sync_scalars(c);
     const int64_t n = c.nslots[s];
-    const int64_t chunk = 1 << 20;
+    const int64_t chunk = kExportChunk;
     Soa raw{};
     alloc_soa(raw, chunk, c.st);
-    unsigned long long* dc = nullptr;
-    FOPIS_CUDA(cudaMalloc(&dc, sizeof(unsigned long long)));
+    int32_t* dc = nullptr;
+    FOPIS_CUDA(cudaMalloc(&dc, sizeof(int32_t) * (kExportTiles + 1)));
     int64_t total = 0;
     for (int64_t lo = 0; lo < n; lo += chunk) {
         const int64_t hi = std::min(n, lo + chunk);
@@ -1257,44 +1400,48 @@ int brick_count(const Ctx& c) {
     return g.nb[0] * g.nb[1] * g.nb[2];
 }
 
-// Counting sort of every species by brick, then by cell inside the brick
-// (key = brick_key); invalid slots are dropped. Records each brick's first
-// slot for push_tile_kernel.
+// Sort of every species by brick (brick_index), then by cell inside the
+// brick (local_cell); invalid slots are dropped. Records each brick's first slot
+// for push_tile_kernel. The particles end in c.sp[s]; c.sp2[s] holds the
+// brick-grouped intermediate.
 void particles_sort(Ctx& c) {
     sync_scalars(c);
     const Grid g = make_grid(c);
-    const long long K = brick_keys(c);
     const int nbricks = brick_count(c);
-    const int tiles = (int)((K + 1 + kScanTile - 1) / kScanTile);
+    const int tiles = (int)((nbricks + 1 + kScanTile - 1) / kScanTile);
     for (int s = 0; s < c.nsp; ++s) {
         if (c.cap[s] == 0) continue;
         if (!c.brick_start[s]) FOPIS_CUDA(cudaMalloc(&c.brick_start[s], sizeof(int32_t) * (nbricks + 1)));
-        FOPIS_CUDA(cudaMemsetAsync(c.sort_count, 0, sizeof(int32_t) * (K + 1), c.st));
+        FOPIS_CUDA(cudaMemsetAsync(c.sort_count, 0, sizeof(int32_t) * (nbricks + 1), c.st));
         ++c.launches;
         sort_count_kernel<<<grid_for(std::max<int64_t>(c.nslots[s], 1)), kThreads, 0, c.st>>>(
             c.sp[s], c.cap[s], &c.d_sc->count[s], g, c.sort_count);
         FOPIS_LAUNCH_CHECK();
         ++c.launches;
-        scan_tiles_kernel<<<tiles, kScanThreads, 0, c.st>>>(c.sort_count, K + 1, c.scan_partials);
+        scan_tiles_kernel<<<tiles, kScanThreads, 0, c.st>>>(c.sort_count, nbricks + 1, c.scan_partials);
         ++c.launches;
         scan_partials_kernel<<<1, kScanThreads, 0, c.st>>>(c.scan_partials, tiles);
         ++c.launches;
-        scan_apply_kernel<<<tiles, kScanThreads, 0, c.st>>>(c.sort_count, K + 1, c.scan_partials, c.sort_offset);
-        ++c.launches;
-        brick_start_kernel<<<(nbricks + 256) / 256, 256, 0, c.st>>>(c.sort_offset, nbricks, c.brick_start[s]);
+        scan_apply_kernel<<<tiles, kScanThreads, 0, c.st>>>(c.sort_count, nbricks + 1, c.scan_partials,
+                                                            c.brick_start[s]);
         FOPIS_LAUNCH_CHECK();
+        FOPIS_CUDA(cudaMemcpyAsync(c.sort_offset, c.brick_start[s], sizeof(int32_t) * (nbricks + 1),
+                                   cudaMemcpyDeviceToDevice, c.st));
         ++c.launches;
         {
             const long long chunks = (std::max<int64_t>(c.nslots[s], 1) + kSortChunk - 1) / kSortChunk;
             const int grid = (int)std::max<long long>(1, std::min<long long>(chunks, 148LL * 8));
-            sort_scatter_chunk_kernel<<<grid, kSortThreads, 0, c.st>>>(c.sp[s], c.sp2[s], c.cap[s], &c.d_sc->count[s], g,
-                                                                      c.sort_offset);
+            sort_brick_scatter_kernel<<<grid, kSortThreads, 0, c.st>>>(c.sp[s], c.sp2[s], c.cap[s],
+                                                                      &c.d_sc->count[s], g, c.sort_offset);
         }
+        FOPIS_LAUNCH_CHECK();
+        ++c.launches;
+        sort_cell_kernel<<<std::min(nbricks, 148 * 8), kCellThreads, 0, c.st>>>(c.sp2[s], c.sp[s], c.brick_start[s],
+                                                                                nbricks);
         FOPIS_LAUNCH_CHECK();
         // the new count is the total of valid particles: the scan's grand total
         FOPIS_CUDA(cudaMemcpyAsync(&c.d_sc->count[s], c.scan_partials + tiles, sizeof(int32_t), cudaMemcpyDeviceToDevice, c.st));
         FOPIS_CUDA(cudaMemsetAsync(((char*)&c.d_sc->count[s]) + 4, 0, 4, c.st));
-        std::swap(c.sp[s], c.sp2[s]);
     }
     sync_scalars(c);
     for (int s = 0; s < c.nsp; ++s) {
