@@ -97,6 +97,64 @@ __global__ void __launch_bounds__(kRowThreads) rb_smooth_kernel(Lv L, int color)
     }
 }
 
+// The same half sweep for large levels: a block of 32 x 4 threads covers 64
+// columns (one node pair per thread) of 4 rows b, and each thread updates its
+// colour's node at A consecutive a, issuing all loads before the stores.
+constexpr int kMarchX = 32, kMarchY = 4;
+
+__device__ __forceinline__ float march_nsum(const Lv& L, const float* u, int a, int b, int c) {
+    const long long row = ((long long)a * L.n1 + b) * L.n2;
+    const int am = wrap_or_out(a - 1, L.n0, L.p0), ap = wrap_or_out(a + 1, L.n0, L.p0);
+    const int bm = wrap_or_out(b - 1, L.n1, L.p1), bp = wrap_or_out(b + 1, L.n1, L.p1);
+    const int cm = wrap_or_out(c - 1, L.n2, L.p2), cp = wrap_or_out(c + 1, L.n2, L.p2);
+    float s = am >= 0 ? u[((long long)am * L.n1 + b) * L.n2 + c] : 0.0f;
+    s += ap >= 0 ? u[((long long)ap * L.n1 + b) * L.n2 + c] : 0.0f;
+    s += bm >= 0 ? u[((long long)a * L.n1 + bm) * L.n2 + c] : 0.0f;
+    s += bp >= 0 ? u[((long long)a * L.n1 + bp) * L.n2 + c] : 0.0f;
+    s += cm >= 0 ? u[row + cm] : 0.0f;
+    s += cp >= 0 ? u[row + cp] : 0.0f;
+    return s;
+}
+
+template <int A>
+__global__ void __launch_bounds__(kMarchX * kMarchY) rb_march_kernel(Lv L, int color) {
+    const int pair = blockIdx.x * kMarchX + threadIdx.x;
+    const int b = blockIdx.y * kMarchY + threadIdx.y;
+    const int a0 = blockIdx.z * A;
+    if (b >= L.n1) return;
+    float v[A];
+    long long at[A];
+#pragma unroll
+    for (int e = 0; e < A; ++e) {
+        const int a = a0 + e, c = 2 * pair + ((a + b + color) & 1);
+        at[e] = -1;
+        if (a < L.n0 && c < L.n2) {
+            at[e] = ((long long)a * L.n1 + b) * L.n2 + c;
+            v[e] = (1.0f - kOmega) * L.u[at[e]] +
+                   kOmega * (march_nsum(L, L.u, a, b, c) + L.f[at[e]] * L.inv_scale) * (1.0f / 6.0f);
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < A; ++e)
+        if (at[e] >= 0) L.u[at[e]] = v[e];
+}
+
+// r = f - A u for large levels: one node per thread at A consecutive a.
+template <int A>
+__global__ void __launch_bounds__(kMarchX * kMarchY) residual_march_kernel(Lv L) {
+    const int c = blockIdx.x * kMarchX + threadIdx.x;
+    const int b = blockIdx.y * kMarchY + threadIdx.y;
+    const int a0 = blockIdx.z * A;
+    if (b >= L.n1 || c >= L.n2) return;
+#pragma unroll
+    for (int e = 0; e < A; ++e) {
+        const int a = a0 + e;
+        if (a >= L.n0) break;
+        const long long at = ((long long)a * L.n1 + b) * L.n2 + c;
+        L.r[at] = L.f[at] - (6.0f * L.u[at] - march_nsum(L, L.u, a, b, c)) / L.inv_scale;
+    }
+}
+
 // Weighted Jacobi sweep into r, for levels whose periodic axes are odd.
 __global__ void __launch_bounds__(kRowThreads) jacobi_kernel(Lv L, float omega) {
     const int rows = L.n0 * L.n1;
@@ -742,12 +800,46 @@ bool level_rb(const MGLevel& m) {
     return true;
 }
 
+// Levels at least kMarchMin nodes along a use the marching kernels; each
+// thread takes march_depth consecutive a (more per thread on larger levels,
+// where the grid still fills the GPU).
+constexpr int kMarchMin = 24;
+int march_depth(const MGLevel& m) { return m.n[0] >= 96 ? 4 : (m.n[0] >= 48 ? 2 : 1); }
+
+void residual(Ctx& c, const MGLevel& m) {
+    ++c.launches;
+    if (m.n[0] >= kMarchMin) {
+        const int A = march_depth(m);
+        const dim3 blk(kMarchX, kMarchY);
+        const dim3 grd((unsigned)((m.n[2] + kMarchX - 1) / kMarchX), (unsigned)((m.n[1] + kMarchY - 1) / kMarchY),
+                       (unsigned)((m.n[0] + A - 1) / A));
+        if (A == 4) residual_march_kernel<4><<<grd, blk, 0, c.st>>>(lv(m));
+        else if (A == 2) residual_march_kernel<2><<<grd, blk, 0, c.st>>>(lv(m));
+        else residual_march_kernel<1><<<grd, blk, 0, c.st>>>(lv(m));
+    } else {
+        residual_kernel<<<row_blocks((long long)m.n[0] * m.n[1]), std::min(kRowThreads, ((m.n[2] + 31) / 32) * 32), 0,
+                          c.st>>>(lv(m));
+    }
+}
+
 void smooth(Ctx& c, int l, int sweeps) {
     MGLevel& m = c.mg[l];
     const Lv L = lv(m);
     const int rb = row_blocks((long long)m.n[0] * m.n[1]);
     const int th = std::min(kRowThreads, ((m.n[2] + 31) / 32) * 32);
-    if (level_rb(m)) {
+    if (level_rb(m) && m.n[0] >= kMarchMin) {
+        const int A = march_depth(m);
+        const dim3 blk(kMarchX, kMarchY);
+        const dim3 grd((unsigned)((m.n[2] + 2 * kMarchX - 1) / (2 * kMarchX)), (unsigned)((m.n[1] + kMarchY - 1) / kMarchY),
+                       (unsigned)((m.n[0] + A - 1) / A));
+        for (int s = 0; s < sweeps; ++s)
+            for (int color = 0; color < 2; ++color) {
+                ++c.launches;
+                if (A == 4) rb_march_kernel<4><<<grd, blk, 0, c.st>>>(L, color);
+                else if (A == 2) rb_march_kernel<2><<<grd, blk, 0, c.st>>>(L, color);
+                else rb_march_kernel<1><<<grd, blk, 0, c.st>>>(L, color);
+            }
+    } else if (level_rb(m)) {
         const int th2 = std::min(kRowThreads, ((m.n[2] / 2 + 32) / 32) * 32);
         for (int s = 0; s < sweeps; ++s)
             for (int color = 0; color < 2; ++color) {
@@ -792,9 +884,7 @@ void vcycle(Ctx& c, int l) {
     MGLevel& n = c.mg[l + 1];
     FOPIS_CUDA(cudaMemsetAsync(m.u, 0, sizeof(float) * m.size(), c.st));
     smooth(c, l, kPreSweeps);
-    ++c.launches;
-    residual_kernel<<<row_blocks((long long)m.n[0] * m.n[1]), std::min(kRowThreads, ((m.n[2] + 31) / 32) * 32), 0,
-                      c.st>>>(lv(m));
+    residual(c, m);
     ++c.launches;
     restrict_kernel<<<row_blocks((long long)n.n[0] * n.n[1]), std::min(kRowThreads, ((n.n[2] + 31) / 32) * 32), 0,
                       c.st>>>(lv(m), lv(n));
@@ -971,7 +1061,6 @@ void mg_free(Ctx& c) {
 static void ensure_cycle_graph(Ctx& c) {
     if (c.mg_exec) return;
     Outer O = make_outer(c);
-    const long long M = (long long)O.n0 * O.n1 * O.n2;
     const int64_t before = c.launches;
     FOPIS_CUDA(cudaStreamBeginCapture(c.st, cudaStreamCaptureModeThreadLocal));
     try {
