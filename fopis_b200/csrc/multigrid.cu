@@ -155,6 +155,23 @@ __global__ void __launch_bounds__(kMarchX * kMarchY) residual_march_kernel(Lv L)
     }
 }
 
+// The first red half sweep from u = 0, which also zeroes the black nodes: red
+// nodes get omega (f/scale) / 6 (their neighbours are all zero).
+template <int A>
+__global__ void __launch_bounds__(kMarchX * kMarchY) rb_first_march_kernel(Lv L) {
+    const int c = blockIdx.x * kMarchX + threadIdx.x;
+    const int b = blockIdx.y * kMarchY + threadIdx.y;
+    const int a0 = blockIdx.z * A;
+    if (b >= L.n1 || c >= L.n2) return;
+#pragma unroll
+    for (int e = 0; e < A; ++e) {
+        const int a = a0 + e;
+        if (a >= L.n0) break;
+        const long long at = ((long long)a * L.n1 + b) * L.n2 + c;
+        L.u[at] = ((a + b + c) & 1) ? 0.0f : kOmega * (L.f[at] * L.inv_scale) * (1.0f / 6.0f);
+    }
+}
+
 // Weighted Jacobi sweep into r, for levels whose periodic axes are odd.
 __global__ void __launch_bounds__(kRowThreads) jacobi_kernel(Lv L, float omega) {
     const int rows = L.n0 * L.n1;
@@ -252,6 +269,81 @@ __global__ void __launch_bounds__(kRowThreads) prolong_kernel(Lv C, Lv F) {
             F.u[(long long)row * F.n2 + c] += s;
         }
     }
+}
+
+// Full weighting for large levels: one coarse node per thread at A
+// consecutive coarse A.
+template <int A>
+__global__ void __launch_bounds__(kMarchX * kMarchY) restrict_march_kernel(Lv F, Lv C) {
+    const int Cc = blockIdx.x * kMarchX + threadIdx.x;
+    const int B = blockIdx.y * kMarchY + threadIdx.y;
+    const int A0 = blockIdx.z * A;
+    if (B >= C.n1 || Cc >= C.n2) return;
+    const float w[3] = {0.25f, 0.5f, 0.25f};
+    const int fb = fine_of(B, F.p1), fc = fine_of(Cc, F.p2);
+    int bs[3], cs[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { bs[d] = wrap_or_out(fb + d - 1, F.n1, F.p1); cs[d] = wrap_or_out(fc + d - 1, F.n2, F.p2); }
+    float out[A];
+#pragma unroll
+    for (int e = 0; e < A; ++e) {
+        const int Ac = A0 + e;
+        out[e] = 0.0f;
+        if (Ac >= C.n0) continue;
+        const int fa = fine_of(Ac, F.p0);
+        float s = 0.0f;
+#pragma unroll
+        for (int da = 0; da < 3; ++da) {
+            const int a = wrap_or_out(fa + da - 1, F.n0, F.p0);
+            if (a < 0) continue;
+#pragma unroll
+            for (int db = 0; db < 3; ++db) {
+                if (bs[db] < 0) continue;
+                const float* fr = F.r + ((long long)a * F.n1 + bs[db]) * F.n2;
+                const float wab = w[da] * w[db];
+#pragma unroll
+                for (int dc = 0; dc < 3; ++dc)
+                    if (cs[dc] >= 0) s += wab * w[dc] * fr[cs[dc]];
+            }
+        }
+        out[e] = s;
+    }
+#pragma unroll
+    for (int e = 0; e < A; ++e)
+        if (A0 + e < C.n0) C.f[((long long)(A0 + e) * C.n1 + B) * C.n2 + Cc] = out[e];
+}
+
+// Trilinear prolongation for large levels: one fine node per thread at A
+// consecutive fine a.
+template <int A>
+__global__ void __launch_bounds__(kMarchX * kMarchY) prolong_march_kernel(Lv C, Lv F) {
+    const int c = blockIdx.x * kMarchX + threadIdx.x;
+    const int b = blockIdx.y * kMarchY + threadIdx.y;
+    const int a0 = blockIdx.z * A;
+    if (b >= F.n1 || c >= F.n2) return;
+    int Ib[2], Ic[2];
+    float wb[2], wc[2];
+    const int nbv = coarse_src(b, F.p1, C.n1, Ib, wb), nc = coarse_src(c, F.p2, C.n2, Ic, wc);
+    float add[A];
+#pragma unroll
+    for (int e = 0; e < A; ++e) {
+        const int a = a0 + e;
+        add[e] = 0.0f;
+        if (a >= F.n0) continue;
+        int Ia[2];
+        float wa[2];
+        const int na = coarse_src(a, F.p0, C.n0, Ia, wa);
+        float s = 0.0f;
+        for (int x = 0; x < na; ++x)
+            for (int y = 0; y < nbv; ++y) {
+                const float* cr = C.u + ((long long)Ia[x] * C.n1 + Ib[y]) * C.n2;
+                for (int z = 0; z < nc; ++z) s += wa[x] * wb[y] * wc[z] * cr[Ic[z]];
+            }
+        add[e] = s;
+    }
+#pragma unroll
+    for (int e = 0; e < A; ++e)
+        if (a0 + e < F.n0) F.u[((long long)(a0 + e) * F.n1 + b) * F.n2 + c] += add[e];
 }
 
 // Coarsest level in one CTA, FP64 in shared memory: red-black Gauss-Seidel
@@ -806,13 +898,18 @@ bool level_rb(const MGLevel& m) {
 constexpr int kMarchMin = 24;
 int march_depth(const MGLevel& m) { return m.n[0] >= 96 ? 4 : (m.n[0] >= 48 ? 2 : 1); }
 
+// Launch grid of the marching kernels over n[2]/cols_per_thread columns.
+dim3 march_grid(const int n[3], int A, int cols_per_thread) {
+    return dim3((unsigned)((n[2] + cols_per_thread * kMarchX - 1) / (cols_per_thread * kMarchX)),
+                (unsigned)((n[1] + kMarchY - 1) / kMarchY), (unsigned)((n[0] + A - 1) / A));
+}
+
 void residual(Ctx& c, const MGLevel& m) {
     ++c.launches;
     if (m.n[0] >= kMarchMin) {
         const int A = march_depth(m);
         const dim3 blk(kMarchX, kMarchY);
-        const dim3 grd((unsigned)((m.n[2] + kMarchX - 1) / kMarchX), (unsigned)((m.n[1] + kMarchY - 1) / kMarchY),
-                       (unsigned)((m.n[0] + A - 1) / A));
+        const dim3 grd = march_grid(m.n, A, 1);
         if (A == 4) residual_march_kernel<4><<<grd, blk, 0, c.st>>>(lv(m));
         else if (A == 2) residual_march_kernel<2><<<grd, blk, 0, c.st>>>(lv(m));
         else residual_march_kernel<1><<<grd, blk, 0, c.st>>>(lv(m));
@@ -822,19 +919,29 @@ void residual(Ctx& c, const MGLevel& m) {
     }
 }
 
-void smooth(Ctx& c, int l, int sweeps) {
+// `sweeps` red-black sweeps on level l; with from_zero the level's u is
+// first set to zero (on marching levels the first red half sweep does it).
+void smooth(Ctx& c, int l, int sweeps, bool from_zero = false) {
     MGLevel& m = c.mg[l];
     const Lv L = lv(m);
     const int rb = row_blocks((long long)m.n[0] * m.n[1]);
     const int th = std::min(kRowThreads, ((m.n[2] + 31) / 32) * 32);
-    if (level_rb(m) && m.n[0] >= kMarchMin) {
+    const bool march = level_rb(m) && m.n[0] >= kMarchMin;
+    if (from_zero && !march) FOPIS_CUDA(cudaMemsetAsync(m.u, 0, sizeof(float) * m.size(), c.st));
+    if (march) {
         const int A = march_depth(m);
         const dim3 blk(kMarchX, kMarchY);
-        const dim3 grd((unsigned)((m.n[2] + 2 * kMarchX - 1) / (2 * kMarchX)), (unsigned)((m.n[1] + kMarchY - 1) / kMarchY),
-                       (unsigned)((m.n[0] + A - 1) / A));
+        const dim3 grd = march_grid(m.n, A, 2);
         for (int s = 0; s < sweeps; ++s)
             for (int color = 0; color < 2; ++color) {
                 ++c.launches;
+                if (from_zero && s == 0 && color == 0) {
+                    const dim3 g1 = march_grid(m.n, A, 1);
+                    if (A == 4) rb_first_march_kernel<4><<<g1, blk, 0, c.st>>>(L);
+                    else if (A == 2) rb_first_march_kernel<2><<<g1, blk, 0, c.st>>>(L);
+                    else rb_first_march_kernel<1><<<g1, blk, 0, c.st>>>(L);
+                    continue;
+                }
                 if (A == 4) rb_march_kernel<4><<<grd, blk, 0, c.st>>>(L, color);
                 else if (A == 2) rb_march_kernel<2><<<grd, blk, 0, c.st>>>(L, color);
                 else rb_march_kernel<1><<<grd, blk, 0, c.st>>>(L, color);
@@ -882,17 +989,33 @@ void vcycle(Ctx& c, int l) {
     if (l == L - 1) { coarse_solve(c, l); return; }
     MGLevel& m = c.mg[l];
     MGLevel& n = c.mg[l + 1];
-    FOPIS_CUDA(cudaMemsetAsync(m.u, 0, sizeof(float) * m.size(), c.st));
-    smooth(c, l, kPreSweeps);
+    smooth(c, l, kPreSweeps, true);
     residual(c, m);
+    const dim3 blk(kMarchX, kMarchY);
     ++c.launches;
-    restrict_kernel<<<row_blocks((long long)n.n[0] * n.n[1]), std::min(kRowThreads, ((n.n[2] + 31) / 32) * 32), 0,
-                      c.st>>>(lv(m), lv(n));
+    if (n.n[0] >= kMarchMin) {
+        const int A = march_depth(n);
+        const dim3 grd = march_grid(n.n, A, 1);
+        if (A == 4) restrict_march_kernel<4><<<grd, blk, 0, c.st>>>(lv(m), lv(n));
+        else if (A == 2) restrict_march_kernel<2><<<grd, blk, 0, c.st>>>(lv(m), lv(n));
+        else restrict_march_kernel<1><<<grd, blk, 0, c.st>>>(lv(m), lv(n));
+    } else {
+        restrict_kernel<<<row_blocks((long long)n.n[0] * n.n[1]), std::min(kRowThreads, ((n.n[2] + 31) / 32) * 32), 0,
+                          c.st>>>(lv(m), lv(n));
+    }
     FOPIS_LAUNCH_CHECK();
     vcycle(c, l + 1);
     ++c.launches;
-    prolong_kernel<<<row_blocks((long long)m.n[0] * m.n[1]), std::min(kRowThreads, ((m.n[2] + 31) / 32) * 32), 0,
-                     c.st>>>(lv(n), lv(m));
+    if (m.n[0] >= kMarchMin) {
+        const int A = march_depth(m);
+        const dim3 grd = march_grid(m.n, A, 1);
+        if (A == 4) prolong_march_kernel<4><<<grd, blk, 0, c.st>>>(lv(n), lv(m));
+        else if (A == 2) prolong_march_kernel<2><<<grd, blk, 0, c.st>>>(lv(n), lv(m));
+        else prolong_march_kernel<1><<<grd, blk, 0, c.st>>>(lv(n), lv(m));
+    } else {
+        prolong_kernel<<<row_blocks((long long)m.n[0] * m.n[1]), std::min(kRowThreads, ((m.n[2] + 31) / 32) * 32), 0,
+                         c.st>>>(lv(n), lv(m));
+    }
     FOPIS_LAUNCH_CHECK();
     smooth(c, l, kPostSweeps);
 }
