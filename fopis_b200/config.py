@@ -159,7 +159,7 @@ def _species_struct(sp: SpeciesInfo, norm: Normalizer, dx: float) -> _abi.Specie
 def make_params(nxyz: Tuple[int, int, int], boundary: str, dx: float, dt: float, species: List[SpeciesInfo],
                 bfield_nT=(0.0, 0.0, 0.0), shine=(0.0, 0.0, 0.0), seed: int = 12345, tol: float = 1e-8,
                 max_vcycles: int = 100, sort_interval: int = 8, guess: int = _abi.GUESS_WARM,
-                capacity_factor: float = 1.5) -> Tuple[_abi.Params, Normalizer]:
+                capacity_factor: float = 1.5, precision: int = _abi.MIXED) -> Tuple[_abi.Params, Normalizer]:
     norm = Normalizer(dx, dt)
     p = _abi.Params()
     p.nx, p.ny, p.nz = (int(v) for v in nxyz)
@@ -180,7 +180,7 @@ def make_params(nxyz: Tuple[int, int, int], boundary: str, dx: float, dt: float,
     p.sort_interval = sort_interval
     p.remove_interval = 50
     p.capacity_factor = capacity_factor
-    p.precision = _abi.MIXED
+    p.precision = precision
     p.seed = seed
     return p, norm
 

@@ -230,7 +230,9 @@ int fopis_create(const fopis_params* p, int device, void** out) {
             if (b != 'D' && b != 'N' && b != 'P')
                 throw ApiError{FOPIS_ERR_ARG, "Unknown boundary condition type was used"};  // Field.cpp:25-28
         }
-        if (p->precision != FOPIS_MIXED) throw ApiError{FOPIS_ERR_ARG, "only the mixed-precision path is built"};
+        if (p->precision != FOPIS_MIXED && p->precision != FOPIS_FP64)
+            throw ApiError{FOPIS_ERR_ARG, "precision must be FOPIS_MIXED or FOPIS_FP64"};
+        x.fp64 = p->precision == FOPIS_FP64;
         for (int s = 0; s < p->nspecies; ++s)
             if (!(p->species[s].mass > 0.0)) throw ApiError{FOPIS_ERR_ARG, "species mass must be positive"};
         int ndev = 0;
@@ -258,6 +260,10 @@ int fopis_create(const fopis_params* p, int device, void** out) {
         FOPIS_CUDA(cudaMalloc(&x.phi_obj, sizeof(double) * x.N));
         FOPIS_CUDA(cudaMalloc(&x.scratch64, sizeof(double) * x.N));
         FOPIS_CUDA(cudaMalloc(&x.E, sizeof(float4) * x.N));
+        if (x.fp64) {
+            FOPIS_CUDA(cudaMalloc(&x.E64, sizeof(Vec4d) * x.N));
+            FOPIS_CUDA(cudaMemset(x.E64, 0, sizeof(Vec4d) * x.N));
+        }
         FOPIS_CUDA(cudaMalloc(&x.cellmap, x.N));
         FOPIS_CUDA(cudaMalloc(&x.node_cmat, sizeof(int32_t) * x.N));
         const size_t keys = std::max<size_t>(x.N, (size_t)brick_keys(x));
@@ -277,8 +283,8 @@ int fopis_create(const fopis_params* p, int device, void** out) {
         // absorbed list: generous for conductor-heavy steps
         x.ab.cap = std::max<int64_t>(1 << 20, (int64_t)x.N / 2);
         FOPIS_CUDA(cudaMalloc(&x.ab.cell, sizeof(int32_t) * x.ab.cap));
-        float** fl[6] = {&x.ab.ox, &x.ab.oy, &x.ab.oz, &x.ab.vx, &x.ab.vy, &x.ab.vz};
-        for (auto* q : fl) FOPIS_CUDA(cudaMalloc(q, sizeof(float) * x.ab.cap));
+        double** fl[6] = {&x.ab.ox, &x.ab.oy, &x.ab.oz, &x.ab.vx, &x.ab.vy, &x.ab.vz};
+        for (auto* q : fl) FOPIS_CUDA(cudaMalloc(q, sizeof(double) * x.ab.cap));
         FOPIS_CUDA(cudaMalloc(&x.ab.species, x.ab.cap));
         FOPIS_CUDA(cudaMalloc(&x.ab.object, x.ab.cap));
         FOPIS_CUDA(cudaMalloc(&x.d_sc, sizeof(DevScalars)));
@@ -311,6 +317,11 @@ void fopis_destroy(void* h) {
             void* arr[7] = {q->cell, q->ox, q->oy, q->oz, q->vx, q->vy, q->vz};
             for (void* a : arr) if (a) cudaFreeAsync(a, c->st);
         }
+        Soa64* w[2] = {&c->dp[s], &c->dp2[s]};
+        for (Soa64* q : w) {
+            void* arr[7] = {q->cell, q->ox, q->oy, q->oz, q->vx, q->vy, q->vz};
+            for (void* a : arr) if (a) cudaFreeAsync(a, c->st);
+        }
     }
     if (c->st) cudaStreamSynchronize(c->st);
     for (int s = 0; s < FOPIS_MAX_SPECIES; ++s) if (c->brick_start[s]) cudaFree(c->brick_start[s]);
@@ -319,7 +330,7 @@ void fopis_destroy(void* h) {
         cudaFree(o.charge_map); cudaFree(o.phis); cudaFree(o.scal); cudaFree(o.lit);
     }
     mg_free(*c);
-    void* ptrs[] = {c->rho_i64, c->rho0, c->phi, c->phi_prev, c->phi_prev2, c->phi_obj, c->scratch64, c->E, c->cellmap,
+    void* ptrs[] = {c->rho_i64, c->rho0, c->phi, c->phi_prev, c->phi_prev2, c->phi_obj, c->scratch64, c->E, c->E64, c->cellmap,
                     c->node_cmat, c->sort_count, c->sort_offset, c->scan_partials, c->ab.cell, c->ab.ox,
                     c->ab.oy, c->ab.oz, c->ab.vx, c->ab.vy, c->ab.vz, c->ab.species, c->ab.object, c->d_sc};
     for (void* q : ptrs) if (q) cudaFree(q);
@@ -414,6 +425,7 @@ int fopis_get_particles_raw(void* h, int s, int32_t* cell, float* ox, float* oy,
     return guarded(h, [&](Ctx& c) -> int {
         if (s < 0 || s >= c.nsp) throw ApiError{FOPIS_ERR_ARG, "species"};
         if (cap > 0 && !(cell && ox && oy && oz && vx && vy && vz)) throw ApiError{FOPIS_ERR_ARG, "buffers"};
+        if (c.fp64) throw ApiError{FOPIS_ERR_ARG, "raw split-precision state exists only in the mixed mode"};
         const int64_t n = c.cap[s] ? particles_export_raw(c, s, cell, ox, oy, oz, vx, vy, vz, cap) : 0;
         if (n_out) *n_out = n;
         return FOPIS_OK;

@@ -34,7 +34,8 @@ int blocks(long long n) {
 // MPIw::Environment::sendRecvNodeScalar self-exchange, glue size 2
 // (src/MPI/Communicator.cpp:497-574): node 0 and node n both become their sum,
 // node 1 and node n+1 likewise.
-__global__ void fold_kernel(unsigned long long* rho, int nsp, long long N, G g, int axis) {
+template <typename W>
+__global__ void fold_kernel(W* rho, int nsp, long long N, G g, int axis) {
     const int dims[3] = {g.cx, g.cy, g.cz};
     const int a1 = axis == 0 ? 1 : 0, a2 = axis == 2 ? 1 : 2;
     const long long plane = (long long)dims[a1] * dims[a2];
@@ -45,31 +46,38 @@ __global__ void fold_kernel(unsigned long long* rho, int nsp, long long N, G g, 
         int idx[3];
         idx[a1] = (int)(r / dims[a2]);
         idx[a2] = (int)(r % dims[a2]);
-        unsigned long long* a = rho + (long long)s * N;
+        W* a = rho + (long long)s * N;
         const int X = dims[axis];
         idx[axis] = 0; const long long p0 = L(g, idx[0], idx[1], idx[2]);
         idx[axis] = X - 2; const long long pn = L(g, idx[0], idx[1], idx[2]);
         idx[axis] = 1; const long long p1 = L(g, idx[0], idx[1], idx[2]);
         idx[axis] = X - 1; const long long pn1 = L(g, idx[0], idx[1], idx[2]);
-        const unsigned long long s0 = a[p0] + a[pn], s1 = a[p1] + a[pn1];
+        const W s0 = a[p0] + a[pn], s1 = a[p1] + a[pn1];
         a[p0] = s0; a[pn] = s0; a[p1] = s1; a[pn1] = s1;
     }
 }
 
 struct Scales { double v[FOPIS_MAX_SPECIES]; };
 
-// rho[0] = sum_s q_s size_s W_s 2^-51 (RootGridField.cpp:1206-1214).
-__global__ void convert_kernel(const unsigned long long* rho, int nsp, long long N, Scales sc, double* rho0) {
+// A species accumulator as a number: int64 fixed point (mixed mode) or the
+// FP64 weight sum (FP64 mode).
+__device__ __forceinline__ double weight_value(unsigned long long w) { return (double)(long long)w; }
+__device__ __forceinline__ double weight_value(double w) { return w; }
+
+// rho[0] = sum_s q_s size_s W_s (x 2^-51 in fixed point) (RootGridField.cpp:1206-1214).
+template <typename W>
+__global__ void convert_kernel(const W* rho, int nsp, long long N, Scales sc, double* rho0) {
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
         double r = 0.0;
-        for (int s = 0; s < nsp; ++s) r += sc.v[s] * (double)(long long)rho[(long long)s * N + t];
+        for (int s = 0; s < nsp; ++s) r += sc.v[s] * weight_value(rho[(long long)s * N + t]);
         rho0[t] = r;
     }
 }
 
-__global__ void convert_species_kernel(const unsigned long long* rho, long long N, double scale, double* out) {
+template <typename W>
+__global__ void convert_species_kernel(const W* rho, long long N, double scale, double* out) {
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x)
-        out[t] = scale * (double)(long long)rho[t];
+        out[t] = scale * weight_value(rho[t]);
 }
 
 // Glue copy of one axis: node 0 <- node n, node n+1 <- node 1
@@ -117,6 +125,11 @@ __device__ __forceinline__ int wrapi(const G& g, int axis, int idx) {
     return idx;
 }
 
+__device__ __forceinline__ void store_e(float4* o, const double e[3]) {
+    *o = make_float4((float)e[0], (float)e[1], (float)e[2], 0.0f);
+}
+__device__ __forceinline__ void store_e(Vec4d* o, const double e[3]) { *o = Vec4d{e[0], e[1], e[2], 0.0}; }
+
 // Nodal E of RootGrid::updateEfield + updateReferenceEfield
 // (RootGridField.cpp:456-582): centred 0.5 (phi[i-1] - phi[i+1]) per axis,
 // one-sided second order on Dirichlet/Neumann faces, zero glue on those axes,
@@ -154,7 +167,7 @@ __global__ void efield_kernel(const double* phi, G g, Out* out, double* outx, do
                 }
             }
         }
-        if (out) out[t] = make_float4((float)e[0], (float)e[1], (float)e[2], 0.0f);
+        if (out) store_e(out + t, e);
         if (outx) { outx[t] = e[0]; outy[t] = e[1]; outz[t] = e[2]; }
     }
 }
@@ -201,6 +214,12 @@ __global__ void sum_partials_kernel(const double* partial, int n, double* out) {
 
 }  // namespace
 
+// Charge of one unit of a species' accumulator: q size 2^-51 for the
+// fixed-point weights, q size for the FP64 weights.
+double species_rho_scale(const Ctx& c, int s) {
+    return c.p.species[s].charge * c.p.species[s].size * (c.fp64 ? 1.0 : kDepositUnit);
+}
+
 void rho_zero(Ctx& c) {
     FOPIS_CUDA(cudaMemsetAsync(c.rho_i64, 0, sizeof(unsigned long long) * c.N * c.nsp, c.st));
 }
@@ -222,13 +241,21 @@ void rho_finalize(Ctx& c) {
     for (int axis = 0; axis < 3; ++axis) {
         if (!c.per[2 * axis]) continue;
         ++c.launches;
-        fold_kernel<<<blocks(planes[axis] * c.nsp), kT, 0, c.st>>>(c.rho_i64, c.nsp, (long long)c.N, g, axis);
+        if (c.fp64)
+            fold_kernel<<<blocks(planes[axis] * c.nsp), kT, 0, c.st>>>(reinterpret_cast<double*>(c.rho_i64), c.nsp,
+                                                                       (long long)c.N, g, axis);
+        else
+            fold_kernel<<<blocks(planes[axis] * c.nsp), kT, 0, c.st>>>(c.rho_i64, c.nsp, (long long)c.N, g, axis);
         FOPIS_LAUNCH_CHECK();
     }
     Scales sc{};
-    for (int s = 0; s < c.nsp; ++s) sc.v[s] = c.p.species[s].charge * c.p.species[s].size * kDepositUnit;
+    for (int s = 0; s < c.nsp; ++s) sc.v[s] = species_rho_scale(c, s);
     ++c.launches;
-    convert_kernel<<<blocks((long long)c.N), kT, 0, c.st>>>(c.rho_i64, c.nsp, (long long)c.N, sc, c.rho0);
+    if (c.fp64)
+        convert_kernel<<<blocks((long long)c.N), kT, 0, c.st>>>(reinterpret_cast<const double*>(c.rho_i64), c.nsp,
+                                                                (long long)c.N, sc, c.rho0);
+    else
+        convert_kernel<<<blocks((long long)c.N), kT, 0, c.st>>>(c.rho_i64, c.nsp, (long long)c.N, sc, c.rho0);
     FOPIS_LAUNCH_CHECK();
 }
 
@@ -250,7 +277,8 @@ void phi_boundary(Ctx& c) {
 void efield_update(Ctx& c) {
     const G g = make_g(c);
     ++c.launches;
-    efield_kernel<float4><<<blocks((long long)c.N), kT, 0, c.st>>>(c.phi, g, c.E, nullptr, nullptr, nullptr);
+    if (c.fp64) efield_kernel<Vec4d><<<blocks((long long)c.N), kT, 0, c.st>>>(c.phi, g, c.E64, nullptr, nullptr, nullptr);
+    else efield_kernel<float4><<<blocks((long long)c.N), kT, 0, c.st>>>(c.phi, g, c.E, nullptr, nullptr, nullptr);
     FOPIS_LAUNCH_CHECK();
 }
 
@@ -271,10 +299,14 @@ void field_export(Ctx& c, int which, double* host) {
         FOPIS_CUDA(cudaFreeAsync(tmp, c.st));
     } else if (which >= FOPIS_FIELD_RHO_SPECIES && which < FOPIS_FIELD_RHO_SPECIES + c.nsp) {
         const int s = which - FOPIS_FIELD_RHO_SPECIES;
-        const double scale = c.p.species[s].charge * c.p.species[s].size * kDepositUnit;
+        const double scale = species_rho_scale(c, s);
         ++c.launches;
-        convert_species_kernel<<<blocks((long long)c.N), kT, 0, c.st>>>(c.rho_i64 + (size_t)s * c.N, (long long)c.N, scale,
-                                                                       c.scratch64);
+        if (c.fp64)
+            convert_species_kernel<<<blocks((long long)c.N), kT, 0, c.st>>>(
+                reinterpret_cast<const double*>(c.rho_i64) + (size_t)s * c.N, (long long)c.N, scale, c.scratch64);
+        else
+            convert_species_kernel<<<blocks((long long)c.N), kT, 0, c.st>>>(c.rho_i64 + (size_t)s * c.N, (long long)c.N,
+                                                                           scale, c.scratch64);
         FOPIS_LAUNCH_CHECK();
         FOPIS_CUDA(cudaMemcpyAsync(host, c.scratch64, bytes, cudaMemcpyDeviceToHost, c.st));
     } else {

@@ -88,11 +88,19 @@ __device__ __forceinline__ void box_muller(double u1, double u2, double& n0, dou
 }
 
 // ------------------------------------------------------------------ device data
-struct Soa {
+// Particles of one species as structure of arrays: packed node cell plus
+// in-cell offsets and velocities, FP32 in the mixed mode, FP64 in FOPIS_FP64.
+template <typename T>
+struct SoaT {
     int32_t* cell = nullptr;
-    float *ox = nullptr, *oy = nullptr, *oz = nullptr;
-    float *vx = nullptr, *vy = nullptr, *vz = nullptr;
+    T *ox = nullptr, *oy = nullptr, *oz = nullptr;
+    T *vx = nullptr, *vy = nullptr, *vz = nullptr;
 };
+using Soa = SoaT<float>;
+using Soa64 = SoaT<double>;
+
+// Nodal E of the FP64 mode (one 32-byte record per node; w unused).
+struct alignas(32) Vec4d { double x, y, z, w; };
 
 // Scalars the kernels update; one copy lives on the device and is mirrored to
 // pinned host memory after each API call.
@@ -109,10 +117,11 @@ struct DevScalars {
     double red[16];                                     // scratch reduction slots
 };
 
-// Absorbed-particle list, written by the deposit paths, read by absorb_kernel.
+// Absorbed-particle list, written by the deposit paths, read by absorb_kernel
+// (FP64 so that both particle precisions store their state exactly).
 struct AbsorbList {
     int32_t* cell = nullptr;
-    float *ox = nullptr, *oy = nullptr, *oz = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;
+    double *ox = nullptr, *oy = nullptr, *oz = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;
     uint8_t* species = nullptr;
     uint8_t* object = nullptr;
     int64_t cap = 0;
@@ -159,14 +168,17 @@ struct Ctx {
     int per[6] = {0};             // isNotBoundary per side
     int nsp = 0;
     // particles
+    bool fp64 = false;            // FOPIS_FP64: particles in dp/dp2, E in E64
     Soa sp[FOPIS_MAX_SPECIES];
     Soa sp2[FOPIS_MAX_SPECIES];   // sort targets
+    Soa64 dp[FOPIS_MAX_SPECIES];
+    Soa64 dp2[FOPIS_MAX_SPECIES];
     int64_t cap[FOPIS_MAX_SPECIES] = {0};
     int64_t nslots[FOPIS_MAX_SPECIES] = {0};   // host mirror of DevScalars::count
     int64_t sorted_n[FOPIS_MAX_SPECIES] = {0}; // slots [0, sorted_n) are brick-sorted
     int32_t* brick_start[FOPIS_MAX_SPECIES] = {nullptr};  // first slot of each brick
     // fields
-    unsigned long long* rho_i64 = nullptr;  // [nsp][N] two's complement fixed point
+    unsigned long long* rho_i64 = nullptr;  // [nsp][N] two's complement fixed point (FP64 mode: double weights)
     double* rho0 = nullptr;
     double* phi = nullptr;
     double* phi_prev = nullptr;      // first-solve phi of the previous step
@@ -174,6 +186,7 @@ struct Ctx {
     double* phi_obj = nullptr;       // previous step's conductor response
     double* scratch64 = nullptr;     // [N] residual / field export
     float4* E = nullptr;             // nodal E (FP32) for the gather
+    Vec4d* E64 = nullptr;            // nodal E (FP64) for the gather of the FP64 mode
     uint8_t* cellmap = nullptr;      // [N] object id + 1 of the node cell, 0 outside
     int32_t* node_cmat = nullptr;    // [N] (object << 24) | cmat, -1 elsewhere
     // sort
@@ -243,6 +256,7 @@ void sync_scalars(Ctx& c);
 // fields.cu
 void rho_zero(Ctx& c);
 void rho_finalize(Ctx& c);
+double species_rho_scale(const Ctx& c, int s);
 void efield_update(Ctx& c);
 void field_export(Ctx& c, int which, double* host);
 double efield_energy(Ctx& c);

@@ -57,12 +57,13 @@ __device__ __forceinline__ long long lin(const Grid& g, int i, int j, int k) {
 // the coordinate is (ci-1)+o. Restates RootGrid::checkX/Y/ZBoundary
 // (include/grid.hpp:309-395) plus the single-rank periodic migration
 // (src/Grid/GridParticleTreatmentES.cpp:115-177). Returns false to invalidate.
-__device__ __forceinline__ bool axis_boundary(const Grid& g, int axis, int& ci, float o) {
+template <typename T>
+__device__ __forceinline__ bool axis_boundary(const Grid& g, int axis, int& ci, T o) {
     const int n = g.n[axis];
     if (ci <= 0) {                                 // x < 0
         if (g.per[2 * axis]) { if (ci <= -1) ci += n; }   // x < -1 -> x + sl
         else return false;
-    } else if (ci > n || (ci == n && o > 0.0f)) {  // x > sl - 1
+    } else if (ci > n || (ci == n && o > (T)0)) {  // x > sl - 1
         if (g.per[2 * axis + 1]) { if (ci >= n + 1) ci -= n; }  // x >= sl -> x - sl
         else return false;
     }
@@ -82,12 +83,26 @@ __device__ __forceinline__ bool axis_boundary_d(const Grid& g, int axis, double&
     return true;
 }
 
-// Split an FP64 coordinate into node cell index and FP32 offset.
-__device__ __forceinline__ void split(double x, int& ci, float& o) {
+// Split an FP64 coordinate into node cell index and in-cell offset (FP32 in
+// the mixed mode, where rounding can reach 1 and carries into the cell).
+template <typename T>
+__device__ __forceinline__ void split(double x, int& ci, T& o) {
     const double f = floor(x);
     ci = (int)f + 1;
-    o = (float)(x - f);
-    if (o >= 1.0f) { o = 0.0f; ci += 1; }
+    o = (T)(x - f);
+    if (o >= (T)1) { o = (T)0; ci += 1; }
+}
+
+// FP64 CIC deposit of the FP64 mode: the eight corner weights of a particle
+// (corner order of corner_offset) added to the species' FP64 weight sums.
+__device__ __forceinline__ void deposit_f64(double* rho, long long base, const long long off[8], double ox, double oy,
+                                            double oz) {
+    const double wx[2] = {1.0 - ox, ox}, wy[2] = {1.0 - oy, oy}, wz[2] = {1.0 - oz, oz};
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        const double w = wx[t >> 2] * wy[(t >> 1) & 1] * wz[t & 1];
+        if (w != 0.0) atomicAdd(rho + base + off[t], w);
+    }
 }
 
 __device__ __forceinline__ bool cell_in_range(const Grid& g, int i, int j, int k) {
@@ -179,49 +194,65 @@ __device__ __forceinline__ double block_sum(double v) {
     return v;
 }
 
-struct PushArgs {
-    Soa p;
+template <typename T> struct NodeE;
+template <> struct NodeE<float> { using type = float4; };
+template <> struct NodeE<double> { using type = Vec4d; };
+__device__ __forceinline__ float4 load_e(const float4* p) { return __ldg(p); }
+__device__ __forceinline__ Vec4d load_e(const Vec4d* p) { return *p; }
+
+template <typename T>
+struct PushArgsT {
+    SoaT<T> p;
     int s;
     long long cap;
     long long lo;             // first slot of the pass (the unsorted tail in the fused step)
     const unsigned long long* count;
-    const float4* E;
+    const typename NodeE<T>::type* E;
     Grid g;
-    float qm;                 // 0.5 q/m
-    float bx, by, bz, boris;  // static B as the reference uses it, 2/(1+|b|^2)
+    T qm;                     // 0.5 q/m
+    T bx, by, bz, boris;      // static B as the reference uses it, 2/(1+|b|^2)
     const uint8_t* cellmap;   // nullptr without objects
-    unsigned long long* rho;  // species rho (fixed point)
+    unsigned long long* rho;  // species accumulator: int64 fixed point, or FP64 weights in the FP64 mode
     AbsorbList ab;
     DevScalars* sc;
 };
+using PushArgs = PushArgsT<float>;
 
-struct PState {
+template <typename T>
+struct PStateT {
     int i, j, k;
-    float ox, oy, oz, vx, vy, vz;
+    T ox, oy, oz, vx, vy, vz;
 };
+using PState = PStateT<float>;
+
+__device__ __forceinline__ float floor_of(float x) { return floorf(x); }
+__device__ __forceinline__ double floor_of(double x) { return floor(x); }
+__device__ __forceinline__ int int_of(float x) { return __float2int_rd(x); }
+__device__ __forceinline__ int int_of(double x) { return __double2int_rd(x); }
 
 // CIC gather of nodal E and the Boris kick/rotate/kick of
 // Grid::updateParticleVelocityES (GridParticleTreatmentES.cpp:13-88): weights
 // qm dx2 dy2 dz2 ... on the eight nodes, B used as given.
-__device__ __forceinline__ void gather_boris(const PushArgs& a, PState& s) {
+template <typename T>
+__device__ __forceinline__ void gather_boris(const PushArgsT<T>& a, PStateT<T>& s) {
     const long long b = lin(a.g, s.i, s.j, s.k);
-    const float x1 = s.ox, x2 = 1.0f - s.ox, y1 = s.oy, y2 = 1.0f - s.oy, z1 = s.oz, z2 = 1.0f - s.oz;
-    const float4 e000 = __ldg(a.E + b), e001 = __ldg(a.E + b + 1);
-    const float4 e010 = __ldg(a.E + b + a.g.sj), e011 = __ldg(a.E + b + a.g.sj + 1);
-    const float4 e100 = __ldg(a.E + b + a.g.si), e101 = __ldg(a.E + b + a.g.si + 1);
-    const float4 e110 = __ldg(a.E + b + a.g.si + a.g.sj), e111 = __ldg(a.E + b + a.g.si + a.g.sj + 1);
-    const float w000 = x2 * y2 * z2, w100 = x1 * y2 * z2, w010 = x2 * y1 * z2, w110 = x1 * y1 * z2;
-    const float w001 = x2 * y2 * z1, w101 = x1 * y2 * z1, w011 = x2 * y1 * z1, w111 = x1 * y1 * z1;
-    const float ex = a.qm * (w000 * e000.x + w100 * e100.x + w010 * e010.x + w110 * e110.x +
-                             w001 * e001.x + w101 * e101.x + w011 * e011.x + w111 * e111.x);
-    const float ey = a.qm * (w000 * e000.y + w100 * e100.y + w010 * e010.y + w110 * e110.y +
-                             w001 * e001.y + w101 * e101.y + w011 * e011.y + w111 * e111.y);
-    const float ez = a.qm * (w000 * e000.z + w100 * e100.z + w010 * e010.z + w110 * e110.z +
-                             w001 * e001.z + w101 * e101.z + w011 * e011.z + w111 * e111.z);
-    const float vx1 = s.vx + ex, vy1 = s.vy + ey, vz1 = s.vz + ez;
-    const float vxt = vx1 + vy1 * a.bz - vz1 * a.by;
-    const float vyt = vy1 + vz1 * a.bx - vx1 * a.bz;
-    const float vzt = vz1 + vx1 * a.by - vy1 * a.bx;
+    const T x1 = s.ox, x2 = (T)1 - s.ox, y1 = s.oy, y2 = (T)1 - s.oy, z1 = s.oz, z2 = (T)1 - s.oz;
+    const auto e000 = load_e(a.E + b), e001 = load_e(a.E + b + 1);
+    const auto e010 = load_e(a.E + b + a.g.sj), e011 = load_e(a.E + b + a.g.sj + 1);
+    const auto e100 = load_e(a.E + b + a.g.si), e101 = load_e(a.E + b + a.g.si + 1);
+    const auto e110 = load_e(a.E + b + a.g.si + a.g.sj), e111 = load_e(a.E + b + a.g.si + a.g.sj + 1);
+    const T w000 = x2 * y2 * z2, w100 = x1 * y2 * z2, w010 = x2 * y1 * z2, w110 = x1 * y1 * z2;
+    const T w001 = x2 * y2 * z1, w101 = x1 * y2 * z1, w011 = x2 * y1 * z1, w111 = x1 * y1 * z1;
+    const T ex = a.qm * (w000 * e000.x + w100 * e100.x + w010 * e010.x + w110 * e110.x +
+                         w001 * e001.x + w101 * e101.x + w011 * e011.x + w111 * e111.x);
+    const T ey = a.qm * (w000 * e000.y + w100 * e100.y + w010 * e010.y + w110 * e110.y +
+                         w001 * e001.y + w101 * e101.y + w011 * e011.y + w111 * e111.y);
+    const T ez = a.qm * (w000 * e000.z + w100 * e100.z + w010 * e010.z + w110 * e110.z +
+                         w001 * e001.z + w101 * e101.z + w011 * e011.z + w111 * e111.z);
+    const T vx1 = s.vx + ex, vy1 = s.vy + ey, vz1 = s.vz + ez;
+    const T vxt = vx1 + vy1 * a.bz - vz1 * a.by;
+    const T vyt = vy1 + vz1 * a.bx - vx1 * a.bz;
+    const T vzt = vz1 + vx1 * a.by - vy1 * a.bx;
     s.vx = vx1 + (ex + a.boris * (vyt * a.bz - vzt * a.by));
     s.vy = vy1 + (ey + a.boris * (vzt * a.bx - vxt * a.bz));
     s.vz = vz1 + (ez + a.boris * (vxt * a.by - vyt * a.bx));
@@ -230,11 +261,12 @@ __device__ __forceinline__ void gather_boris(const PushArgs& a, PState& s) {
 // x += v with the cell carry, then the boundary rules; false invalidates.
 // Cells 1..n-1 of every axis are away from both faces (the rules only act on
 // cells <= 0 and >= n), so most particles skip them.
-__device__ __forceinline__ bool move_boundary(const PushArgs& a, PState& s) {
+template <typename T>
+__device__ __forceinline__ bool move_boundary(const PushArgsT<T>& a, PStateT<T>& s) {
     s.ox += s.vx; s.oy += s.vy; s.oz += s.vz;
-    const float fx = floorf(s.ox), fy = floorf(s.oy), fz = floorf(s.oz);
+    const T fx = floor_of(s.ox), fy = floor_of(s.oy), fz = floor_of(s.oz);
     s.ox -= fx; s.oy -= fy; s.oz -= fz;
-    s.i += __float2int_rd(fx); s.j += __float2int_rd(fy); s.k += __float2int_rd(fz);
+    s.i += int_of(fx); s.j += int_of(fy); s.k += int_of(fz);
     if ((unsigned)(s.i - 1) < (unsigned)(a.g.n[0] - 1) && (unsigned)(s.j - 1) < (unsigned)(a.g.n[1] - 1) &&
         (unsigned)(s.k - 1) < (unsigned)(a.g.n[2] - 1))
         return true;
@@ -249,7 +281,8 @@ __device__ __forceinline__ bool move_boundary(const PushArgs& a, PState& s) {
 
 // Body test and absorbed-list append of RootGrid::updateRho's per-particle
 // part (RootGridField.cpp:1173-1178); every lane of the warp calls it.
-__device__ __forceinline__ bool absorb_check(const PushArgs& a, const PState& s, bool live) {
+template <typename T>
+__device__ __forceinline__ bool absorb_check(const PushArgsT<T>& a, const PStateT<T>& s, bool live) {
     uint8_t ob = 0;
     if (live && a.cellmap) ob = a.cellmap[lin(a.g, s.i, s.j, s.k)];
     const bool absorbed = ob != 0;
@@ -277,8 +310,8 @@ __device__ __forceinline__ bool absorb_check(const PushArgs& a, const PState& s,
 // Spacecraft.cpp:512-592, finished by absorb_kernel); the rest deposit their CIC
 // weights with warp-aggregated atomics. The fused step runs it only on the
 // unsorted tail; push_tile_kernel takes the sorted bricks.
-template <bool VEL, bool POS, bool DEP>
-__global__ void __launch_bounds__(kThreads) push_kernel(PushArgs a) {
+template <typename T, bool VEL, bool POS, bool DEP>
+__global__ void __launch_bounds__(kThreads) push_kernel(PushArgsT<T> a) {
     const long long n = (long long)min(*a.count, (unsigned long long)a.cap);
     const long long stride = (long long)gridDim.x * blockDim.x;
     double e2 = 0.0;
@@ -287,7 +320,7 @@ __global__ void __launch_bounds__(kThreads) push_kernel(PushArgs a) {
         const bool inb = idx < n;
         const int32_t cell = inb ? a.p.cell[idx] : -1;
         bool live = cell >= 0;
-        PState st{0, 0, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        PStateT<T> st{0, 0, 0, (T)0, (T)0, (T)0, (T)0, (T)0, (T)0};
         if (live) {
             unpack_cell(cell, st.i, st.j, st.k);
             st.ox = a.p.ox[idx]; st.oy = a.p.oy[idx]; st.oz = a.p.oz[idx];
@@ -297,7 +330,14 @@ __global__ void __launch_bounds__(kThreads) push_kernel(PushArgs a) {
         if (POS && live) live = move_boundary(a, st);
         if (DEP) {
             if (absorb_check(a, st, live)) live = false;
-            warp_deposit(a.rho, a.g, live, live ? lin(a.g, st.i, st.j, st.k) : 0, st.ox, st.oy, st.oz);
+            if constexpr (sizeof(T) == 4) {
+                warp_deposit(a.rho, a.g, live, live ? lin(a.g, st.i, st.j, st.k) : 0, st.ox, st.oy, st.oz);
+            } else if (live) {
+                long long off[8];
+#pragma unroll
+                for (int t = 0; t < 8; ++t) off[t] = corner_offset(a.g, t);
+                deposit_f64(reinterpret_cast<double*>(a.rho), lin(a.g, st.i, st.j, st.k), off, st.ox, st.oy, st.oz);
+            }
             if (live && VEL) e2 += (double)st.vx * st.vx + (double)st.vy * st.vy + (double)st.vz * st.vz;
         }
         if (inb && cell >= 0) {
@@ -479,15 +519,17 @@ __global__ void __launch_bounds__(kTileThreads, MINB) push_tile_kernel(PushArgs 
 }
 
 // Writes a particle created in FP64 into a species slot (split precision).
-__device__ __forceinline__ void store_split(Soa p, long long slot, int i, int j, int k, float ox, float oy, float oz,
+template <typename T>
+__device__ __forceinline__ void store_split(SoaT<T> p, long long slot, int i, int j, int k, T ox, T oy, T oz,
                                             double vx, double vy, double vz) {
     p.cell[slot] = pack_cell(i, j, k);
     p.ox[slot] = ox; p.oy[slot] = oy; p.oz[slot] = oz;
-    p.vx[slot] = (float)vx; p.vy[slot] = (float)vy; p.vz[slot] = (float)vz;
+    p.vx[slot] = (T)vx; p.vy[slot] = (T)vy; p.vz[slot] = (T)vz;
 }
 
-struct SourceArgs {
-    Soa p[FOPIS_MAX_SPECIES];
+template <typename T>
+struct SourceArgsT {
+    SoaT<T> p[FOPIS_MAX_SPECIES];
     long long cap[FOPIS_MAX_SPECIES];
     Grid g;
     const uint8_t* cellmap;
@@ -504,11 +546,12 @@ struct SourceArgs {
 // active lane of the warp calls it: slots are reserved with one atomic per
 // species per warp, and the kinetic energy goes to the block's accumulator
 // s_energy (flushed once per block by the caller).
-__device__ void finish_source(const SourceArgs& a, int s, double x, double y, double z, double vx, double vy,
+template <typename T>
+__device__ void finish_source(const SourceArgsT<T>& a, int s, double x, double y, double z, double vx, double vy,
                               double vz, bool move, bool want, double* s_energy) {
     bool live = want;
     int i = 0, j = 0, k = 0;
-    float ox = 0.f, oy = 0.f, oz = 0.f;
+    T ox = (T)0, oy = (T)0, oz = (T)0;
     if (live && a.fused && move) {
         x += vx; y += vy; z += vz;
         live = axis_boundary_d(a.g, 0, x) && axis_boundary_d(a.g, 1, y) && axis_boundary_d(a.g, 2, z);
@@ -524,7 +567,7 @@ __device__ void finish_source(const SourceArgs& a, int s, double x, double y, do
         if ((long long)slot < a.ab.cap) {
             a.ab.cell[slot] = pack_cell(i, j, k);
             a.ab.ox[slot] = ox; a.ab.oy[slot] = oy; a.ab.oz[slot] = oz;
-            a.ab.vx[slot] = (float)vx; a.ab.vy[slot] = (float)vy; a.ab.vz[slot] = (float)vz;
+            a.ab.vx[slot] = (T)vx; a.ab.vy[slot] = (T)vy; a.ab.vz[slot] = (T)vz;
             a.ab.species[slot] = (uint8_t)s;
             a.ab.object[slot] = (uint8_t)(a.cellmap[lin(a.g, i, j, k)] - 1);
         } else {
@@ -533,13 +576,20 @@ __device__ void finish_source(const SourceArgs& a, int s, double x, double y, do
         live = false;
     }
     if (live && a.fused) {
-        unsigned long long w[8];
-        corner_weights(ox, oy, oz, w);
-        unsigned long long* rho = a.rho + (long long)s * a.N;
         const long long b = lin(a.g, i, j, k);
+        if constexpr (sizeof(T) == 4) {
+            unsigned long long w[8];
+            corner_weights(ox, oy, oz, w);
+            unsigned long long* rho = a.rho + (long long)s * a.N;
 #pragma unroll
-        for (int t = 0; t < 8; ++t) if (w[t]) atomicAdd(rho + b + corner_offset(a.g, t), w[t]);
-        const float fx = (float)vx, fy = (float)vy, fz = (float)vz;
+            for (int t = 0; t < 8; ++t) if (w[t]) atomicAdd(rho + b + corner_offset(a.g, t), w[t]);
+        } else {
+            long long off[8];
+#pragma unroll
+            for (int t = 0; t < 8; ++t) off[t] = corner_offset(a.g, t);
+            deposit_f64(reinterpret_cast<double*>(a.rho) + (long long)s * a.N, b, off, ox, oy, oz);
+        }
+        const T fx = (T)vx, fy = (T)vy, fz = (T)vz;
         atomicAdd(&s_energy[s], (double)fx * fx + (double)fy * fy + (double)fz * fz);
     }
     const unsigned act = __activemask();
@@ -558,7 +608,8 @@ __device__ __forceinline__ void energy_init(double* s_energy) {
     for (int t = threadIdx.x; t < FOPIS_MAX_SPECIES; t += blockDim.x) s_energy[t] = 0.0;
     __syncthreads();
 }
-__device__ __forceinline__ void energy_flush(const SourceArgs& a, const double* s_energy) {
+template <typename T>
+__device__ __forceinline__ void energy_flush(const SourceArgsT<T>& a, const double* s_energy) {
     __syncthreads();
     for (int t = threadIdx.x; t < FOPIS_MAX_SPECIES; t += blockDim.x)
         if (s_energy[t] != 0.0) atomicAdd(&a.sc->energy[t], s_energy[t]);
@@ -580,7 +631,8 @@ struct InjectTable {
 // (AmbientParticleType.cpp:101-157, rejection redrawing all three components)
 // and generateNewParticle with the slab ranges of
 // RootGrid::injectParticlesFromBoundary (RootGridParticle.cpp:212-302).
-__global__ void inject_kernel(SourceArgs a, InjectTable tb) {
+template <typename T>
+__global__ void inject_kernel(SourceArgsT<T> a, InjectTable tb) {
     __shared__ double s_energy[FOPIS_MAX_SPECIES];
     energy_init(s_energy);
     const long long total = tb.start[tb.n];
@@ -677,7 +729,8 @@ __device__ bool surface_charge(const Grid& g, const int32_t* node_cmat, int obj,
 // (PhotoElectronParticleType.cpp:9-101) at a lit node of the emitting face,
 // its charge taken off the surface at its next crossing point
 // (Spacecraft::emitParticles, Spacecraft.cpp:882-899).
-__global__ void emit_kernel(SourceArgs a, EmitArgs e) {
+template <typename T>
+__global__ void emit_kernel(SourceArgsT<T> a, EmitArgs e) {
     __shared__ double s_energy[FOPIS_MAX_SPECIES];
     energy_init(s_energy);
     const long long total = (long long)e.n_lit * e.K;
@@ -854,8 +907,9 @@ __global__ void absorb_kernel(AbsorbArgs a) {
 }
 
 // ------------------------------------------------------------------ loading
+template <typename T>
 struct AmbientArgs {
-    Soa p;
+    SoaT<T> p;
     long long cap;
     int s;
     long long total;
@@ -870,13 +924,14 @@ struct AmbientArgs {
 // RootGrid::RootGrid uniform loading (RootGrid.cpp:59-79): positions uniform in
 // [0,max), velocities Maxwellian about the drift, particles inside a body
 // dropped (Spacecraft::removeInnerParticle, Spacecraft.cpp:508-510).
-__global__ void ambient_kernel(AmbientArgs a) {
+template <typename T>
+__global__ void ambient_kernel(AmbientArgs<T> a) {
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < a.total; base += stride) {
         const long long t = base + (threadIdx.x & 31);
         bool keep = t < a.total;
         int i = 0, j = 0, k = 0;
-        float ox = 0, oy = 0, oz = 0;
+        T ox = 0, oy = 0, oz = 0;
         double vx = 0, vy = 0, vz = 0;
         if (keep) {
             const uint32_t c0 = (uint32_t)t, c1 = (uint32_t)(t >> 32), c2 = (uint32_t)a.s, dt = TAG_LOAD << 24;
@@ -900,14 +955,15 @@ __global__ void ambient_kernel(AmbientArgs a) {
 
 struct Rec56 { double x, y, z, vx, vy, vz; int typeId, isValid; };
 
-__global__ void load56_kernel(Soa p, long long cap, unsigned long long* count, const Rec56* in, long long n, Grid g,
+template <typename T>
+__global__ void load56_kernel(SoaT<T> p, long long cap, unsigned long long* count, const Rec56* in, long long n, Grid g,
                               DevScalars* sc) {
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
         const long long t = base + (threadIdx.x & 31);
         bool keep = t < n && in[t].isValid;
         int i = 0, j = 0, k = 0;
-        float ox = 0, oy = 0, oz = 0;
+        T ox = 0, oy = 0, oz = 0;
         if (keep) {
             split(in[t].x, i, ox); split(in[t].y, j, oy); split(in[t].z, k, oz);
             if (!cell_in_range(g, i, j, k)) { keep = false; atomicOr(&sc->status, (unsigned)FOPIS_DEV_NONFINITE); }
@@ -920,8 +976,9 @@ __global__ void load56_kernel(Soa p, long long cap, unsigned long long* count, c
     }
 }
 
-// Compacts the valid particles of [lo, hi) into AoS56 records or raw arrays.
-__global__ void energy_kernel(Soa p, long long cap, const unsigned long long* count, double* out) {
+// Sum of v^2 over the valid particles of a species.
+template <typename T>
+__global__ void energy_kernel(SoaT<T> p, long long cap, const unsigned long long* count, double* out) {
     const long long n = (long long)min(*count, (unsigned long long)cap);
     double e = 0.0;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
@@ -939,7 +996,8 @@ __global__ void energy_kernel(Soa p, long long cap, const unsigned long long* co
 // leave sectors partial cost a DRAM fill and a write-back each.
 
 // cnt[b] += particles of brick b (valid slots only), one atomic per warp and brick.
-__global__ void sort_count_kernel(Soa p, long long cap, const unsigned long long* count, Grid g, int32_t* cnt) {
+template <typename T>
+__global__ void sort_count_kernel(SoaT<T> p, long long cap, const unsigned long long* count, Grid g, int32_t* cnt) {
     const long long n = (long long)min(*count, (unsigned long long)cap);
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
@@ -1009,7 +1067,8 @@ __global__ void scan_apply_kernel(const int32_t* in, long long n, const int32_t*
 // counts its valid particles, the tile totals are scanned, and each tile
 // writes its particles at its offset plus their rank inside the tile, so the
 // records come out in slot order.
-__global__ void export_count_kernel(Soa p, long long lo, long long hi, int32_t* partial) {
+template <typename T>
+__global__ void export_count_kernel(SoaT<T> p, long long lo, long long hi, int32_t* partial) {
     const long long base = lo + (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
     int n = 0;
     for (int q = 0; q < kScanItems; ++q) if (base + q < hi && p.cell[base + q] >= 0) ++n;
@@ -1018,7 +1077,8 @@ __global__ void export_count_kernel(Soa p, long long lo, long long hi, int32_t* 
     if (threadIdx.x == 0) partial[blockIdx.x] = tot;
 }
 
-__global__ void export_kernel(Soa p, long long lo, long long hi, int s, Rec56* out56, Soa raw,
+template <typename T>
+__global__ void export_kernel(SoaT<T> p, long long lo, long long hi, int s, Rec56* out56, SoaT<T> raw,
                               const int32_t* partial) {
     const long long base = lo + (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
     int32_t cell[kScanItems];
@@ -1070,7 +1130,8 @@ __device__ __forceinline__ int sort_slot(int* keys, int b) {
     return -1;   // unreachable: at most kSortChunk distinct bricks in kSortSlots slots
 }
 
-__global__ void __launch_bounds__(kSortThreads) sort_brick_scatter_kernel(Soa src, Soa dst, long long cap,
+template <typename T>
+__global__ void __launch_bounds__(kSortThreads) sort_brick_scatter_kernel(SoaT<T> src, SoaT<T> dst, long long cap,
                                                                           const unsigned long long* count, Grid g,
                                                                           int32_t* cursor) {
     static_assert(kSortSlots == 2048, "sort_slot hashes to 11 bits");
@@ -1083,7 +1144,7 @@ __global__ void __launch_bounds__(kSortThreads) sort_brick_scatter_kernel(Soa sr
     __syncthreads();
     for (long long c0 = (long long)blockIdx.x * kSortChunk; c0 < n; c0 += (long long)gridDim.x * kSortChunk) {
         int32_t cell[kSortItems];
-        float f[kSortItems][6];
+        T f[kSortItems][6];
         int slot[kSortItems], rank[kSortItems];
 #pragma unroll
         for (int e = 0; e < kSortItems; ++e) {
@@ -1141,7 +1202,8 @@ __device__ __forceinline__ int cell_rank(int* counter, int lc, bool valid) {
     return __shfl_sync(kFull, r0, leader) + __popc(grp & ((1u << lane) - 1u));
 }
 
-__global__ void __launch_bounds__(kCellThreads) sort_cell_kernel(Soa src, Soa dst, const int32_t* brick_start,
+template <typename T>
+__global__ void __launch_bounds__(kCellThreads) sort_cell_kernel(SoaT<T> src, SoaT<T> dst, const int32_t* brick_start,
                                                                  int nbricks) {
     __shared__ uint8_t s_lc[kCellCap];
     __shared__ uint16_t s_perm[kCellCap];
@@ -1194,7 +1256,7 @@ __global__ void __launch_bounds__(kCellThreads) sort_cell_kernel(Soa src, Soa ds
             __syncthreads();
             for (int r0 = 0; r0 < n; r0 += kStep) {
                 int32_t c[kCellBatch];
-                float v[kCellBatch][6];
+                T v[kCellBatch][6];
 #pragma unroll
                 for (int e = 0; e < kCellBatch; ++e) {
                     const int r = r0 + e * kCellThreads + tid;
@@ -1243,23 +1305,50 @@ int grid_for(long long n, int threads = kThreads) {
 
 // Particle arrays come from the device's stream-ordered pool, so growing them
 // mid-run neither synchronises the device nor returns memory to the driver.
-void alloc_soa(Soa& s, int64_t cap, cudaStream_t st) {
+template <typename T>
+void alloc_soa(SoaT<T>& s, int64_t cap, cudaStream_t st) {
     FOPIS_CUDA(cudaMallocAsync((void**)&s.cell, sizeof(int32_t) * cap, st));
-    float** f[6] = {&s.ox, &s.oy, &s.oz, &s.vx, &s.vy, &s.vz};
-    for (auto* q : f) FOPIS_CUDA(cudaMallocAsync((void**)q, sizeof(float) * cap, st));
+    T** f[6] = {&s.ox, &s.oy, &s.oz, &s.vx, &s.vy, &s.vz};
+    for (auto* q : f) FOPIS_CUDA(cudaMallocAsync((void**)q, sizeof(T) * cap, st));
 }
-void free_soa(Soa& s, cudaStream_t st) {
+template <typename T>
+void free_soa(SoaT<T>& s, cudaStream_t st) {
     if (s.cell) cudaFreeAsync(s.cell, st);
-    float* f[6] = {s.ox, s.oy, s.oz, s.vx, s.vy, s.vz};
+    T* f[6] = {s.ox, s.oy, s.oz, s.vx, s.vy, s.vz};
     for (auto* q : f) if (q) cudaFreeAsync(q, st);
-    s = Soa{};
+    s = SoaT<T>{};
 }
-void copy_soa(Soa& d, const Soa& s, int64_t n, cudaStream_t st) {
+template <typename T>
+void copy_soa(SoaT<T>& d, const SoaT<T>& s, int64_t n, cudaStream_t st) {
     if (n <= 0) return;
     FOPIS_CUDA(cudaMemcpyAsync(d.cell, s.cell, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st));
-    float* df[6] = {d.ox, d.oy, d.oz, d.vx, d.vy, d.vz};
-    float* sf[6] = {s.ox, s.oy, s.oz, s.vx, s.vy, s.vz};
-    for (int t = 0; t < 6; ++t) FOPIS_CUDA(cudaMemcpyAsync(df[t], sf[t], sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+    T* df[6] = {d.ox, d.oy, d.oz, d.vx, d.vy, d.vz};
+    T* sf[6] = {s.ox, s.oy, s.oz, s.vx, s.vy, s.vz};
+    for (int t = 0; t < 6; ++t) FOPIS_CUDA(cudaMemcpyAsync(df[t], sf[t], sizeof(T) * n, cudaMemcpyDeviceToDevice, st));
+}
+
+// The particle arrays of a precision: the live set and the sort target.
+template <typename T> SoaT<T>* parts(Ctx& c);
+template <> Soa* parts<float>(Ctx& c) { return c.sp; }
+template <> Soa64* parts<double>(Ctx& c) { return c.dp; }
+template <typename T> SoaT<T>* parts2(Ctx& c);
+template <> Soa* parts2<float>(Ctx& c) { return c.sp2; }
+template <> Soa64* parts2<double>(Ctx& c) { return c.dp2; }
+
+template <typename T>
+void alloc_species(Ctx& c, int s, int64_t cap) {
+    SoaT<T> a{}, b{};
+    alloc_soa(a, cap, c.st);
+    alloc_soa(b, cap, c.st);
+    FOPIS_CUDA(cudaMemsetAsync(a.cell, 0xff, sizeof(int32_t) * cap, c.st));
+    if (c.cap[s] > 0) {
+        sync_scalars(c);
+        copy_soa(a, parts<T>(c)[s], std::min<int64_t>(c.nslots[s], c.cap[s]), c.st);
+        free_soa(parts<T>(c)[s], c.st);
+        free_soa(parts2<T>(c)[s], c.st);
+    }
+    parts<T>(c)[s] = a;
+    parts2<T>(c)[s] = b;
 }
 
 }  // namespace
@@ -1267,19 +1356,9 @@ void copy_soa(Soa& d, const Soa& s, int64_t n, cudaStream_t st) {
 // Makes sure species s can hold at least `need` slots (grows both buffers).
 void particles_alloc(Ctx& c, int s, int64_t need) {
     if (need <= c.cap[s]) return;
-    int64_t cap = std::max<int64_t>(need, 1024);
-    Soa a{}, b{};
-    alloc_soa(a, cap, c.st);
-    alloc_soa(b, cap, c.st);
-    FOPIS_CUDA(cudaMemsetAsync(a.cell, 0xff, sizeof(int32_t) * cap, c.st));
-    if (c.cap[s] > 0) {
-        sync_scalars(c);
-        copy_soa(a, c.sp[s], std::min<int64_t>(c.nslots[s], c.cap[s]), c.st);
-        free_soa(c.sp[s], c.st);
-        free_soa(c.sp2[s], c.st);
-    }
-    c.sp[s] = a;
-    c.sp2[s] = b;
+    const int64_t cap = std::max<int64_t>(need, 1024);
+    if (c.fp64) alloc_species<double>(c, s, cap);
+    else alloc_species<float>(c, s, cap);
     c.cap[s] = cap;
 }
 
@@ -1289,7 +1368,8 @@ void sync_scalars(Ctx& c) {
     for (int s = 0; s < c.nsp; ++s) c.nslots[s] = (int64_t)std::min<unsigned long long>(c.h_sc->count[s], (unsigned long long)c.cap[s]);
 }
 
-void particles_append_aos(Ctx& c, int s, const void* host56, int64_t n) {
+template <typename T>
+static void append_aos(Ctx& c, int s, const void* host56, int64_t n) {
     sync_scalars(c);
     particles_alloc(c, s, (int64_t)((c.nslots[s] + n) * std::max(1.0, c.p.capacity_factor)) + 4096);
     const int64_t chunk = 1 << 20;
@@ -1300,7 +1380,7 @@ void particles_append_aos(Ctx& c, int s, const void* host56, int64_t n) {
         const int64_t m = std::min(chunk, n - off);
         FOPIS_CUDA(cudaMemcpyAsync(d, (const char*)host56 + 56 * off, 56 * m, cudaMemcpyHostToDevice, c.st));
         ++c.launches;
-        load56_kernel<<<grid_for(m), kThreads, 0, c.st>>>(c.sp[s], c.cap[s], &c.d_sc->count[s], d, m, g, c.d_sc);
+        load56_kernel<<<grid_for(m), kThreads, 0, c.st>>>(parts<T>(c)[s], c.cap[s], &c.d_sc->count[s], d, m, g, c.d_sc);
         FOPIS_LAUNCH_CHECK();
     }
     FOPIS_CUDA(cudaStreamSynchronize(c.st));
@@ -1308,18 +1388,24 @@ void particles_append_aos(Ctx& c, int s, const void* host56, int64_t n) {
     sync_scalars(c);
 }
 
+void particles_append_aos(Ctx& c, int s, const void* host56, int64_t n) {
+    if (c.fp64) append_aos<double>(c, s, host56, n);
+    else append_aos<float>(c, s, host56, n);
+}
+
 // Export chunks hold kExportChunk slots; `partial` has kExportTiles + 1 entries.
 constexpr int64_t kExportChunk = 1 << 20;
 constexpr int kExportTiles = (int)((kExportChunk + kScanTile - 1) / kScanTile);
 
-static int64_t export_range(Ctx& c, int s, Rec56* d56, Soa* raw, int64_t lo, int64_t hi, int32_t* partial) {
+template <typename T>
+static int64_t export_range(Ctx& c, int s, Rec56* d56, SoaT<T>* raw, int64_t lo, int64_t hi, int32_t* partial) {
     const int tiles = (int)((hi - lo + kScanTile - 1) / kScanTile);
     ++c.launches;
-    export_count_kernel<<<tiles, kScanThreads, 0, c.st>>>(c.sp[s], lo, hi, partial);
+    export_count_kernel<<<tiles, kScanThreads, 0, c.st>>>(parts<T>(c)[s], lo, hi, partial);
     ++c.launches;
     scan_partials_kernel<<<1, kScanThreads, 0, c.st>>>(partial, tiles);
     ++c.launches;
-    export_kernel<<<tiles, kScanThreads, 0, c.st>>>(c.sp[s], lo, hi, s, d56, raw ? *raw : Soa{}, partial);
+    export_kernel<<<tiles, kScanThreads, 0, c.st>>>(parts<T>(c)[s], lo, hi, s, d56, raw ? *raw : SoaT<T>{}, partial);
     FOPIS_LAUNCH_CHECK();
     int32_t k = 0;
     FOPIS_CUDA(cudaMemcpyAsync(&k, partial + tiles, sizeof(k), cudaMemcpyDeviceToHost, c.st));
@@ -1338,7 +1424,8 @@ int64_t particles_export_aos(Ctx& c, int s, void* host56, int64_t cap) {
     int64_t total = 0;
     for (int64_t lo = 0; lo < n; lo += chunk) {
         const int64_t hi = std::min(n, lo + chunk);
-        const int64_t k = export_range(c, s, d, nullptr, lo, hi, dc);
+        const int64_t k = c.fp64 ? export_range<double>(c, s, d, nullptr, lo, hi, dc)
+                                 : export_range<float>(c, s, d, nullptr, lo, hi, dc);
         const int64_t w = std::max<int64_t>(0, std::min(k, cap - total));
         if (w > 0) FOPIS_CUDA(cudaMemcpy((char*)host56 + 56 * total, d, 56 * w, cudaMemcpyDeviceToHost));
         total += k;
@@ -1380,7 +1467,8 @@ static double max_extent(const Ctx& c, int axis) {
     return c.per[2 * axis + 1] ? (double)n : n - 1.0;
 }
 
-void particles_generate_ambient(Ctx& c) {
+template <typename T>
+static void generate_ambient(Ctx& c) {
     const Grid g = make_grid(c);
     for (int s = 0; s < c.nsp; ++s) {
         const fopis_species& sp = c.p.species[s];
@@ -1390,8 +1478,8 @@ void particles_generate_ambient(Ctx& c) {
         const int64_t total = cxn * cyn * czn * (int64_t)sp.particle_per_cell;
         sync_scalars(c);
         particles_alloc(c, s, (int64_t)((c.nslots[s] + total) * std::max(1.0, c.p.capacity_factor)) + 4096);
-        AmbientArgs a;
-        a.p = c.sp[s]; a.cap = c.cap[s]; a.s = s; a.total = total;
+        AmbientArgs<T> a;
+        a.p = parts<T>(c)[s]; a.cap = c.cap[s]; a.s = s; a.total = total;
         for (int q = 0; q < 3; ++q) { a.maxe[q] = max_extent(c, q); a.drift[q] = sp.drift[q]; }
         a.dev = sp.deviation; a.seed = c.p.seed; a.g = g;
         a.cellmap = c.objs.empty() ? nullptr : c.cellmap;
@@ -1401,6 +1489,11 @@ void particles_generate_ambient(Ctx& c) {
         FOPIS_LAUNCH_CHECK();
     }
     sync_scalars(c);
+}
+
+void particles_generate_ambient(Ctx& c) {
+    if (c.fp64) generate_ambient<double>(c);
+    else generate_ambient<float>(c);
 }
 
 int64_t brick_keys(const Ctx& c) {
@@ -1415,9 +1508,10 @@ int brick_count(const Ctx& c) {
 
 // Sort of every species by brick (brick_index), then by cell inside the
 // brick (local_cell); invalid slots are dropped. Records each brick's first slot
-// for push_tile_kernel. The particles end in c.sp[s]; c.sp2[s] holds the
-// brick-grouped intermediate.
-void particles_sort(Ctx& c) {
+// for push_tile_kernel. The particles end in the live arrays; the sort
+// targets hold the brick-grouped intermediate.
+template <typename T>
+static void sort_all(Ctx& c) {
     sync_scalars(c);
     const Grid g = make_grid(c);
     const int nbricks = brick_count(c);
@@ -1428,7 +1522,7 @@ void particles_sort(Ctx& c) {
         FOPIS_CUDA(cudaMemsetAsync(c.sort_count, 0, sizeof(int32_t) * (nbricks + 1), c.st));
         ++c.launches;
         sort_count_kernel<<<grid_for(std::max<int64_t>(c.nslots[s], 1)), kThreads, 0, c.st>>>(
-            c.sp[s], c.cap[s], &c.d_sc->count[s], g, c.sort_count);
+            parts<T>(c)[s], c.cap[s], &c.d_sc->count[s], g, c.sort_count);
         FOPIS_LAUNCH_CHECK();
         ++c.launches;
         scan_tiles_kernel<<<tiles, kScanThreads, 0, c.st>>>(c.sort_count, nbricks + 1, c.scan_partials);
@@ -1444,13 +1538,13 @@ void particles_sort(Ctx& c) {
         {
             const long long chunks = (std::max<int64_t>(c.nslots[s], 1) + kSortChunk - 1) / kSortChunk;
             const int grid = (int)std::max<long long>(1, std::min<long long>(chunks, 148LL * 8));
-            sort_brick_scatter_kernel<<<grid, kSortThreads, 0, c.st>>>(c.sp[s], c.sp2[s], c.cap[s],
+            sort_brick_scatter_kernel<<<grid, kSortThreads, 0, c.st>>>(parts<T>(c)[s], parts2<T>(c)[s], c.cap[s],
                                                                       &c.d_sc->count[s], g, c.sort_offset);
         }
         FOPIS_LAUNCH_CHECK();
         ++c.launches;
-        sort_cell_kernel<<<std::min(nbricks, 148 * 8), kCellThreads, 0, c.st>>>(c.sp2[s], c.sp[s], c.brick_start[s],
-                                                                                nbricks);
+        sort_cell_kernel<<<std::min(nbricks, 148 * 8), kCellThreads, 0, c.st>>>(parts2<T>(c)[s], parts<T>(c)[s],
+                                                                                c.brick_start[s], nbricks);
         FOPIS_LAUNCH_CHECK();
         // the new count is the total of valid particles: the scan's grand total
         FOPIS_CUDA(cudaMemcpyAsync(&c.d_sc->count[s], c.scan_partials + tiles, sizeof(int32_t), cudaMemcpyDeviceToDevice, c.st));
@@ -1461,55 +1555,79 @@ void particles_sort(Ctx& c) {
         if (c.cap[s] == 0) continue;
         const int64_t n = c.nslots[s];
         c.sorted_n[s] = n;
-        if (n < c.cap[s]) FOPIS_CUDA(cudaMemsetAsync(c.sp[s].cell + n, 0xff, sizeof(int32_t) * (c.cap[s] - n), c.st));
+        if (n < c.cap[s]) FOPIS_CUDA(cudaMemsetAsync(parts<T>(c)[s].cell + n, 0xff, sizeof(int32_t) * (c.cap[s] - n), c.st));
         // keep head room for the appends of the coming steps
         const int64_t want = (int64_t)(n * 1.25) + 65536;
         if (want > c.cap[s]) particles_alloc(c, s, (int64_t)(n * std::max(1.5, c.p.capacity_factor)) + 65536);
     }
 }
 
-static PushArgs push_args(Ctx& c, int s) {
-    PushArgs a;
-    a.p = c.sp[s]; a.s = s; a.cap = c.cap[s]; a.lo = 0; a.count = &c.d_sc->count[s];
-    a.E = c.E; a.g = make_grid(c);
-    a.qm = (float)(0.5 * c.p.species[s].charge / c.p.species[s].mass);
-    a.bx = (float)c.p.static_bfield[0]; a.by = (float)c.p.static_bfield[1]; a.bz = (float)c.p.static_bfield[2];
+void particles_sort(Ctx& c) {
+    if (c.fp64) sort_all<double>(c);
+    else sort_all<float>(c);
+}
+
+template <typename T> const typename NodeE<T>::type* node_e(const Ctx& c);
+template <> const float4* node_e<float>(const Ctx& c) { return c.E; }
+template <> const Vec4d* node_e<double>(const Ctx& c) { return c.E64; }
+
+template <typename T>
+static PushArgsT<T> push_args(Ctx& c, int s) {
+    PushArgsT<T> a;
+    a.p = parts<T>(c)[s]; a.s = s; a.cap = c.cap[s]; a.lo = 0; a.count = &c.d_sc->count[s];
+    a.E = node_e<T>(c); a.g = make_grid(c);
+    a.qm = (T)(0.5 * c.p.species[s].charge / c.p.species[s].mass);
+    a.bx = (T)c.p.static_bfield[0]; a.by = (T)c.p.static_bfield[1]; a.bz = (T)c.p.static_bfield[2];
     const double b2 = c.p.static_bfield[0] * c.p.static_bfield[0] + c.p.static_bfield[1] * c.p.static_bfield[1] +
                       c.p.static_bfield[2] * c.p.static_bfield[2];
-    a.boris = (float)(2.0 / (1.0 + b2));
+    a.boris = (T)(2.0 / (1.0 + b2));
     a.cellmap = c.objs.empty() ? nullptr : c.cellmap;
     a.rho = c.rho_i64 + (size_t)s * c.N;
     a.ab = c.ab; a.sc = c.d_sc;
     return a;
 }
 
+template <typename T>
+static void push_generic(Ctx& c, const PushArgsT<T>& a, int grid, bool vel, bool pos, bool dep) {
+    if (vel && pos && dep) push_kernel<T, true, true, true><<<grid, kThreads, 0, c.st>>>(a);
+    else if (vel && !pos && !dep) push_kernel<T, true, false, false><<<grid, kThreads, 0, c.st>>>(a);
+    else if (!vel && pos && !dep) push_kernel<T, false, true, false><<<grid, kThreads, 0, c.st>>>(a);
+    else if (!vel && !pos && dep) push_kernel<T, false, false, true><<<grid, kThreads, 0, c.st>>>(a);
+    else throw ApiError{FOPIS_ERR_ARG, "unsupported push combination"};
+}
+
+// The fused step takes the brick-sorted slots with push_tile_kernel and the
+// appended tail with push_kernel (mixed mode); the FP64 mode and the single
+// phases run push_kernel over every slot.
 void launch_push(Ctx& c, bool vel, bool pos, bool dep) {
     for (int s = 0; s < c.nsp; ++s) {
         if (c.cap[s] == 0) continue;
-        PushArgs a = push_args(c, s);
         const int grid = grid_for(c.cap[s]);
-        if (vel && pos && dep && c.sorted_n[s] > 0 && c.brick_start[s]) {
+        if (c.fp64) {
+            ++c.launches;
+            push_generic<double>(c, push_args<double>(c, s), grid, vel, pos, dep);
+        } else if (vel && pos && dep && c.sorted_n[s] > 0 && c.brick_start[s]) {
+            PushArgs a = push_args<float>(c, s);
             ++c.launches;
             push_tile_kernel<kPushRun, 4><<<brick_count(c), kTileThreads, TileChunk<kPushRun>::kSmem, c.st>>>(
                 a, c.brick_start[s]);
             a.lo = c.sorted_n[s];
             ++c.launches;
-            push_kernel<true, true, true><<<grid_for(std::max<int64_t>(c.cap[s] - a.lo, 1)), kThreads, 0, c.st>>>(a);
+            push_kernel<float, true, true, true><<<grid_for(std::max<int64_t>(c.cap[s] - a.lo, 1)), kThreads, 0, c.st>>>(a);
+        } else {
+            ++c.launches;
+            push_generic<float>(c, push_args<float>(c, s), grid, vel, pos, dep);
         }
-        else if (vel && pos && dep) { ++c.launches; push_kernel<true, true, true><<<grid, kThreads, 0, c.st>>>(a); }
-        else if (vel && !pos && !dep) { ++c.launches; push_kernel<true, false, false><<<grid, kThreads, 0, c.st>>>(a); }
-        else if (!vel && pos && !dep) { ++c.launches; push_kernel<false, true, false><<<grid, kThreads, 0, c.st>>>(a); }
-        else if (!vel && !pos && dep) { ++c.launches; push_kernel<false, false, true><<<grid, kThreads, 0, c.st>>>(a); }
-        else throw ApiError{FOPIS_ERR_ARG, "unsupported push combination"};
         FOPIS_LAUNCH_CHECK();
     }
 }
 
 void launch_deposit_all(Ctx& c) { launch_push(c, false, false, true); }
 
-static SourceArgs source_args(Ctx& c, bool fused) {
-    SourceArgs a;
-    for (int s = 0; s < FOPIS_MAX_SPECIES; ++s) { a.p[s] = c.sp[s]; a.cap[s] = c.cap[s]; }
+template <typename T>
+static SourceArgsT<T> source_args(Ctx& c, bool fused) {
+    SourceArgsT<T> a;
+    for (int s = 0; s < FOPIS_MAX_SPECIES; ++s) { a.p[s] = parts<T>(c)[s]; a.cap[s] = c.cap[s]; }
     a.g = make_grid(c);
     a.cellmap = c.objs.empty() ? nullptr : c.cellmap;
     a.rho = c.rho_i64; a.N = (long long)c.N; a.ab = c.ab; a.sc = c.d_sc; a.seed = c.p.seed;
@@ -1531,7 +1649,6 @@ void launch_emit(Ctx& c, bool fused) {
         sync_scalars(c);
         if (c.nslots[s] + add > c.cap[s])
             particles_alloc(c, s, std::max<int64_t>((int64_t)((c.nslots[s] + add) * 1.5), add * 2048) + 65536);
-        SourceArgs a = source_args(c, fused);
         EmitArgs e;
         e.obj = (int)o; e.s = s; e.K = K; e.eaxis = eaxis;
         for (int q = 0; q < 3; ++q) e.ev[q] = -c.p.shine_vector[q];
@@ -1539,7 +1656,8 @@ void launch_emit(Ctx& c, bool fused) {
         e.n_lit = ob.n_lit; e.lit = ob.lit; e.lit_ijk = ob.lit + ob.n_lit;
         e.node_cmat = c.node_cmat; e.charge_tmp = ob.charge_tmp; e.n_cmat = ob.n; e.step = c.timestep;
         ++c.launches;
-        emit_kernel<<<grid_for(add), kThreads, 0, c.st>>>(a, e);
+        if (c.fp64) emit_kernel<<<grid_for(add), kThreads, 0, c.st>>>(source_args<double>(c, fused), e);
+        else emit_kernel<<<grid_for(add), kThreads, 0, c.st>>>(source_args<float>(c, fused), e);
         FOPIS_LAUNCH_CHECK();
     }
 }
@@ -1586,9 +1704,9 @@ void launch_inject(Ctx& c, bool fused) {
         for (int s = 0; s < c.nsp; ++s)
             if (need[s] && c.nslots[s] + need[s] > c.cap[s]) particles_alloc(c, s, (int64_t)((c.nslots[s] + need[s]) * 1.5) + 65536);
     }
-    SourceArgs a = source_args(c, fused);
     ++c.launches;
-    inject_kernel<<<grid_for(tb.start[tb.n]), kThreads, 0, c.st>>>(a, tb);
+    if (c.fp64) inject_kernel<<<grid_for(tb.start[tb.n]), kThreads, 0, c.st>>>(source_args<double>(c, fused), tb);
+    else inject_kernel<<<grid_for(tb.start[tb.n]), kThreads, 0, c.st>>>(source_args<float>(c, fused), tb);
     FOPIS_LAUNCH_CHECK();
 }
 
@@ -1608,8 +1726,12 @@ void launch_energy(Ctx& c) {
     for (int s = 0; s < c.nsp; ++s) {
         if (c.cap[s] == 0) continue;
         ++c.launches;
-        energy_kernel<<<grid_for(c.cap[s]), kThreads, 0, c.st>>>(c.sp[s], c.cap[s], &c.d_sc->count[s],
-                                                                  &c.d_sc->energy[s]);
+        if (c.fp64)
+            energy_kernel<<<grid_for(c.cap[s]), kThreads, 0, c.st>>>(c.dp[s], c.cap[s], &c.d_sc->count[s],
+                                                                      &c.d_sc->energy[s]);
+        else
+            energy_kernel<<<grid_for(c.cap[s]), kThreads, 0, c.st>>>(c.sp[s], c.cap[s], &c.d_sc->count[s],
+                                                                      &c.d_sc->energy[s]);
         FOPIS_LAUNCH_CHECK();
     }
 }

@@ -84,7 +84,10 @@ typedef struct fopis_species {
 typedef enum fopis_precision {
     FOPIS_MIXED = 0,   /* int32 cell + FP32 offset/velocity particles, int64 fixed-point rho,
                           FP32 smoother inside FP64 iterative refinement */
-    FOPIS_FP64 = 1     /* FP64 particles, FP64 deposit and FP64 smoother */
+    FOPIS_FP64 = 1     /* int32 cell + FP64 offset/velocity particles, FP64 E gather and push,
+                          FP64 CIC deposit (atomic sums), phi from the same FP64 residual
+                          refinement to the requested tolerance; the reference run for
+                          the mixed mode's error */
 } fopis_precision;
 
 typedef enum fopis_guess_mode {

@@ -13,7 +13,7 @@ from helpers import match, rel_err
 pytestmark = pytest.mark.gpu
 
 
-def cube_cfg(n=25, half=2, ppc=8, photo=True, tol=1e-10, fixed=None):
+def cube_cfg(n=25, half=2, ppc=8, photo=True, tol=1e-10, fixed=None, precision=_abi.MIXED):
     dx, dt = plasma_units()
     sp = [SpeciesInfo("Electron", "ambient", 1.0, -1.0, 1e7, 1.0, ppc),
           SpeciesInfo("Ion", "ambient", 100.0, 1.0, 1e7, 1.0, ppc)]
@@ -24,7 +24,8 @@ def cube_cfg(n=25, half=2, ppc=8, photo=True, tol=1e-10, fixed=None):
         sp.append(SpeciesInfo("Photo", "photoelectron", 1.0, -1.0, 1e7, 0.2, ppc,
                               current_density=10.0 * config.E * 1e7 * vbar / 4.0))
         shine = (-1.0, 0.0, 0.0)
-    p, norm = make_params((n, n, n), "DDDDDD", dx, dt, sp, shine=shine, tol=tol, sort_interval=1000000, seed=4242)
+    p, norm = make_params((n, n, n), "DDDDDD", dx, dt, sp, shine=shine, tol=tol, sort_interval=1000000, seed=4242,
+                          precision=precision)
     emit = 2 if photo else -1
     obj = objects_from_boxes([((-half,) * 3, (half,) * 3)], (n, n, n), emit_species=emit, fixed=fixed)
     return config.SimConfig(params=p, norm=norm, species=sp, objects=[obj])
