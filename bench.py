@@ -34,6 +34,12 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 PUSH_BYTES_PER_PARTICLE = 56.0   # 28 B split-precision state read + 28 B written (gather+push+deposit fused)
+PUSH_BYTES_FP64 = 104.0          # FP64 mode: 4 B cell + 48 B offsets and velocities, read and written
+
+
+def precision_of(args):
+    from fopis_b200 import _abi
+    return _abi.FP64 if args.precision == "fp64" else _abi.MIXED
 
 
 def peaks():
@@ -158,7 +164,8 @@ def guess_mode(args):
 
 def build_sim(args, rank, local):
     from fopis_b200 import RootGrid, config
-    cfg = config.workload(args.workload, ppc=args.ppc, seed=20251203 + 7919 * rank, sort_interval=args.sort_interval)
+    cfg = config.workload(args.workload, ppc=args.ppc, seed=20251203 + 7919 * rank, sort_interval=args.sort_interval,
+                          precision=precision_of(args))
     g = RootGrid(cfg, device=local)
     g.set_guess_mode(guess_mode(args))
     t0 = time.time()
@@ -392,6 +399,8 @@ def main():
     ap.add_argument("--workload", default="cube128")
     ap.add_argument("--ppc", type=int, default=None, help="particles per cell per species (workload default)")
     ap.add_argument("--sort-interval", type=int, default=8)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+                    help="mixed: FP32 split-precision particles (the headline); fp64: FP64 particles and deposit")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu", dest="cpu", action="store_false")
     ap.add_argument("--cpu-steps", type=int, default=1)
@@ -409,7 +418,8 @@ def main():
     hbm, peak_kind = peaks()
     base = {"metric": "particle-steps/s", "unit": "particle-steps/s", "n_gpus": world, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "data": "synthetic (Philox-seeded Maxwellian plasma)",
-            "dtype": "fp32 particles, int64 fixed-point rho, fp32 smoother in fp64 refinement",
+            "dtype": ("fp32 particles, int64 fixed-point rho, fp32 smoother in fp64 refinement" if args.precision == "mixed"
+                      else "fp64 particles, fp64 deposit, fp32 smoother in fp64 refinement"),
             "config": {"workload": workload_desc(args.workload, args.ppc),
                        "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (particle state ~3.8 GB)",
                        "sort_interval": args.sort_interval,
@@ -440,19 +450,22 @@ def main():
         return
     res, cfg = run_gpu(args, world, rank, local)
     value = res["psteps"] / (res["ms"] * 1e-3)
-    achieved = PUSH_BYTES_PER_PARTICLE * res["pushed"] / (res["push_ms"] * 1e-3) / 1e9
+    push_bytes = PUSH_BYTES_PER_PARTICLE if args.precision == "mixed" else PUSH_BYTES_FP64
+    achieved = push_bytes * res["pushed"] / (res["push_ms"] * 1e-3) / 1e9
     traffic = None
     prof = ROOT / "profiles" / "push_kernel_cube64.md"
-    if prof.exists():
+    if prof.exists() and args.precision == "mixed":
         # DRAM bytes per particle of one push_tile_kernel launch, from the committed ncu summary
         m = re.search(r"\| dram_bytes_per_particle \| ([0-9.]+) \|", prof.read_text())
         if m:
             traffic = float(m.group(1)) * res["pushed"]
     line = dict(base, value=value, steps=args.steps, warmup=args.warmup, ms_per_step=res["ms"] / args.steps)
     line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                        "traffic": traffic, "kernel": "push_tile_kernel + tail push_kernel (all species)",
+                        "traffic": traffic,
+                        "kernel": ("push_tile_kernel + tail push_kernel (all species)" if args.precision == "mixed"
+                                   else "push_kernel<double> (all species)"),
                         "peak_kind": peak_kind,
-                        "bytes_per_particle": PUSH_BYTES_PER_PARTICLE}
+                        "bytes_per_particle": push_bytes}
     line["clocks"] = res["clocks"]
     line["gpu_launches"] = res["launches"]
     line["vcycles_per_step"] = res["vcycles_per_step"]
