@@ -361,6 +361,8 @@ constexpr int kTile = kWX * kWY * kWZ;             // 9 x 9 x 13 nodes
 // Adds one integer corner weight (< 2^52) to the shared tile, held as three
 // 32-bit planes of 17-bit chunks so the additions are native 32-bit shared
 // atomics; a plane overflows only after 2^15 full-weight additions to a node.
+// (A 64-bit tile with one 64-bit shared atomicAdd per corner made the 128^3
+// push 4.05 -> 5.75 ms.)
 __device__ __forceinline__ void tile_add(unsigned* t0, unsigned* t1, unsigned* t2, int idx, unsigned long long w) {
     atomicAdd(t0 + idx, (unsigned)(w & 0x1FFFFull));
     atomicAdd(t1 + idx, (unsigned)((w >> 17) & 0x1FFFFull));
