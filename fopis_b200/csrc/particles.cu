@@ -49,8 +49,10 @@ __device__ __forceinline__ int local_cell(int i, int j, int k) {
     return ((i % kBX) * kBY + (j % kBY)) * kBZ + (k % kBZ);
 }
 
-__device__ __forceinline__ long long lin(const Grid& g, int i, int j, int k) {
-    return (long long)i * g.si + (long long)j * g.sj + k;
+// Linear node index. fopis_create caps every axis at 1022 nodes with glue, so
+// indices stay below 2^31 and are formed in 32-bit arithmetic.
+__device__ __forceinline__ int lin(const Grid& g, int i, int j, int k) {
+    return i * (int)g.si + j * (int)g.sj + k;
 }
 
 // Boundary rule of one axis on the split position (cell index ci, offset o):
@@ -235,12 +237,14 @@ __device__ __forceinline__ int int_of(double x) { return __double2int_rd(x); }
 // qm dx2 dy2 dz2 ... on the eight nodes, B used as given.
 template <typename T>
 __device__ __forceinline__ void gather_boris(const PushArgsT<T>& a, PStateT<T>& s) {
-    const long long b = lin(a.g, s.i, s.j, s.k);
+    const int b = lin(a.g, s.i, s.j, s.k);
+    const int sj = (int)a.g.sj, si = (int)a.g.si;
     const T x1 = s.ox, x2 = (T)1 - s.ox, y1 = s.oy, y2 = (T)1 - s.oy, z1 = s.oz, z2 = (T)1 - s.oz;
-    const auto e000 = load_e(a.E + b), e001 = load_e(a.E + b + 1);
-    const auto e010 = load_e(a.E + b + a.g.sj), e011 = load_e(a.E + b + a.g.sj + 1);
-    const auto e100 = load_e(a.E + b + a.g.si), e101 = load_e(a.E + b + a.g.si + 1);
-    const auto e110 = load_e(a.E + b + a.g.si + a.g.sj), e111 = load_e(a.E + b + a.g.si + a.g.sj + 1);
+    const auto* e = a.E + b;
+    const auto e000 = load_e(e), e001 = load_e(e + 1);
+    const auto e010 = load_e(e + sj), e011 = load_e(e + sj + 1);
+    const auto e100 = load_e(e + si), e101 = load_e(e + si + 1);
+    const auto e110 = load_e(e + si + sj), e111 = load_e(e + si + sj + 1);
     const T w000 = x2 * y2 * z2, w100 = x1 * y2 * z2, w010 = x2 * y1 * z2, w110 = x1 * y1 * z2;
     const T w001 = x2 * y2 * z1, w101 = x1 * y2 * z1, w011 = x2 * y1 * z1, w111 = x1 * y1 * z1;
     const T ex = a.qm * (w000 * e000.x + w100 * e100.x + w010 * e010.x + w110 * e110.x +
