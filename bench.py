@@ -406,8 +406,9 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--profile", action="store_true", help="cudaProfilerStart/Stop around the timed steps")
     ap.add_argument("--phases", action="store_true", help="report the phase times of every timed step")
-    ap.add_argument("--learned-train", type=int, default=200,
-                    help="online training steps before the learned-guess comparison (0: skip it)")
+    ap.add_argument("--learned-train", type=int, default=2000,
+                    help="online training steps before the learned-guess comparison (0: skip it); "
+                         "2000 as in the learned-guess configuration")
     ap.add_argument("--learned-lr", type=float, default=1e-3)
     ap.add_argument("--guess", default="history", choices=["warm", "history"],
                     help="Poisson start of the timed run: the reference's warm start or the per-solve history")
