@@ -1,6 +1,8 @@
 """GPU parity of the conductor path against the FP64 oracle: capacity matrix,
 ambient loading, photoemission, boundary injection, absorption and the
-equipotential redistribution."""
+equipotential redistribution (RootGrid::injectParticlesFromBoundary,
+Spacecraft::emitParticles, distributeInnerParticleCharge, sumWholeCharge,
+redistributeChargeForPerfectConductor, RootGrid::initializeObjectsCmatrix)."""
 import numpy as np
 import pytest
 

@@ -1,6 +1,6 @@
 """GPU parity: libfopis_gpu.so through its C ABI against the FP64 oracle.
 
-Tolerances (north star): particle positions and velocities within 1e-5
+Tolerances: particle positions and velocities within 1e-5
 relative after a step; rho bit-exact against the fixed-point replay of the
 same split-precision particles; phi within 1e-7 relative of the converged FP64
 solve (solver tolerance 1e-10 here; the 1e-8 default is checked separately);
