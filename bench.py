@@ -227,6 +227,8 @@ def run_gpu(args, world, rank, local):
         "vcycles_per_step": float(np.mean(vcyc)), "phases_last": phases, "t_cmat": t_cmat,
         "particles": total_particles(st, nsp), "n_cmat": [len(o.nodes) for o in cfg.objects],
         "step_ms": [round(x, 3) for x in step_ms], "phases_all": phases_all,
+        "solve_mode": ["host loop", "device-loop graph", "device-loop graph with programmatic dependent launch"][
+            st.solve_mode],
     }
     Cm = g.get_cmatrix(0) if cfg.objects else None
     V, Q, cur = g.getObject(0) if cfg.objects else (0.0, 0.0, None)
@@ -469,6 +471,7 @@ def main():
                         "bytes_per_particle": push_bytes}
     line["clocks"] = res["clocks"]
     line["gpu_launches"] = res["launches"]
+    line["solve_mode"] = res["solve_mode"]
     line["vcycles_per_step"] = res["vcycles_per_step"]
     line["particles"] = res["particles"]
     line["phases_ms_last_step"] = dict(zip(["push", "emit", "inject", "absorb", "rho+solve1", "solve2", "efield",

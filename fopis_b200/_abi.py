@@ -117,6 +117,8 @@ class Stats(C.Structure):
         ("learned_used", C.c_int),
         ("ms_phase", C.c_double * 8),
         ("kernel_launches", C.c_int64),
+        ("solve_mode", C.c_int),
+        ("pad", C.c_int),
     ]
 
 

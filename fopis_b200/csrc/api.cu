@@ -597,6 +597,7 @@ int fopis_get_stats(void* h, fopis_stats* st) {
         st->learned_used = c.learned_used;
         for (int q = 0; q < 8; ++q) st->ms_phase[q] = c.ms_phase[q];
         st->kernel_launches = c.launches;
+        st->solve_mode = c.solve_state == 1 ? (c.pdl ? 2 : 1) : 0;
         return FOPIS_OK;
     });
 }

@@ -206,6 +206,7 @@ struct Ctx {
     cudaGraphExec_t solve_exec = nullptr;
     cudaStream_t body_st = nullptr;
     int solve_state = 0;
+    bool pdl = true;                 // solver kernels launched with programmatic dependent launch
     int64_t solve_pre_launches = 0, solve_post_launches = 0;
     int64_t cycle_launches = 0;      // kernels in that graph
     int mg_cta_start = -1;           // first level whose V-cycle runs inside one CTA

@@ -161,6 +161,9 @@ typedef struct fopis_stats {
     int learned_used;            /* the learned guess seeded the last step's solves */
     double ms_phase[8];          /* last step: push, emit, inject, absorb, rho, solve, efield, sort */
     int64_t kernel_launches;     /* kernels this context has launched since creation */
+    int solve_mode;              /* 0: host-driven V-cycle loop; 1: one CUDA graph with a device-side
+                                    loop; 2: the same graph with programmatic dependent launches */
+    int pad;
 } fopis_stats;
 
 /* ---- lifetime ----------------------------------------------------------- */
