@@ -362,16 +362,18 @@ constexpr int kHalo = 2;                           // cells a particle may drift
 constexpr int kWX = kBX + 1 + 2 * kHalo, kWY = kBY + 1 + 2 * kHalo, kWZ = kBZ + 1 + 2 * kHalo;
 constexpr int kTile = kWX * kWY * kWZ;             // 9 x 9 x 13 nodes
 
-// Adds one integer corner weight (< 2^52) to the shared tile, held as three
-// 32-bit planes of 17-bit chunks so the additions are native 32-bit shared
-// atomics; a plane overflows only after 2^15 full-weight additions to a node.
-// (A 64-bit tile with one 64-bit shared atomicAdd per corner made the 128^3
-// push 4.05 -> 5.75 ms.)
-__device__ __forceinline__ void tile_add(unsigned* t0, unsigned* t1, unsigned* t2, int idx, unsigned long long w) {
-    atomicAdd(t0 + idx, (unsigned)(w & 0x1FFFFull));
-    atomicAdd(t1 + idx, (unsigned)((w >> 17) & 0x1FFFFull));
-    const unsigned c2 = (unsigned)(w >> 34);
-    if (c2) atomicAdd(t2 + idx, c2);
+// Adds one integer corner weight to the shared tile, held as a low and a high
+// 32-bit plane with native 32-bit shared atomics: the low word's addition
+// returns the old value, its carry goes into the high word with the weight's
+// high bits. The tile thus holds each node's sum modulo 2^64, exactly what the
+// 64-bit global accumulator holds. (A 64-bit tile with one 64-bit shared
+// atomicAdd per corner made the 128^3 push 4.05 -> 5.75 ms; three planes of
+// 17-bit chunks took 4.05 ms.)
+__device__ __forceinline__ void tile_add(unsigned* lo, unsigned* hi, int idx, unsigned long long w) {
+    const unsigned wl = (unsigned)w, wh = (unsigned)(w >> 32);
+    const unsigned old = atomicAdd(lo + idx, wl);
+    const unsigned carry = (old + wl < old) ? 1u : 0u;
+    if (wh + carry) atomicAdd(hi + idx, wh + carry);
 }
 
 // RUN consecutive particles per thread; a pass stages kTileThreads * RUN
@@ -388,12 +390,11 @@ __device__ __forceinline__ int padi(int q) { return q + (q >> 5); }
 // 0.2-0.9 ms slower per 128^3 step; runs of 2 the same.
 constexpr int kPushRun = 4;
 
-__device__ __forceinline__ void tile_flush(unsigned* t0, unsigned* t1, unsigned* t2, int tb,
-                                           const unsigned long long acc[8]) {
+__device__ __forceinline__ void tile_flush(unsigned* lo, unsigned* hi, int tb, const unsigned long long acc[8]) {
 #pragma unroll
     for (int t = 0; t < 8; ++t) {
         const int off = ((t >> 2) ? kWY * kWZ : 0) + (((t >> 1) & 1) ? kWZ : 0) + (t & 1);
-        if (acc[t]) tile_add(t0, t1, t2, tb + off, acc[t]);
+        if (acc[t]) tile_add(lo, hi, tb + off, acc[t]);
     }
 }
 
@@ -404,13 +405,13 @@ __device__ __forceinline__ void tile_flush(unsigned* t0, unsigned* t1, unsigned*
 // at l*(kChunk/32) + w*kRun, so the lanes of a warp sit kChunk/32 particles (about one cell)
 // apart while each thread walks a run of particles that mostly share a cell. A
 // thread sums its run's corner weights in registers and adds them to the shared
-// tile (brick + 2-cell halo, three 32-bit planes of 17-bit chunks) when the
+// tile (brick + 2-cell halo, a low and a high 32-bit plane) when the
 // cell changes; particles that drifted beyond the halo add straight to HBM. The
 // tile is flushed with one 64-bit atomic per nonzero node.
 template <int RUN, int MINB>
 __global__ void __launch_bounds__(kTileThreads, MINB) push_tile_kernel(PushArgs a, const int32_t* brick_start) {
     constexpr int kRun = RUN, kChunk = TileChunk<RUN>::kChunk, kChunkPad = TileChunk<RUN>::kChunkPad;
-    __shared__ unsigned t0[kTile], t1[kTile], t2[kTile];
+    __shared__ unsigned t_lo[kTile], t_hi[kTile];
     extern __shared__ float s_stage[];
     int32_t* s_cell = reinterpret_cast<int32_t*>(s_stage);
     float* const s_f[6] = {s_stage + kChunkPad, s_stage + 2 * kChunkPad, s_stage + 3 * kChunkPad,
@@ -421,7 +422,7 @@ __global__ void __launch_bounds__(kTileThreads, MINB) push_tile_kernel(PushArgs 
     const int wx0 = bi * kBX - kHalo, wy0 = bj * kBY - kHalo, wz0 = bk * kBZ - kHalo;
     int body = 0;
     for (int t = tid; t < kTile; t += kTileThreads) {
-        t0[t] = 0u; t1[t] = 0u; t2[t] = 0u;
+        t_lo[t] = 0u; t_hi[t] = 0u;
         // a body cell anywhere in the window (cells wx0 .. wx0 + kWX - 2 per axis)?
         const int x = wx0 + t / (kWY * kWZ), y = wy0 + (t / kWZ) % kWY, z = wz0 + t % kWZ;
         if (a.cellmap && x >= wx0 && x - wx0 < kWX - 1 && y - wy0 < kWY - 1 && z - wz0 < kWZ - 1 && x >= 0 && y >= 0 &&
@@ -431,9 +432,6 @@ __global__ void __launch_bounds__(kTileThreads, MINB) push_tile_kernel(PushArgs 
     // particles that stay inside a body-free window need no body test
     const bool window_body = __syncthreads_or(body) != 0;
     const long long p0 = brick_start[b], p1 = brick_start[b + 1];
-    // every particle adds at most once to a node, so fewer than 2^15 particles
-    // cannot overflow a 32-bit chunk plane; denser bricks deposit to HBM
-    const bool tile_ok = (p1 - p0) < 32768;
     double e2 = 0.0;
     __syncthreads();
     for (long long c0 = p0; c0 < p1; c0 += kChunk) {
@@ -476,10 +474,10 @@ __global__ void __launch_bounds__(kTileThreads, MINB) push_tile_kernel(PushArgs 
                 const unsigned qd = (unsigned)__float2int_rn(st.oz * kDepositScale);
                 const unsigned wx[2] = {(unsigned)kDepositOne - qa, qa}, wy[2] = {(unsigned)kDepositOne - qb, qb};
                 const unsigned wz[2] = {(unsigned)kDepositOne - qd, qd};
-                if (tile_ok && inwin) {
+                if (inwin) {
                     const int tb = (li * kWY + lj) * kWZ + lk;
                     if (tb != cur) {
-                        if (cur >= 0) tile_flush(t0, t1, t2, cur, acc);
+                        if (cur >= 0) tile_flush(t_lo, t_hi, cur, acc);
                         cur = tb;
 #pragma unroll
                         for (int t = 0; t < 8; ++t) acc[t] = 0ull;
@@ -503,7 +501,7 @@ __global__ void __launch_bounds__(kTileThreads, MINB) push_tile_kernel(PushArgs 
                 s_f[3][d] = st.vx; s_f[4][d] = st.vy; s_f[5][d] = st.vz;
             }
         }
-        if (cur >= 0) tile_flush(t0, t1, t2, cur, acc);
+        if (cur >= 0) tile_flush(t_lo, t_hi, cur, acc);
         __syncthreads();
         for (int q = tid; q < m; q += kTileThreads) {
             const int d = padi(q);
@@ -514,8 +512,7 @@ __global__ void __launch_bounds__(kTileThreads, MINB) push_tile_kernel(PushArgs 
         __syncthreads();
     }
     for (int t = tid; t < kTile; t += kTileThreads) {
-        const unsigned long long v = (unsigned long long)t0[t] + ((unsigned long long)t1[t] << 17) +
-                                     ((unsigned long long)t2[t] << 34);
+        const unsigned long long v = (unsigned long long)t_lo[t] | ((unsigned long long)t_hi[t] << 32);
         if (!v) continue;
         const int x = wx0 + t / (kWY * kWZ), y = wy0 + (t / kWZ) % kWY, z = wz0 + t % kWZ;
         atomicAdd(a.rho + lin(a.g, x, y, z), v);
