@@ -148,7 +148,8 @@ WORKLOADS = {
 
 def workload_desc(name: str, ppc) -> str:
     text, default_ppc = WORKLOADS[name]
-    return f"{name}: {text}, {ppc or default_ppc} ppc/species, MG to ||r||/||f|| <= 1e-8, 2 solves/step"
+    solves = "1 solve/step" if name == "periodic32" else "2 solves/step"
+    return f"{name}: {text}, {ppc or default_ppc} ppc/species, MG to ||r||/||f|| <= 1e-8, {solves}"
 
 
 def barrier(world: int):
@@ -371,9 +372,12 @@ def reference_cmatrix(cfg):
     return orc.dirichlet_capacity_matrix(cfg.params, cfg.objects[0].nodes)
 
 
-def run_oracle(cfg, Cm, threads: int, steps: int):
+def run_oracle(cfg, Cm, threads: int, steps: int, warmup: int = 0, budget_s: float = float("inf")):
     """The oracle (FP64 CPU restatement of the reference path, reference PSOR with
-    its 1000-sweep cap) on the same workload, capacity matrix preloaded."""
+    its 1000-sweep cap) on the same workload, capacity matrix preloaded: `warmup`
+    untimed steps, then up to `steps` timed steps, stopping early once the timed
+    steps pass `budget_s` seconds. Returns (particle-steps/s, seconds, particles,
+    PSOR sweeps of the last solve, steps timed)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as orc
     orc.lib().orc_set_threads(threads)
@@ -383,13 +387,18 @@ def run_oracle(cfg, Cm, threads: int, steps: int):
         o.set_cmatrix(0, Cm)
     o.generate_ambient()
     o.initialize()
+    if warmup > 0:
+        o.main_loop(warmup)
     n = sum(o.L.orc_num_particles(o.h, s) for s in range(cfg.params.nspecies))
-    t0 = time.perf_counter()
-    o.main_loop(steps)
-    dt = time.perf_counter() - t0
+    done, dt = 0, 0.0
+    while done < steps and dt < budget_s:
+        t0 = time.perf_counter()
+        o.main_loop(1)
+        dt += time.perf_counter() - t0
+        done += 1
     it, _ = o.solver_stats()
     o.close()
-    return n * steps / dt, dt, n, it
+    return n * done / dt, dt, n, it, done
 
 
 def main():
@@ -406,6 +415,8 @@ def main():
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu", dest="cpu", action="store_false")
     ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--ref-budget-s", type=float, default=180.0,
+                    help="--impl reference: stop the timed CPU steps once they pass this many seconds")
     ap.add_argument("--profile", action="store_true", help="cudaProfilerStart/Stop around the timed steps")
     ap.add_argument("--phases", action="store_true", help="report the phase times of every timed step")
     ap.add_argument("--learned-train", type=int, default=2000,
@@ -441,13 +452,18 @@ def main():
         except NotImplementedError as e:
             print(json.dumps({"impl": "reference", "unavailable": f"capacity matrix of this body: {e}"}))
             return
-        v, dt, n, it = run_oracle(cfg, Cm, threads, args.cpu_steps)
-        line = dict(base, impl="reference", value=v, steps=args.cpu_steps, warmup=0, ms_per_step=dt * 1e3 / args.cpu_steps,
-                    n_gpus=1)
-        line["config"] = dict(base["config"], poisson_start="the reference's PSOR continues from the previous phi")
+        warm = min(args.warmup, 1)   # the CPU path has nothing to warm beyond its first step
+        v, dt, n, it, done = run_oracle(cfg, Cm, threads, args.steps, warm, args.ref_budget_s)
+        line = dict(base, impl="reference", value=v, steps=done, warmup=warm, ms_per_step=dt * 1e3 / done, n_gpus=1)
+        line["dtype"] = "fp64 particles and fields (CPU restatement of the reference path)"
+        line["config"] = dict(base["config"], poisson_start="the reference's PSOR continues from the previous phi",
+                              l2="CPU run (no GPU caches involved)")
         line["cpu_baseline"] = {"value": v, "unit": "particle-steps/s", "cores": threads, "kind": "port",
-                                "sample": f"{args.cpu_steps} full step(s) of the workload ({n} particles), "
-                                          f"reference PSOR ({it} sweeps last solve)"}
+                                "sample": f"{done} full step(s) of the workload ({n} particles) after {warm} untimed, "
+                                          f"reference PSOR ({it} sweeps last solve)"
+                                          + ("" if done == args.steps else
+                                             f"; stopped after {done} of {args.steps} steps at the "
+                                             f"{args.ref_budget_s:.0f} s budget")}
         line["e2e"] = {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
         print(json.dumps(line))
         return
@@ -470,6 +486,10 @@ def main():
                         "peak_kind": peak_kind,
                         "bytes_per_particle": push_bytes}
     line["clocks"] = res["clocks"]
+    state_gb = res["particles"] * (28 if args.precision == "mixed" else 52) / 1e9
+    line["config"] = dict(line["config"], l2=(f"inputs larger than L2: particle state {state_gb:.2f} GB, L2 126 MB"
+                                              if state_gb > 0.126 else
+                                              f"particle state {state_gb:.3f} GB fits in L2 (126 MB)"))
     line["gpu_launches"] = res["launches"]
     line["solve_mode"] = res["solve_mode"]
     line["vcycles_per_step"] = res["vcycles_per_step"]
@@ -497,7 +517,7 @@ def main():
             Cref = reference_cmatrix(cfg)
         except NotImplementedError:
             Cref = res["cmatrix"]       # irregular body: the GPU-built matrix, checked against solves in the tests
-        v, dt, n, it = run_oracle(cfg, Cref, os.cpu_count() or 1, args.cpu_steps)
+        v, dt, n, it, _ = run_oracle(cfg, Cref, os.cpu_count() or 1, args.cpu_steps)
         line["cpu_baseline"] = {"value": v, "unit": "particle-steps/s", "cores": os.cpu_count() or 1, "kind": "port",
                                 "sample": f"{args.cpu_steps} full step(s) of the same workload ({n} particles) on the "
                                           f"oracle: FP64 AoS, OpenMP, reference PSOR ({it} sweeps last solve)",
