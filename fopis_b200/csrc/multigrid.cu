@@ -841,46 +841,87 @@ __global__ void __launch_bounds__(kT) fstats_kernel(Outer O, const double* rho0,
     if (threadIdx.x == 0) { partial[2 * blockIdx.x] = s; partial[2 * blockIdx.x + 1] = s2; }
 }
 
-// r = f - A phi in FP64; stores r to the level-0 right-hand side (FP32) and
-// per-block partial sums of r^2.
-__global__ void __launch_bounds__(kT) outer_residual_kernel(Outer O, const double* rho0, const double* phi, float* f0,
-                                                           double* partial) {
+// The FP64 outer kernels on tiles of 32 unknowns along c, 4 rows b and
+// kOuterA consecutive a: a fixed grid of kRedBlocks blocks of 128 threads
+// strides over the tiles, each thread issuing its kOuterA nodes' loads
+// together (the per-block partial sums keep a fixed order).
+constexpr int kOuterA = 4, kOuterThreads = 128;
+
+struct OuterTile {
+    int ntc, ntb, nta;
+    long long tiles;
+};
+__host__ __device__ __forceinline__ OuterTile outer_tiles(const Outer& O) {
+    OuterTile t;
+    t.ntc = (O.n2 + 31) / 32;
+    t.ntb = (O.n1 + 3) / 4;
+    t.nta = (O.n0 + kOuterA - 1) / kOuterA;
+    t.tiles = (long long)t.ntc * t.ntb * t.nta;
+    return t;
+}
+
+// r = f - A phi in FP64 at every unknown; the level-0 right-hand side (FP32)
+// and per-block partial sums of r^2.
+__global__ void __launch_bounds__(kOuterThreads) outer_residual_march_kernel(Outer O, const double* rho0,
+                                                                              const double* phi, float* f0,
+                                                                              double* partial) {
     pdl_entry();
     __shared__ double red[32];
-    const int rows = O.n0 * O.n1;
+    const OuterTile T = outer_tiles(O);
     const double fm = *O.fmean;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     double s2 = 0.0;
-    for (int row = blockIdx.x; row < rows; row += gridDim.x) {
-        const int a = row / O.n1, b = row - a * O.n1;
-        const int i = a + O.o0, j = b + O.o1;
-        const double* p0 = phi + gl(O, i, j, 0);
-        const double* pim = phi + gl(O, wrapn(i - 1, O.p0, O.nref0), j, 0);
-        const double* pip = phi + gl(O, wrapn(i + 1, O.p0, O.nref0), j, 0);
-        const double* pjm = phi + gl(O, i, wrapn(j - 1, O.p1, O.nref1), 0);
-        const double* pjp = phi + gl(O, i, wrapn(j + 1, O.p1, O.nref1), 0);
-        const double* rr = rho0 + gl(O, i, j, 0);
-        float* fr = f0 + (long long)row * O.n2;
-        for (int c = threadIdx.x; c < O.n2; c += blockDim.x) {
-            const int k = c + O.o2;
-            const double s = pim[k] + pip[k] + pjm[k] + pjp[k] + p0[wrapn(k - 1, O.p2, O.nref2)] +
-                             p0[wrapn(k + 1, O.p2, O.nref2)];
-            const double r = (rr[k] * O.inv_eps0 - fm) - (6.0 * p0[k] - s);
-            fr[c] = (float)r;
-            s2 += r * r;
+    for (long long t = blockIdx.x; t < T.tiles; t += gridDim.x) {
+        const int tc = (int)(t % T.ntc);
+        const long long rest = t / T.ntc;
+        const int tb = (int)(rest % T.ntb), ta = (int)(rest / T.ntb);
+        const int c = tc * 32 + tx, b = tb * 4 + ty;
+        if (c >= O.n2 || b >= O.n1) continue;
+        const int j = b + O.o1, k = c + O.o2;
+        const int jm = wrapn(j - 1, O.p1, O.nref1), jp = wrapn(j + 1, O.p1, O.nref1);
+        const int km = wrapn(k - 1, O.p2, O.nref2), kp = wrapn(k + 1, O.p2, O.nref2);
+        double r[kOuterA];
+#pragma unroll
+        for (int e = 0; e < kOuterA; ++e) {
+            const int a = ta * kOuterA + e;
+            r[e] = 0.0;
+            if (a >= O.n0) continue;
+            const int i = a + O.o0;
+            const int im = wrapn(i - 1, O.p0, O.nref0), ip = wrapn(i + 1, O.p0, O.nref0);
+            const double p = phi[gl(O, i, j, k)];
+            const double sn = phi[gl(O, im, j, k)] + phi[gl(O, ip, j, k)] + phi[gl(O, i, jm, k)] +
+                              phi[gl(O, i, jp, k)] + phi[gl(O, i, j, km)] + phi[gl(O, i, j, kp)];
+            r[e] = (rho0[gl(O, i, j, k)] * O.inv_eps0 - fm) - (6.0 * p - sn);
+        }
+#pragma unroll
+        for (int e = 0; e < kOuterA; ++e) {
+            const int a = ta * kOuterA + e;
+            if (a >= O.n0) continue;
+            f0[((long long)a * O.n1 + b) * O.n2 + c] = (float)r[e];
+            s2 += r[e] * r[e];
         }
     }
     s2 = bsum(s2, red);
     if (threadIdx.x == 0) partial[blockIdx.x] = s2;
 }
 
-__global__ void __launch_bounds__(kT) correct_kernel(Outer O, double* phi, const float* e) {
+// phi += e at every unknown.
+__global__ void __launch_bounds__(kOuterThreads) correct_march_kernel(Outer O, double* phi, const float* e) {
     pdl_entry();
-    const int rows = O.n0 * O.n1;
-    for (int row = blockIdx.x; row < rows; row += gridDim.x) {
-        const int a = row / O.n1, b = row - a * O.n1;
-        double* pr = phi + gl(O, a + O.o0, b + O.o1, O.o2);
-        const float* er = e + (long long)row * O.n2;
-        for (int c = threadIdx.x; c < O.n2; c += blockDim.x) pr[c] += (double)er[c];
+    const OuterTile T = outer_tiles(O);
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (long long t = blockIdx.x; t < T.tiles; t += gridDim.x) {
+        const int tc = (int)(t % T.ntc);
+        const long long rest = t / T.ntc;
+        const int tb = (int)(rest % T.ntb), ta = (int)(rest / T.ntb);
+        const int c = tc * 32 + tx, b = tb * 4 + ty;
+        if (c >= O.n2 || b >= O.n1) continue;
+#pragma unroll
+        for (int q = 0; q < kOuterA; ++q) {
+            const int a = ta * kOuterA + q;
+            if (a >= O.n0) continue;
+            phi[gl(O, a + O.o0, b + O.o1, c + O.o2)] += (double)e[((long long)a * O.n1 + b) * O.n2 + c];
+        }
     }
 }
 
@@ -1234,9 +1275,9 @@ static void ensure_cycle_graph(Ctx& c) {
     try {
         vcycle(c, 0);
         ++c.launches;
-        launch_k(c.pdl, correct_kernel, row_blocks((long long)O.n0 * O.n1), outer_threads(O), 0, c.st, O, c.phi, c.mg[0].u);
+        launch_k(c.pdl, correct_march_kernel, kRedBlocks, kOuterThreads, 0, c.st, O, c.phi, c.mg[0].u);
         ++c.launches;
-        launch_k(c.pdl, outer_residual_kernel, kRedBlocks, outer_threads(O), 0, c.st, O, c.rho0, c.phi, c.mg[0].f, c.red_partials);
+        launch_k(c.pdl, outer_residual_march_kernel, kRedBlocks, kOuterThreads, 0, c.st, O, c.rho0, c.phi, c.mg[0].f, c.red_partials);
         ++c.launches;
         launch_k(c.pdl, reduce_partials_kernel, 1, 1024, 0, c.st, c.red_partials, kRedBlocks, 1, 0, &c.d_sc->red[2]);
         FOPIS_LAUNCH_CHECK();
@@ -1311,7 +1352,7 @@ void build_solve_graph(Ctx& c) {
         ++c.launches;
         launch_k(c.pdl, solve_prep_kernel, 1, 1, 0, main_st, c.d_sc, (double)M, allper ? 1 : 0);
         ++c.launches;
-        launch_k(c.pdl, outer_residual_kernel, kRedBlocks, outer_threads(O), 0, main_st, O, c.rho0, c.phi, c.mg[0].f, c.red_partials);
+        launch_k(c.pdl, outer_residual_march_kernel, kRedBlocks, kOuterThreads, 0, main_st, O, c.rho0, c.phi, c.mg[0].f, c.red_partials);
         ++c.launches;
         launch_k(c.pdl, reduce_partials_kernel, 1, 1024, 0, main_st, c.red_partials, kRedBlocks, 1, 0, &c.d_sc->red[2]);
         FOPIS_LAUNCH_CHECK();
@@ -1343,9 +1384,9 @@ void build_solve_graph(Ctx& c) {
         const int64_t b0 = c.launches;
         vcycle(c, 0);
         ++c.launches;
-        launch_k(c.pdl, correct_kernel, row_blocks((long long)O.n0 * O.n1), outer_threads(O), 0, c.st, O, c.phi, c.mg[0].u);
+        launch_k(c.pdl, correct_march_kernel, kRedBlocks, kOuterThreads, 0, c.st, O, c.phi, c.mg[0].u);
         ++c.launches;
-        launch_k(c.pdl, outer_residual_kernel, kRedBlocks, outer_threads(O), 0, c.st, O, c.rho0, c.phi, c.mg[0].f, c.red_partials);
+        launch_k(c.pdl, outer_residual_march_kernel, kRedBlocks, kOuterThreads, 0, c.st, O, c.rho0, c.phi, c.mg[0].f, c.red_partials);
         ++c.launches;
         launch_k(c.pdl, reduce_partials_kernel, 1, 1024, 0, c.st, c.red_partials, kRedBlocks, 1, 0, &c.d_sc->red[2]);
         ++c.launches;
@@ -1407,7 +1448,7 @@ void mg_solve_host_loop(Ctx& c, double tol, int max_cycles, double* res_out, dou
     double fnorm = std::sqrt(std::max(0.0, fsq - (allper ? fsum * fsum / (double)M : 0.0)));
     if (!(fnorm > 0.0)) fnorm = 1.0;
     ++c.launches;
-    launch_k(c.pdl, outer_residual_kernel, kRedBlocks, outer_threads(O), 0, c.st, O, c.rho0, c.phi, c.mg[0].f, c.red_partials);
+    launch_k(c.pdl, outer_residual_march_kernel, kRedBlocks, kOuterThreads, 0, c.st, O, c.rho0, c.phi, c.mg[0].f, c.red_partials);
     ++c.launches;
     launch_k(c.pdl, reduce_partials_kernel, 1, 1024, 0, c.st, c.red_partials, kRedBlocks, 1, 0, &c.d_sc->red[2]);
     FOPIS_LAUNCH_CHECK();
