@@ -83,8 +83,10 @@ int solve_cap(const Ctx& c) { return c.p.max_vcycles > 0 ? c.p.max_vcycles : 100
 //  WARM     the current phi (the reference's PSOR continues from it).
 //  HISTORY  the first solve of a step (plasma charge only) starts from the
 //           previous step's first solve, the second solve (after the
-//           capacity-matrix redistribution) from the first plus the previous
-//           step's conductor response phi_final - phi_first.
+//           capacity-matrix redistribution) from the first plus the two
+//           previous steps' conductor responses phi_final - phi_first, scaled
+//           by the least-squares fit of this step's redistributed surface
+//           charge to theirs.
 //  LEARNED  HISTORY with the first solve seeded by the U-Net's increment.
 // Every start converges to the same tolerance. A solve that fails to converge
 // from the learned guess is redone from the history start, and one from a
@@ -109,7 +111,7 @@ int solve(Ctx& c, int kind) {
         learned = unet_before_solve(c) != 0;
         c.learned_used = learned ? 1 : 0;
     } else if (hist && c.hist_ok) {
-        phi_axpy(c, c.phi, c.phi, c.phi_obj, 1.0);
+        conductor_start(c);
     }
     if (mode == FOPIS_GUESS_ZERO) FOPIS_CUDA(cudaMemsetAsync(c.phi, 0, sizeof(double) * c.N, c.st));
     int rc = mg_solve(c, solve_tol(c), solve_cap(c));
@@ -133,10 +135,10 @@ int solve(Ctx& c, int kind) {
             if (kind == SOLVE_ONLY) history_valid(c);
         }
     } else if (track) {
-        phi_axpy(c, c.phi_obj, c.phi, c.phi_prev, -1.0);
+        conductor_record(c, c.phi_prev);
         history_valid(c);
     }
-    if (!track) c.hist_ok = false;
+    if (!track) { c.hist_ok = false; c.obj_hist = 0; }
     return rc;
 }
 
@@ -258,6 +260,7 @@ int fopis_create(const fopis_params* p, int device, void** out) {
         FOPIS_CUDA(cudaMalloc(&x.phi_prev, sizeof(double) * x.N));
         FOPIS_CUDA(cudaMalloc(&x.phi_prev2, sizeof(double) * x.N));
         FOPIS_CUDA(cudaMalloc(&x.phi_obj, sizeof(double) * x.N));
+        FOPIS_CUDA(cudaMalloc(&x.phi_obj2, sizeof(double) * x.N));
         FOPIS_CUDA(cudaMalloc(&x.scratch64, sizeof(double) * x.N));
         FOPIS_CUDA(cudaMalloc(&x.E, sizeof(float4) * x.N));
         if (x.fp64) {
@@ -277,6 +280,7 @@ int fopis_create(const fopis_params* p, int device, void** out) {
         FOPIS_CUDA(cudaMemset(x.phi_prev, 0, sizeof(double) * x.N));
         FOPIS_CUDA(cudaMemset(x.phi_prev2, 0, sizeof(double) * x.N));
         FOPIS_CUDA(cudaMemset(x.phi_obj, 0, sizeof(double) * x.N));
+        FOPIS_CUDA(cudaMemset(x.phi_obj2, 0, sizeof(double) * x.N));
         FOPIS_CUDA(cudaMemset(x.E, 0, sizeof(float4) * x.N));
         FOPIS_CUDA(cudaMemset(x.cellmap, 0, x.N));
         FOPIS_CUDA(cudaMemset(x.node_cmat, 0xff, sizeof(int32_t) * x.N));
@@ -327,10 +331,10 @@ void fopis_destroy(void* h) {
     for (int s = 0; s < FOPIS_MAX_SPECIES; ++s) if (c->brick_start[s]) cudaFree(c->brick_start[s]);
     for (auto& o : c->objs) {
         cudaFree(o.nodes); cudaFree(o.C); cudaFree(o.colsum); cudaFree(o.charge_tmp);
-        cudaFree(o.charge_map); cudaFree(o.phis); cudaFree(o.scal); cudaFree(o.lit);
+        cudaFree(o.charge_map); cudaFree(o.phis); cudaFree(o.scal); cudaFree(o.lit); cudaFree(o.drho_buf);
     }
     mg_free(*c);
-    void* ptrs[] = {c->rho_i64, c->rho0, c->phi, c->phi_prev, c->phi_prev2, c->phi_obj, c->scratch64, c->E, c->E64, c->cellmap,
+    void* ptrs[] = {c->rho_i64, c->rho0, c->phi, c->phi_prev, c->phi_prev2, c->phi_obj, c->phi_obj2, c->scratch64, c->E, c->E64, c->cellmap,
                     c->node_cmat, c->sort_count, c->sort_offset, c->scan_partials, c->ab.cell, c->ab.ox,
                     c->ab.oy, c->ab.oz, c->ab.vx, c->ab.vy, c->ab.vz, c->ab.species, c->ab.object, c->d_sc};
     for (void* q : ptrs) if (q) cudaFree(q);
@@ -457,6 +461,7 @@ int fopis_initialize(void* h) {
         rho_zero(c);
         launch_deposit_all(c);
         c.hist_ok = false;
+        c.obj_hist = 0;
         int rc1 = FOPIS_OK;
         rho_tail(c, &rc1);
         const int rc2 = solve(c, solve_kind_after_rho(c));

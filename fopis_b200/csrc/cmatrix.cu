@@ -127,9 +127,10 @@ __global__ void potential_kernel(const double* phi, const int32_t* nodes, const 
     }
 }
 
-// delta rho_i = sum_j C_ij (V - phi_j), added to rho0 at surface node i.
+// delta rho_i = sum_j C_ij (V - phi_j), added to rho0 at surface node i and
+// kept in drho_out for the start of the second solve.
 __global__ void drho_kernel(const double* C, int n, const double* phis, const double* scal, const int32_t* nodes,
-                            double* rho0) {
+                            double* rho0, double* drho_out) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     const double V = scal[0];
@@ -138,8 +139,51 @@ __global__ void drho_kernel(const double* C, int n, const double* phis, const do
         const double* row = C + (long long)i * n;
         for (int j = lane; j < n; j += 32) s += row[j] * (V - phis[j]);
         s = wsum(s);
-        if (lane == 0) rho0[nodes[i]] += s;
+        if (lane == 0) { rho0[nodes[i]] += s; drho_out[i] = s; }
     }
+}
+
+// Start of the second solve: this step's redistributed charge d0 fitted in
+// least squares by the two previous steps' (d1, d2) over the surface nodes of
+// every object; the coefficients scale the conductor responses those charges
+// produced. One term while only one response is recorded, and alpha = 1 (the
+// previous response as it is) when the fit is degenerate.
+struct ConductorFit {
+    int nobj;
+    int terms;
+    const double* d0[FOPIS_MAX_OBJECTS];
+    const double* d1[FOPIS_MAX_OBJECTS];
+    const double* d2[FOPIS_MAX_OBJECTS];
+    int n[FOPIS_MAX_OBJECTS];
+};
+
+__global__ void conductor_fit_kernel(ConductorFit f, double* alpha) {
+    double s11 = 0.0, s12 = 0.0, s22 = 0.0, b1 = 0.0, b2 = 0.0;
+    for (int o = 0; o < f.nobj; ++o)
+        for (int i = threadIdx.x; i < f.n[o]; i += blockDim.x) {
+            const double x0 = f.d0[o][i], x1 = f.d1[o][i], x2 = f.terms > 1 ? f.d2[o][i] : 0.0;
+            s11 += x1 * x1; s12 += x1 * x2; s22 += x2 * x2; b1 += x0 * x1; b2 += x0 * x2;
+        }
+    s11 = bsum(s11); s12 = bsum(s12); s22 = bsum(s22); b1 = bsum(b1); b2 = bsum(b2);
+    if (threadIdx.x == 0) {
+        double a1 = 1.0, a2 = 0.0;
+        const double det = s11 * s22 - s12 * s12;
+        if (f.terms > 1 && det > 1e-10 * s11 * s22) {
+            a1 = (b1 * s22 - b2 * s12) / det;
+            a2 = (b2 * s11 - b1 * s12) / det;
+        } else if (s11 > 0.0) {
+            a1 = b1 / s11;
+        }
+        alpha[0] = a1;
+        alpha[1] = a2;
+    }
+}
+
+__global__ void conductor_start_kernel(double* phi, const double* r1, const double* r2, const double* alpha,
+                                       long long N) {
+    const double a1 = alpha[0], a2 = alpha[1];
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x)
+        phi[t] += a1 * r1[t] + (a2 != 0.0 ? a2 * r2[t] : 0.0);
 }
 
 // Spacecraft::is{X,Y,Z}surfacePoint at an integer node (dx1 = 0), host side.
@@ -212,6 +256,9 @@ void object_upload(Ctx& c, ObjectDev& o, const fopis_object_desc* d, int id) {
     FOPIS_CUDA(cudaMalloc(&o.charge_tmp, sizeof(long long) * (size_t)c.nsp * o.n));
     FOPIS_CUDA(cudaMalloc(&o.charge_map, sizeof(double) * (size_t)c.nsp * o.n));
     FOPIS_CUDA(cudaMalloc(&o.phis, sizeof(double) * o.n));
+    FOPIS_CUDA(cudaMalloc(&o.drho_buf, sizeof(double) * 3 * o.n));
+    FOPIS_CUDA(cudaMemset(o.drho_buf, 0, sizeof(double) * 3 * o.n));
+    for (int q = 0; q < 3; ++q) o.drho[q] = o.drho_buf + (size_t)q * o.n;
     FOPIS_CUDA(cudaMalloc(&o.scal, sizeof(double) * 8));
     FOPIS_CUDA(cudaMemset(o.charge_tmp, 0, sizeof(long long) * (size_t)c.nsp * o.n));
     FOPIS_CUDA(cudaMemset(o.charge_map, 0, sizeof(double) * (size_t)c.nsp * o.n));
@@ -341,7 +388,7 @@ void redistribute(Ctx& c) {
         potential_kernel<<<1, 1024, 0, c.st>>>(c.phi, o.nodes, o.colsum, o.n, o.total, o.is_fixed, o.fixed_potential,
                                                 o.phis, o.scal);
         ++c.launches;
-        drho_kernel<<<grid1((long long)o.n * 32), kT, 0, c.st>>>(o.C, o.n, o.phis, o.scal, o.nodes, c.rho0);
+        drho_kernel<<<grid1((long long)o.n * 32), kT, 0, c.st>>>(o.C, o.n, o.phis, o.scal, o.nodes, c.rho0, o.drho[0]);
         FOPIS_LAUNCH_CHECK();
         double sc[2];
         FOPIS_CUDA(cudaMemcpyAsync(sc, o.scal, sizeof(double) * 2, cudaMemcpyDeviceToHost, c.st));
@@ -350,6 +397,38 @@ void redistribute(Ctx& c) {
         o.total_charge = sc[1];
     }
     glue_copy(c, c.rho0);
+}
+
+// phi (the first solve's result) += the fitted conductor responses.
+void conductor_start(Ctx& c) {
+    if (c.obj_hist < 1 || c.objs.empty()) return;
+    ConductorFit f{};
+    f.nobj = (int)c.objs.size();
+    f.terms = c.obj_hist >= 2 ? 2 : 1;
+    for (int o = 0; o < f.nobj; ++o) {
+        f.d0[o] = c.objs[o].drho[0]; f.d1[o] = c.objs[o].drho[1]; f.d2[o] = c.objs[o].drho[2];
+        f.n[o] = c.objs[o].n;
+    }
+    double* alpha = &c.d_sc->red[12];
+    ++c.launches;
+    conductor_fit_kernel<<<1, 1024, 0, c.st>>>(f, alpha);
+    ++c.launches;
+    conductor_start_kernel<<<grid1((long long)c.N), kT, 0, c.st>>>(c.phi, c.phi_obj, c.phi_obj2, alpha, (long long)c.N);
+    FOPIS_LAUNCH_CHECK();
+}
+
+// After the second solve: the response phi_final - phi_first becomes the
+// newest history entry, with this step's redistributed charge.
+void conductor_record(Ctx& c, const double* phi_first) {
+    std::swap(c.phi_obj, c.phi_obj2);
+    phi_axpy(c, c.phi_obj, c.phi, phi_first, -1.0);
+    for (auto& o : c.objs) {
+        double* oldest = o.drho[2];
+        o.drho[2] = o.drho[1];
+        o.drho[1] = o.drho[0];
+        o.drho[0] = oldest;
+    }
+    c.obj_hist = std::min(2, c.obj_hist + 1);
 }
 
 }  // namespace fopis

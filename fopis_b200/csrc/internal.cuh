@@ -137,6 +137,8 @@ struct ObjectDev {
     long long* charge_tmp = nullptr;   // [nsp][n] fixed point (2^-40)
     double* charge_map = nullptr;      // [nsp][n]
     double* phis = nullptr;            // phi at the surface nodes
+    double* drho_buf = nullptr;        // [3][n] redistributed surface charge of the last three steps
+    double* drho[3] = {nullptr, nullptr, nullptr};   // this step, one and two steps back
     double* scal = nullptr;            // [4]: potential, total charge, sum C phi
     int is_fixed = 0;
     double fixed_potential = 0.0, offset = 0.0;
@@ -184,6 +186,8 @@ struct Ctx {
     double* phi_prev = nullptr;      // first-solve phi of the previous step
     double* phi_prev2 = nullptr;     // first-solve phi two steps back
     double* phi_obj = nullptr;       // previous step's conductor response
+    double* phi_obj2 = nullptr;      // the one before it
+    int obj_hist = 0;                // conductor responses recorded (0..2)
     double* scratch64 = nullptr;     // [N] residual / field export
     float4* E = nullptr;             // nodal E (FP32) for the gather
     Vec4d* E64 = nullptr;            // nodal E (FP64) for the gather of the FP64 mode
@@ -274,6 +278,8 @@ void object_upload(Ctx& c, ObjectDev& o, const fopis_object_desc* d, int id);
 void cmatrix_build(Ctx& c, int id);
 void cmatrix_set(Ctx& c, int id, const double* hostC);
 void redistribute(Ctx& c);
+void conductor_start(Ctx& c);
+void conductor_record(Ctx& c, const double* phi_first);
 void objects_step_begin(Ctx& c);
 void objects_step_end(Ctx& c);
 // unet.cu (learned initial guess)
