@@ -652,7 +652,13 @@ struct PadLv {
     int size;         // padded nodes
     int off;          // float offset of u; f and r follow
     float inv_scale;
+    int n2h;          // (n2 + 1) / 2: node pairs along c
+    // x / d as __umulhi(x, m) with m = ceil(2^32 / d), exact for x, d < 2^16;
+    // m = 0 stands for d = 1 (whose multiplier 2^32 does not fit)
+    unsigned m2, m12, m2h, m12h;   // d = n2, n1 n2, n2h, n1 n2h
 };
+__host__ inline unsigned div_magic(unsigned d) { return d <= 1 ? 0u : (unsigned)((0x100000000ull + d - 1) / d); }
+__device__ __forceinline__ int qdiv(int x, unsigned m) { return m ? (int)__umulhi((unsigned)x, m) : x; }
 struct PadCycle {
     int nl;
     PadLv lv[kMaxSmLevels];
@@ -670,17 +676,43 @@ __device__ __forceinline__ void pad_for_each(const PadLv& L, Body body) {
     const int bd = blockDim.x, t = threadIdx.x;
     if (n12 >= bd) {
         for (int q = t; q < n12; q += bd) {
-            const int b = q / L.n2, c = q - b * L.n2;
+            const int b = qdiv(q, L.m2), c = q - b * L.n2;
             const int p0 = L.si + (b + 1) * L.sj + (c + 1);
             for (int a = 0; a < L.n0; ++a) body(p0 + a * L.si, a, b, c);
         }
     } else {
         const int astep = bd / n12;
         if (t < astep * n12) {
-            const int a0 = t / n12, q = t - a0 * n12;
-            const int b = q / L.n2, c = q - b * L.n2;
+            const int a0 = qdiv(t, L.m12), q = t - a0 * n12;
+            const int b = qdiv(q, L.m2), c = q - b * L.n2;
             const int p0 = (a0 + 1) * L.si + (b + 1) * L.sj + (c + 1);
             for (int a = a0; a < L.n0; a += astep) body(p0 + (a - a0) * L.si, a, b, c);
+        }
+    }
+}
+// The nodes of one colour ((a + b + c) % 2 == color): threads take node pairs
+// along c, so every active thread updates a node at each a it visits.
+template <typename Body>
+__device__ __forceinline__ void pad_for_each_color(const PadLv& L, int color, Body body) {
+    const int n12 = L.n1 * L.n2h;
+    const int bd = blockDim.x, t = threadIdx.x;
+    if (n12 >= bd) {
+        for (int q = t; q < n12; q += bd) {
+            const int b = qdiv(q, L.m2h), h = q - b * L.n2h;
+            for (int a = 0; a < L.n0; ++a) {
+                const int c = 2 * h + ((a + b + color) & 1);
+                if (c < L.n2) body((a + 1) * L.si + (b + 1) * L.sj + (c + 1));
+            }
+        }
+    } else {
+        const int astep = bd / n12;
+        if (t < astep * n12) {
+            const int a0 = qdiv(t, L.m12h), q = t - a0 * n12;
+            const int b = qdiv(q, L.m2h), h = q - b * L.n2h;
+            for (int a = a0; a < L.n0; a += astep) {
+                const int c = 2 * h + ((a + b + color) & 1);
+                if (c < L.n2) body((a + 1) * L.si + (b + 1) * L.sj + (c + 1));
+            }
         }
     }
 }
@@ -693,8 +725,7 @@ template <typename T>
 __device__ void pad_smooth(const PadLv& L, T* u, const T* f, int sweeps, T inv_scale, T omega) {
     for (int sw = 0; sw < sweeps; ++sw)
         for (int color = 0; color < 2; ++color) {
-            pad_for_each(L, [&](int p, int a, int b, int c) {
-                if (((a + b + c) & 1) != color) return;
+            pad_for_each_color(L, color, [&](int p) {
                 u[p] = ((T)1 - omega) * u[p] + omega * (pad_nsum(u, p, L.sj, L.si) + f[p] * inv_scale) * (T)(1.0 / 6.0);
             });
             __syncthreads();
@@ -1149,6 +1180,11 @@ void coarse_cycle(Ctx& c) {
             L.size = (int)padded_size(m);
             L.off = off;
             L.inv_scale = (float)(1.0 / m.scale);
+            L.n2h = (L.n2 + 1) / 2;
+            L.m2 = div_magic((unsigned)L.n2);
+            L.m12 = div_magic((unsigned)(L.n1 * L.n2));
+            L.m2h = div_magic((unsigned)L.n2h);
+            L.m12h = div_magic((unsigned)(L.n1 * L.n2h));
             off += 3 * L.size;
         }
         d.floats = off;
