@@ -1016,6 +1016,7 @@ bool level_rb(const MGLevel& m) {
 // thread takes march_depth consecutive a (more per thread on larger levels,
 // where the grid still fills the GPU).
 constexpr int kMarchMin = 24;
+constexpr int kRestrictMarchMin = 8;   // restriction onto levels this size and up marches too
 int march_depth(const MGLevel& m) { return m.n[0] >= 96 ? 4 : (m.n[0] >= 48 ? 2 : 1); }
 
 // Launch grid of the marching kernels over n[2]/cols_per_thread columns.
@@ -1112,7 +1113,7 @@ void vcycle(Ctx& c, int l) {
     residual(c, m);
     const dim3 blk(kMarchX, kMarchY);
     ++c.launches;
-    if (n.n[0] >= kMarchMin) {
+    if (n.n[0] >= kRestrictMarchMin) {
         const int A = march_depth(n);
         const dim3 grd = march_grid(n.n, A, 1);
         if (A == 4) launch_k(c.pdl, restrict_march_kernel<4>, grd, blk, 0, c.st, lv(m), lv(n));
@@ -1351,13 +1352,23 @@ __global__ void solve_init_kernel(DevScalars* sc, cudaGraphConditionalHandle h) 
     const bool go = isfinite(res) && res > sc->red[6] * sc->red[5] && sc->red[7] > 0.0;
     cudaGraphSetConditional(h, go ? 1u : 0u);
 }
-__global__ void solve_decide_kernel(DevScalars* sc, cudaGraphConditionalHandle h) {
+// End of a refinement iteration: the squared residual norm from the outer
+// residual's block partials (one block), then the loop condition.
+__global__ void solve_decide_kernel(const double* partial, int nparts, DevScalars* sc,
+                                    cudaGraphConditionalHandle h) {
     pdl_entry();
-    const double n = sc->red[8] + 1.0;
-    sc->red[8] = n;
-    const double res = sqrt(sc->red[2]);
-    const bool go = isfinite(res) && res > sc->red[6] * sc->red[5] && n < sc->red[7];
-    cudaGraphSetConditional(h, go ? 1u : 0u);
+    __shared__ double red[32];
+    double v = 0.0;
+    for (int t = threadIdx.x; t < nparts; t += blockDim.x) v += partial[t];
+    v = bsum(v, red);
+    if (threadIdx.x == 0) {
+        sc->red[2] = v;
+        const double n = sc->red[8] + 1.0;
+        sc->red[8] = n;
+        const double res = sqrt(v);
+        const bool go = isfinite(res) && res > sc->red[6] * sc->red[5] && n < sc->red[7];
+        cudaGraphSetConditional(h, go ? 1u : 0u);
+    }
 }
 
 // Records the whole solve once per context: norms of f, initial residual, a
@@ -1424,9 +1435,8 @@ void build_solve_graph(Ctx& c) {
         ++c.launches;
         launch_k(c.pdl, outer_residual_march_kernel, kRedBlocks, kOuterThreads, 0, c.st, O, c.rho0, c.phi, c.mg[0].f, c.red_partials);
         ++c.launches;
-        launch_k(c.pdl, reduce_partials_kernel, 1, 1024, 0, c.st, c.red_partials, kRedBlocks, 1, 0, &c.d_sc->red[2]);
-        ++c.launches;
-        launch_k(c.pdl, solve_decide_kernel, 1, 1, 0, c.st, c.d_sc, handle);
+        launch_k(c.pdl, solve_decide_kernel, 1, 1024, 0, c.st, (const double*)c.red_partials, kRedBlocks, c.d_sc,
+                 handle);
         FOPIS_LAUNCH_CHECK();
         body = c.launches - b0;
         c.st = main_st;
