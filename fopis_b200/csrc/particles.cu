@@ -436,7 +436,9 @@ __global__ void __launch_bounds__(kTileThreads, MINB) push_tile_kernel(PushArgs 
     __syncthreads();
     for (long long c0 = p0; c0 < p1; c0 += kChunk) {
         const int m = (int)min((long long)kChunk, p1 - c0);
-        for (int q = tid; q < kChunk; q += kTileThreads) {
+#pragma unroll
+        for (int rr = 0; rr < kRun; ++rr) {
+            const int q = tid + rr * kTileThreads;
             const int d = padi(q);
             if (q < m) {
                 s_cell[d] = a.p.cell[c0 + q];
@@ -503,7 +505,10 @@ __global__ void __launch_bounds__(kTileThreads, MINB) push_tile_kernel(PushArgs 
         }
         if (cur >= 0) tile_flush(t_lo, t_hi, cur, acc);
         __syncthreads();
-        for (int q = tid; q < m; q += kTileThreads) {
+#pragma unroll
+        for (int rr = 0; rr < kRun; ++rr) {
+            const int q = tid + rr * kTileThreads;
+            if (q >= m) break;
             const int d = padi(q);
             a.p.cell[c0 + q] = s_cell[d];
             a.p.ox[c0 + q] = s_f[0][d]; a.p.oy[c0 + q] = s_f[1][d]; a.p.oz[c0 + q] = s_f[2][d];
