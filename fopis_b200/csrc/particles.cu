@@ -372,8 +372,7 @@ constexpr int kTile = kWX * kWY * kWZ;             // 9 x 9 x 13 nodes
 __device__ __forceinline__ void tile_add(unsigned* lo, unsigned* hi, int idx, unsigned long long w) {
     const unsigned wl = (unsigned)w, wh = (unsigned)(w >> 32);
     const unsigned old = atomicAdd(lo + idx, wl);
-    const unsigned carry = (old + wl < old) ? 1u : 0u;
-    if (wh + carry) atomicAdd(hi + idx, wh + carry);
+    atomicAdd(hi + idx, wh + ((old + wl < old) ? 1u : 0u));
 }
 
 // RUN consecutive particles per thread; a pass stages kTileThreads * RUN
@@ -390,11 +389,13 @@ __device__ __forceinline__ int padi(int q) { return q + (q >> 5); }
 // 0.2-0.9 ms slower per 128^3 step; runs of 2 the same.
 constexpr int kPushRun = 4;
 
+// Every corner is added, zero weights included (they are rare, and adding
+// zero changes nothing): the tests cost more than the atomics they skip.
 __device__ __forceinline__ void tile_flush(unsigned* lo, unsigned* hi, int tb, const unsigned long long acc[8]) {
 #pragma unroll
     for (int t = 0; t < 8; ++t) {
         const int off = ((t >> 2) ? kWY * kWZ : 0) + (((t >> 1) & 1) ? kWZ : 0) + (t & 1);
-        if (acc[t]) tile_add(lo, hi, tb + off, acc[t]);
+        tile_add(lo, hi, tb + off, acc[t]);
     }
 }
 
