@@ -479,15 +479,17 @@ __global__ void __launch_bounds__(kTileThreads, MINB) push_tile_kernel(PushArgs 
                 const unsigned wz[2] = {(unsigned)kDepositOne - qd, qd};
                 if (inwin) {
                     const int tb = (li * kWY + lj) * kWZ + lk;
-                    if (tb != cur) {
+                    if (tb != cur) {   // a new run starts with this particle's weights
                         if (cur >= 0) tile_flush(t_lo, t_hi, cur, acc);
                         cur = tb;
 #pragma unroll
-                        for (int t = 0; t < 8; ++t) acc[t] = 0ull;
-                    }
+                        for (int t = 0; t < 8; ++t)
+                            acc[t] = (unsigned long long)wx[t >> 2] * wy[(t >> 1) & 1] * wz[t & 1];
+                    } else {
 #pragma unroll
-                    for (int t = 0; t < 8; ++t)
-                        acc[t] += (unsigned long long)wx[t >> 2] * wy[(t >> 1) & 1] * wz[t & 1];
+                        for (int t = 0; t < 8; ++t)
+                            acc[t] += (unsigned long long)wx[t >> 2] * wy[(t >> 1) & 1] * wz[t & 1];
+                    }
                 } else {
                     const long long gb = lin(a.g, st.i, st.j, st.k);
 #pragma unroll
