@@ -51,32 +51,86 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock and throttle reasons sampled during the timed region: NVML read
+    every 10 ms from a thread (so a timed region of ~0.1 s still gives about ten
+    samples), nvidia-smi every 200 ms where NVML is unavailable. Reading only:
+    no clock or other GPU setting is changed."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
-    def __init__(self, index: int):
+    def __init__(self, index: int, period_s: float = 0.01):
         self.index = index
+        self.period = period_s
         self.proc = None
         self.lines = []
+        self.samples = []          # (sm_mhz, max_mhz, set of reason names)
+        self.stop = threading.Event()
+        self.thread = None
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _poll_nvml(self, nv, h):
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((float(sm), float(mx), {k for k, b in bits.items() if r & b}))
+            except Exception:
+                pass
+            self.stop.wait(self.period)
 
     def __enter__(self):
+        try:
+            nv, h = self._nvml_handle()
+            self.thread = threading.Thread(target=self._poll_nvml, args=(nv, h), daemon=True)
+            self.thread.start()
+            self.source = "nvml 10 ms"
+            return self
+        except Exception:
+            pass
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             threading.Thread(target=self._read, daemon=True).start()
+            self.source = "nvidia-smi 200 ms"
         except OSError:
             self.proc = None
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            f = [x.strip() for x in line.strip().split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                self.samples.append((float(f[1]), float(f[2]),
+                                     {nm for nm, v in zip(self.NAMES, f[5:9]) if v.lower() == "active"}))
+            except ValueError:
+                continue
 
     def __exit__(self, *a):
+        self.stop.set()
+        if self.thread:
+            self.thread.join(timeout=5)
         if self.proc:
             self.proc.terminate()
             try:
@@ -85,22 +139,13 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
+        sm = [x[0] for x in self.samples]
+        mx = self.samples[-1][1] if self.samples else None
+        reasons = set()
+        for x in self.samples:
+            reasons |= x[2]
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": self.source}
 
 
 def dist_setup():
@@ -434,17 +479,18 @@ def main():
             "scaling": "weak", "vs_baseline": None, "data": "synthetic (Philox-seeded Maxwellian plasma)",
             "dtype": ("fp32 particles, int64 fixed-point rho, fp32 smoother in fp64 refinement" if args.precision == "mixed"
                       else "fp64 particles, fp64 deposit, fp32 smoother in fp64 refinement"),
+            # the same dict on both arms: what is run, not how each arm runs it
             "config": {"workload": workload_desc(args.workload, args.ppc),
-                       "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (particle state ~3.8 GB)",
-                       "sort_interval": args.sort_interval,
-                       "poisson_start": {"warm": "previous phi (the reference's)",
-                                         "history": "per-solve history (first solve from the previous first "
-                                                    "solve, second from it + previous conductor response)"}[args.guess]}}
+                       "parallelism": f"replicas x{world}", "sort_interval": args.sort_interval}}
     if args.impl == "reference":
         if rank != 0:
             return
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle as orc
         from fopis_b200 import config
-        cfg = config.workload(args.workload, ppc=args.ppc, seed=20251203)
+        # bodies parsed by the oracle's own .obj loader: nothing of libfopis_gpu.so
+        # is loaded on this arm
+        cfg = config.workload(args.workload, ppc=args.ppc, seed=20251203, obj_parser=orc.parse_obj)
         # untimed setup: the capacity matrix the reference would load from its
         # cache, computed exactly on the host (six Dirichlet faces)
         try:
@@ -452,12 +498,12 @@ def main():
         except NotImplementedError as e:
             print(json.dumps({"impl": "reference", "unavailable": f"capacity matrix of this body: {e}"}))
             return
-        warm = min(args.warmup, 1)   # the CPU path has nothing to warm beyond its first step
+        warm = args.warmup
         v, dt, n, it, done = run_oracle(cfg, Cm, threads, args.steps, warm, args.ref_budget_s)
         line = dict(base, impl="reference", value=v, steps=done, warmup=warm, ms_per_step=dt * 1e3 / done, n_gpus=1)
         line["dtype"] = "fp64 particles and fields (CPU restatement of the reference path)"
-        line["config"] = dict(base["config"], poisson_start="the reference's PSOR continues from the previous phi",
-                              l2="CPU run (no GPU caches involved)")
+        line["poisson_start"] = "the reference's PSOR continues from the previous phi"
+        line["l2"] = "CPU run (no GPU caches involved)"
         line["cpu_baseline"] = {"value": v, "unit": "particle-steps/s", "cores": threads, "kind": "port",
                                 "sample": f"{done} full step(s) of the workload ({n} particles) after {warm} untimed, "
                                           f"reference PSOR ({it} sweeps last solve)"
@@ -487,9 +533,11 @@ def main():
                         "bytes_per_particle": push_bytes}
     line["clocks"] = res["clocks"]
     state_gb = res["particles"] * (28 if args.precision == "mixed" else 52) / 1e9
-    line["config"] = dict(line["config"], l2=(f"inputs larger than L2: particle state {state_gb:.2f} GB, L2 126 MB"
-                                              if state_gb > 0.126 else
-                                              f"particle state {state_gb:.3f} GB fits in L2 (126 MB)"))
+    line["l2"] = (f"inputs larger than L2: particle state {state_gb:.2f} GB, L2 126 MB" if state_gb > 0.126 else
+                  f"particle state {state_gb:.3f} GB fits in L2 (126 MB)")
+    line["poisson_start"] = {"warm": "previous phi (the reference's)",
+                             "history": "per-solve history (first solve from the previous first solve, second from "
+                                        "it + previous conductor response)"}[args.guess]
     line["gpu_launches"] = res["launches"]
     line["solve_mode"] = res["solve_mode"]
     line["vcycles_per_step"] = res["vcycles_per_step"]

@@ -250,12 +250,16 @@ def box_obj_text(boxes: Sequence[Tuple[Tuple[int, int, int], Tuple[int, int, int
     return "\n".join(out) + "\n"
 
 
-def objects_from_boxes(boxes, nxyz, name="Spacecraft", emit_species=-1, fixed=None, offset=0.0) -> ObjectInfo:
+def objects_from_boxes(boxes, nxyz, name="Spacecraft", emit_species=-1, fixed=None, offset=0.0,
+                       obj_parser=None) -> ObjectInfo:
+    """The conductor made of `boxes`, written as a MagicaVoxel .obj and parsed by
+    `obj_parser(path, nx, ny, nz) -> (nodes, cells)` (default: fopis_parse_obj
+    of this library)."""
     fd, path = tempfile.mkstemp(suffix=".obj")
     with os.fdopen(fd, "w") as f:
         f.write(box_obj_text(boxes))
     try:
-        nodes, cells = parse_obj(path, *nxyz)
+        nodes, cells = (obj_parser or parse_obj)(path, *nxyz)
     finally:
         os.unlink(path)
     return ObjectInfo(name=name, nodes=nodes, cells=cells, is_potential_fixed=int(fixed is not None),
@@ -270,8 +274,9 @@ def plasma_units(n0: float = 1e7, te_ev: float = 1.0, dt_omega: float = 0.1):
     return lam * (1.0 - 1e-6), dt_omega / wpe
 
 
-def workload(name: str, ppc: Optional[int] = None, seed: int = 20251203, **kw) -> SimConfig:
-    """Synthetic configurations:
+def workload(name: str, ppc: Optional[int] = None, seed: int = 20251203, obj_parser=None, **kw) -> SimConfig:
+    """Synthetic configurations (obj_parser: the .obj loader for the bodies,
+    default this library's fopis_parse_obj):
     periodic32   32^3 cells periodic, 16 ppc/species, no object (CPU-runnable case);
     cube64       64^3 cells Dirichlet + injection, 8^3 cube conductor, 32 ppc;
     cube128      128^3 cells Dirichlet + injection, 16^3 cube, photoemission from +x;
@@ -313,7 +318,7 @@ def workload(name: str, ppc: Optional[int] = None, seed: int = 20251203, **kw) -
     objs = []
     if boxes:
         emit = next((k for k, s in enumerate(species) if s.kind == "photoelectron"), -1)
-        objs.append(objects_from_boxes(boxes, nxyz, emit_species=emit))
+        objs.append(objects_from_boxes(boxes, nxyz, emit_species=emit, obj_parser=obj_parser))
     return SimConfig(params=p, norm=norm, species=species, objects=objs, dx=dx, dt=dt)
 
 

@@ -295,17 +295,19 @@ int fopis_unet_tensor(void* ctx, int which, float* host, int64_t cap, int64_t* c
 
 /* Field::getEfieldEnergy's value (the quantity fopis_get_energy reports as
  * efield_energy) for a potential the caller owns, computed without allocating
- * any device memory. For callers that cannot call cudaMalloc: code recorded
- * into a CUDA graph by stream capture, hosts that give the library only memory
- * from their own pool, loops that forbid allocator calls after start-up.
+ * any device memory. For callers that cannot call cudaMalloc once their run
+ * loop has started: hosts that give the library only memory from their own
+ * pool allocator, and real-time loops that forbid allocator calls because
+ * cudaMalloc/cudaFree synchronise the device.
  * phi: device pointer, (nx+2)(ny+2)(nz+2) doubles in the glue layout;
  * energy: device pointer to one double, written as 0.5 eps0 sum(edge E^2);
  * stream: a cudaStream_t (NULL = legacy default stream); work is enqueued, not
- * waited for. Scratch is a 32 KB file-scope device array held by every GPU
- * that loads the library until exit, so nx*ny*nz may not exceed 33,554,432
- * (FOPIS_ERR_ARG beyond). All calls share that array: calls that overlap on
- * the GPU race. The first call on a device looks the array's address up with
- * cudaGetSymbolAddress and should come before any stream capture. This entry
+ * waited for. Scratch is a 32 KB file-scope device array held by every CUDA
+ * context that loads the library until that context ends, so nx*ny*nz may not
+ * exceed 33,554,432 (FOPIS_ERR_ARG beyond). All calls share that array: calls
+ * that overlap on the GPU race. The first call in a context (on a device)
+ * looks the array's address up with cudaGetSymbolAddress, keyed by the
+ * context's unique id, and should come before any stream capture. This entry
  * point has no counterpart in the reference. */
 int fopis_efield_energy_noalloc(const double* phi, int nx, int ny, int nz, double eps0, double* energy,
                                 void* stream);

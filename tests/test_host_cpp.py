@@ -2,6 +2,7 @@
 normalised parameters and object node lists as the Python loader, for a
 generated input and for the reference's own sample input."""
 import ctypes as C
+import os
 import subprocess
 from pathlib import Path
 
@@ -14,7 +15,9 @@ from host_input import write_input
 
 ROOT = Path(__file__).resolve().parent.parent
 RUN = ROOT / "fopis_b200" / "fopis_run"
-SAMPLE = Path("/root/reference/input_samples/input.json")
+# the reference checkout's sample input (FOPIS_REFERENCE), where given
+_REF = os.environ.get("FOPIS_REFERENCE")
+SAMPLE = Path(_REF) / "input_samples" / "input.json" if _REF else None
 
 
 def dump(path, tmp_path):
@@ -66,6 +69,6 @@ def test_cpp_loader_matches_python(built, tmp_path, photo):
 
 
 def test_cpp_loader_on_reference_sample(built, tmp_path):
-    if not SAMPLE.exists():
+    if SAMPLE is None or not SAMPLE.exists():
         pytest.skip("reference sample input not available")
     compare(dump(SAMPLE, tmp_path), config.load_input(str(SAMPLE)))

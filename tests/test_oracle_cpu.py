@@ -2,6 +2,7 @@
 Position header and analytic physics; the C ABI library's exports; the
 host-side set-up code. None of these touch a GPU."""
 import math
+import os
 import re
 from pathlib import Path
 
@@ -15,7 +16,8 @@ from fopis_b200.config import SpeciesInfo, make_params, plasma_units
 from helpers import random_particles
 
 ROOT = Path(__file__).resolve().parent.parent
-REFERENCE = Path("/root/reference")
+# the reference checkout, for its sample inputs (tests that need it skip when unset)
+REFERENCE = Path(os.environ["FOPIS_REFERENCE"]) if os.environ.get("FOPIS_REFERENCE") else None
 
 
 def test_philox_known_answers():
@@ -99,7 +101,8 @@ def test_obj_parser_matches_oracle(tmp_path, boxes, nxyz, n_cmat):
                         assert tuple(q) in surface
 
 
-@pytest.mark.skipif(not (REFERENCE / "input_samples/objects").exists(), reason="reference samples absent")
+@pytest.mark.skipif(REFERENCE is None or not (REFERENCE / "input_samples/objects").exists(),
+                    reason="FOPIS_REFERENCE unset or its sample inputs absent")
 @pytest.mark.parametrize("name", ["cube.obj", "4x4x4_Sphere.obj", "8x8x8_Sphere.obj", "20x2x2_Line.obj",
                                   "test_solar_array.obj"])
 def test_obj_parser_on_reference_samples(name):

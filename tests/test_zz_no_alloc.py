@@ -1,12 +1,13 @@
 """The allocation-free field-energy entry point, called through the C ABI.
 
-Callers that cannot allocate device memory — stream-captured CUDA graphs,
-hosts that only hand over memory from their own pool, loops that forbid
-allocator calls — get the field energy of a potential they own from
-fopis_efield_energy_noalloc, whose scratch is a file-scope device array. Its
-result must equal what fopis_get_energy reports for the same potential, on
-two calls in a row (the second call reuses the scratch the first one filled).
-This file sorts last so a stop-at-first-failure run has done every other test.
+Callers that cannot allocate device memory once their loop runs — hosts that
+only hand over memory from their own pool, real-time loops in which a
+device-synchronising cudaMalloc is not allowed — get the field energy of a
+potential they own from fopis_efield_energy_noalloc, whose scratch is a
+file-scope device array. Its result must equal what fopis_get_energy reports
+for the same potential, on two calls in a row (the second call reuses the
+scratch the first one filled). This file sorts last so a
+stop-at-first-failure run has done every other test.
 """
 import ctypes as C
 
