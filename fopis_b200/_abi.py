@@ -29,6 +29,7 @@ DEV_BAD_CMAT_NODE = 0x4
 DEV_SURFACE_NOT_FOUND = 0x8
 DEV_INJECT_REJECTS = 0x10
 DEV_NONFINITE = 0x20
+DEV_RHO_OVERFLOW = 0x40
 
 SPECIES_AMBIENT = 0
 SPECIES_PHOTOELECTRON = 1

@@ -17,7 +17,7 @@ namespace {
 thread_local std::string g_create_error;
 
 constexpr uint32_t kFatalBits = FOPIS_DEV_PARTICLE_OVERFLOW | FOPIS_DEV_ABSORB_OVERFLOW | FOPIS_DEV_BAD_CMAT_NODE |
-                                FOPIS_DEV_NONFINITE;
+                                FOPIS_DEV_NONFINITE | FOPIS_DEV_RHO_OVERFLOW;
 
 template <typename F>
 int guarded(void* h, F&& f) {
@@ -47,6 +47,11 @@ int check_device(Ctx& c) {
     if (st & (FOPIS_DEV_PARTICLE_OVERFLOW | FOPIS_DEV_ABSORB_OVERFLOW)) {
         c.err = "particle or absorbed-list capacity exceeded (device status " + std::to_string(st) + ")";
         return FOPIS_ERR_CAPACITY;
+    }
+    if (st & FOPIS_DEV_RHO_OVERFLOW) {
+        c.err = "device status " + std::to_string(st) + ": a node's fixed-point charge sum passed 2^64 "
+                "(more than 8192 full particle weights of one species on one node)";
+        return FOPIS_ERR_DEVICE;
     }
     if (st & kFatalBits) {
         c.err = "device status " + std::to_string(st) + ": invalid surface node or non-finite particle state";

@@ -34,8 +34,13 @@ int blocks(long long n) {
 // MPIw::Environment::sendRecvNodeScalar self-exchange, glue size 2
 // (src/MPI/Communicator.cpp:497-574): node 0 and node n both become their sum,
 // node 1 and node n+1 likewise.
+// A fixed-point fold sum that passed 2^64 (unsigned wrap) is latched as
+// FOPIS_DEV_RHO_OVERFLOW; FP64 sums have no such limit.
+__device__ __forceinline__ bool fold_wrapped(unsigned long long sum, unsigned long long a) { return sum < a; }
+__device__ __forceinline__ bool fold_wrapped(double, double) { return false; }
+
 template <typename W>
-__global__ void fold_kernel(W* rho, int nsp, long long N, G g, int axis) {
+__global__ void fold_kernel(W* rho, int nsp, long long N, G g, int axis, unsigned* status) {
     const int dims[3] = {g.cx, g.cy, g.cz};
     const int a1 = axis == 0 ? 1 : 0, a2 = axis == 2 ? 1 : 2;
     const long long plane = (long long)dims[a1] * dims[a2];
@@ -53,15 +58,17 @@ __global__ void fold_kernel(W* rho, int nsp, long long N, G g, int axis) {
         idx[axis] = 1; const long long p1 = L(g, idx[0], idx[1], idx[2]);
         idx[axis] = X - 1; const long long pn1 = L(g, idx[0], idx[1], idx[2]);
         const W s0 = a[p0] + a[pn], s1 = a[p1] + a[pn1];
+        if (fold_wrapped(s0, a[p0]) || fold_wrapped(s1, a[p1])) atomicOr(status, (unsigned)FOPIS_DEV_RHO_OVERFLOW);
         a[p0] = s0; a[pn] = s0; a[p1] = s1; a[pn1] = s1;
     }
 }
 
 struct Scales { double v[FOPIS_MAX_SPECIES]; };
 
-// A species accumulator as a number: int64 fixed point (mixed mode) or the
-// FP64 weight sum (FP64 mode).
-__device__ __forceinline__ double weight_value(unsigned long long w) { return (double)(long long)w; }
+// A species accumulator as a number: unsigned 64-bit fixed point (mixed mode;
+// the weights are nonnegative and the deposit latches any wrap) or the FP64
+// weight sum (FP64 mode).
+__device__ __forceinline__ double weight_value(unsigned long long w) { return (double)w; }
 __device__ __forceinline__ double weight_value(double w) { return w; }
 
 // rho[0] = sum_s q_s size_s W_s (x 2^-51 in fixed point) (RootGridField.cpp:1206-1214).
@@ -243,9 +250,10 @@ void rho_finalize(Ctx& c) {
         ++c.launches;
         if (c.fp64)
             fold_kernel<<<blocks(planes[axis] * c.nsp), kT, 0, c.st>>>(reinterpret_cast<double*>(c.rho_i64), c.nsp,
-                                                                       (long long)c.N, g, axis);
+                                                                       (long long)c.N, g, axis, &c.d_sc->status);
         else
-            fold_kernel<<<blocks(planes[axis] * c.nsp), kT, 0, c.st>>>(c.rho_i64, c.nsp, (long long)c.N, g, axis);
+            fold_kernel<<<blocks(planes[axis] * c.nsp), kT, 0, c.st>>>(c.rho_i64, c.nsp, (long long)c.N, g, axis,
+                                                                       &c.d_sc->status);
         FOPIS_LAUNCH_CHECK();
     }
     Scales sc{};

@@ -130,7 +130,8 @@ __device__ __forceinline__ long long corner_offset(const Grid& g, int t) {
 // their eight weights directly; lanes sharing a cell are reduced first with
 // three 17-bit-chunk redux.sync sums per corner (exact), then their leader adds.
 // Every lane of the warp must call this (dep selects the depositing ones).
-__device__ __forceinline__ void warp_deposit(unsigned long long* rho, const Grid& g, bool dep, long long base,
+// Returns true when one of this lane's additions wrapped a node past 2^64.
+__device__ __forceinline__ bool warp_deposit(unsigned long long* rho, const Grid& g, bool dep, long long base,
                                              float ox, float oy, float oz) {
     const int lane = threadIdx.x & 31;
     unsigned long long w[8];
@@ -142,10 +143,14 @@ __device__ __forceinline__ void warp_deposit(unsigned long long* rho, const Grid
     const long long key = dep ? base : -1ll - lane;
     const unsigned grp = __match_any_sync(kFull, key);
     const bool single = __popc(grp) == 1;
+    bool wrap = false;
     if (dep && single) {
 #pragma unroll
         for (int t = 0; t < 8; ++t)
-            if (w[t]) atomicAdd(rho + base + corner_offset(g, t), w[t]);
+            if (w[t]) {
+                const unsigned long long old = atomicAdd(rho + base + corner_offset(g, t), w[t]);
+                wrap |= old + w[t] < old;
+            }
     }
     unsigned multi = __ballot_sync(kFull, dep && !single);
     while (multi) {
@@ -161,11 +166,15 @@ __device__ __forceinline__ void warp_deposit(unsigned long long* rho, const Grid
             if (lane == leader) {
                 const unsigned long long tot = (unsigned long long)s0 + ((unsigned long long)s1 << 17) +
                                                ((unsigned long long)s2 << 34);
-                if (tot) atomicAdd(rho + base + corner_offset(g, t), tot);
+                if (tot) {
+                    const unsigned long long old = atomicAdd(rho + base + corner_offset(g, t), tot);
+                    wrap |= old + tot < old;
+                }
             }
         }
         multi &= ~members;
     }
+    return wrap;
 }
 
 // Warp-aggregated slot reservation on a 64-bit counter.
@@ -313,7 +322,7 @@ __device__ __forceinline__ bool absorb_check(const PushArgsT<T>& a, const PState
 // to the absorbed list (Spacecraft::distributeInnerParticleCharge,
 // Spacecraft.cpp:512-592, finished by absorb_kernel); the rest deposit their CIC
 // weights with warp-aggregated atomics. The fused step runs it only on the
-// unsorted tail; push_tile_kernel takes the sorted bricks.
+// unsorted tail; push_brick_kernel takes the sorted bricks.
 template <typename T, bool VEL, bool POS, bool DEP>
 __global__ void __launch_bounds__(kThreads) push_kernel(PushArgsT<T> a) {
     const long long n = (long long)min(*a.count, (unsigned long long)a.cap);
@@ -335,7 +344,8 @@ __global__ void __launch_bounds__(kThreads) push_kernel(PushArgsT<T> a) {
         if (DEP) {
             if (absorb_check(a, st, live)) live = false;
             if constexpr (sizeof(T) == 4) {
-                warp_deposit(a.rho, a.g, live, live ? lin(a.g, st.i, st.j, st.k) : 0, st.ox, st.oy, st.oz);
+                if (warp_deposit(a.rho, a.g, live, live ? lin(a.g, st.i, st.j, st.k) : 0, st.ox, st.oy, st.oz))
+                    atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_RHO_OVERFLOW);
             } else if (live) {
                 long long off[8];
 #pragma unroll
@@ -356,175 +366,246 @@ __global__ void __launch_bounds__(kThreads) push_kernel(PushArgsT<T> a) {
     }
 }
 
-// ------------------------------------------------------------------ brick-tiled fused push
-constexpr int kTileThreads = 256;
-constexpr int kHalo = 2;                           // cells a particle may drift out of its brick
-constexpr int kWX = kBX + 1 + 2 * kHalo, kWY = kBY + 1 + 2 * kHalo, kWZ = kBZ + 1 + 2 * kHalo;
-constexpr int kTile = kWX * kWY * kWZ;             // 9 x 9 x 13 nodes
+// ------------------------------------------------------------------ brick push
+// push_brick_kernel: the fused push (gather + Boris + move + boundaries +
+// absorption flag + deposit + kinetic energy) over the brick-sorted particles,
+// one brick per CTA.
+//
+// Push. Lanes hold consecutive particles. Between sorts a warp's 32 particles
+// start in one or two cells, so the eight corner loads of the field gather are
+// broadcasts (measured on B200: eight float4 loads cost ~1.9 SM cycles per warp
+// instruction when lanes share a node, ~12 when all 32 lanes read different
+// nodes), and the state loads and stores are coalesced 128-byte rows.
+//
+// Deposit. The charge of a cell's particles reaches the cell's eight corner
+// nodes as sums of the in-cell moments 1, a, b, d, ab, ad, bd, abd (a, b, d the
+// offsets in 17-bit fixed point): the corner (ex,ey,ez) weight of one particle
+// is prod(e ? q : 2^17 - q), a polynomial in those moments. Each lane packs its
+// particle's new window cell and offsets into one 64-bit word of a batch buffer
+// (kBatch particles, sorted order); the buffer is then read with lanes
+// kBatch/32 particles apart, i.e. in different cells, and every particle adds
+// its moments, cut into 17-bit pieces, to the CTA's moment tile over the
+// brick's cells plus a two-cell halo (13 planes of 32-bit words, no-return
+// shared atomics; lanes on the same word would serialise, lanes on distinct
+// words cost ~1.4 SM cycles per instruction). After each segment of at most
+// kSegment particles the occupied cells turn their moments into corner weights
+// (exact modulo 2^64), summed per node in a tile (low/high 32-bit planes with
+// carry, in the batch buffer's memory) that is then added to the species'
+// int64 accumulator. A segment holds fewer than 2^13 particles, so no corner
+// sum of one cell reaches 2^64 and no moment plane reaches 2^32; a wrap of a
+// node sum (more than 2^13 full weights on one node) is detected and latched
+// as FOPIS_DEV_RHO_OVERFLOW. Particles that leave the halo add their eight
+// corner weights straight to the global accumulator.
+constexpr int kBrickThreads = 256;
+constexpr int kPer = 2;                                  // particles per thread per compute pass (64 registers)
+constexpr int kPass = kBrickThreads * kPer;              // 512
+constexpr int kBatch = 1024;                             // particles per deposit batch (two passes)
+constexpr int kBatchPad = kBatch + kBatch / 32;          // one pad word per 32 entries: conflict-free reads
+constexpr int kHalo = 2;                                 // cells a particle may drift out of its brick
+constexpr int kCX = kBX + 2 * kHalo, kCY = kBY + 2 * kHalo, kCZ = kBZ + 2 * kHalo;   // window cells
+constexpr int kWinCells = kCX * kCY * kCZ;               // 8 x 8 x 12 = 768
+constexpr int kNX = kCX + 1, kNY = kCY + 1, kNZ = kCZ + 1;                           // window nodes
+constexpr int kWinNodes = kNX * kNY * kNZ;               // 9 x 9 x 13 = 1053
+constexpr int kPlanes = 13;                              // N, A, B, D, AB lo/hi, AD lo/hi, BD lo/hi, ABD x3
+constexpr int kSegment = 7 * kBatch;                     // 7168 < 2^13 particles per moment segment
+constexpr unsigned kChunk17 = 0x1FFFFu;
+constexpr unsigned long long kNoDeposit = 0x3FFull;      // batch entry without a deposit (cell field all ones)
+static_assert(kBatch == 2 * kPass, "a batch is two compute passes");
+static_assert(kWinCells < 0x3FF, "window cell fits the 10-bit field of a batch entry");
+static_assert(2 * kWinNodes <= 2 * kBatchPad, "the node tile fits in the batch buffer");
+__device__ __forceinline__ int bpad(int q) { return q + (q >> 5); }
 
-// Adds one integer corner weight to the shared tile, held as a low and a high
-// 32-bit plane with native 32-bit shared atomics: the low word's addition
-// returns the old value, its carry goes into the high word with the weight's
-// high bits. The tile thus holds each node's sum modulo 2^64, exactly what the
-// 64-bit global accumulator holds. (A 64-bit tile with one 64-bit shared
-// atomicAdd per corner made the 128^3 push 4.05 -> 5.75 ms; three planes of
-// 17-bit chunks took 4.05 ms.)
-__device__ __forceinline__ void tile_add(unsigned* lo, unsigned* hi, int idx, unsigned long long w) {
+// Adds one corner weight (a value below 2^64) to the node tile held as a low
+// and a high 32-bit plane; returns true when the node's sum wrapped past 2^64.
+__device__ __forceinline__ bool tile_add_checked(unsigned* lo, unsigned* hi, int idx, unsigned long long w) {
     const unsigned wl = (unsigned)w, wh = (unsigned)(w >> 32);
     const unsigned old = atomicAdd(lo + idx, wl);
-    atomicAdd(hi + idx, wh + ((old + wl < old) ? 1u : 0u));
+    const unsigned add = wh + ((old + wl < old) ? 1u : 0u);
+    const unsigned oldh = atomicAdd(hi + idx, add);
+    return add < wh || oldh + add < oldh;
 }
 
-// RUN consecutive particles per thread; a pass stages kTileThreads * RUN
-// particles (one pad word per 32 entries) in dynamic shared memory.
-template <int RUN>
-struct TileChunk {
-    static constexpr int kChunk = kTileThreads * RUN;
-    static constexpr int kChunkPad = kChunk + kChunk / 32;
-    static constexpr size_t kSmem = sizeof(float) * 7 * kChunkPad;
-};
-__device__ __forceinline__ int padi(int q) { return q + (q >> 5); }
-// Runs of 4 at four 256-thread CTAs per SM (64 registers): runs of 8 (three
-// CTAs per SM) and register caps for five or six CTAs (spilling) measured
-// 0.2-0.9 ms slower per 128^3 step; runs of 2 the same.
-constexpr int kPushRun = 4;
-
-// Every corner is added, zero weights included (they are rare, and adding
-// zero changes nothing): the tests cost more than the atomics they skip.
-__device__ __forceinline__ void tile_flush(unsigned* lo, unsigned* hi, int tb, const unsigned long long acc[8]) {
+// Adds a particle's eight corner weights straight to the global accumulator.
+__device__ __forceinline__ bool global_deposit(unsigned long long* rho, const Grid& g, int base, unsigned qa,
+                                               unsigned qb, unsigned qd) {
+    const unsigned wx[2] = {(unsigned)kDepositOne - qa, qa}, wy[2] = {(unsigned)kDepositOne - qb, qb};
+    const unsigned wz[2] = {(unsigned)kDepositOne - qd, qd};
+    bool wrap = false;
 #pragma unroll
     for (int t = 0; t < 8; ++t) {
-        const int off = ((t >> 2) ? kWY * kWZ : 0) + (((t >> 1) & 1) ? kWZ : 0) + (t & 1);
-        tile_add(lo, hi, tb + off, acc[t]);
+        const unsigned long long w = (unsigned long long)wx[t >> 2] * wy[(t >> 1) & 1] * wz[t & 1];
+        if (w) {
+            const unsigned long long old = atomicAdd(rho + base + corner_offset(g, t), w);
+            wrap |= old + w < old;
+        }
     }
+    return wrap;
 }
 
-// The fused push (gather + Boris + move + boundaries + absorption flag +
-// deposit + kinetic energy) over the brick-sorted particles, one brick per CTA.
-// A chunk of kChunk particles is staged through shared memory with coalesced
-// loads; thread (warp w, lane l) then owns the kRun consecutive entries starting
-// at l*(kChunk/32) + w*kRun, so the lanes of a warp sit kChunk/32 particles (about one cell)
-// apart while each thread walks a run of particles that mostly share a cell. A
-// thread sums its run's corner weights in registers and adds them to the shared
-// tile (brick + 2-cell halo, a low and a high 32-bit plane) when the
-// cell changes; particles that drifted beyond the halo add straight to HBM. The
-// tile is flushed with one 64-bit atomic per nonzero node.
-template <int RUN, int MINB>
-__global__ void __launch_bounds__(kTileThreads, MINB) push_tile_kernel(PushArgs a, const int32_t* brick_start) {
-    constexpr int kRun = RUN, kChunk = TileChunk<RUN>::kChunk, kChunkPad = TileChunk<RUN>::kChunkPad;
-    __shared__ unsigned t_lo[kTile], t_hi[kTile];
-    extern __shared__ float s_stage[];
-    int32_t* s_cell = reinterpret_cast<int32_t*>(s_stage);
-    float* const s_f[6] = {s_stage + kChunkPad, s_stage + 2 * kChunkPad, s_stage + 3 * kChunkPad,
-                           s_stage + 4 * kChunkPad, s_stage + 5 * kChunkPad, s_stage + 6 * kChunkPad};
+// Adds one particle's moments, cut into 17-bit pieces, to the moment tile of
+// window cell wc: 13 no-return 32-bit shared atomics.
+__device__ __forceinline__ void moment_deposit(unsigned* mom, int wc, unsigned qa, unsigned qb, unsigned qd) {
+    const unsigned long long ab = (unsigned long long)qa * qb, ad = (unsigned long long)qa * qd;
+    const unsigned long long bd = (unsigned long long)qb * qd, abd = ab * qd;
+    unsigned* m = mom + wc;
+    atomicAdd(m, 1u);
+    atomicAdd(m + 1 * kWinCells, qa);
+    atomicAdd(m + 2 * kWinCells, qb);
+    atomicAdd(m + 3 * kWinCells, qd);
+    atomicAdd(m + 4 * kWinCells, (unsigned)ab & kChunk17);
+    atomicAdd(m + 5 * kWinCells, (unsigned)(ab >> 17));
+    atomicAdd(m + 6 * kWinCells, (unsigned)ad & kChunk17);
+    atomicAdd(m + 7 * kWinCells, (unsigned)(ad >> 17));
+    atomicAdd(m + 8 * kWinCells, (unsigned)bd & kChunk17);
+    atomicAdd(m + 9 * kWinCells, (unsigned)(bd >> 17));
+    atomicAdd(m + 10 * kWinCells, (unsigned)abd & kChunk17);
+    atomicAdd(m + 11 * kWinCells, (unsigned)(abd >> 17) & kChunk17);
+    atomicAdd(m + 12 * kWinCells, (unsigned)(abd >> 34));
+}
+
+// Corner (ex,ey,ez) weight sum of a cell from its moments: the sum over the
+// axis subsets T containing E = {axes with e = 1} of (-1)^|T\E| O^(3-|T|) M_T,
+// evaluated modulo 2^64 (exact: the true value lies in [0, 2^64)).
+__device__ __forceinline__ unsigned long long corner_from_moments(int t, const unsigned long long M[8]) {
+    constexpr unsigned long long O = (unsigned long long)kDepositOne;
+    unsigned long long w = 0;
+#pragma unroll
+    for (int T = 0; T < 8; ++T) {                 // T bits: 4 = x, 2 = y, 1 = z (M index)
+        if ((T & t) != t) continue;
+        const int extra = __popc(T & ~t), size = __popc(T);
+        unsigned long long term = M[T];
+        for (int q = size; q < 3; ++q) term *= O;
+        w += (extra & 1) ? (0ull - term) : term;
+    }
+    return w;
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(kBrickThreads, MINB) push_brick_kernel(PushArgs a, const int32_t* brick_start) {
+    __shared__ __align__(16) unsigned s_mom[kPlanes * kWinCells];
+    __shared__ __align__(16) unsigned long long s_batch[kBatchPad];    // batch entries; node tile in the epilogue
+    unsigned* const t_lo = reinterpret_cast<unsigned*>(s_batch);
+    unsigned* const t_hi = t_lo + kWinNodes;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int b = blockIdx.x;
     const int bi = b / (a.g.nb[1] * a.g.nb[2]), bj = (b / a.g.nb[2]) % a.g.nb[1], bk = b % a.g.nb[2];
     const int wx0 = bi * kBX - kHalo, wy0 = bj * kBY - kHalo, wz0 = bk * kBZ - kHalo;
     int body = 0;
-    for (int t = tid; t < kTile; t += kTileThreads) {
-        t_lo[t] = 0u; t_hi[t] = 0u;
-        // a body cell anywhere in the window (cells wx0 .. wx0 + kWX - 2 per axis)?
-        const int x = wx0 + t / (kWY * kWZ), y = wy0 + (t / kWZ) % kWY, z = wz0 + t % kWZ;
-        if (a.cellmap && x >= wx0 && x - wx0 < kWX - 1 && y - wy0 < kWY - 1 && z - wz0 < kWZ - 1 && x >= 0 && y >= 0 &&
-            z >= 0 && x < a.g.cx - 1 && y < a.g.cy - 1 && z < a.g.cz - 1 && a.cellmap[lin(a.g, x, y, z)] != 0)
+    for (int t = tid; t < kWinCells; t += kBrickThreads) {
+        // a body cell anywhere in the window?
+        const int x = wx0 + t / (kCY * kCZ), y = wy0 + (t / kCZ) % kCY, z = wz0 + t % kCZ;
+        if (a.cellmap && x >= 0 && y >= 0 && z >= 0 && x < a.g.cx - 1 && y < a.g.cy - 1 && z < a.g.cz - 1 &&
+            a.cellmap[lin(a.g, x, y, z)] != 0)
             body = 1;
     }
     // particles that stay inside a body-free window need no body test
     const bool window_body = __syncthreads_or(body) != 0;
     const long long p0 = brick_start[b], p1 = brick_start[b + 1];
     double e2 = 0.0;
-    __syncthreads();
-    for (long long c0 = p0; c0 < p1; c0 += kChunk) {
-        const int m = (int)min((long long)kChunk, p1 - c0);
-#pragma unroll
-        for (int rr = 0; rr < kRun; ++rr) {
-            const int q = tid + rr * kTileThreads;
-            const int d = padi(q);
-            if (q < m) {
-                s_cell[d] = a.p.cell[c0 + q];
-                s_f[0][d] = a.p.ox[c0 + q]; s_f[1][d] = a.p.oy[c0 + q]; s_f[2][d] = a.p.oz[c0 + q];
-                s_f[3][d] = a.p.vx[c0 + q]; s_f[4][d] = a.p.vy[c0 + q]; s_f[5][d] = a.p.vz[c0 + q];
-            } else {
-                s_cell[d] = -1;
-            }
-        }
-        __syncthreads();
-        int cur = -1;
-        unsigned long long acc[8];
-#pragma unroll
-        for (int t = 0; t < 8; ++t) acc[t] = 0ull;
+    bool wrap = false;
+    for (long long s0 = p0; s0 < p1; s0 += kSegment) {
+        const long long s1 = min(p1, s0 + (long long)kSegment);
+        static_assert((kPlanes * kWinCells) % 4 == 0, "moment tile cleared in 16-byte stores");
+        for (int t = tid; t < kPlanes * kWinCells / 4; t += kBrickThreads)
+            reinterpret_cast<uint4*>(s_mom)[t] = make_uint4(0u, 0u, 0u, 0u);
+        for (long long c0 = s0; c0 < s1; c0 += kBatch) {
 #pragma unroll 1
-        for (int r = 0; r < kRun; ++r) {
-            const int d = padi(lane * (kChunk / 32) + warp * kRun + r);
-            const int32_t cell = s_cell[d];
-            bool live = cell >= 0;
-            PState st{0, 0, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            if (live) {
-                unpack_cell(cell, st.i, st.j, st.k);
-                st.ox = s_f[0][d]; st.oy = s_f[1][d]; st.oz = s_f[2][d];
-                st.vx = s_f[3][d]; st.vy = s_f[4][d]; st.vz = s_f[5][d];
-                gather_boris(a, st);
-                live = move_boundary(a, st);
-            }
-            const int li = st.i - wx0, lj = st.j - wy0, lk = st.k - wz0;
-            const bool inwin = li >= 0 && lj >= 0 && lk >= 0 && li < kWX - 1 && lj < kWY - 1 && lk < kWZ - 1;
-            const bool test = live && (window_body || !inwin);
-            if (__any_sync(kFull, test) && absorb_check(a, st, test)) live = false;
-            if (live) {
-                const unsigned qa = (unsigned)__float2int_rn(st.ox * kDepositScale);
-                const unsigned qb = (unsigned)__float2int_rn(st.oy * kDepositScale);
-                const unsigned qd = (unsigned)__float2int_rn(st.oz * kDepositScale);
-                const unsigned wx[2] = {(unsigned)kDepositOne - qa, qa}, wy[2] = {(unsigned)kDepositOne - qb, qb};
-                const unsigned wz[2] = {(unsigned)kDepositOne - qd, qd};
-                if (inwin) {
-                    const int tb = (li * kWY + lj) * kWZ + lk;
-                    if (tb != cur) {   // a new run starts with this particle's weights
-                        if (cur >= 0) tile_flush(t_lo, t_hi, cur, acc);
-                        cur = tb;
+            for (int h = 0; h < 2; ++h) {
+                const long long cp = c0 + h * kPass;
+                int32_t cell[kPer];
+                float f[kPer][6];
 #pragma unroll
-                        for (int t = 0; t < 8; ++t)
-                            acc[t] = (unsigned long long)wx[t >> 2] * wy[(t >> 1) & 1] * wz[t & 1];
-                    } else {
-#pragma unroll
-                        for (int t = 0; t < 8; ++t)
-                            acc[t] += (unsigned long long)wx[t >> 2] * wy[(t >> 1) & 1] * wz[t & 1];
-                    }
-                } else {
-                    const long long gb = lin(a.g, st.i, st.j, st.k);
-#pragma unroll
-                    for (int t = 0; t < 8; ++t) {
-                        const unsigned long long w = (unsigned long long)wx[t >> 2] * wy[(t >> 1) & 1] * wz[t & 1];
-                        if (w) atomicAdd(a.rho + gb + corner_offset(a.g, t), w);
+                for (int r = 0; r < kPer; ++r) {
+                    const long long idx = cp + (r * (kBrickThreads / 32) + warp) * 32 + lane;
+                    cell[r] = idx < s1 ? a.p.cell[idx] : -1;
+                    if (cell[r] >= 0) {
+                        f[r][0] = a.p.ox[idx]; f[r][1] = a.p.oy[idx]; f[r][2] = a.p.oz[idx];
+                        f[r][3] = a.p.vx[idx]; f[r][4] = a.p.vy[idx]; f[r][5] = a.p.vz[idx];
                     }
                 }
-                e2 += (double)st.vx * st.vx + (double)st.vy * st.vy + (double)st.vz * st.vz;
-            }
-            if (cell >= 0) {
-                s_cell[d] = live ? pack_cell(st.i, st.j, st.k) : -1;
-                s_f[0][d] = st.ox; s_f[1][d] = st.oy; s_f[2][d] = st.oz;
-                s_f[3][d] = st.vx; s_f[4][d] = st.vy; s_f[5][d] = st.vz;
-            }
-        }
-        if (cur >= 0) tile_flush(t_lo, t_hi, cur, acc);
-        __syncthreads();
 #pragma unroll
-        for (int rr = 0; rr < kRun; ++rr) {
-            const int q = tid + rr * kTileThreads;
-            if (q >= m) break;
-            const int d = padi(q);
-            a.p.cell[c0 + q] = s_cell[d];
-            a.p.ox[c0 + q] = s_f[0][d]; a.p.oy[c0 + q] = s_f[1][d]; a.p.oz[c0 + q] = s_f[2][d];
-            a.p.vx[c0 + q] = s_f[3][d]; a.p.vy[c0 + q] = s_f[4][d]; a.p.vz[c0 + q] = s_f[5][d];
+                for (int r = 0; r < kPer; ++r) {
+                    const int q = h * kPass + (r * (kBrickThreads / 32) + warp) * 32 + lane;   // place in the batch
+                    const long long idx = c0 + q;
+                    bool live = cell[r] >= 0;
+                    PState st{0, 0, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                    if (live) {
+                        unpack_cell(cell[r], st.i, st.j, st.k);
+                        st.ox = f[r][0]; st.oy = f[r][1]; st.oz = f[r][2];
+                        st.vx = f[r][3]; st.vy = f[r][4]; st.vz = f[r][5];
+                        gather_boris(a, st);
+                        live = move_boundary(a, st);
+                    }
+                    const int li = st.i - wx0, lj = st.j - wy0, lk = st.k - wz0;
+                    const bool inwin = (unsigned)li < (unsigned)kCX && (unsigned)lj < (unsigned)kCY &&
+                                       (unsigned)lk < (unsigned)kCZ;
+                    const bool test = live && (window_body || !inwin);
+                    if (__any_sync(kFull, test) && absorb_check(a, st, test)) live = false;
+                    const unsigned qa = (unsigned)__float2int_rn(st.ox * kDepositScale);
+                    const unsigned qb = (unsigned)__float2int_rn(st.oy * kDepositScale);
+                    const unsigned qd = (unsigned)__float2int_rn(st.oz * kDepositScale);
+                    s_batch[bpad(q)] = (live && inwin)
+                                           ? ((unsigned long long)((li * kCY + lj) * kCZ + lk) |
+                                              ((unsigned long long)qa << 10) | ((unsigned long long)qb << 28) |
+                                              ((unsigned long long)qd << 46))
+                                           : kNoDeposit;
+                    if (live && !inwin) wrap |= global_deposit(a.rho, a.g, lin(a.g, st.i, st.j, st.k), qa, qb, qd);
+                    if (live) e2 += (double)(st.vx * st.vx + st.vy * st.vy + st.vz * st.vz);
+                    if (cell[r] >= 0) {
+                        a.p.cell[idx] = live ? pack_cell(st.i, st.j, st.k) : -1;
+                        a.p.ox[idx] = st.ox; a.p.oy[idx] = st.oy; a.p.oz[idx] = st.oz;
+                        a.p.vx[idx] = st.vx; a.p.vy[idx] = st.vy; a.p.vz[idx] = st.vz;
+                    }
+                }
+            }
+            __syncthreads();
+            // deposit: lane l takes entries l*32 + warp*4 + r, 32 sorted places apart
+#pragma unroll
+            for (int r = 0; r < kBatch / kBrickThreads; ++r) {
+                const unsigned long long e = s_batch[bpad(lane * (kBatch / 32) + warp * (kBatch / kBrickThreads) + r)];
+                const int wc = (int)(e & 0x3FFull);
+                if (wc != (int)kNoDeposit)
+                    moment_deposit(s_mom, wc, (unsigned)(e >> 10) & 0x3FFFFu, (unsigned)(e >> 28) & 0x3FFFFu,
+                                   (unsigned)(e >> 46));
+            }
+            __syncthreads();
+        }
+        // occupied cells: moments -> corner weights -> node tile (in the batch buffer)
+        for (int t = tid; t < 2 * kWinNodes; t += kBrickThreads) t_lo[t] = 0u;
+        __syncthreads();
+        for (int t = tid; t < kWinCells; t += kBrickThreads) {
+            const unsigned n = s_mom[t];
+            if (!n) continue;
+            const unsigned* m = s_mom + t;
+            unsigned long long M[8];
+            M[0] = n;                                                      // {}
+            M[4] = m[1 * kWinCells];                                       // {x}: A
+            M[2] = m[2 * kWinCells];                                       // {y}: B
+            M[1] = m[3 * kWinCells];                                       // {z}: D
+            M[6] = m[4 * kWinCells] + ((unsigned long long)m[5 * kWinCells] << 17);    // {x,y}: AB
+            M[5] = m[6 * kWinCells] + ((unsigned long long)m[7 * kWinCells] << 17);    // {x,z}: AD
+            M[3] = m[8 * kWinCells] + ((unsigned long long)m[9 * kWinCells] << 17);    // {y,z}: BD
+            M[7] = m[10 * kWinCells] + ((unsigned long long)m[11 * kWinCells] << 17) +
+                   ((unsigned long long)m[12 * kWinCells] << 34);                      // {x,y,z}: ABD
+            const int x = t / (kCY * kCZ), y = (t / kCZ) % kCY, z = t % kCZ;
+            const int nb = (x * kNY + y) * kNZ + z;
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                const int off = ((c >> 2) ? kNY * kNZ : 0) + (((c >> 1) & 1) ? kNZ : 0) + (c & 1);
+                wrap |= tile_add_checked(t_lo, t_hi, nb + off, corner_from_moments(c, M));
+            }
+        }
+        __syncthreads();
+        for (int t = tid; t < kWinNodes; t += kBrickThreads) {
+            const unsigned long long v = (unsigned long long)t_lo[t] | ((unsigned long long)t_hi[t] << 32);
+            if (!v) continue;
+            const int x = wx0 + t / (kNY * kNZ), y = wy0 + (t / kNZ) % kNY, z = wz0 + t % kNZ;
+            const unsigned long long old = atomicAdd(a.rho + lin(a.g, x, y, z), v);
+            wrap |= old + v < old;
         }
         __syncthreads();
     }
-    for (int t = tid; t < kTile; t += kTileThreads) {
-        const unsigned long long v = (unsigned long long)t_lo[t] | ((unsigned long long)t_hi[t] << 32);
-        if (!v) continue;
-        const int x = wx0 + t / (kWY * kWZ), y = wy0 + (t / kWZ) % kWY, z = wz0 + t % kWZ;
-        atomicAdd(a.rho + lin(a.g, x, y, z), v);
-    }
+    if (wrap) atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_RHO_OVERFLOW);
     const double tot = block_sum(e2);
     if (tid == 0 && tot != 0.0) atomicAdd(&a.sc->energy[a.s], tot);
 }
@@ -592,8 +673,14 @@ __device__ void finish_source(const SourceArgsT<T>& a, int s, double x, double y
             unsigned long long w[8];
             corner_weights(ox, oy, oz, w);
             unsigned long long* rho = a.rho + (long long)s * a.N;
+            bool wrap = false;
 #pragma unroll
-            for (int t = 0; t < 8; ++t) if (w[t]) atomicAdd(rho + b + corner_offset(a.g, t), w[t]);
+            for (int t = 0; t < 8; ++t)
+                if (w[t]) {
+                    const unsigned long long old = atomicAdd(rho + b + corner_offset(a.g, t), w[t]);
+                    wrap |= old + w[t] < old;
+                }
+            if (wrap) atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_RHO_OVERFLOW);
         } else {
             long long off[8];
 #pragma unroll
@@ -1519,7 +1606,7 @@ int brick_count(const Ctx& c) {
 
 // Sort of every species by brick (brick_index), then by cell inside the
 // brick (local_cell); invalid slots are dropped. Records each brick's first slot
-// for push_tile_kernel. The particles end in the live arrays; the sort
+// for push_brick_kernel. The particles end in the live arrays; the sort
 // targets hold the brick-grouped intermediate.
 template <typename T>
 static void sort_all(Ctx& c) {
@@ -1607,7 +1694,7 @@ static void push_generic(Ctx& c, const PushArgsT<T>& a, int grid, bool vel, bool
     else throw ApiError{FOPIS_ERR_ARG, "unsupported push combination"};
 }
 
-// The fused step takes the brick-sorted slots with push_tile_kernel and the
+// The fused step takes the brick-sorted slots with push_brick_kernel and the
 // appended tail with push_kernel (mixed mode); the FP64 mode and the single
 // phases run push_kernel over every slot.
 void launch_push(Ctx& c, bool vel, bool pos, bool dep) {
@@ -1620,8 +1707,7 @@ void launch_push(Ctx& c, bool vel, bool pos, bool dep) {
         } else if (vel && pos && dep && c.sorted_n[s] > 0 && c.brick_start[s]) {
             PushArgs a = push_args<float>(c, s);
             ++c.launches;
-            push_tile_kernel<kPushRun, 4><<<brick_count(c), kTileThreads, TileChunk<kPushRun>::kSmem, c.st>>>(
-                a, c.brick_start[s]);
+            push_brick_kernel<4><<<brick_count(c), kBrickThreads, 0, c.st>>>(a, c.brick_start[s]);
             a.lo = c.sorted_n[s];
             ++c.launches;
             push_kernel<float, true, true, true><<<grid_for(std::max<int64_t>(c.cap[s] - a.lo, 1)), kThreads, 0, c.st>>>(a);

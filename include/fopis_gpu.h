@@ -59,6 +59,8 @@ typedef enum fopis_status {
 #define FOPIS_DEV_SURFACE_NOT_FOUND   0x8   /* absorbed particle without a crossing face (Spacecraft.cpp:573-582) */
 #define FOPIS_DEV_INJECT_REJECTS      0x10  /* injection rejection sampling hit its attempt cap */
 #define FOPIS_DEV_NONFINITE           0x20  /* NaN/Inf met in a reduction */
+#define FOPIS_DEV_RHO_OVERFLOW        0x40  /* a node's int64 fixed-point charge sum passed 2^64
+                                               (more than 2^13 full particle weights on one node) */
 
 typedef enum fopis_species_kind {
     FOPIS_SPECIES_AMBIENT = 0,        /* AmbientParticleType */
