@@ -170,6 +170,7 @@ SIGNATURES = {
     "fopis_parse_obj": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.POINTER(C.c_int32)),
                                   C.POINTER(C.c_int), C.POINTER(C.POINTER(C.c_int32)), C.POINTER(C.c_int)]),
     "fopis_free": (None, [_VP]),
+    "fopis_check_bounded_wait": (C.c_int, [C.c_int, C.c_uint32, C.c_int, C.POINTER(C.c_uint32)]),
     "fopis_efield_energy_noalloc": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, C.c_double, _VP, _VP]),
 }
 

@@ -1571,7 +1571,16 @@ int mg_solve(Ctx& c, double tol, int max_cycles) {
     c.last_converged = (res <= tol * fnorm) ? 1 : 0;
     c.step_vcycles += cycles;
     c.step_solves += 1;
-    if (!std::isfinite(res)) return FOPIS_ERR_DEVICE;
+    if (!std::isfinite(res)) {
+        // NaN or Inf in the charge or the potential: latched like the particle
+        // kernels' non-finite state, so fopis_get_stats shows it too
+        sync_scalars(c);
+        c.h_sc->status |= FOPIS_DEV_NONFINITE;
+        FOPIS_CUDA(cudaMemcpyAsync(&c.d_sc->status, &c.h_sc->status, sizeof(unsigned), cudaMemcpyHostToDevice, c.st));
+        FOPIS_CUDA(cudaStreamSynchronize(c.st));
+        c.err = "non-finite Poisson residual: NaN or Inf in rho or phi";
+        return FOPIS_ERR_DEVICE;
+    }
     return c.last_converged ? FOPIS_OK : FOPIS_ERR_NOT_CONVERGED;
 }
 

@@ -222,6 +222,7 @@ struct PushArgsT {
     Grid g;
     T qm;                     // 0.5 q/m
     T bx, by, bz, boris;      // static B as the reference uses it, 2/(1+|b|^2)
+    int bzero;                // B = 0: the rotation adds exact zeros and is skipped
     const uint8_t* cellmap;   // nullptr without objects
     unsigned long long* rho;  // species accumulator: int64 fixed point, or FP64 weights in the FP64 mode
     AbsorbList ab;
@@ -263,6 +264,10 @@ __device__ __forceinline__ void gather_boris(const PushArgsT<T>& a, PStateT<T>& 
     const T ez = a.qm * (w000 * e000.z + w100 * e100.z + w010 * e010.z + w110 * e110.z +
                          w001 * e001.z + w101 * e101.z + w011 * e011.z + w111 * e111.z);
     const T vx1 = s.vx + ex, vy1 = s.vy + ey, vz1 = s.vz + ez;
+    if (a.bzero) {
+        s.vx = vx1 + ex; s.vy = vy1 + ey; s.vz = vz1 + ez;
+        return;
+    }
     const T vxt = vx1 + vy1 * a.bz - vz1 * a.by;
     const T vyt = vy1 + vz1 * a.bx - vx1 * a.bz;
     const T vzt = vz1 + vx1 * a.by - vy1 * a.bx;
@@ -383,11 +388,12 @@ __global__ void __launch_bounds__(kThreads) push_kernel(PushArgsT<T> a) {
 // is prod(e ? q : 2^17 - q), a polynomial in those moments. Each lane packs its
 // particle's new window cell and offsets into one 64-bit word of a batch buffer
 // (kBatch particles, sorted order); the buffer is then read with lanes
-// kBatch/32 particles apart, i.e. in different cells, and every particle adds
-// its moments, cut into 17-bit pieces, to the CTA's moment tile over the
-// brick's cells plus a two-cell halo (13 planes of 32-bit words, no-return
-// shared atomics; lanes on the same word would serialise, lanes on distinct
-// words cost ~1.4 SM cycles per instruction). After each segment of at most
+// kBatch/32 particles apart, i.e. in different cells, each thread summing the
+// moments of its run of consecutive entries in registers and adding them,
+// cut into 17-bit pieces, to the CTA's moment tile over the brick's cells plus
+// a two-cell halo (13 planes of 32-bit words, no-return shared atomics; lanes
+// on the same word would serialise, lanes on distinct words cost ~1.4 SM
+// cycles per instruction). After each segment of at most
 // kSegment particles the occupied cells turn their moments into corner weights
 // (exact modulo 2^64), summed per node in a tile (low/high 32-bit planes with
 // carry, in the batch buffer's memory) that is then added to the species'
@@ -442,42 +448,48 @@ __device__ __forceinline__ bool global_deposit(unsigned long long* rho, const Gr
     return wrap;
 }
 
-// Adds one particle's moments, cut into 17-bit pieces, to the moment tile of
-// window cell wc: 13 no-return 32-bit shared atomics.
-__device__ __forceinline__ void moment_deposit(unsigned* mom, int wc, unsigned qa, unsigned qb, unsigned qd) {
-    const unsigned long long ab = (unsigned long long)qa * qb, ad = (unsigned long long)qa * qd;
-    const unsigned long long bd = (unsigned long long)qb * qd, abd = ab * qd;
-    unsigned* m = mom + wc;
-    atomicAdd(m, 1u);
-    atomicAdd(m + 1 * kWinCells, qa);
-    atomicAdd(m + 2 * kWinCells, qb);
-    atomicAdd(m + 3 * kWinCells, qd);
-    atomicAdd(m + 4 * kWinCells, (unsigned)ab & kChunk17);
-    atomicAdd(m + 5 * kWinCells, (unsigned)(ab >> 17));
-    atomicAdd(m + 6 * kWinCells, (unsigned)ad & kChunk17);
-    atomicAdd(m + 7 * kWinCells, (unsigned)(ad >> 17));
-    atomicAdd(m + 8 * kWinCells, (unsigned)bd & kChunk17);
-    atomicAdd(m + 9 * kWinCells, (unsigned)(bd >> 17));
-    atomicAdd(m + 10 * kWinCells, (unsigned)abd & kChunk17);
-    atomicAdd(m + 11 * kWinCells, (unsigned)(abd >> 17) & kChunk17);
-    atomicAdd(m + 12 * kWinCells, (unsigned)(abd >> 34));
-}
-
-// Corner (ex,ey,ez) weight sum of a cell from its moments: the sum over the
-// axis subsets T containing E = {axes with e = 1} of (-1)^|T\E| O^(3-|T|) M_T,
-// evaluated modulo 2^64 (exact: the true value lies in [0, 2^64)).
-__device__ __forceinline__ unsigned long long corner_from_moments(int t, const unsigned long long M[8]) {
-    constexpr unsigned long long O = (unsigned long long)kDepositOne;
-    unsigned long long w = 0;
-#pragma unroll
-    for (int T = 0; T < 8; ++T) {                 // T bits: 4 = x, 2 = y, 1 = z (M index)
-        if ((T & t) != t) continue;
-        const int extra = __popc(T & ~t), size = __popc(T);
-        unsigned long long term = M[T];
-        for (int q = size; q < 3; ++q) term *= O;
-        w += (extra & 1) ? (0ull - term) : term;
+// Moment sums of a few particles of one cell; flush() adds them to the cell's
+// words of the moment tile (13 no-return 32-bit shared atomics). Each 64-bit
+// moment is cut into 17-bit pieces; every piece a flush adds stays below 2^20,
+// so a plane word, summed over one segment, stays below 2^32.
+struct MomentSum {
+    unsigned n = 0, a = 0, b = 0, d = 0;
+    unsigned long long ab = 0, ad = 0, bd = 0, abd = 0;
+    __device__ __forceinline__ void add(unsigned qa, unsigned qb, unsigned qd) {
+        const unsigned long long pab = (unsigned long long)qa * qb;
+        n += 1u; a += qa; b += qb; d += qd;
+        ab += pab; ad += (unsigned long long)qa * qd; bd += (unsigned long long)qb * qd; abd += pab * qd;
     }
-    return w;
+    __device__ __forceinline__ void flush(unsigned* mom, int wc) const {
+        unsigned* m = mom + wc;
+        atomicAdd(m, n);
+        atomicAdd(m + 1 * kWinCells, a);
+        atomicAdd(m + 2 * kWinCells, b);
+        atomicAdd(m + 3 * kWinCells, d);
+        atomicAdd(m + 4 * kWinCells, (unsigned)ab & kChunk17);
+        atomicAdd(m + 5 * kWinCells, (unsigned)(ab >> 17));
+        atomicAdd(m + 6 * kWinCells, (unsigned)ad & kChunk17);
+        atomicAdd(m + 7 * kWinCells, (unsigned)(ad >> 17));
+        atomicAdd(m + 8 * kWinCells, (unsigned)bd & kChunk17);
+        atomicAdd(m + 9 * kWinCells, (unsigned)(bd >> 17));
+        atomicAdd(m + 10 * kWinCells, (unsigned)abd & kChunk17);
+        atomicAdd(m + 11 * kWinCells, (unsigned)(abd >> 17) & kChunk17);
+        atomicAdd(m + 12 * kWinCells, (unsigned)(abd >> 34));
+    }
+};
+
+// The eight corner weight sums of a cell from its moments M[T] (T bits: 4 = x,
+// 2 = y, 1 = z; M[T] = sum over the particles of the product of the offsets
+// of the axes in T). Per axis, a set T without the axis becomes the "0" corner
+// side O M_T - M_{T+axis} and the set with it the "1" side: after the three
+// axes M[t] holds the corner t = (ex,ey,ez) sum of prod(e ? q : O - q).
+// Modulo 2^64 and exact: every true corner sum lies in [0, 2^64).
+__device__ __forceinline__ void corners_from_moments(unsigned long long M[8]) {
+#pragma unroll
+    for (int axis = 4; axis >= 1; axis >>= 1)
+#pragma unroll
+        for (int T = 0; T < 8; ++T)
+            if (!(T & axis)) M[T] = (M[T] << kDepositBits) - M[T | axis];
 }
 
 template <int MINB>
@@ -559,14 +571,26 @@ __global__ void __launch_bounds__(kBrickThreads, MINB) push_brick_kernel(PushArg
                 }
             }
             __syncthreads();
-            // deposit: lane l takes entries l*32 + warp*4 + r, 32 sorted places apart
+            // deposit: lane l takes the run of entries l*32 + warp*4 + r (r = 0..3), runs of
+            // different lanes 32 sorted places (about one cell) apart; a run's particles
+            // mostly share a cell and are summed in registers, two cells at a time
+            {
+                MomentSum ma, mb;
+                int ca = -1, cb = -1;
 #pragma unroll
-            for (int r = 0; r < kBatch / kBrickThreads; ++r) {
-                const unsigned long long e = s_batch[bpad(lane * (kBatch / 32) + warp * (kBatch / kBrickThreads) + r)];
-                const int wc = (int)(e & 0x3FFull);
-                if (wc != (int)kNoDeposit)
-                    moment_deposit(s_mom, wc, (unsigned)(e >> 10) & 0x3FFFFu, (unsigned)(e >> 28) & 0x3FFFFu,
-                                   (unsigned)(e >> 46));
+                for (int r = 0; r < kBatch / kBrickThreads; ++r) {
+                    const unsigned long long e =
+                        s_batch[bpad(lane * (kBatch / 32) + warp * (kBatch / kBrickThreads) + r)];
+                    const int wc = (int)(e & 0x3FFull);
+                    if (wc == (int)kNoDeposit) continue;
+                    const unsigned qa = (unsigned)(e >> 10) & 0x3FFFFu, qb = (unsigned)(e >> 28) & 0x3FFFFu;
+                    const unsigned qd = (unsigned)(e >> 46);
+                    if (ca < 0 || wc == ca) { ca = wc; ma.add(qa, qb, qd); }
+                    else if (cb < 0 || wc == cb) { cb = wc; mb.add(qa, qb, qd); }
+                    else { MomentSum one; one.add(qa, qb, qd); one.flush(s_mom, wc); }
+                }
+                if (ca >= 0) ma.flush(s_mom, ca);
+                if (cb >= 0) mb.flush(s_mom, cb);
             }
             __syncthreads();
         }
@@ -587,12 +611,13 @@ __global__ void __launch_bounds__(kBrickThreads, MINB) push_brick_kernel(PushArg
             M[3] = m[8 * kWinCells] + ((unsigned long long)m[9 * kWinCells] << 17);    // {y,z}: BD
             M[7] = m[10 * kWinCells] + ((unsigned long long)m[11 * kWinCells] << 17) +
                    ((unsigned long long)m[12 * kWinCells] << 34);                      // {x,y,z}: ABD
+            corners_from_moments(M);
             const int x = t / (kCY * kCZ), y = (t / kCZ) % kCY, z = t % kCZ;
             const int nb = (x * kNY + y) * kNZ + z;
 #pragma unroll
             for (int c = 0; c < 8; ++c) {
                 const int off = ((c >> 2) ? kNY * kNZ : 0) + (((c >> 1) & 1) ? kNZ : 0) + (c & 1);
-                wrap |= tile_add_checked(t_lo, t_hi, nb + off, corner_from_moments(c, M));
+                wrap |= tile_add_checked(t_lo, t_hi, nb + off, M[c]);
             }
         }
         __syncthreads();
@@ -1679,6 +1704,7 @@ static PushArgsT<T> push_args(Ctx& c, int s) {
     const double b2 = c.p.static_bfield[0] * c.p.static_bfield[0] + c.p.static_bfield[1] * c.p.static_bfield[1] +
                       c.p.static_bfield[2] * c.p.static_bfield[2];
     a.boris = (T)(2.0 / (1.0 + b2));
+    a.bzero = b2 == 0.0 ? 1 : 0;
     a.cellmap = c.objs.empty() ? nullptr : c.cellmap;
     a.rho = c.rho_i64 + (size_t)s * c.N;
     a.ab = c.ab; a.sc = c.d_sc;

@@ -47,10 +47,14 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    for (uint32_t i = 0; i < kWaitPolls; ++i)
+// Polls the phase of `parity` up to `polls` times; false when it never completed.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint32_t polls = kWaitPolls) {
+    for (uint32_t i = 0; i < polls; ++i)
         if (mbar_try(bar, parity)) return true;
     return false;
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
 // Tensor memory: one warp allocates / frees; ncols is a power of two >= 32.

@@ -98,6 +98,21 @@ __device__ __forceinline__ void report(unsigned int* err, unsigned int code) {
     if (err) atomicOr(err, code);
 }
 
+// The bounded mbarrier wait of the tensor-core kernels, run on its own: one
+// thread initialises an mbarrier that expects one arrival and, when `arrive`
+// is 0, waits for a phase that nothing completes. With nothing asynchronous
+// in flight the wait can only run out: it gives up after `polls` polls and
+// reports code 1 through the same path the convolution kernels use.
+__global__ void bounded_wait_check_kernel(uint32_t polls, int arrive, unsigned int* err) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x != 0) return;
+    const uint32_t b = tc::saddr(&bar);
+    tc::mbar_init(b, 1);
+    tc::fence_mbar_init();
+    if (arrive) tc::mbar_arrive(b);
+    if (!tc::mbar_wait(b, 0u, polls)) report(err, 1u);
+}
+
 __device__ __forceinline__ void unpack8(uint4 u, float* f) {
     const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
 #pragma unroll
@@ -1315,3 +1330,26 @@ int unet_tensor(Ctx& c, int which, float* host, int64_t cap, int64_t* count) {
 }
 
 }  // namespace fopis
+
+// Device self-check of the bounded wait (include/fopis_gpu.h).
+extern "C" int fopis_check_bounded_wait(int device, uint32_t polls, int arrive, uint32_t* status) {
+    using namespace fopis;
+    if (!status) return FOPIS_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return FOPIS_ERR_NO_CUDA;
+    if (device < 0 || device >= ndev || cudaSetDevice(device) != cudaSuccess) return FOPIS_ERR_ARG;
+    unsigned int* d = nullptr;
+    if (cudaMalloc(&d, sizeof(unsigned int)) != cudaSuccess) return FOPIS_ERR_NOMEM;
+    int rc = FOPIS_OK;
+    unsigned int h = 0;
+    if (cudaMemset(d, 0, sizeof(unsigned int)) != cudaSuccess) rc = FOPIS_ERR_CUDA;
+    if (rc == FOPIS_OK) {
+        bounded_wait_check_kernel<<<1, 32>>>(polls, arrive, d);
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = FOPIS_ERR_CUDA;
+    }
+    cudaFree(d);
+    *status = h;
+    return rc;
+}

@@ -293,6 +293,16 @@ int fopis_unet_params(void* ctx, float* get, const float* set, int64_t* count);
  * With host null only *count (values) is set. */
 int fopis_unet_tensor(void* ctx, int which, float* host, int64_t cap, int64_t* count);
 
+/* ---- device self-check (no reference counterpart) ----------------------- */
+
+/* Runs the bounded mbarrier wait that guards every tensor-core pipeline stage
+ * of the learned guess, alone, on `device`: a barrier expecting one arrival is
+ * waited on for up to `polls` polls; with arrive = 0 nothing arrives, so the
+ * wait runs out and *status receives 1 (the kernels' error report), with
+ * arrive = 1 the phase completes and *status receives 0. Nothing asynchronous
+ * is in flight, so the device stays usable either way. */
+int fopis_check_bounded_wait(int device, uint32_t polls, int arrive, uint32_t* status);
+
 /* ---- allocation-free variant (no reference counterpart) ------------------ */
 
 /* Field::getEfieldEnergy's value (the quantity fopis_get_energy reports as
