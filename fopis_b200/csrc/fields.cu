@@ -267,8 +267,14 @@ void rho_finalize(Ctx& c) {
     FOPIS_LAUNCH_CHECK();
 }
 
+// After a solve: the periodic glue copies first (the last halo exchange of the
+// reference's doPSOR), then Field::setBoundaryConditionPhi on the D/N faces
+// (RootGridField.cpp:65-103 calls it after the sweeps and exchanges nothing
+// afterwards), so a glue node beside a Neumann face keeps the value it had
+// before the face copy, as in the reference.
 void phi_boundary(Ctx& c) {
     const G g = make_g(c);
+    glue_copy(c, c.phi);
     for (int axis = 0; axis < 3; ++axis)
         for (int side = 0; side < 2; ++side) {
             const char b = c.p.boundary[2 * axis + side];
@@ -279,7 +285,6 @@ void phi_boundary(Ctx& c) {
             phi_face_kernel<<<blocks(m), kT, 0, c.st>>>(c.phi, g, axis, side, b == 'N');
             FOPIS_LAUNCH_CHECK();
         }
-    glue_copy(c, c.phi);
 }
 
 void efield_update(Ctx& c) {

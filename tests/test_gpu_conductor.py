@@ -102,7 +102,9 @@ def test_phased_step_with_conductor_matches_oracle(pair):
         assert abs(Qg - Qo) <= 1e-3 * abs(Qo) + 1e-6 * abs(cfg.params.species[0].size), (step, Qg, Qo)
         assert np.allclose(Ig, Io, rtol=0.05, atol=abs(cfg.params.species[0].size) * 2.5)
     cm_g, cm_o = g.getChargeMap(0), o.charge_map(0)
-    assert rel_err(cm_g.sum(0), cm_o.sum(0)) < 0.05
+    cm_err = rel_err(cm_g.sum(0), cm_o.sum(0))
+    print(f"\nmixed precision, 3 phased steps: charge map {cm_err:.2e}")
+    assert cm_err < 1e-5
     st = g.stats()
     assert st.device_status & ~_abi.DEV_SURFACE_NOT_FOUND == 0
 

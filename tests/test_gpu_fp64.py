@@ -86,7 +86,13 @@ def test_fp64_conductor_run_tracks_oracle(gpu_available):
     for s in range(3):
         a, b, d = match(g.getParticles(s), o.particles(s))
         assert np.max(d) < 1e-8
-    print(f"\nFP64 GPU vs oracle, 30 steps: max |dV|/max|V| {np.max(np.abs(Vg - Vo)) / np.max(np.abs(Vo)):.2e}")
+    # surface charge per node and species (Spacecraft charge_map): the same absorptions and
+    # emissions, the GPU's bilinear weights in 20-bit fixed point
+    cm_g, cm_o = g.getChargeMap(0), o.charge_map(0)
+    cm_err = rel_err(cm_g, cm_o)
+    assert cm_err < 1e-5, cm_err
+    print(f"\nFP64 GPU vs oracle, 30 steps: max |dV|/max|V| {np.max(np.abs(Vg - Vo)) / np.max(np.abs(Vo)):.2e}, "
+          f"charge map {cm_err:.2e}")
     g.close()
     o.close()
 
