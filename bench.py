@@ -238,7 +238,7 @@ def run_gpu(args, world, rank, local):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     launches0 = g.stats().kernel_launches
     psteps = 0
-    push_ms, vcyc, pushed, phases_all = [], [], [], []
+    push_ms, vcyc, pushed, phases_all, pointwise = [], [], [], [], []
     barrier(world)
     torch.cuda.synchronize(local)
     if args.profile:
@@ -256,6 +256,7 @@ def run_gpu(args, world, rank, local):
             push_ms.append(st.ms_phase[0])
             phases_all.append([round(x, 3) for x in st.ms_phase])
             vcyc.append(st.vcycles_step)
+            pointwise.append(st.residual_pointwise)
         ev1.record(stream)
         torch.cuda.synchronize(local)
     if args.profile:
@@ -271,6 +272,7 @@ def run_gpu(args, world, rank, local):
         "ms": ms_max, "psteps": psteps_all, "launches": launches, "clocks": clk.summary(),
         "push_ms": float(np.mean(push_ms)), "pushed": float(np.mean(pushed)),
         "vcycles_per_step": float(np.mean(vcyc)), "phases_last": phases, "t_cmat": t_cmat,
+        "pointwise_max": float(np.max(pointwise)),
         "particles": total_particles(st, nsp), "n_cmat": [len(o.nodes) for o in cfg.objects],
         "step_ms": [round(x, 3) for x in step_ms], "phases_all": phases_all,
         "solve_mode": ["host loop", "device-loop graph", "device-loop graph with programmatic dependent launch"][
@@ -407,6 +409,88 @@ def learned_comparison(args, rank, local, Cm):
             "policy_history_learned_enabled": list(pol)}
 
 
+def mixed_vs_fp64(args, local, Cm, steps: int = 100):
+    """The mixed-precision step against the FP64 GPU mode on the same seed and
+    workload: rho, phi and E after one step (max |difference| / max |FP64
+    value|), and the spacecraft-potential history over `steps` steps."""
+    from fopis_b200 import RootGrid, _abi, config
+    gs = []
+    for prec in (_abi.MIXED, _abi.FP64):
+        cfg = config.workload(args.workload, ppc=args.ppc, seed=20251203, sort_interval=args.sort_interval,
+                              precision=prec)
+        g = RootGrid(cfg, device=local)
+        g.set_guess_mode(_abi.GUESS_HISTORY)
+        if Cm is not None:
+            g.set_cmatrix(0, Cm)
+        g.generate_ambient()
+        g.initialize()
+        gs.append(g)
+    for g in gs:
+        g.mainLoopES(1)
+
+    def rel(a, b):
+        return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+    out = {"steps": steps, "rho": rel(gs[0].getRho(), gs[1].getRho()), "phi": rel(gs[0].getPhi(), gs[1].getPhi()),
+           "E": max(rel(a, b) for a, b in zip(gs[0].getEref(), gs[1].getEref()))}
+    if cfg.objects:
+        V = [(gs[0].getObject(0)[0], gs[1].getObject(0)[0])]
+        for _ in range(steps - 1):
+            for g in gs:
+                g.mainLoopES(1)
+            V.append((gs[0].getObject(0)[0], gs[1].getObject(0)[0]))
+        V = np.array(V)
+        out["potential_history"] = float(np.max(np.abs(V[:, 0] - V[:, 1])) / np.max(np.abs(V[:, 1])))
+        out["potential_V_last"] = [cfg.norm.unpotential(float(v)) for v in V[-1]]
+    for g in gs:
+        g.close()
+    out["note"] = ("mixed (fp32 split-precision particles, int64 fixed-point rho) against the fp64 GPU mode, "
+                   "same seed; field errors after one step as max|diff|/max|fp64|; potential over the steps")
+    return out
+
+
+def craft256_block(args, local, steps: int = 8, warmup: int = 2):
+    """The 256^3 spacecraft workload (32x16x16 body + 48x4x16 panel, photoemission,
+    ~1.07e9 particles): ms/step, particle-steps/s and the push roofline fraction,
+    with the capacity-matrix build time. Timed with CUDA events on the library stream."""
+    import torch
+    from fopis_b200 import RootGrid, _abi, config
+    cfg = config.workload("craft256", seed=20251203, sort_interval=args.sort_interval)
+    g = RootGrid(cfg, device=local)
+    g.set_guess_mode(_abi.GUESS_HISTORY)
+    t0 = time.time()
+    g.initializeObjectsCmatrix(0)
+    t_cmat = time.time() - t0
+    g.generate_ambient()
+    g.initialize()
+    for _ in range(warmup):
+        g.mainLoopES(1)
+    stream = torch.cuda.ExternalStream(g.stream_ptr(), device=torch.device("cuda", local))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    psteps, push, pushed = 0, [], []
+    torch.cuda.synchronize(local)
+    e0.record(stream)
+    for _ in range(steps):
+        st = g.stats()
+        n = total_particles(st, cfg.params.nspecies)
+        g.mainLoopES(1)
+        psteps += n
+        pushed.append(n)
+        push.append(g.stats().ms_phase[0])
+    e1.record(stream)
+    torch.cuda.synchronize(local)
+    ms = e0.elapsed_time(e1)
+    st = g.stats()
+    hbm, _ = peaks()
+    achieved = PUSH_BYTES_PER_PARTICLE * float(np.mean(pushed)) / (float(np.mean(push)) * 1e-3) / 1e9
+    out = {"workload": workload_desc("craft256", None), "steps": steps, "warmup": warmup,
+           "ms_per_step": ms / steps, "particle_steps_per_s": psteps / (ms * 1e-3),
+           "particles": total_particles(st, cfg.params.nspecies), "n_cmat": len(cfg.objects[0].nodes),
+           "setup_cmatrix_s": round(t_cmat, 2), "vcycles_per_step": st.vcycles_step,
+           "push_roofline": {"achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm}}
+    g.close()
+    return out
+
+
 def reference_cmatrix(cfg):
     """Capacity matrix for the CPU arms, as the reference's use_existing_capacity_matrix
     would load it: the exact sine-basis build of the oracle (host only, untimed)."""
@@ -468,6 +552,10 @@ def main():
                     help="online training steps before the learned-guess comparison (0: skip it); "
                          "2000 as in the learned-guess configuration")
     ap.add_argument("--learned-lr", type=float, default=1e-3)
+    ap.add_argument("--mixed-vs-fp64", type=int, default=100,
+                    help="steps of the mixed-precision run against the FP64 GPU mode on the same seed (0: skip)")
+    ap.add_argument("--no-craft256", dest="craft256", action="store_false",
+                    help="skip the 256^3 spacecraft block")
     ap.add_argument("--guess", default="history", choices=["warm", "history"],
                     help="Poisson start of the timed run: the reference's warm start or the per-solve history")
     args = ap.parse_args()
@@ -549,10 +637,17 @@ def main():
     if args.phases:
         line["phases_all"] = res["phases_all"]
     line["setup_cmatrix_s"] = round(res["t_cmat"], 2)
+    line["residual_pointwise_max"] = res["pointwise_max"]
+    line["residual_note"] = ("solves stop at ||r||2/||f||2 <= 1e-8; residual_pointwise_max is the largest over the "
+                             "timed solves of the reference's checkPhiResidual measure max|L phi + rho/eps0|/|rho/eps0|")
     if "e2e" in res:
         line["e2e"] = res["e2e"]
     if args.learned_train > 0 and world == 1:
         line["learned_guess"] = learned_comparison(args, rank, local, res["cmatrix"])
+    if args.mixed_vs_fp64 > 0 and world == 1 and args.precision == "mixed":
+        line["mixed_vs_fp64"] = mixed_vs_fp64(args, local, res["cmatrix"], args.mixed_vs_fp64)
+    if args.craft256 and world == 1 and args.workload != "craft256":
+        line["craft256"] = craft256_block(args, local)
     if rank == 0 and res["cmatrix"] is not None:
         try:
             Cx = reference_cmatrix(cfg)

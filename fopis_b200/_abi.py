@@ -120,6 +120,7 @@ class Stats(C.Structure):
         ("kernel_launches", C.c_int64),
         ("solve_mode", C.c_int),
         ("pad", C.c_int),
+        ("residual_pointwise", C.c_double),
     ]
 
 

@@ -608,6 +608,12 @@ int fopis_get_stats(void* h, fopis_stats* st) {
         for (int q = 0; q < 8; ++q) st->ms_phase[q] = c.ms_phase[q];
         st->kernel_launches = c.launches;
         st->solve_mode = c.solve_state == 1 ? (c.pdl ? 2 : 1) : 0;
+        {
+            const unsigned long long bits = c.h_sc->pointwise_bits;
+            double v;
+            std::memcpy(&v, &bits, sizeof(v));
+            st->residual_pointwise = v;
+        }
         return FOPIS_OK;
     });
 }

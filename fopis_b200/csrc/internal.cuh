@@ -113,6 +113,7 @@ struct DevScalars {
     unsigned long long not_found;
     unsigned int status;                                // FOPIS_DEV_* bits
     unsigned int pad;
+    unsigned long long pointwise_bits;                  // last solve's pointwise residual (double bits)
     double energy[FOPIS_MAX_SPECIES];                   // sum of v^2 of live particles
     double red[16];                                     // scratch reduction slots
 };

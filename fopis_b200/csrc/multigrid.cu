@@ -994,6 +994,45 @@ __global__ void reduce_partials_kernel(const double* partial, int n, int stride,
 // Threads of the row-walking FP64 kernels: one row of the contiguous axis per pass.
 int outer_threads(const Outer& O) { return std::min(kT, std::max(32, ((O.n2 + 31) / 32) * 32)); }
 
+// RootGrid::checkPhiResidual's measure (src/Grid/RootGrid/RootGridField.cpp:
+// 267-317): max over the unknown nodes with a nonzero source of
+// |L phi + rho/eps0| / |rho/eps0|, L the 7-point operator with dx = 1 (the
+// Dirichlet/Neumann face planes are not unknowns and are skipped, as there).
+// Periodic neighbours wrap (the reference reads its freshly exchanged glue);
+// with every axis periodic the source is the solve's mean-free one. Nonnegative
+// doubles order like their bit patterns, so the block maxima combine with an
+// integer atomicMax.
+__global__ void __launch_bounds__(kT) pointwise_residual_kernel(Outer O, const double* rho0, const double* phi,
+                                                                unsigned long long* out) {
+    __shared__ double red[32];
+    const long long total = (long long)O.n0 * O.n1 * O.n2;
+    const double fm = (O.p0 && O.p1 && O.p2) ? *O.fmean : 0.0;
+    double m = 0.0;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int a = (int)(t / ((long long)O.n1 * O.n2));
+        const int b = (int)((t / O.n2) % O.n1), cc = (int)(t % O.n2);
+        const int i = a + O.o0, j = b + O.o1, k = cc + O.o2;
+        const double src = rho0[gl(O, i, j, k)] * O.inv_eps0 - fm;
+        if (!(fabs(src) > 0.0)) continue;
+        const double op = phi[gl(O, wrapn(i - 1, O.p0, O.nref0), j, k)] + phi[gl(O, wrapn(i + 1, O.p0, O.nref0), j, k)] +
+                          phi[gl(O, i, wrapn(j - 1, O.p1, O.nref1), k)] + phi[gl(O, i, wrapn(j + 1, O.p1, O.nref1), k)] +
+                          phi[gl(O, i, j, wrapn(k - 1, O.p2, O.nref2))] + phi[gl(O, i, j, wrapn(k + 1, O.p2, O.nref2))] -
+                          6.0 * phi[gl(O, i, j, k)];
+        const double r = fabs((op + src) / src);
+        m = r > m ? r : m;            // a NaN residual stays out of the maximum
+    }
+    for (int o = 16; o; o >>= 1) { const double v = __shfl_down_sync(0xffffffffu, m, o); m = v > m ? v : m; }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) red[w] = m;
+    __syncthreads();
+    if (w == 0) {
+        m = (l < (int)(blockDim.x >> 5)) ? red[l] : 0.0;
+        for (int o = 16; o; o >>= 1) { const double v = __shfl_down_sync(0xffffffffu, m, o); m = v > m ? v : m; }
+        if (l == 0 && m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
 Outer make_outer(const Ctx& c) {
     Outer O;
     O.cx = c.cx; O.cy = c.cy; O.cz = c.cz;
@@ -1564,6 +1603,13 @@ int mg_solve(Ctx& c, double tol, int max_cycles) {
         c.launches += c.solve_pre_launches + (int64_t)cycles * c.cycle_launches + c.solve_post_launches;
     } else {
         mg_solve_host_loop(c, tol, max_cycles, &res, &fnorm, &cycles);
+    }
+    {   // the reference's pointwise measure on the state the solve reached (faces still held)
+        const Outer O = make_outer(c);
+        FOPIS_CUDA(cudaMemsetAsync(&c.d_sc->pointwise_bits, 0, sizeof(unsigned long long), c.st));
+        ++c.launches;
+        pointwise_residual_kernel<<<kRedBlocks, kT, 0, c.st>>>(O, c.rho0, c.phi, &c.d_sc->pointwise_bits);
+        FOPIS_LAUNCH_CHECK();
     }
     phi_boundary(c);
     c.last_vcycles = cycles;

@@ -166,6 +166,10 @@ typedef struct fopis_stats {
     int solve_mode;              /* 0: host-driven V-cycle loop; 1: one CUDA graph with a device-side
                                     loop; 2: the same graph with programmatic dependent launches */
     int pad;
+    double residual_pointwise;   /* last solve, RootGrid::checkPhiResidual's measure
+                                    (RootGridField.cpp:267-317): max over unknown nodes with a
+                                    nonzero source of |L phi + rho/eps0| / |rho/eps0| (mean-free
+                                    source when every axis is periodic) */
 } fopis_stats;
 
 /* ---- lifetime ----------------------------------------------------------- */

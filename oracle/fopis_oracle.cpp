@@ -1246,6 +1246,13 @@ void orc_set_solver(void* h, int mode, int max_post_loop, double exact_tol) {
 void orc_solver_stats(void* h, int* iterations, double* residual) {
     Ctx* c = (Ctx*)h; *iterations = c->last_iterations; *residual = c->last_residual;
 }
+// RootGrid::checkPhiResidual on the current phi and rho (glue of periodic axes
+// refreshed first, as the PSOR's exchanges leave it).
+double orc_pointwise_residual(void* h) {
+    Ctx* c = (Ctx*)h;
+    copy_field_glue(*c, c->phi);
+    return check_phi_residual(*c);
+}
 
 int orc_add_object(void* h, const fopis_object_desc* d) {
     Ctx* c = (Ctx*)h;

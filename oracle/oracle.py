@@ -37,6 +37,7 @@ def lib():
             "orc_philox": (None, [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
             "orc_set_solver": (None, [vp, C.c_int, C.c_int, C.c_double]),
             "orc_solver_stats": (None, [vp, C.POINTER(C.c_int), dp]),
+            "orc_pointwise_residual": (C.c_double, [vp]),
             "orc_add_object": (C.c_int, [vp, vp]), "orc_build_cmatrix": (C.c_int, [vp, C.c_int]),
             "orc_set_cmatrix": (C.c_int, [vp, C.c_int, dp, C.c_int]),
             "orc_get_cmatrix": (C.c_int, [vp, C.c_int, dp, C.c_int]),
@@ -218,6 +219,10 @@ class Oracle:
         it, res = C.c_int(), C.c_double()
         self.L.orc_solver_stats(self.h, C.byref(it), C.byref(res))
         return it.value, res.value
+
+    def pointwise_residual(self):
+        """RootGrid::checkPhiResidual's measure on the current phi and rho."""
+        return self.L.orc_pointwise_residual(self.h)
 
     def build_cmatrix(self, obj=0):
         rc = self.L.orc_build_cmatrix(self.h, obj)
