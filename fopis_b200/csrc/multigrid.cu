@@ -205,6 +205,50 @@ __global__ void __launch_bounds__(kMarchX * kMarchY) rb_first_march_kernel(Lv L)
     }
 }
 
+// Red value of the first half sweep from u = 0 (rb_first_march_kernel's formula).
+__device__ __forceinline__ float red_from_zero(float f, float inv_scale) {
+    return kOmega * (f * inv_scale) * (1.0f / 6.0f);
+}
+
+// The first full red-black sweep from u = 0 in one pass: red nodes as
+// rb_first_march_kernel sets them, black nodes as rb_march_kernel's black half
+// sweep then updates them, with the six red neighbours evaluated from f in
+// place (on red-black levels every neighbour of a black node is red). The
+// additions run in march_nsum's order, so the values equal the two passes'.
+template <int A>
+__global__ void __launch_bounds__(kMarchX * kMarchY) rb_first2_march_kernel(Lv L) {
+    pdl_entry();
+    const int c = blockIdx.x * kMarchX + threadIdx.x;
+    const int b = blockIdx.y * kMarchY + threadIdx.y;
+    const int a0 = blockIdx.z * A;
+    if (b >= L.n1 || c >= L.n2) return;
+    const int bm = wrap_or_out(b - 1, L.n1, L.p1), bp = wrap_or_out(b + 1, L.n1, L.p1);
+    const int cm = wrap_or_out(c - 1, L.n2, L.p2), cp = wrap_or_out(c + 1, L.n2, L.p2);
+    float v[A];
+#pragma unroll
+    for (int e = 0; e < A; ++e) {
+        const int a = a0 + e;
+        v[e] = 0.0f;
+        if (a >= L.n0) continue;
+        const long long row = ((long long)a * L.n1 + b) * L.n2;
+        if (((a + b + c) & 1) == 0) {
+            v[e] = red_from_zero(L.f[row + c], L.inv_scale);
+        } else {
+            const int am = wrap_or_out(a - 1, L.n0, L.p0), ap = wrap_or_out(a + 1, L.n0, L.p0);
+            float sum = am >= 0 ? red_from_zero(L.f[((long long)am * L.n1 + b) * L.n2 + c], L.inv_scale) : 0.0f;
+            sum += ap >= 0 ? red_from_zero(L.f[((long long)ap * L.n1 + b) * L.n2 + c], L.inv_scale) : 0.0f;
+            sum += bm >= 0 ? red_from_zero(L.f[((long long)a * L.n1 + bm) * L.n2 + c], L.inv_scale) : 0.0f;
+            sum += bp >= 0 ? red_from_zero(L.f[((long long)a * L.n1 + bp) * L.n2 + c], L.inv_scale) : 0.0f;
+            sum += cm >= 0 ? red_from_zero(L.f[row + cm], L.inv_scale) : 0.0f;
+            sum += cp >= 0 ? red_from_zero(L.f[row + cp], L.inv_scale) : 0.0f;
+            v[e] = (1.0f - kOmega) * 0.0f + kOmega * (sum + L.f[row + c] * L.inv_scale) * (1.0f / 6.0f);
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < A; ++e)
+        if (a0 + e < L.n0) L.u[((long long)(a0 + e) * L.n1 + b) * L.n2 + c] = v[e];
+}
+
 // Weighted Jacobi sweep into r, for levels whose periodic axes are odd.
 __global__ void __launch_bounds__(kRowThreads) jacobi_kernel(Lv L, float omega) {
     pdl_entry();
@@ -937,6 +981,44 @@ __global__ void __launch_bounds__(kOuterThreads) outer_residual_march_kernel(Out
 }
 
 // phi += e at every unknown.
+// rb_march_kernel's half sweep on level 0, then phi += e at both nodes of the
+// thread's pair: the other colour's node is not written in this half sweep, so
+// after it every node's correction is final (replaces correct_march_kernel
+// after the V-cycle).
+template <int A>
+__global__ void __launch_bounds__(kMarchX * kMarchY) rb_march_correct_kernel(Lv L, int color, Outer O, double* phi) {
+    pdl_entry();
+    const int pair = blockIdx.x * kMarchX + threadIdx.x;
+    const int b = blockIdx.y * kMarchY + threadIdx.y;
+    const int a0 = blockIdx.z * A;
+    if (b >= L.n1) return;
+    float v[A];
+    long long at[A];
+#pragma unroll
+    for (int e = 0; e < A; ++e) {
+        const int a = a0 + e, c = 2 * pair + ((a + b + color) & 1);
+        at[e] = -1;
+        if (a < L.n0 && c < L.n2) {
+            at[e] = ((long long)a * L.n1 + b) * L.n2 + c;
+            v[e] = (1.0f - kOmega) * L.u[at[e]] +
+                   kOmega * (march_nsum(L, L.u, a, b, c) + L.f[at[e]] * L.inv_scale) * (1.0f / 6.0f);
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < A; ++e) {
+        const int a = a0 + e;
+        if (a >= L.n0) continue;
+        if (at[e] >= 0) {
+            L.u[at[e]] = v[e];
+            const int c = 2 * pair + ((a + b + color) & 1);
+            phi[gl(O, a + O.o0, b + O.o1, c + O.o2)] += (double)v[e];
+        }
+        const int co = 2 * pair + ((a + b + color + 1) & 1);   // the other colour's node of the pair
+        if (co < L.n2)
+            phi[gl(O, a + O.o0, b + O.o1, co + O.o2)] += (double)L.u[((long long)a * L.n1 + b) * L.n2 + co];
+    }
+}
+
 __global__ void __launch_bounds__(kOuterThreads) correct_march_kernel(Outer O, double* phi, const float* e) {
     pdl_entry();
     const OuterTile T = outer_tiles(O);
@@ -1080,7 +1162,12 @@ void residual(Ctx& c, const MGLevel& m) {
 
 // `sweeps` red-black sweeps on level l; with from_zero the level's u is
 // first set to zero (on marching levels the first red half sweep does it).
-void smooth(Ctx& c, int l, int sweeps, bool from_zero = false) {
+struct FoldCorrect {
+    Outer O;
+    double* phi;
+};
+
+void smooth(Ctx& c, int l, int sweeps, bool from_zero = false, const FoldCorrect* fold = nullptr) {
     MGLevel& m = c.mg[l];
     const Lv L = lv(m);
     const int rb = row_blocks((long long)m.n[0] * m.n[1]);
@@ -1093,12 +1180,24 @@ void smooth(Ctx& c, int l, int sweeps, bool from_zero = false) {
         const dim3 grd = march_grid(m.n, A, 2);
         for (int s = 0; s < sweeps; ++s)
             for (int color = 0; color < 2; ++color) {
-                ++c.launches;
-                if (from_zero && s == 0 && color == 0) {
+                if (from_zero && s == 0) {
+                    // the first sweep from zero: both colours in one pass
+                    if (color == 1) continue;
+                    ++c.launches;
                     const dim3 g1 = march_grid(m.n, A, 1);
-                    if (A == 4) launch_k(c.pdl, rb_first_march_kernel<4>, g1, blk, 0, c.st, L);
-                    else if (A == 2) launch_k(c.pdl, rb_first_march_kernel<2>, g1, blk, 0, c.st, L);
-                    else launch_k(c.pdl, rb_first_march_kernel<1>, g1, blk, 0, c.st, L);
+                    if (A == 4) launch_k(c.pdl, rb_first2_march_kernel<4>, g1, blk, 0, c.st, L);
+                    else if (A == 2) launch_k(c.pdl, rb_first2_march_kernel<2>, g1, blk, 0, c.st, L);
+                    else launch_k(c.pdl, rb_first2_march_kernel<1>, g1, blk, 0, c.st, L);
+                    continue;
+                }
+                ++c.launches;
+                const bool last = s == sweeps - 1 && color == 1;
+                if (last && fold) {
+                    // the level-0 post-smoothing's last half sweep adds the finished
+                    // correction to the FP64 potential as it goes
+                    if (A == 4) launch_k(c.pdl, rb_march_correct_kernel<4>, grd, blk, 0, c.st, L, color, fold->O, fold->phi);
+                    else if (A == 2) launch_k(c.pdl, rb_march_correct_kernel<2>, grd, blk, 0, c.st, L, color, fold->O, fold->phi);
+                    else launch_k(c.pdl, rb_march_correct_kernel<1>, grd, blk, 0, c.st, L, color, fold->O, fold->phi);
                     continue;
                 }
                 if (A == 4) launch_k(c.pdl, rb_march_kernel<4>, grd, blk, 0, c.st, L, color);
@@ -1142,6 +1241,13 @@ void coarse_solve(Ctx& c, int l) {
 
 void coarse_cycle(Ctx& c);
 
+// Whether vcycle(c, 0) adds the correction to phi itself (the level-0
+// post-smoothing marches); otherwise the caller launches correct_march_kernel.
+bool folds_correction(const Ctx& c) {
+    const MGLevel& m = c.mg[0];
+    return c.mg.size() > 1 && c.mg_cta_start != 0 && level_rb(m) && m.n[0] >= kMarchMin;
+}
+
 void vcycle(Ctx& c, int l) {
     const int L = (int)c.mg.size();
     if (l == c.mg_cta_start) { coarse_cycle(c); return; }
@@ -1174,7 +1280,12 @@ void vcycle(Ctx& c, int l) {
         launch_k(c.pdl, prolong_kernel, row_blocks((long long)m.n[0] * m.n[1]), std::min(kRowThreads, ((m.n[2] + 31) / 32) * 32), 0, c.st, lv(n), lv(m));
     }
     FOPIS_LAUNCH_CHECK();
-    smooth(c, l, kPostSweeps);
+    if (l == 0 && folds_correction(c)) {
+        const FoldCorrect fold{make_outer(c), c.phi};
+        smooth(c, l, kPostSweeps, false, &fold);
+    } else {
+        smooth(c, l, kPostSweeps);
+    }
 }
 
 
@@ -1350,8 +1461,10 @@ static void ensure_cycle_graph(Ctx& c) {
     FOPIS_CUDA(cudaStreamBeginCapture(c.st, cudaStreamCaptureModeThreadLocal));
     try {
         vcycle(c, 0);
-        ++c.launches;
-        launch_k(c.pdl, correct_march_kernel, kRedBlocks, kOuterThreads, 0, c.st, O, c.phi, c.mg[0].u);
+        if (!folds_correction(c)) {
+            ++c.launches;
+            launch_k(c.pdl, correct_march_kernel, kRedBlocks, kOuterThreads, 0, c.st, O, c.phi, c.mg[0].u);
+        }
         ++c.launches;
         launch_k(c.pdl, outer_residual_march_kernel, kRedBlocks, kOuterThreads, 0, c.st, O, c.rho0, c.phi, c.mg[0].f, c.red_partials);
         ++c.launches;
@@ -1469,8 +1582,10 @@ void build_solve_graph(Ctx& c) {
         c.st = c.body_st;
         const int64_t b0 = c.launches;
         vcycle(c, 0);
-        ++c.launches;
-        launch_k(c.pdl, correct_march_kernel, kRedBlocks, kOuterThreads, 0, c.st, O, c.phi, c.mg[0].u);
+        if (!folds_correction(c)) {
+            ++c.launches;
+            launch_k(c.pdl, correct_march_kernel, kRedBlocks, kOuterThreads, 0, c.st, O, c.phi, c.mg[0].u);
+        }
         ++c.launches;
         launch_k(c.pdl, outer_residual_march_kernel, kRedBlocks, kOuterThreads, 0, c.st, O, c.rho0, c.phi, c.mg[0].f, c.red_partials);
         ++c.launches;
