@@ -222,7 +222,13 @@ def build_sim(args, rank, local):
 
 
 def total_particles(st, nsp):
-    return int(sum(st.num_particles[s] for s in range(nsp)))
+    """Valid particles after the last step or sort."""
+    return int(sum(st.valid_particles[s] for s in range(nsp)))
+
+
+def pushed_particles(st, nsp):
+    """Valid particles the last step's push moved (its particle-steps)."""
+    return int(sum(st.pushed_step[s] for s in range(nsp)))
 
 
 def run_gpu(args, world, rank, local):
@@ -247,12 +253,12 @@ def run_gpu(args, world, rank, local):
     with ClockSampler(local) as clk:
         ev0.record(stream)
         for t in range(args.steps):
-            n_before = total_particles(g.stats(), nsp)
             g.mainLoopES(1)
             step_ev[t].record(stream)
             st = g.stats()
-            psteps += n_before
-            pushed.append(n_before)
+            n = pushed_particles(st, nsp)
+            psteps += n
+            pushed.append(n)
             push_ms.append(st.ms_phase[0])
             phases_all.append([round(x, 3) for x in st.ms_phase])
             vcyc.append(st.vcycles_step)
@@ -311,12 +317,11 @@ def run_gpu(args, world, rank, local):
         ps2 = 0
         d2h = 0
         for _ in range(args.steps):
-            n_before = total_particles(g2.stats(), nsp)
             g2.mainLoopES(1)
             g2.getEnergy()
             if cfg.objects:
                 g2.getObject(0)
-            ps2 += n_before
+            ps2 += pushed_particles(g2.stats(), nsp)
             d2h += 16 + (16 + 8 * nsp if cfg.objects else 0)
         e1.record(stream2)
         torch.cuda.synchronize(local)
@@ -470,12 +475,12 @@ def craft256_block(args, local, steps: int = 8, warmup: int = 2):
     torch.cuda.synchronize(local)
     e0.record(stream)
     for _ in range(steps):
-        st = g.stats()
-        n = total_particles(st, cfg.params.nspecies)
         g.mainLoopES(1)
+        st = g.stats()
+        n = pushed_particles(st, cfg.params.nspecies)
         psteps += n
         pushed.append(n)
-        push.append(g.stats().ms_phase[0])
+        push.append(st.ms_phase[0])
     e1.record(stream)
     torch.cuda.synchronize(local)
     ms = e0.elapsed_time(e1)

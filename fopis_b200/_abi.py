@@ -121,6 +121,8 @@ class Stats(C.Structure):
         ("solve_mode", C.c_int),
         ("pad", C.c_int),
         ("residual_pointwise", C.c_double),
+        ("valid_particles", C.c_int64 * MAX_SPECIES),
+        ("pushed_step", C.c_int64 * MAX_SPECIES),
     ]
 
 
@@ -170,6 +172,10 @@ SIGNATURES = {
     "fopis_unet_tensor": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_float), C.c_int64, C.POINTER(C.c_int64)]),
     "fopis_parse_obj": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.POINTER(C.c_int32)),
                                   C.POINTER(C.c_int), C.POINTER(C.POINTER(C.c_int32)), C.POINTER(C.c_int)]),
+    "fopis_set_charge_map": (C.c_int, [_VP, C.c_int, _DP, C.c_int]),
+    "fopis_set_timestep": (C.c_int, [_VP, C.c_int64]),
+    "fopis_get_injection_carry": (C.c_int, [_VP, _DP, C.c_int]),
+    "fopis_set_injection_carry": (C.c_int, [_VP, _DP, C.c_int]),
     "fopis_free": (None, [_VP]),
     "fopis_check_bounded_wait": (C.c_int, [C.c_int, C.c_uint32, C.c_int, C.POINTER(C.c_uint32)]),
     "fopis_efield_energy_noalloc": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, C.c_double, _VP, _VP]),

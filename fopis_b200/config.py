@@ -116,6 +116,7 @@ class ObjectInfo:
     fixed_potential: float = 0.0     # volts
     initial_potential_offset: float = 0.0
     emit_species: int = -1
+    file_name: str = ""              # the .obj file's name without directories (capacity-matrix cache name)
 
 
 @dataclass
@@ -364,7 +365,8 @@ def load_input(path: str) -> SimConfig:
                 emit = names.index(pname)
         objs.append(ObjectInfo(oname, nodes, cells, int(o.get("is_potential_fixed", False)),
                                norm.potential(float(o.get("fixed_potential", 0.0))),
-                               norm.potential(float(o.get("initial_potential_offset", 0.0))), emit))
+                               norm.potential(float(o.get("initial_potential_offset", 0.0))), emit,
+                               file_name=os.path.basename(o["file_name"])))
     return SimConfig(params=p, norm=norm, species=species, objects=objs, max_timestep=int(env.get("max_timestep", 0)),
                      dx=dx, dt=dt, use_existing_capacity_matrix=bool(opts.get("use_existing_capacity_matrix", False)),
                      maximum_poisson_post_loop=int(opts.get("maximum_poisson_post_loop", 1000)))

@@ -172,6 +172,7 @@ void record(Ctx& c, int k) {
 // The fused RootGrid::mainLoopES (RootGrid.cpp:82-143).
 int one_step(Ctx& c) {
     step_begin(c);
+    FOPIS_CUDA(cudaMemsetAsync(c.d_sc->pushed, 0, 3 * sizeof(c.d_sc->pushed), c.st));
     FOPIS_CUDA(cudaMemsetAsync(&c.d_sc->absorbed_n, 0, sizeof(unsigned long long), c.st));
     rho_zero(c);
     record(c, 0);
@@ -193,6 +194,11 @@ int one_step(Ctx& c) {
     record(c, 8);
     int rc = check_device(c);
     update_currents(c);
+    for (int s = 0; s < c.nsp; ++s) {
+        c.pushed_step[s] = (int64_t)c.h_sc->pushed[s];
+        // after a sort step the sort's exact count stands; otherwise survivors plus new particles
+        if (c.timestep % si != 0) c.valid[s] = (int64_t)(c.h_sc->survived[s] + c.h_sc->added[s]);
+    }
     c.energy_valid = true;
     c.timestep += 1;
     if (c.ev[0]) {
@@ -411,6 +417,38 @@ int fopis_get_charge_map(void* h, int id, double* out, int n) {
     });
 }
 
+int fopis_set_charge_map(void* h, int id, const double* in, int n) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (id < 0 || id >= (int)c.objs.size() || !in || n != c.nsp * c.objs[id].n) throw ApiError{FOPIS_ERR_ARG, "object id or size"};
+        FOPIS_CUDA(cudaMemcpy(c.objs[id].charge_map, in, sizeof(double) * n, cudaMemcpyHostToDevice));
+        return FOPIS_OK;
+    });
+}
+
+int fopis_set_timestep(void* h, int64_t t) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (t < 1) throw ApiError{FOPIS_ERR_ARG, "timestep must be >= 1"};
+        c.timestep = t;
+        return FOPIS_OK;
+    });
+}
+
+int fopis_get_injection_carry(void* h, double* out, int n) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (!out || n != 6 * c.nsp) throw ApiError{FOPIS_ERR_ARG, "carry size must be 6 * nspecies"};
+        for (int s = 0; s < c.nsp; ++s) for (int f = 0; f < 6; ++f) out[6 * s + f] = c.inject_residual[s][f];
+        return FOPIS_OK;
+    });
+}
+
+int fopis_set_injection_carry(void* h, const double* in, int n) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (!in || n != 6 * c.nsp) throw ApiError{FOPIS_ERR_ARG, "carry size must be 6 * nspecies"};
+        for (int s = 0; s < c.nsp; ++s) for (int f = 0; f < 6; ++f) c.inject_residual[s][f] = in[6 * s + f];
+        return FOPIS_OK;
+    });
+}
+
 int fopis_load_particles(void* h, int s, const void* p56, int64_t n) {
     return guarded(h, [&](Ctx& c) -> int {
         if (s < 0 || s >= c.nsp || (n > 0 && !p56) || n < 0) throw ApiError{FOPIS_ERR_ARG, "species or buffer"};
@@ -599,7 +637,12 @@ int fopis_get_stats(void* h, fopis_stats* st) {
         st->converged = c.last_converged;
         st->residual_last = c.last_res;
         st->residual_initial = c.first_res;
-        for (int s = 0; s < c.nsp; ++s) { st->num_particles[s] = c.nslots[s]; st->capacity[s] = c.cap[s]; }
+        for (int s = 0; s < c.nsp; ++s) {
+            st->num_particles[s] = c.nslots[s];
+            st->capacity[s] = c.cap[s];
+            st->valid_particles[s] = c.valid[s];
+            st->pushed_step[s] = c.pushed_step[s];
+        }
         st->absorbed_step = c.absorbed_step;
         st->injected_step = c.injected_step;
         st->emitted_step = c.emitted_step;

@@ -114,6 +114,9 @@ struct DevScalars {
     unsigned int status;                                // FOPIS_DEV_* bits
     unsigned int pad;
     unsigned long long pointwise_bits;                  // last solve's pointwise residual (double bits)
+    // per species in the current fused step: valid particles the push moved, those that
+    // stayed valid (in the domain, not absorbed), and particles injected or emitted
+    unsigned long long pushed[FOPIS_MAX_SPECIES], survived[FOPIS_MAX_SPECIES], added[FOPIS_MAX_SPECIES];
     double energy[FOPIS_MAX_SPECIES];                   // sum of v^2 of live particles
     double red[16];                                     // scratch reduction slots
 };
@@ -179,6 +182,8 @@ struct Ctx {
     int64_t cap[FOPIS_MAX_SPECIES] = {0};
     int64_t nslots[FOPIS_MAX_SPECIES] = {0};   // host mirror of DevScalars::count
     int64_t sorted_n[FOPIS_MAX_SPECIES] = {0}; // slots [0, sorted_n) are brick-sorted
+    int64_t valid[FOPIS_MAX_SPECIES] = {0};    // valid particles after the last fused step or sort
+    int64_t pushed_step[FOPIS_MAX_SPECIES] = {0};   // valid particles the last fused step pushed
     int32_t* brick_start[FOPIS_MAX_SPECIES] = {nullptr};  // first slot of each brick
     // fields
     unsigned long long* rho_i64 = nullptr;  // [nsp][N] two's complement fixed point (FP64 mode: double weights)

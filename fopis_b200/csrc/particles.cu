@@ -332,7 +332,7 @@ template <typename T, bool VEL, bool POS, bool DEP>
 __global__ void __launch_bounds__(kThreads) push_kernel(PushArgsT<T> a) {
     const long long n = (long long)min(*a.count, (unsigned long long)a.cap);
     const long long stride = (long long)gridDim.x * blockDim.x;
-    double e2 = 0.0;
+    double e2 = 0.0, npushed = 0.0, nkept = 0.0;
     for (long long base = a.lo + (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
         const long long idx = base + (threadIdx.x & 31);
         const bool inb = idx < n;
@@ -358,6 +358,7 @@ __global__ void __launch_bounds__(kThreads) push_kernel(PushArgsT<T> a) {
                 deposit_f64(reinterpret_cast<double*>(a.rho), lin(a.g, st.i, st.j, st.k), off, st.ox, st.oy, st.oz);
             }
             if (live && VEL) e2 += (double)st.vx * st.vx + (double)st.vy * st.vy + (double)st.vz * st.vz;
+            if (VEL && POS) { npushed += cell >= 0 ? 1.0 : 0.0; nkept += live ? 1.0 : 0.0; }
         }
         if (inb && cell >= 0) {
             if (POS || DEP) a.p.cell[idx] = live ? pack_cell(st.i, st.j, st.k) : -1;
@@ -368,6 +369,13 @@ __global__ void __launch_bounds__(kThreads) push_kernel(PushArgsT<T> a) {
     if (DEP && VEL) {
         const double t = block_sum(e2);
         if (threadIdx.x == 0 && t != 0.0) atomicAdd(&a.sc->energy[a.s], t);
+    }
+    if (DEP && VEL && POS) {   // the fused pass: counts of the step (exact in FP64 below 2^53)
+        const double np = block_sum(npushed), nk = block_sum(nkept);
+        if (threadIdx.x == 0) {
+            if (np > 0.0) atomicAdd(&a.sc->pushed[a.s], (unsigned long long)np);
+            if (nk > 0.0) atomicAdd(&a.sc->survived[a.s], (unsigned long long)nk);
+        }
     }
 }
 
@@ -513,7 +521,7 @@ __global__ void __launch_bounds__(kBrickThreads, MINB) push_brick_kernel(PushArg
     // particles that stay inside a body-free window need no body test
     const bool window_body = __syncthreads_or(body) != 0;
     const long long p0 = brick_start[b], p1 = brick_start[b + 1];
-    double e2 = 0.0;
+    double e2 = 0.0, npushed = 0.0, nkept = 0.0;
     bool wrap = false;
     for (long long s0 = p0; s0 < p1; s0 += kSegment) {
         const long long s1 = min(p1, s0 + (long long)kSegment);
@@ -563,6 +571,8 @@ __global__ void __launch_bounds__(kBrickThreads, MINB) push_brick_kernel(PushArg
                                            : kNoDeposit;
                     if (live && !inwin) wrap |= global_deposit(a.rho, a.g, lin(a.g, st.i, st.j, st.k), qa, qb, qd);
                     if (live) e2 += (double)(st.vx * st.vx + st.vy * st.vy + st.vz * st.vz);
+                    npushed += cell[r] >= 0 ? 1.0 : 0.0;
+                    nkept += live ? 1.0 : 0.0;
                     if (cell[r] >= 0) {
                         a.p.cell[idx] = live ? pack_cell(st.i, st.j, st.k) : -1;
                         a.p.ox[idx] = st.ox; a.p.oy[idx] = st.oy; a.p.oz[idx] = st.oz;
@@ -633,6 +643,11 @@ __global__ void __launch_bounds__(kBrickThreads, MINB) push_brick_kernel(PushArg
     if (wrap) atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_RHO_OVERFLOW);
     const double tot = block_sum(e2);
     if (tid == 0 && tot != 0.0) atomicAdd(&a.sc->energy[a.s], tot);
+    const double np = block_sum(npushed), nk = block_sum(nkept);
+    if (tid == 0) {
+        if (np > 0.0) atomicAdd(&a.sc->pushed[a.s], (unsigned long long)np);
+        if (nk > 0.0) atomicAdd(&a.sc->survived[a.s], (unsigned long long)nk);
+    }
 }
 
 // Writes a particle created in FP64 into a species slot (split precision).
@@ -720,7 +735,10 @@ __device__ void finish_source(const SourceArgsT<T>& a, int s, double x, double y
     if (!live) return;
     const int lane = threadIdx.x & 31, leader = __ffs(grp) - 1;
     unsigned long long base = 0;
-    if (lane == leader) base = atomicAdd(&a.sc->count[s], (unsigned long long)__popc(grp));
+    if (lane == leader) {
+        base = atomicAdd(&a.sc->count[s], (unsigned long long)__popc(grp));
+        atomicAdd(&a.sc->added[s], (unsigned long long)__popc(grp));
+    }
     base = __shfl_sync(grp, base, leader);
     const unsigned long long slot = base + __popc(grp & ((1u << lane) - 1u));
     if ((long long)slot < a.cap[s]) store_split(a.p[s], (long long)slot, i, j, k, ox, oy, oz, vx, vy, vz);
@@ -1678,6 +1696,7 @@ static void sort_all(Ctx& c) {
         if (c.cap[s] == 0) continue;
         const int64_t n = c.nslots[s];
         c.sorted_n[s] = n;
+        c.valid[s] = n;             // the sort keeps exactly the valid particles
         if (n < c.cap[s]) FOPIS_CUDA(cudaMemsetAsync(parts<T>(c)[s].cell + n, 0xff, sizeof(int32_t) * (c.cap[s] - n), c.st));
         // keep head room for the appends of the coming steps
         const int64_t want = (int64_t)(n * 1.25) + 65536;

@@ -1,5 +1,8 @@
 // fopis_host.cpp — the host classes of fopis_host.hpp over the C ABI.
+#include <iostream>
+
 #include "fopis_host.hpp"
+#include "datafile.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -93,6 +96,9 @@ Input load_input(const std::string& path) {
     if (env.integer_or("proc_x", 1) * env.integer_or("proc_y", 1) * env.integer_or("proc_z", 1) != 1)
         throw Error(FOPIS_ERR_ARG, "the whole domain lives on one GPU: proc_x = proc_y = proc_z = 1");
     in.max_timestep = env.integer_or("max_timestep", 0);
+    in.job_type = env.str_or("job_type", "new");
+    if (in.job_type != "new" && in.job_type != "load")
+        throw Error(FOPIS_ERR_ARG, "Unknown jobtype, neither ``new'' or ``load'', was inputted.");   // Initialize.cpp:97-99
     in.norm = Normalizer(in.dx, in.dt);
     const Normalizer& norm = in.norm;
 
@@ -157,6 +163,7 @@ Input load_input(const std::string& path) {
             ObjectSpec spec;
             spec.name = kv.first;
             std::string file = o["file_name"].str();
+            spec.file_name = file.substr(file.find_last_of('/') == std::string::npos ? 0 : file.find_last_of('/') + 1);
             if (!file.empty() && file[0] != '/') file = base + "/" + file;
             parse_obj(file, nxyz[0], nxyz[1], nxyz[2], spec);
             spec.is_potential_fixed = o.boolean_or("is_potential_fixed", false) ? 1 : 0;
@@ -226,32 +233,101 @@ void RootGrid::check(int rc, bool allow_not_converged) const {
     throw Error(rc, fopis_last_error(ctx_));
 }
 
-void RootGrid::initializeObjectsCmatrix(const std::string& cache_dir) {
+void RootGrid::initializeObjectsCmatrix(const std::string& resume_dir) {
     for (size_t k = 0; k < in_.objects.size(); ++k) {
-        const int id = object_ids_[k];
-        const int n = in_.objects[k].n_cmat();
-        const std::string file = cache_dir.empty() ? "" : cache_dir + "/cmatrix_" + in_.objects[k].name + ".bin";
-        if (!file.empty() && in_.use_existing_capacity_matrix) {
-            std::ifstream f(file, std::ios::binary);
-            int64_t m = 0;
-            if (f && f.read(reinterpret_cast<char*>(&m), sizeof m) && m == n) {
-                std::vector<double> C((size_t)n * n);
-                if (f.read(reinterpret_cast<char*>(C.data()), sizeof(double) * C.size())) {
-                    check(fopis_set_capacity_matrix(ctx_, id, C.data(), n));
-                    continue;
-                }
-            }
+        if (!resume_dir.empty() && in_.use_existing_capacity_matrix && io::loadCmatrixData(*this, (int)k, resume_dir))
+            continue;
+        check(fopis_build_capacity_matrix(ctx_, object_ids_[k]));
+        if (!resume_dir.empty()) io::writeCmatrixData(*this, (int)k, resume_dir);
+    }
+}
+
+void RootGrid::setTimestep(int64_t t) { check(fopis_set_timestep(ctx_, t)); }
+
+void RootGrid::saveResumeData(const std::string& dir) const {
+    make_dirs(dir);
+    DataFile f;
+    const int nsp = in_.params.nspecies;
+    std::vector<double> carry(6 * (size_t)nsp);
+    check(fopis_get_injection_carry(ctx_, carry.data(), 6 * nsp));
+    for (int s = 0; s < nsp; ++s) {
+        const std::string g = in_.species[s].name + "/";
+        const std::vector<Particle> p = getParticles(s);
+        const uint64_t n = p.size();
+        std::vector<double> col[6];
+        for (auto& c : col) c.resize(n);
+        for (uint64_t i = 0; i < n; ++i) {
+            col[0][i] = p[i].x; col[1][i] = p[i].y; col[2][i] = p[i].z;
+            col[3][i] = p[i].vx; col[4][i] = p[i].vy; col[5][i] = p[i].vz;
         }
-        check(fopis_build_capacity_matrix(ctx_, id));
-        if (!file.empty()) {
-            std::vector<double> C((size_t)n * n);
-            check(fopis_get_capacity_matrix(ctx_, id, C.data(), n));
-            std::ofstream f(file, std::ios::binary);
-            const int64_t m = n;
-            f.write(reinterpret_cast<const char*>(&m), sizeof m);
-            f.write(reinterpret_cast<const char*>(C.data()), sizeof(double) * C.size());
+        f.put_f64(g + "size", (double)n);                     // the reference writes the count as a double
+        const char* keys[6] = {"x", "y", "z", "vx", "vy", "vz"};
+        for (int q = 0; q < 6; ++q) f.put_f64(g + keys[q], {n}, col[q].data());
+        // the reference records its mt19937 draw counts here; the Philox draws are keyed
+        // by (seed, timestep), so the seed and the timestep take their place
+        const int64_t counts[2] = {(int64_t)in_.params.seed, timestep()};
+        f.put_i64(g + "generated_counts", {2}, counts);
+        f.put_f64(g + "injection_carry", {6}, carry.data() + 6 * s);
+    }
+    const uint64_t dims[3] = {(uint64_t)in_.params.nx + 2, (uint64_t)in_.params.ny + 2, (uint64_t)in_.params.nz + 2};
+    const std::vector<uint64_t> shape(dims, dims + 3);
+    f.put_f64("Potential/phi", shape, getField(FOPIS_FIELD_PHI).data());
+    // nodal E (the reference stores its edge E; here it follows from phi)
+    f.put_f64("Efield/exref", shape, getField(FOPIS_FIELD_EXREF).data());
+    f.put_f64("Efield/eyref", shape, getField(FOPIS_FIELD_EYREF).data());
+    f.put_f64("Efield/ezref", shape, getField(FOPIS_FIELD_EZREF).data());
+    for (size_t k = 0; k < in_.objects.size(); ++k) {
+        const int n = in_.objects[k].n_cmat();
+        std::vector<double> cm((size_t)nsp * n);
+        check(fopis_get_charge_map(ctx_, object_ids_[k], cm.data(), nsp * n));
+        f.put_f64(in_.objects[k].name + "/charge_map", {(uint64_t)nsp, (uint64_t)n}, cm.data());
+    }
+    f.save(dir + "/grid_id_0.bin");
+}
+
+void RootGrid::loadResumeData(const std::string& dir) {
+    const DataFile f = DataFile::load(dir + "/grid_id_0.bin");
+    const int nsp = in_.params.nspecies;
+    std::vector<double> carry(6 * (size_t)nsp, 0.0);
+    for (int s = 0; s < nsp; ++s) {
+        const std::string g = in_.species[s].name + "/";
+        const uint64_t n = (uint64_t)f.f64_scalar(g + "size");
+        if (n == 0) continue;
+        const char* keys[6] = {"x", "y", "z", "vx", "vy", "vz"};
+        std::vector<double> col[6];
+        for (int q = 0; q < 6; ++q) {
+            col[q] = f.f64(g + keys[q]);
+            if (col[q].size() != n) throw std::runtime_error("resume data: " + g + keys[q] + " has the wrong length");
+        }
+        std::vector<Particle> p(n);
+        for (uint64_t i = 0; i < n; ++i)
+            p[i] = Particle{col[0][i], col[1][i], col[2][i], col[3][i], col[4][i], col[5][i], s, 1};
+        loadParticles(s, p);
+        if (f.has(g + "injection_carry")) {
+            const std::vector<double> c = f.f64(g + "injection_carry");
+            if (c.size() == 6) for (int q = 0; q < 6; ++q) carry[6 * s + q] = c[q];
         }
     }
+    check(fopis_set_injection_carry(ctx_, carry.data(), 6 * nsp));
+    const std::vector<double> phi = f.f64("Potential/phi");
+    const size_t N = (size_t)(in_.params.nx + 2) * (in_.params.ny + 2) * (in_.params.nz + 2);
+    if (phi.size() != N) throw std::runtime_error("resume data: Potential/phi has the wrong size");
+    check(fopis_set_field(ctx_, FOPIS_FIELD_PHI, phi.data(), N));
+    for (size_t k = 0; k < in_.objects.size(); ++k) {
+        const int n = in_.objects[k].n_cmat();
+        const std::vector<double> cm = f.f64(in_.objects[k].name + "/charge_map");
+        if (cm.size() != (size_t)nsp * n) throw std::runtime_error("resume data: charge_map of " + in_.objects[k].name);
+        check(fopis_set_charge_map(ctx_, object_ids_[k], cm.data(), nsp * n));
+    }
+}
+
+// Grid::initializeForLoad (Grid.cpp:38-50): nodal E from the saved potential
+// (the reference reads its saved edge E), then updateRho, which with objects
+// runs the first solve and the redistribution of the restored charge map.
+void RootGrid::initializeForLoad() {
+    updateEfield();
+    check(fopis_sort_particles(ctx_));
+    updateRho();
 }
 
 void RootGrid::generateAmbientParticles() { check(fopis_generate_ambient(ctx_)); }
@@ -377,6 +453,90 @@ void plot_particle_numbers(const RootGrid& g, int timestep, const std::string& d
     put_log(file, timestep, timestep * g.input().dt, e);
 }
 }  // namespace io
+
+namespace io {
+
+std::string cmatrix_file(const std::string& resume_dir, const ObjectSpec& o) {
+    return resume_dir + "/objects/" + (o.file_name.empty() ? o.name : o.file_name) + ".bin";
+}
+
+void writeCmatrixData(const RootGrid& g, int k, const std::string& resume_dir) {
+    const ObjectSpec& o = g.input().objects[k];
+    const int n = o.n_cmat();
+    std::vector<double> C((size_t)n * n);
+    const int rc = fopis_get_capacity_matrix(g.context(), g.objectId(k), C.data(), n);
+    if (rc != FOPIS_OK) throw Error(rc, fopis_last_error(g.context()));
+    DataFile f;
+    f.put_f64("capacity_matrix", {(uint64_t)n, (uint64_t)n}, C.data());
+    f.put_f64("grid_spacing", g.input().dx);
+    f.put_f64("time_spacing", g.input().dt);
+    make_dirs(resume_dir + "/objects");
+    f.save(cmatrix_file(resume_dir, o));
+}
+
+bool loadCmatrixData(RootGrid& g, int k, const std::string& resume_dir) {
+    const ObjectSpec& o = g.input().objects[k];
+    const std::string file = cmatrix_file(resume_dir, o);
+    if (!file_exists(file)) {
+        std::cout << "[WARNING] File " << file << " does not exist." << std::endl;
+        return false;
+    }
+    DataFile f;
+    try {
+        f = DataFile::load(file);
+    } catch (const std::runtime_error& e) {
+        std::cout << "[WARNING] " << e.what() << std::endl;
+        return false;
+    }
+    if (!f.has("capacity_matrix")) {
+        std::cout << "[WARNING] Dataset capacity_matrix does not exist in the file " << file << "." << std::endl;
+        return false;
+    }
+    const int n = o.n_cmat();
+    const DataFile::Entry& e = f.get("capacity_matrix");
+    const bool valid = e.dims.size() == 2 && e.dims[0] == (uint64_t)n && e.dims[1] == (uint64_t)n &&
+                       f.f64_scalar("grid_spacing") == g.input().dx && f.f64_scalar("time_spacing") == g.input().dt;
+    if (!valid) return false;
+    const std::vector<double> C = f.f64("capacity_matrix");
+    const int rc = fopis_set_capacity_matrix(g.context(), g.objectId(k), C.data(), n);
+    if (rc != FOPIS_OK) throw Error(rc, fopis_last_error(g.context()));
+    return true;
+}
+
+}  // namespace io
+
+namespace env {
+
+void saveInfo(const Input& in, int64_t timestep, const std::string& resume_dir) {
+    make_dirs(resume_dir);
+    DataFile f;
+    f.put_f64("dx", in.dx);
+    f.put_f64("dt", in.dt);
+    f.put_i64("timestep", timestep);
+    f.save(resume_dir + "/environment.bin");
+}
+
+int64_t loadInfo(const Input& in, const std::string& resume_dir) {
+    const std::string file = resume_dir + "/environment.bin";
+    if (!file_exists(file))
+        throw std::invalid_argument("[ERROR] resume file_name " + file + " does not exist.");
+    const DataFile f = DataFile::load(file);
+    const double dx = f.f64_scalar("dx"), dt = f.f64_scalar("dt");
+    char msg[256];
+    if (dx != in.dx) {
+        std::snprintf(msg, sizeof msg, "[ERROR] dx %.17g in the resume data does not match the dx %.17g from input.json.",
+                      dx, in.dx);
+        throw std::invalid_argument(msg);
+    }
+    if (dt != in.dt) {
+        std::snprintf(msg, sizeof msg, "[ERROR] dt %.17g in the resume data does not match the dt %.17g from input.json.",
+                      dt, in.dt);
+        throw std::invalid_argument(msg);
+    }
+    return f.i64_scalar("timestep");
+}
+
+}  // namespace env
 
 }  // namespace host
 }  // namespace fopis

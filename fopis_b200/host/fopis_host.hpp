@@ -60,6 +60,7 @@ void calc_flux(double vth, double density_norm, double size, const double drift[
 // One conductor as the C ABI takes it (ObjectDataFromFile + Spacecraft::construct).
 struct ObjectSpec {
     std::string name;
+    std::string file_name;         // the .obj file's name without directories (Spacecraft::file_name)
     std::vector<int32_t> nodes;    // [n_cmat][3] glue-layout
     std::vector<int32_t> cells;    // [n_cells][3] glue-layout
     int is_potential_fixed = 0;
@@ -78,6 +79,7 @@ struct Input {
     int max_timestep = 0;
     double dx = 1.0, dt = 1.0;
     bool use_existing_capacity_matrix = false;
+    std::string job_type = "new";        // Environment.job_type: "new" or "load"
 };
 
 // Initializer::initTDPIC's parsing (src/Initializer/Initialize.cpp:158-421) for
@@ -120,11 +122,22 @@ public:
 
     void* context() const { return ctx_; }
     const Input& input() const { return in_; }
+    int objectId(int k) const { return object_ids_[k]; }
 
-    // RootGrid::initializeObjectsCmatrix (RootGridObject.cpp:77-148); with a
-    // cache directory, reuses data/cmatrix_<name>.bin when it fits
-    // (Options::use_existing_capacity_matrix) and writes it after a build.
-    void initializeObjectsCmatrix(const std::string& cache_dir = "");
+    // RootGrid::initializeObjectsCmatrix (RootGridObject.cpp:77-148): with
+    // Options::use_existing_capacity_matrix the matrix is read from
+    // <resume_dir>/objects/<file_name> (io::loadCmatrixData) when it fits,
+    // otherwise built and written there (io::writeCmatrixData).
+    void initializeObjectsCmatrix(const std::string& resume_dir = "");
+    // RootGrid::saveResumeData / loadResumeData (RootGridIO.cpp:25-50): the
+    // particles of every species, phi and E, and each object's charge map in
+    // <resume_dir>/grid_id_0.bin; Grid::initializeForLoad (Grid.cpp:38-50)
+    // rebuilds rho and the conductor state from them.
+    void saveResumeData(const std::string& resume_dir) const;
+    void loadResumeData(const std::string& resume_dir);
+    void initializeForLoad();
+    int64_t timestep() const { return stats().timestep; }   // Environment::timestep of the next step
+    void setTimestep(int64_t t);
     void generateAmbientParticles();                 // Initializer's ambient loading
     void loadParticles(int species, const std::vector<Particle>& p);
     void initialize();                               // Grid::initialize (Grid.cpp:23-36)
@@ -161,10 +174,26 @@ private:
 // IO::plotEnergy / plotObjectsData / plotValidParticleNumber (src/Misc/IO.cpp:150-300):
 // files data/energy.txt, data/object_<name>.txt, data/total_particle_number.txt.
 namespace io {
+// IO::writeCmatrixData / loadCmatrixData (src/Misc/IO.cpp:28-120): datasets
+// capacity_matrix [n][n], grid_spacing, time_spacing. A file is valid when the
+// matrix size and dx, dt match (IO.cpp:88-90); loadCmatrixData then sets the
+// object's matrix and returns true.
+std::string cmatrix_file(const std::string& resume_dir, const ObjectSpec& o);
+void writeCmatrixData(const RootGrid& g, int object, const std::string& resume_dir);
+bool loadCmatrixData(RootGrid& g, int object, const std::string& resume_dir);
 void plot_energy(const RootGrid& g, int timestep, const std::string& dir);
 void plot_objects(const RootGrid& g, int timestep, const std::string& dir);
 void plot_particle_numbers(const RootGrid& g, int timestep, const std::string& dir);
 }  // namespace io
+
+// Environment::saveInfo / loadInfo (src/Misc/Environment.cpp:379-438):
+// <resume_dir>/environment.bin holds dx, dt and the timestep of the next step;
+// loadInfo rejects a file whose dx or dt differs from input.json's
+// (std::invalid_argument, as the reference) and returns the timestep.
+namespace env {
+void saveInfo(const Input& in, int64_t timestep, const std::string& resume_dir);
+int64_t loadInfo(const Input& in, const std::string& resume_dir);
+}  // namespace env
 
 }  // namespace host
 }  // namespace fopis

@@ -1,19 +1,26 @@
 // fopis_run — the reference's main loop (src/main.cpp:16-72) on the GPU
-// library: read input.json, set up the conductors (capacity matrix built or
-// read from the cache), load the ambient plasma, initialize, then per step
-// RootGrid::mainLoop and the energy / object / particle-number logs.
+// library: read input.json, set up the conductors (capacity matrix built, or
+// read from <resume>/objects with Options.use_existing_capacity_matrix), then
+// for job_type "new" load the ambient plasma and initialize, for "load" read
+// <resume>/environment.bin and grid_id_0.bin and Grid::initializeForLoad
+// (Initialize.cpp:75-99); per step RootGrid::mainLoop and the energy / object /
+// particle-number logs; at the end Environment::saveInfo and
+// RootGrid::saveResumeData into <resume>.
 //
-//   fopis_run [input.json] [--steps N] [--out DIR] [--device D]
+//   fopis_run [input.json] [--steps N] [--out DIR] [--resume DIR] [--device D]
 //             [--guess warm|history] [--dump-params FILE]
 //
-// --dump-params writes the normalised parameters and object node lists that
-// input.json produces (no GPU work) and exits.
+// --steps N runs N steps (default: up to max_timestep, as the reference's
+// loop); --resume defaults to "resume". --dump-params writes the normalised
+// parameters and object node lists that input.json produces (no GPU work) and
+// exits.
 #include <cstdio>
 #include <cstring>
 #include <fstream>
 #include <iostream>
 #include <string>
 
+#include "datafile.hpp"
 #include "fopis_host.hpp"
 
 using namespace fopis::host;
@@ -37,7 +44,7 @@ void dump_params(const Input& in, const std::string& file) {
 }  // namespace
 
 int main(int argc, char** argv) {
-    std::string input = "input.json", out = "data", dump;
+    std::string input = "input.json", out = "data", dump, resume = "resume";
     int steps = -1, device = 0, guess = FOPIS_GUESS_WARM;
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
@@ -47,8 +54,21 @@ int main(int argc, char** argv) {
         };
         if (a == "--steps") steps = std::stoi(next());
         else if (a == "--out") out = next();
+        else if (a == "--resume") resume = next();
         else if (a == "--device") device = std::stoi(next());
         else if (a == "--dump-params") dump = next();
+        else if (a == "--datafile-echo") {
+            // reads a data file and writes its datasets to another (no GPU work): a
+            // check of the file format against other writers and readers
+            const std::string src = next(), dst = next();
+            try {
+                fopis::host::DataFile::load(src).save(dst);
+            } catch (const std::exception& e) {
+                std::fprintf(stderr, "fopis_run: %s\n", e.what());
+                return 1;
+            }
+            return 0;
+        }
         else if (a == "--guess") {
             const std::string g = next();
             guess = g == "history" ? FOPIS_GUESS_HISTORY : FOPIS_GUESS_WARM;
@@ -60,22 +80,33 @@ int main(int argc, char** argv) {
             dump_params(in, dump);
             return 0;
         }
-        if (steps < 0) steps = in.max_timestep;
         RootGrid grid(in, device);
         grid.setGuessMode(guess);
-        grid.initializeObjectsCmatrix(out);
-        grid.generateAmbientParticles();
-        grid.initialize();
-        std::cout << "===== Begin Main Loop =====" << std::endl;
-        for (int t = 1; t <= steps; ++t) {
-            grid.mainLoop();
-            io::plot_energy(grid, t, out);
-            io::plot_objects(grid, t, out);
-            io::plot_particle_numbers(grid, t, out);
+        grid.initializeObjectsCmatrix(resume);
+        int64_t first = 1;
+        if (in.job_type == "load") {
+            first = env::loadInfo(in, resume);
+            std::cout << "--  Resume Data (t = " << first << ") Loading --" << std::endl;
+            grid.setTimestep(first);
+            grid.loadResumeData(resume);
+            grid.initializeForLoad();
+        } else {
+            grid.generateAmbientParticles();
+            grid.initialize();
         }
+        const int64_t last = steps >= 0 ? first + steps - 1 : (int64_t)in.max_timestep;
+        std::cout << "===== Begin Main Loop =====" << std::endl;
+        for (int64_t t = first; t <= last; ++t) {
+            grid.mainLoop();
+            io::plot_energy(grid, (int)t, out);
+            io::plot_objects(grid, (int)t, out);
+            io::plot_particle_numbers(grid, (int)t, out);
+        }
+        env::saveInfo(in, grid.timestep(), resume);
+        grid.saveResumeData(resume);
         const fopis_stats st = grid.stats();
-        std::cout << "===== End Main Loop ===== steps " << steps << ", V-cycles in the last step " << st.vcycles_step
-                  << std::endl;
+        std::cout << "===== End Main Loop ===== steps " << (last - first + 1) << ", V-cycles in the last step "
+                  << st.vcycles_step << std::endl;
     } catch (const std::exception& e) {
         std::fprintf(stderr, "fopis_run: %s\n", e.what());
         return 1;

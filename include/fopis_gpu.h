@@ -154,7 +154,8 @@ typedef struct fopis_stats {
     int converged;               /* last solve reached the tolerance */
     double residual_last;        /* ||r||_2/||f||_2 of the last solve */
     double residual_initial;     /* same, before the first V-cycle of the last solve */
-    int64_t num_particles[FOPIS_MAX_SPECIES];   /* valid particles per species */
+    int64_t num_particles[FOPIS_MAX_SPECIES];   /* slots in use per species: the valid particles plus the
+                                                   slots of particles removed since the last sort */
     int64_t capacity[FOPIS_MAX_SPECIES];
     int64_t absorbed_step;       /* particles absorbed by conductors in the last step */
     int64_t injected_step;
@@ -170,6 +171,10 @@ typedef struct fopis_stats {
                                     (RootGridField.cpp:267-317): max over unknown nodes with a
                                     nonzero source of |L phi + rho/eps0| / |rho/eps0| (mean-free
                                     source when every axis is periodic) */
+    int64_t valid_particles[FOPIS_MAX_SPECIES];  /* valid particles after the last fused step (those the
+                                                    push kept plus the injected and emitted ones) or the
+                                                    last sort */
+    int64_t pushed_step[FOPIS_MAX_SPECIES];      /* valid particles the last fused step's push moved */
 } fopis_stats;
 
 /* ---- lifetime ----------------------------------------------------------- */
@@ -198,6 +203,8 @@ int fopis_get_object(void* ctx, int object_id, double* potential, double* charge
                      double* current_per_species);
 /* Spacecraft::charge_map [nspecies][n_cmat], normalised charge. */
 int fopis_get_charge_map(void* ctx, int object_id, double* charge_map, int n);
+/* Restores it (RootGrid::loadResumeObjectData, RootGridIO.cpp:273-280); n as above. */
+int fopis_set_charge_map(void* ctx, int object_id, const double* charge_map, int n);
 
 /* ---- particles ---------------------------------------------------------- */
 
@@ -242,6 +249,15 @@ int fopis_remove_invalid_particles(void* ctx); /* Grid::removeInvalidParticles *
 /* Ends a step driven through the phase entry points: ++Environment::timestep
  * (src/main.cpp:33), which keys the Philox draws of injection and emission. */
 int fopis_advance_timestep(void* ctx);
+/* Environment::timestep of the next step, as Environment::loadInfo restores it
+ * (src/Misc/Environment.cpp:379-420); the Philox keys of injection and emission
+ * continue from it. */
+int fopis_set_timestep(void* ctx, int64_t timestep);
+/* The fractional injection carry of RootGrid::injectParticlesFromBoundary
+ * (RootGridParticle.cpp:3-130), [nspecies][6 faces]: saved with a resume so that
+ * a continued run injects the same counts. */
+int fopis_get_injection_carry(void* ctx, double* carry, int n);
+int fopis_set_injection_carry(void* ctx, const double* carry, int n);
 
 /* ---- fields and diagnostics --------------------------------------------- */
 

@@ -22,7 +22,8 @@ def test_fopis_run_matches_python_driver(gpu_available, tmp_path):
     steps = 5
     path = write_input(tmp_path / "case", n=25, ppc=4, photo=True, steps=steps)
     out = tmp_path / "data"
-    r = subprocess.run([str(RUN), str(path), "--out", str(out)], capture_output=True, text=True, timeout=600)
+    r = subprocess.run([str(RUN), str(path), "--out", str(out), "--resume", str(tmp_path / "resume")],
+                       capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
     energy = np.loadtxt(out / "energy.txt", skiprows=1)
     obj = np.loadtxt(out / "object_Spacecraft.txt", skiprows=1)
