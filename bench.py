@@ -613,14 +613,14 @@ def main():
     traffic = None
     prof = ROOT / "profiles" / "push_kernel_cube64.md"
     if prof.exists() and args.precision == "mixed":
-        # DRAM bytes per particle of one push_tile_kernel launch, from the committed ncu summary
+        # DRAM bytes per particle of one push_brick_kernel launch, from the committed ncu summary
         m = re.search(r"\| dram_bytes_per_particle \| ([0-9.]+) \|", prof.read_text())
         if m:
             traffic = float(m.group(1)) * res["pushed"]
     line = dict(base, value=value, steps=args.steps, warmup=args.warmup, ms_per_step=res["ms"] / args.steps)
     line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                         "traffic": traffic,
-                        "kernel": ("push_tile_kernel + tail push_kernel (all species)" if args.precision == "mixed"
+                        "kernel": ("push_brick_kernel + tail push_kernel (all species)" if args.precision == "mixed"
                                    else "push_kernel<double> (all species)"),
                         "peak_kind": peak_kind,
                         "bytes_per_particle": push_bytes}
