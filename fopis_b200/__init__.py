@@ -86,6 +86,12 @@ class RootGrid:
         d.fixed_potential = o.fixed_potential
         d.initial_potential_offset = o.initial_potential_offset
         d.emit_species = o.emit_species
+        d.secondary_species = o.secondary_species
+        d.dielectric = o.dielectric
+        if o.dielectric:
+            cap = np.ascontiguousarray(o.capacitance, dtype=np.float64)
+            self._keep.append(cap)
+            d.capacitance = cap.ctypes.data_as(C.POINTER(C.c_double))
         oid = C.c_int()
         self._check(self.lib.fopis_add_object(self.h, C.byref(d), C.byref(oid)))
         self.object_ids.append(oid.value)
@@ -110,6 +116,19 @@ class RootGrid:
         cur = np.zeros(self.nspecies)
         self._check(self.lib.fopis_get_object(self.h, obj, C.byref(V), C.byref(Q), _dp(cur)))
         return V.value, Q.value, cur
+
+    def get_incidents(self) -> np.ndarray:
+        """The pending incident events as an [n, 10] array: object, species, axis,
+        remaining time, crossing point x, y, z, velocity vx, vy, vz."""
+        n = C.c_int64()
+        self._check(self.lib.fopis_get_incidents(self.h, None, 0, C.byref(n)))
+        out = np.zeros((max(n.value, 1), _abi.INCIDENT_DOUBLES))
+        self._check(self.lib.fopis_get_incidents(self.h, _dp(out), n.value, C.byref(n)))
+        return out[: n.value]
+
+    def set_incidents(self, recs: np.ndarray):
+        recs = np.ascontiguousarray(recs, dtype=np.float64).reshape(-1, _abi.INCIDENT_DOUBLES)
+        self._check(self.lib.fopis_set_incidents(self.h, _dp(recs), len(recs)))
 
     def getChargeMap(self, obj: int = 0) -> np.ndarray:
         n = len(self.cfg.objects[obj].nodes)

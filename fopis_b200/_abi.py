@@ -33,6 +33,8 @@ DEV_RHO_OVERFLOW = 0x40
 
 SPECIES_AMBIENT = 0
 SPECIES_PHOTOELECTRON = 1
+SPECIES_SECONDARY = 2
+INCIDENT_DOUBLES = 10
 MIXED = 0
 FP64 = 1
 GUESS_ZERO = 0
@@ -84,6 +86,7 @@ class Params(C.Structure):
         ("precision", C.c_int),
         ("reserved0", C.c_int),
         ("seed", C.c_uint64),
+        ("energy_ev", C.c_double),
     ]
 
 
@@ -97,6 +100,9 @@ class ObjectDesc(C.Structure):
         ("fixed_potential", C.c_double),
         ("initial_potential_offset", C.c_double),
         ("emit_species", C.c_int),
+        ("secondary_species", C.c_int),
+        ("dielectric", C.c_int),
+        ("capacitance", C.POINTER(C.c_double)),
     ]
 
 
@@ -179,6 +185,10 @@ SIGNATURES = {
     "fopis_free": (None, [_VP]),
     "fopis_check_bounded_wait": (C.c_int, [C.c_int, C.c_uint32, C.c_int, C.POINTER(C.c_uint32)]),
     "fopis_efield_energy_noalloc": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, C.c_double, _VP, _VP]),
+    "fopis_get_incidents": (C.c_int, [_VP, _DP, C.c_int64, C.POINTER(C.c_int64)]),
+    "fopis_set_incidents": (C.c_int, [_VP, _DP, C.c_int64]),
+    "fopis_parse_obj_textures": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.POINTER(C.c_int32)),
+                                           C.POINTER(C.POINTER(C.c_int32)), C.POINTER(C.c_int)]),
 }
 
 LIB_PATH = Path(__file__).resolve().parent / "libfopis_gpu.so"

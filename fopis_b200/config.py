@@ -96,7 +96,7 @@ def calc_flux(vth: float, density_norm: float, size: float, drift: Sequence[floa
 @dataclass
 class SpeciesInfo:
     name: str
-    kind: str                 # "ambient" | "photoelectron"
+    kind: str                 # "ambient" | "photoelectron" | "secondary"
     mass: float               # in m_e
     charge: float             # in e
     density: float            # m^-3
@@ -117,6 +117,9 @@ class ObjectInfo:
     initial_potential_offset: float = 0.0
     emit_species: int = -1
     file_name: str = ""              # the .obj file's name without directories (capacity-matrix cache name)
+    secondary_species: int = -1      # secondary-electron species this body emits
+    dielectric: int = 0              # surface_type "dielectric"
+    capacitance: Optional[np.ndarray] = None   # [n_cmat] normalised node capacitance (dielectric)
 
 
 @dataclass
@@ -134,7 +137,8 @@ class SimConfig:
 
 def _species_struct(sp: SpeciesInfo, norm: Normalizer, dx: float) -> _abi.Species:
     s = _abi.Species()
-    s.kind = _abi.SPECIES_AMBIENT if sp.kind == "ambient" else _abi.SPECIES_PHOTOELECTRON
+    s.kind = {"ambient": _abi.SPECIES_AMBIENT, "photoelectron": _abi.SPECIES_PHOTOELECTRON,
+              "secondary": _abi.SPECIES_SECONDARY}[sp.kind]
     s.particle_per_cell = int(sp.ppc)
     s.charge = float(sp.charge)
     s.mass = float(sp.mass)
@@ -151,7 +155,7 @@ def _species_struct(sp: SpeciesInfo, norm: Normalizer, dx: float) -> _abi.Specie
         fl = calc_flux(s.thermal_velocity, dens_norm, s.size, list(s.drift), list(s.injection_axis))
         for a in range(6):
             s.flux[a] = fl[a]
-    else:
+    elif sp.kind == "photoelectron":
         j = norm.current_density(sp.current_density)
         s.emission_amount = 1.0 * j / (abs(sp.charge) * s.size)   # area dx^2 = 1 (Spacecraft.cpp:876-877)
     return s
@@ -169,8 +173,8 @@ def make_params(nxyz: Tuple[int, int, int], boundary: str, dx: float, dt: float,
     for a in range(3):
         p.static_bfield[a] = bfield_nT[a] * norm.bfield(1.0) * 1e-9
         p.shine_vector[a] = float(shine[a])
-    # Environment::resetParticleTypeOrder: ambient first, then photoelectrons
-    ordered = [s for s in species if s.kind == "ambient"] + [s for s in species if s.kind == "photoelectron"]
+    # Environment::resetParticleTypeOrder (Environment.cpp:360-377): ambient, photoelectron, secondary
+    ordered = [s for k in ("ambient", "photoelectron", "secondary") for s in species if s.kind == k]
     species[:] = ordered
     p.nspecies = len(species)
     for i, sp in enumerate(species):
@@ -183,6 +187,7 @@ def make_params(nxyz: Tuple[int, int, int], boundary: str, dx: float, dt: float,
     p.capacity_factor = capacity_factor
     p.precision = precision
     p.seed = seed
+    p.energy_ev = norm.unenergy(1.0) / E                       # Normalizer::unnormalizeEnergy(1, "eV")
     return p, norm
 
 
@@ -201,6 +206,47 @@ def parse_obj(path: str, nx: int, ny: int, nz: int) -> Tuple[np.ndarray, np.ndar
     lib.fopis_free(C.cast(nodes, C.c_void_p))
     lib.fopis_free(C.cast(cells, C.c_void_p))
     return a.astype(np.int32), b.astype(np.int32)
+
+
+def parse_obj_textures(path: str, nx: int, ny: int, nz: int) -> List[List[int]]:
+    """fopis_parse_obj_textures: per surface node (cmat order) the texture index of
+    every quad covering it (ObjectDataFromFile::textures, ObjectUtils.cpp:65-160)."""
+    lib = _abi.library()
+    start = C.POINTER(C.c_int32)()
+    tex = C.POINTER(C.c_int32)()
+    n = C.c_int()
+    rc = lib.fopis_parse_obj_textures(str(path).encode(), nx, ny, nz, C.byref(start), C.byref(tex), C.byref(n))
+    if rc != 0:
+        raise _abi.FopisError(rc, f"cannot parse {path}")
+    st = np.ctypeslib.as_array(start, shape=(n.value + 1,)).copy()
+    tx = np.ctypeslib.as_array(tex, shape=(max(int(st[-1]), 1),))[: int(st[-1])].copy()
+    lib.fopis_free(C.cast(start, C.c_void_p))
+    lib.fopis_free(C.cast(tex, C.c_void_p))
+    return [list(map(int, tx[st[m]:st[m + 1]])) for m in range(n.value)]
+
+
+# Spacecraft::material_property_list (SpacecraftMaterialPropertyList.cpp:3-34).
+RELATIVE_PERMITTIVITY = {"Silicon": 12.0, "Aluminum": 9.5, "EpoxyGlass": 5.0, "Bakelite": 4.8,
+                         "GlassReinforcedTeflon": 2.32, "Teflon": 2.1}
+
+
+def node_capacitance(textures: List[List[int]], materials: dict, norm: Normalizer) -> np.ndarray:
+    """Spacecraft::construct's dielectric capacitance map (Spacecraft.cpp:117-149): per
+    node the mean over its quads of normalizeCapacitance(4 pi eps0 eps_r) of the quad's
+    material (texture index -> material name)."""
+    per_tex = {}
+    out = np.zeros(len(textures))
+    for m, tl in enumerate(textures):
+        acc = 0.0
+        for t in tl:
+            if t not in per_tex:
+                name = materials.get(t)
+                if name not in RELATIVE_PERMITTIVITY:
+                    raise ValueError(f"Invalid material name {name} is specified to be assigned the texture index {t}.")
+                per_tex[t] = 4.0 * math.pi * EPS0 * RELATIVE_PERMITTIVITY[name] * norm.V_unit / norm.e
+            acc += per_tex[t]
+        out[m] = acc / len(tl)
+    return out
 
 
 def box_obj_text(boxes: Sequence[Tuple[Tuple[int, int, int], Tuple[int, int, int]]]) -> str:
@@ -337,7 +383,7 @@ def load_input(path: str) -> SimConfig:
     for name in sorted(js["Plasma"]):                 # picojson objects are std::map (sorted keys)
         pl = js["Plasma"][name]
         kind = pl["type"]
-        if kind not in ("ambient", "photoelectron"):
+        if kind not in ("ambient", "photoelectron", "secondary"):
             raise ValueError(f"species type {kind} is outside the ES hot path")
         species.append(SpeciesInfo(name, kind, float(pl["mass"]), float(pl["charge"]), float(pl["density"]),
                                    float(pl["temperature"]), int(pl["particle_per_cell"]),
@@ -353,20 +399,28 @@ def load_input(path: str) -> SimConfig:
     names = [s.name for s in species]
     for oname in sorted(js.get("Object", {})):
         o = js["Object"][oname]
-        if o.get("surface_type", "perfect") != "perfect":
-            raise ValueError("only perfect conductors are on the ES hot path")
+        surface = o.get("surface_type", "perfect")
+        if surface not in ("perfect", "dielectric"):
+            raise ValueError(f"surface_type {surface} is not perfect or dielectric")
         fpath = o["file_name"]
         if not os.path.isabs(fpath):
             fpath = str(base / fpath)
         nodes, cells = parse_obj(fpath, *nxyz)
-        emit = -1
+        emit, second = -1, -1
         for pname in o.get("emit_particles", {}):
             if pname in names and species[names.index(pname)].kind == "photoelectron":
                 emit = names.index(pname)
+            if pname in names and species[names.index(pname)].kind == "secondary":
+                second = names.index(pname)
+        cap = None
+        if surface == "dielectric":
+            mats = {int(k): v for k, v in o.get("materials", {}).items()}
+            cap = node_capacitance(parse_obj_textures(fpath, *nxyz), mats, norm)
         objs.append(ObjectInfo(oname, nodes, cells, int(o.get("is_potential_fixed", False)),
                                norm.potential(float(o.get("fixed_potential", 0.0))),
                                norm.potential(float(o.get("initial_potential_offset", 0.0))), emit,
-                               file_name=os.path.basename(o["file_name"])))
+                               file_name=os.path.basename(o["file_name"]), secondary_species=second,
+                               dielectric=int(surface == "dielectric"), capacitance=cap))
     return SimConfig(params=p, norm=norm, species=species, objects=objs, max_timestep=int(env.get("max_timestep", 0)),
                      dx=dx, dt=dt, use_existing_capacity_matrix=bool(opts.get("use_existing_capacity_matrix", False)),
                      maximum_poisson_post_loop=int(opts.get("maximum_poisson_post_loop", 1000)))

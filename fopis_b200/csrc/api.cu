@@ -343,6 +343,12 @@ void fopis_destroy(void* h) {
     for (auto& o : c->objs) {
         cudaFree(o.nodes); cudaFree(o.C); cudaFree(o.colsum); cudaFree(o.charge_tmp);
         cudaFree(o.charge_map); cudaFree(o.phis); cudaFree(o.scal); cudaFree(o.lit); cudaFree(o.drho_buf);
+        if (o.capacitance) cudaFree(o.capacitance);
+    }
+    {
+        void* inc[] = {c->inc.x, c->inc.y, c->inc.z, c->inc.vx, c->inc.vy, c->inc.vz, c->inc.trem, c->inc.species,
+                       c->inc.object, c->inc.axis, c->inc.count};
+        for (void* q : inc) if (q) cudaFree(q);
     }
     mg_free(*c);
     void* ptrs[] = {c->rho_i64, c->rho0, c->phi, c->phi_prev, c->phi_prev2, c->phi_obj, c->phi_obj2, c->scratch64, c->E, c->E64, c->cellmap,
@@ -421,6 +427,64 @@ int fopis_set_charge_map(void* h, int id, const double* in, int n) {
     return guarded(h, [&](Ctx& c) -> int {
         if (id < 0 || id >= (int)c.objs.size() || !in || n != c.nsp * c.objs[id].n) throw ApiError{FOPIS_ERR_ARG, "object id or size"};
         FOPIS_CUDA(cudaMemcpy(c.objs[id].charge_map, in, sizeof(double) * n, cudaMemcpyHostToDevice));
+        return FOPIS_OK;
+    });
+}
+
+// Incident records: object, species, axis, remaining time, x, y, z, vx, vy, vz.
+int fopis_get_incidents(void* h, double* out, int64_t cap, int64_t* n_out) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (!n_out || cap < 0 || (cap > 0 && !out)) throw ApiError{FOPIS_ERR_ARG, "null output"};
+        sync_scalars(c);
+        const int64_t n = c.inc.cap ? (int64_t)std::min<unsigned long long>(c.h_sc->incident_n, (unsigned long long)c.inc.cap) : 0;
+        *n_out = n;
+        const int64_t m = std::min(n, cap);
+        if (m == 0) return FOPIS_OK;
+        std::vector<double> col[7];
+        const double* src[7] = {c.inc.trem, c.inc.x, c.inc.y, c.inc.z, c.inc.vx, c.inc.vy, c.inc.vz};
+        for (int q = 0; q < 7; ++q) {
+            col[q].resize(m);
+            FOPIS_CUDA(cudaMemcpy(col[q].data(), src[q], sizeof(double) * m, cudaMemcpyDeviceToHost));
+        }
+        std::vector<uint8_t> ob(m), sp(m), ax(m);
+        FOPIS_CUDA(cudaMemcpy(ob.data(), c.inc.object, m, cudaMemcpyDeviceToHost));
+        FOPIS_CUDA(cudaMemcpy(sp.data(), c.inc.species, m, cudaMemcpyDeviceToHost));
+        FOPIS_CUDA(cudaMemcpy(ax.data(), c.inc.axis, m, cudaMemcpyDeviceToHost));
+        for (int64_t t = 0; t < m; ++t) {
+            double* r = out + FOPIS_INCIDENT_DOUBLES * t;
+            r[0] = ob[t]; r[1] = sp[t]; r[2] = ax[t];
+            for (int q = 0; q < 7; ++q) r[3 + q] = col[q][t];
+        }
+        return FOPIS_OK;
+    });
+}
+
+int fopis_set_incidents(void* h, const double* in, int64_t n) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (n < 0 || (n > 0 && !in)) throw ApiError{FOPIS_ERR_ARG, "null input"};
+        if (c.inc.cap == 0) throw ApiError{FOPIS_ERR_STATE, "no object emits secondaries"};
+        if (n > c.inc.cap) throw ApiError{FOPIS_ERR_CAPACITY, "more incidents than the absorbed-list capacity"};
+        std::vector<double> col[7];
+        std::vector<uint8_t> ob(n), sp(n), ax(n);
+        for (int q = 0; q < 7; ++q) col[q].resize(n);
+        for (int64_t t = 0; t < n; ++t) {
+            const double* r = in + FOPIS_INCIDENT_DOUBLES * t;
+            const int o = (int)r[0], s = (int)r[1], a = (int)r[2];
+            if (o < 0 || o >= (int)c.objs.size() || s < 0 || s >= c.nsp || a < 0 || a > 2)
+                throw ApiError{FOPIS_ERR_ARG, "incident object, species or axis out of range"};
+            ob[t] = (uint8_t)o; sp[t] = (uint8_t)s; ax[t] = (uint8_t)a;
+            for (int q = 0; q < 7; ++q) col[q][t] = r[3 + q];
+        }
+        double* dst[7] = {c.inc.trem, c.inc.x, c.inc.y, c.inc.z, c.inc.vx, c.inc.vy, c.inc.vz};
+        if (n > 0) {
+            for (int q = 0; q < 7; ++q)
+                FOPIS_CUDA(cudaMemcpy(dst[q], col[q].data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+            FOPIS_CUDA(cudaMemcpy(c.inc.object, ob.data(), n, cudaMemcpyHostToDevice));
+            FOPIS_CUDA(cudaMemcpy(c.inc.species, sp.data(), n, cudaMemcpyHostToDevice));
+            FOPIS_CUDA(cudaMemcpy(c.inc.axis, ax.data(), n, cudaMemcpyHostToDevice));
+        }
+        const unsigned long long nn = (unsigned long long)n;
+        FOPIS_CUDA(cudaMemcpy(&c.d_sc->incident_n, &nn, sizeof(nn), cudaMemcpyHostToDevice));
         return FOPIS_OK;
     });
 }

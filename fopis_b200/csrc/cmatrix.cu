@@ -112,11 +112,21 @@ __global__ void sum_charge_kernel(long long* tmp, double* map, int nsp, int n, c
 }
 
 // V of the perfect conductor into scal[0]; scal[2] = sum_j colsum_j phi_j.
+// On a dielectric surface (Spacecraft::redistributeChargeForDielectric,
+// Spacecraft.cpp:641-706) every node with a capacitance sees phi_j - Q_j / c_j,
+// Q_j its accumulated charge over the species: the same formulas then give V
+// and delta rho, so phis holds that effective potential.
 __global__ void potential_kernel(const double* phi, const int32_t* nodes, const double* colsum, int n, double total,
-                                 int fixed, double fixedV, double* phis, double* scal) {
+                                 int fixed, double fixedV, double* phis, double* scal, const double* cap,
+                                 const double* charge_map, int nsp) {
     double s = 0.0;
     for (int j = threadIdx.x; j < n; j += blockDim.x) {
-        const double p = phi[nodes[j]];
+        double p = phi[nodes[j]];
+        if (cap && cap[j] > 0.0) {
+            double q = 0.0;
+            for (int sp = 0; sp < nsp; ++sp) q += charge_map[(long long)sp * n + j];
+            p -= q / cap[j];
+        }
         phis[j] = p;
         s += colsum[j] * p;
     }
@@ -267,6 +277,28 @@ void object_upload(Ctx& c, ObjectDev& o, const fopis_object_desc* d, int id) {
     o.fixed_potential = d->fixed_potential;
     o.offset = d->initial_potential_offset;
     o.emit_species = d->emit_species;
+    o.secondary_species = -1;
+    if (d->secondary_species >= 0) {
+        if (d->secondary_species >= c.nsp || c.p.species[d->secondary_species].kind != FOPIS_SPECIES_SECONDARY)
+            throw ApiError{FOPIS_ERR_ARG, "secondary_species must name a species of kind FOPIS_SPECIES_SECONDARY"};
+        if (!(c.p.energy_ev > 0.0)) throw ApiError{FOPIS_ERR_ARG, "secondary emission needs params.energy_ev"};
+        o.secondary_species = d->secondary_species;
+        if (c.inc.cap == 0) {   // one incident list per context, as long as the absorbed list
+            c.inc.cap = c.ab.cap;
+            double** fl[7] = {&c.inc.x, &c.inc.y, &c.inc.z, &c.inc.vx, &c.inc.vy, &c.inc.vz, &c.inc.trem};
+            for (auto* q : fl) FOPIS_CUDA(cudaMalloc(q, sizeof(double) * c.inc.cap));
+            FOPIS_CUDA(cudaMalloc(&c.inc.species, c.inc.cap));
+            FOPIS_CUDA(cudaMalloc(&c.inc.object, c.inc.cap));
+            FOPIS_CUDA(cudaMalloc(&c.inc.axis, c.inc.cap));
+            FOPIS_CUDA(cudaMalloc(&c.inc.count, sizeof(int32_t) * c.inc.cap));
+        }
+    }
+    o.dielectric = d->dielectric ? 1 : 0;
+    if (o.dielectric) {
+        if (!d->capacitance) throw ApiError{FOPIS_ERR_ARG, "a dielectric surface needs its node capacitances"};
+        FOPIS_CUDA(cudaMalloc(&o.capacitance, sizeof(double) * o.n));
+        FOPIS_CUDA(cudaMemcpy(o.capacitance, d->capacitance, sizeof(double) * o.n, cudaMemcpyHostToDevice));
+    }
     // lit nodes of the emitting face (Spacecraft::emitParticles, Spacecraft.cpp:836-886)
     std::vector<int32_t> lit, lit_ijk;
     if (o.emit_species >= 0 && o.emit_species < c.nsp &&
@@ -386,7 +418,8 @@ void redistribute(Ctx& c) {
         if (!o.has_C) throw ApiError{FOPIS_ERR_STATE, "capacity matrix not built"};
         ++c.launches;
         potential_kernel<<<1, 1024, 0, c.st>>>(c.phi, o.nodes, o.colsum, o.n, o.total, o.is_fixed, o.fixed_potential,
-                                                o.phis, o.scal);
+                                                o.phis, o.scal, o.dielectric ? o.capacitance : nullptr, o.charge_map,
+                                                c.nsp);
         ++c.launches;
         drho_kernel<<<grid1((long long)o.n * 32), kT, 0, c.st>>>(o.C, o.n, o.phis, o.scal, o.nodes, c.rho0, o.drho[0]);
         FOPIS_LAUNCH_CHECK();

@@ -56,7 +56,7 @@ constexpr double kSurfaceUnit = 0x1p-40;
 // ------------------------------------------------------------------ Philox
 // Philox4x32-10 (Salmon et al., SC'11). Identical keying to the oracle so the
 // GPU and CPU draw the same particle sets.
-enum : uint32_t { TAG_LOAD = 1u, TAG_INJECT = 2u, TAG_EMIT = 3u };
+enum : uint32_t { TAG_LOAD = 1u, TAG_INJECT = 2u, TAG_EMIT = 3u, TAG_SECONDARY = 4u };
 
 __host__ __device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
 #pragma unroll
@@ -117,6 +117,8 @@ struct DevScalars {
     // per species in the current fused step: valid particles the push moved, those that
     // stayed valid (in the domain, not absorbed), and particles injected or emitted
     unsigned long long pushed[FOPIS_MAX_SPECIES], survived[FOPIS_MAX_SPECIES], added[FOPIS_MAX_SPECIES];
+    unsigned long long incident_n;                      // entries in the incident list
+    unsigned long long secondary_n;                     // secondaries the pending incidents will emit
     double energy[FOPIS_MAX_SPECIES];                   // sum of v^2 of live particles
     double red[16];                                     // scratch reduction slots
 };
@@ -128,6 +130,18 @@ struct AbsorbList {
     double *ox = nullptr, *oy = nullptr, *oz = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;
     uint8_t* species = nullptr;
     uint8_t* object = nullptr;
+    int64_t cap = 0;
+};
+
+// Incident events of Spacecraft::addIncidentEvent (SecondaryEmission.cpp:14-33):
+// recorded by absorb_kernel for objects that emit secondaries, consumed by the
+// next step's emission.
+struct IncidentList {
+    double *x = nullptr, *y = nullptr, *z = nullptr;      // crossing point
+    double *vx = nullptr, *vy = nullptr, *vz = nullptr;   // incident velocity
+    double* trem = nullptr;                               // remaining time (move ratio since the crossing)
+    uint8_t *species = nullptr, *object = nullptr, *axis = nullptr;
+    int32_t* count = nullptr;                             // secondaries per incident (count pass)
     int64_t cap = 0;
 };
 
@@ -147,6 +161,9 @@ struct ObjectDev {
     int is_fixed = 0;
     double fixed_potential = 0.0, offset = 0.0;
     int emit_species = -1;
+    int secondary_species = -1;        // SecondaryParticleType emitted by this body, -1 = none
+    int dielectric = 0;                // surface_type "dielectric"
+    double* capacitance = nullptr;     // [n] node capacitance (dielectric)
     int n_lit = 0;
     int32_t* lit = nullptr;            // cmat numbers of the lit nodes
     bool has_C = false;
@@ -205,6 +222,7 @@ struct Ctx {
     int32_t* scan_partials = nullptr;
     // absorbed list
     AbsorbList ab;
+    IncidentList inc;
     // multigrid
     std::vector<MGLevel> mg;
     double* coarse64 = nullptr;
@@ -262,6 +280,7 @@ void launch_deposit_all(Ctx& c);
 void launch_emit(Ctx& c, bool fused);
 void launch_inject(Ctx& c, bool fused);
 void launch_absorb(Ctx& c);
+void launch_secondary(Ctx& c, bool fused);   // emission of the pending incidents' secondaries
 void launch_energy(Ctx& c);
 void sync_scalars(Ctx& c);
 // fields.cu

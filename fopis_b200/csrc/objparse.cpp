@@ -30,7 +30,8 @@ struct Dom {
     size_t size() const { return (size_t)n[0] * n[1] * n[2]; }
 };
 
-bool read_obj(const char* path, int shift[3], std::vector<std::array<int, 3>>& v, std::vector<std::array<int, 4>>& f) {
+bool read_obj(const char* path, int shift[3], std::vector<std::array<int, 3>>& v, std::vector<std::array<int, 4>>& f,
+              std::vector<int>* tex = nullptr) {
     std::ifstream in(path);
     if (!in) return false;
     std::string line;
@@ -43,12 +44,18 @@ bool read_obj(const char* path, int shift[3], std::vector<std::array<int, 3>>& v
             v.push_back(p);
         } else if (line[0] == 'f') {
             std::array<int, 4> q{};
+            int vt = 0;
             for (int t = 0; t < 4; ++t) {
                 std::string tok;
                 ss >> tok;
                 q[t] = std::atoi(tok.c_str());   // stops at the first '/'
+                if (t == 0) {
+                    const size_t slash = tok.find('/');
+                    if (slash != std::string::npos) vt = std::atoi(tok.c_str() + slash + 1);
+                }
             }
             f.push_back(q);
+            if (tex) tex->push_back(vt);
         }
     }
     return true;
@@ -130,5 +137,63 @@ extern "C" int fopis_parse_obj(const char* path, int nx, int ny, int nz, int32_t
     if (!*cmat_nodes || !*cells) return FOPIS_ERR_NOMEM;
     std::memcpy(*cmat_nodes, nodes.data(), sizeof(int32_t) * nodes.size());
     std::memcpy(*cells, inner.data(), sizeof(int32_t) * inner.size());
+    return FOPIS_OK;
+}
+
+// Per-node texture lists in the cmat order of fopis_parse_obj: the same quad
+// walk, each covered node appending the quad's texture index.
+extern "C" int fopis_parse_obj_textures(const char* path, int nx, int ny, int nz, int32_t** start, int32_t** tex,
+                                        int* n_cmat) {
+    if (!path || !start || !tex || !n_cmat || nx < 2 || ny < 2 || nz < 2) return FOPIS_ERR_ARG;
+    Dom d{{nx, ny, nz}};
+    int shift[3] = {nx / 2, ny / 2, nz / 2};
+    std::vector<std::array<int, 3>> verts;
+    std::vector<std::array<int, 4>> faces;
+    std::vector<int> ftex;
+    if (!read_obj(path, shift, verts, faces, &ftex)) return FOPIS_ERR_ARG;
+    std::vector<int32_t> node_id(d.size(), -1);
+    std::vector<std::vector<int32_t>> lists;
+    for (size_t fi = 0; fi < faces.size(); ++fi) {
+        const auto& q = faces[fi];
+        std::array<int, 3> p[4];
+        for (int t = 0; t < 4; ++t) {
+            if (q[t] < 1 || q[t] > (int)verts.size()) return FOPIS_ERR_ARG;
+            p[t] = verts[q[t] - 1];
+        }
+        int normal = -1;
+        for (int a = 0; a < 3 && normal < 0; ++a)
+            if (p[0][a] == p[1][a] && p[0][a] == p[2][a] && p[0][a] == p[3][a]) normal = a;
+        if (normal < 0) return FOPIS_ERR_ARG;
+        const int u = normal == 0 ? 1 : 0, w = normal == 2 ? 1 : 2;
+        int lo_u = p[0][u], hi_u = p[0][u], lo_w = p[0][w], hi_w = p[0][w];
+        for (int t = 1; t < 4; ++t) {
+            lo_u = std::min(lo_u, p[t][u]); hi_u = std::max(hi_u, p[t][u]);
+            lo_w = std::min(lo_w, p[t][w]); hi_w = std::max(hi_w, p[t][w]);
+        }
+        for (int a = lo_u; a <= hi_u; ++a)
+            for (int b = lo_w; b <= hi_w; ++b) {
+                int c[3];
+                c[normal] = p[0][normal]; c[u] = a; c[w] = b;
+                if (c[0] < 0 || c[1] < 0 || c[2] < 0 || c[0] >= nx || c[1] >= ny || c[2] >= nz) return FOPIS_ERR_ARG;
+                const size_t id = d.at(c[0], c[1], c[2]);
+                if (node_id[id] < 0) {
+                    node_id[id] = (int32_t)lists.size();
+                    lists.emplace_back();
+                }
+                lists[node_id[id]].push_back(ftex[fi]);
+            }
+    }
+    size_t total = 0;
+    for (const auto& l : lists) total += l.size();
+    *n_cmat = (int)lists.size();
+    *start = (int32_t*)std::malloc(sizeof(int32_t) * (lists.size() + 1));
+    *tex = (int32_t*)std::malloc(sizeof(int32_t) * std::max<size_t>(1, total));
+    if (!*start || !*tex) return FOPIS_ERR_NOMEM;
+    size_t at = 0;
+    for (size_t m = 0; m < lists.size(); ++m) {
+        (*start)[m] = (int32_t)at;
+        for (int32_t t : lists[m]) (*tex)[at++] = t;
+    }
+    (*start)[lists.size()] = (int32_t)at;
     return FOPIS_OK;
 }

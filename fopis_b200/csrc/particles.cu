@@ -931,6 +931,8 @@ struct AbsorbArgs {
     const int32_t* node_cmat;
     long long* charge_tmp[FOPIS_MAX_OBJECTS];
     int n_cmat[FOPIS_MAX_OBJECTS];
+    int secondary[FOPIS_MAX_OBJECTS];   // the body emits secondaries: record its hits
+    IncidentList inc;
     DevScalars* sc;
 };
 
@@ -978,10 +980,67 @@ __device__ __forceinline__ double move_ratio(double d1, double v) {
     return v > 0.0 ? d1 / fabs(v) : (1.0 - d1) / fabs(v);
 }
 
-// Absorbed particle: Particle::computeCrossPoints (particle.cpp:82-204, with the
-// xz-case comparison `mvx <= mvx` that always puts x first) and the first
-// crossing that is a body face (Spacecraft::distributeInnerParticleCharge,
-// Spacecraft.cpp:556-591).
+// Particle::computeCrossPoints (particle.cpp:82-204, with the xz-case
+// comparison `mvx <= mvx` that always puts x first) for the particle at
+// (x, y, z) that moved by v this step, and the first crossing that is a body
+// face whose axis is not `skip` (Spacecraft::distributeInnerParticleCharge,
+// Spacecraft.cpp:556-591; distributeInnerParticleChargeForSecondary skips the
+// axis it was emitted from, SecondaryEmission.cpp:35-110). Returns the face
+// axis (-1: none) with the crossing as a position and as coordinates.
+__device__ int find_body_face(const AbsorbArgs& a, int obj, double x, double y, double z, double vx, double vy,
+                              double vz, int skip, DPos& hit, double hitc[3]) {
+    DPos pos, old;
+    pos.set(x, y, z);
+    old.set(x - vx, y - vy, z - vz);
+    const double ox_[3] = {x - vx, y - vy, z - vz};
+    const double v[3] = {vx, vy, vz};
+    const double mv[3] = {1.0 - move_ratio(pos.d1[0], vx), 1.0 - move_ratio(pos.d1[1], vy), 1.0 - move_ratio(pos.d1[2], vz)};
+    const bool mvd[3] = {pos.i != old.i, pos.j != old.j, pos.k != old.k};
+    int order[3], cnt = 0;
+    const int count = (int)mvd[0] + (int)mvd[1] + (int)mvd[2];
+    const double mvx = mv[0], mvy = mv[1], mvz = mv[2];
+    if (count == 3) {
+        if (mvx <= mvy) {
+            if (mvx <= mvz) { order[0] = 0; if (mvy <= mvz) { order[1] = 1; order[2] = 2; } else { order[1] = 2; order[2] = 1; } }
+            else { order[0] = 2; order[1] = 0; order[2] = 1; }
+        } else {
+            if (mvy <= mvz) { order[0] = 1; if (mvx <= mvz) { order[1] = 0; order[2] = 2; } else { order[1] = 2; order[2] = 0; } }
+            else { order[0] = 2; order[1] = 1; order[2] = 0; }
+        }
+        cnt = 3;
+    } else if (count == 2) {
+        if (mvd[0] && mvd[1]) { if (mvx <= mvy) { order[0] = 0; order[1] = 1; } else { order[0] = 1; order[1] = 0; } }
+        else if (mvd[0]) { order[0] = 0; order[1] = 2; }
+        else { if (mvy <= mvz) { order[0] = 1; order[1] = 2; } else { order[0] = 2; order[1] = 1; } }
+        cnt = 2;
+    } else if (count == 1) {
+        order[0] = mvd[0] ? 0 : (mvd[1] ? 1 : 2);
+        cnt = 1;
+    }
+    const int sgn[3] = {vx > 0.0 ? 1 : -1, vy > 0.0 ? 1 : -1, vz > 0.0 ? 1 : -1};
+    for (int q = 0; q < cnt; ++q) {
+        const int ax0 = order[q];
+        double c[3];
+        for (int r = 0; r < 3; ++r)
+            c[r] = (r == ax0) ? (v[ax0] > 0.0 ? ceil(ox_[r]) : floor(ox_[r])) : ox_[r] + v[r] * mv[ax0];
+        DPos cp;
+        cp.set(c[0], c[1], c[2]);
+        for (int ax = 0; ax < 3; ++ax) {
+            if (ax == skip) continue;
+            if (surface_point(a, obj, cp, ax, sgn[ax])) {
+                hit = cp;
+                hitc[0] = c[0]; hitc[1] = c[1]; hitc[2] = c[2];
+                return ax;
+            }
+        }
+    }
+    return -1;
+}
+
+// Absorbed particle: the charge goes to the first body face it crossed
+// (bilinear, fixed point); for a body that emits secondaries the hit is kept
+// as an incident event (Spacecraft::addIncidentEvent with the move ratio along
+// the face axis as the remaining time, SecondaryEmission.cpp:14-33).
 __global__ void absorb_kernel(AbsorbArgs a) {
     const long long n = (long long)min(a.sc->absorbed_n, (unsigned long long)a.ab.cap);
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
@@ -990,61 +1049,211 @@ __global__ void absorb_kernel(AbsorbArgs a) {
         unpack_cell(a.ab.cell[t], ci, cj, ck);
         const double x = (ci - 1) + (double)a.ab.ox[t], y = (cj - 1) + (double)a.ab.oy[t], z = (ck - 1) + (double)a.ab.oz[t];
         const double vx = a.ab.vx[t], vy = a.ab.vy[t], vz = a.ab.vz[t];
-        DPos pos, old;
-        pos.set(x, y, z);
-        old.set(x - vx, y - vy, z - vz);
-        const double ox_[3] = {x - vx, y - vy, z - vz};
-        const double v[3] = {vx, vy, vz};
-        const double mv[3] = {1.0 - move_ratio(pos.d1[0], vx), 1.0 - move_ratio(pos.d1[1], vy), 1.0 - move_ratio(pos.d1[2], vz)};
-        const bool mvd[3] = {pos.i != old.i, pos.j != old.j, pos.k != old.k};
-        DPos cps[3];
-        auto cross = [&](int ax) {
-            double c[3];
-            for (int q = 0; q < 3; ++q)
-                c[q] = (q == ax) ? (v[ax] > 0.0 ? ceil(ox_[q]) : floor(ox_[q])) : ox_[q] + v[q] * mv[ax];
-            DPos r;
-            r.set(c[0], c[1], c[2]);
-            return r;
-        };
-        int order[3], cnt = 0;
-        const int count = (int)mvd[0] + (int)mvd[1] + (int)mvd[2];
-        const double mvx = mv[0], mvy = mv[1], mvz = mv[2];
-        if (count == 3) {
-            if (mvx <= mvy) {
-                if (mvx <= mvz) { order[0] = 0; if (mvy <= mvz) { order[1] = 1; order[2] = 2; } else { order[1] = 2; order[2] = 1; } }
-                else { order[0] = 2; order[1] = 0; order[2] = 1; }
-            } else {
-                if (mvy <= mvz) { order[0] = 1; if (mvx <= mvz) { order[1] = 0; order[2] = 2; } else { order[1] = 2; order[2] = 0; } }
-                else { order[0] = 2; order[1] = 1; order[2] = 0; }
-            }
-            cnt = 3;
-        } else if (count == 2) {
-            if (mvd[0] && mvd[1]) { if (mvx <= mvy) { order[0] = 0; order[1] = 1; } else { order[0] = 1; order[1] = 0; } }
-            else if (mvd[0]) { order[0] = 0; order[1] = 2; }
-            else { if (mvy <= mvz) { order[0] = 1; order[1] = 2; } else { order[0] = 2; order[1] = 1; } }
-            cnt = 2;
-        } else if (count == 1) {
-            order[0] = mvd[0] ? 0 : (mvd[1] ? 1 : 2);
-            cnt = 1;
-        }
-        for (int q = 0; q < cnt; ++q) cps[q] = cross(order[q]);
-        const int sgn[3] = {vx > 0.0 ? 1 : -1, vy > 0.0 ? 1 : -1, vz > 0.0 ? 1 : -1};
-        bool found = false;
-        long long* tmp = a.charge_tmp[obj] + (long long)s * a.n_cmat[obj];
-        for (int q = 0; q < cnt && !found; ++q) {
-            const DPos& cp = cps[q];
-            for (int ax = 0; ax < 3 && !found; ++ax) {
-                if (surface_point(a, obj, cp, ax, sgn[ax])) {
-                    const int oa = ax == 0 ? 1 : 0, ob = ax == 2 ? 1 : 2;
-                    if (!surface_charge(a.g, a.node_cmat, obj, tmp, ax, cp.i, cp.j, cp.k, cp.d1[oa], cp.d1[ob], 1))
-                        atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_BAD_CMAT_NODE);
-                    found = true;
+        DPos cp;
+        double cc[3];
+        const int ax = find_body_face(a, obj, x, y, z, vx, vy, vz, -1, cp, cc);
+        if (ax >= 0) {
+            long long* tmp = a.charge_tmp[obj] + (long long)s * a.n_cmat[obj];
+            const int oa = ax == 0 ? 1 : 0, ob = ax == 2 ? 1 : 2;
+            if (!surface_charge(a.g, a.node_cmat, obj, tmp, ax, cp.i, cp.j, cp.k, cp.d1[oa], cp.d1[ob], 1))
+                atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_BAD_CMAT_NODE);
+            if (a.secondary[obj]) {
+                const unsigned long long slot = atomicAdd(&a.sc->incident_n, 1ull);
+                if ((long long)slot < a.inc.cap) {
+                    DPos pos;
+                    pos.set(x, y, z);
+                    const double v[3] = {vx, vy, vz};
+                    a.inc.x[slot] = cc[0]; a.inc.y[slot] = cc[1]; a.inc.z[slot] = cc[2];
+                    a.inc.vx[slot] = vx; a.inc.vy[slot] = vy; a.inc.vz[slot] = vz;
+                    a.inc.trem[slot] = move_ratio(pos.d1[ax], v[ax]);
+                    a.inc.species[slot] = (uint8_t)s;
+                    a.inc.object[slot] = (uint8_t)obj;
+                    a.inc.axis[slot] = (uint8_t)ax;
+                } else {
+                    atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_ABSORB_OVERFLOW);
                 }
             }
+        } else {
+            atomicAdd(&a.sc->not_found, 1ull);
+            atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_SURFACE_NOT_FOUND);
         }
-        if (!found) { atomicAdd(&a.sc->not_found, 1ull); atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_SURFACE_NOT_FOUND); }
         atomicAdd(&a.sc->absorbed_by[obj][s], 1ull);
     }
+}
+
+// ------------------------------------------------------------------ secondary electrons
+// Spacecraft::emitParticles' secondary branch (Spacecraft.cpp:901-937) with
+// SecondaryParticleType::generateNewParticles (SecondaryParticleType.cpp:16-51)
+// on the test material the reference hard-codes (Fermi energy 9.1 eV, delta_max
+// 3.0 at 420 eV, Z = 13). Per incident: elastic backscatter with probability r,
+// inelastic backscatter with eta, else floor(delta') + (u < frac) true
+// secondaries, delta' = delta / (1 - r - eta) (Whipple's coefficients,
+// :162-194). The draws are Philox keyed by the incident's own content (its
+// crossing point and velocity rounded to 2^-24, species, axis and object) and
+// the step, so an incident gives the same secondaries wherever it is listed,
+// and runs whose trajectories agree to far below 2^-24 draw the same ones.
+constexpr int kMaxSecondaries = 64;   // per incident; more latch FOPIS_DEV_PARTICLE_OVERFLOW
+struct SeeMaterial {
+    static constexpr double fermi = 9.1, delta_max = 3.0, eps_max = 420.0, z = 13.0;
+};
+
+__device__ inline uint64_t see_mix(uint64_t h, uint64_t w) {
+    h ^= w;
+    h *= 0x100000001B3ull;
+    h ^= h >> 29;
+    return h;
+}
+__device__ inline uint64_t incident_key(double x, double y, double z, double vx, double vy, double vz, int species,
+                                                 int axis, int object) {
+    const double d[6] = {x, y, z, vx, vy, vz};
+    uint64_t h = 0xCBF29CE484222325ull;
+    for (int q = 0; q < 6; ++q) h = see_mix(h, (uint64_t)__double2ll_rn(d[q] * 16777216.0));
+    return see_mix(h, (uint64_t)species | ((uint64_t)axis << 8) | ((uint64_t)object << 16));
+}
+
+struct SecondaryArgs {
+    IncidentList inc;
+    long long n;                           // incidents
+    int sec[FOPIS_MAX_OBJECTS];            // secondary species of each object
+    double mass[FOPIS_MAX_SPECIES], charge[FOPIS_MAX_SPECIES], vth[FOPIS_MAX_SPECIES];
+    double energy_ev;
+    uint64_t seed;
+    long long step;
+};
+
+// What one incident emits: kind (0 none, 1 elastic, 2 inelastic, 3 true) and count.
+struct SeePlan { int kind, count; };
+__device__ SeePlan see_plan(const SecondaryArgs& e, long long t, uint64_t key) {
+    const int s = e.inc.species[t], ax = e.inc.axis[t];
+    const double v[3] = {e.inc.vx[t], e.inc.vy[t], e.inc.vz[t]};
+    const double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    const double E = 0.5 * e.mass[s] * v2 * e.energy_ev;                 // IncidentInfo_t energy in eV
+    const double th = acos(fabs(v[ax]) / sqrt(v2));                       // angle from the normal
+    const double ct = cos(th);
+    using M = SeeMaterial;
+    double r = 0.0, eta = 0.0;
+    if (e.charge[s] < 0.0) {
+        const double f3 = M::fermi * M::fermi * M::fermi;
+        r = (1.0 / 13.54) * (f3 * M::fermi) / (16.0 * ((E + M::fermi) * (E + M::fermi) * (E + M::fermi) + f3));
+        const double eta1 = 1.0 - pow(2.0 / E, 0.037 * M::z);
+        const double eta2 = 0.1 * exp(-E / 5000.0);
+        double eta0 = 0.0;
+        if (E > 50.0 && E < 1000.0) eta0 = log(E / 50.0) / log(20.0);
+        else if (E > 1000.0) eta0 = 1.0;
+        eta = eta0 * (eta1 + eta2) * (7.37 * pow(M::z, -0.56875)) * (1.0 - ct);
+    }
+    const double delta = (1.114 * M::delta_max / ct) * pow(M::eps_max / E, 0.35) *
+                         (1.0 - exp(-2.28 * ct * pow(E / M::eps_max, 1.35)));
+    const U2 u = draw2(e.seed, (uint32_t)key, (uint32_t)(key >> 32), (uint32_t)e.step, TAG_SECONDARY << 24);
+    if (u.a < r) return {1, 1};
+    if (u.a < r + eta) return {2, 1};
+    const double d = delta / (1.0 - r - eta);
+    const double fl = floor(d);
+    int cnt = (int)fl + ((u.b < d - fl) ? 1 : 0);
+    return {3, cnt};
+}
+
+__device__ __forceinline__ uint64_t incident_key_at(const SecondaryArgs& e, long long t) {
+    return incident_key(e.inc.x[t], e.inc.y[t], e.inc.z[t], e.inc.vx[t], e.inc.vy[t], e.inc.vz[t], e.inc.species[t],
+                        e.inc.axis[t], e.inc.object[t]);
+}
+
+// Count pass: the secondaries of every incident, and their total.
+__global__ void see_count_kernel(SecondaryArgs e, DevScalars* sc) {
+    unsigned long long tot = 0;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < e.n; t += (long long)gridDim.x * blockDim.x) {
+        int c = 0;
+        if (e.sec[e.inc.object[t]] >= 0) c = min(see_plan(e, t, incident_key_at(e, t)).count, kMaxSecondaries);
+        e.inc.count[t] = c;
+        tot += (unsigned long long)c;
+    }
+    for (int o = 16; o; o >>= 1) tot += __shfl_xor_sync(kFull, tot, o);
+    if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&sc->secondary_n, tot);
+}
+
+// Emission pass: each secondary leaves the crossing point for the remaining
+// time with its new velocity. Outside the body its charge comes off the face
+// it left, at the next crossing of its back-dated position along the incident
+// axis (Spacecraft::subtractChargeOfParticleFrom{X,Y,Z}surface, :945-970), and
+// it is appended; inside the body it is absorbed at once on a face of another
+// axis (distributeInnerParticleChargeForSecondary). The reference records that
+// re-absorption as an incident too, in the list it is iterating and clears
+// right after, so it emits nothing here.
+template <typename T>
+__global__ void see_emit_kernel(SourceArgsT<T> a, SecondaryArgs e, AbsorbArgs b) {
+    __shared__ double s_energy[FOPIS_MAX_SPECIES];
+    energy_init(s_energy);
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < e.n; t += (long long)gridDim.x * blockDim.x) {
+        const int obj = e.inc.object[t], sec = e.sec[obj];
+        if (sec < 0) continue;
+        const uint64_t key = incident_key_at(e, t);
+        const SeePlan plan = see_plan(e, t, key);
+        if (plan.count > kMaxSecondaries) atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_PARTICLE_OVERFLOW);
+        const int n = min(plan.count, kMaxSecondaries);
+        const int s = e.inc.species[t], ax = e.inc.axis[t];
+        const double vin[3] = {e.inc.vx[t], e.inc.vy[t], e.inc.vz[t]};
+        const double cp[3] = {e.inc.x[t], e.inc.y[t], e.inc.z[t]};
+        const double trem = e.inc.trem[t];
+        double speed = e.vth[sec];                                          // true secondaries: sqrt(2 T / m)
+        if (plan.kind == 2) {
+            const U2 ue = draw2(e.seed, (uint32_t)key, (uint32_t)(key >> 32), (uint32_t)e.step, (TAG_SECONDARY << 24) | 1u);
+            const double v2 = vin[0] * vin[0] + vin[1] * vin[1] + vin[2] * vin[2];
+            speed = sqrt(2.0 * (ue.a * 0.5 * e.mass[s] * v2) / e.mass[sec]);   // uniform share of the incident energy
+        }
+        for (int m = 0; m < n; ++m) {
+            double v[3];
+            if (plan.kind == 1) {
+                v[0] = vin[0]; v[1] = vin[1]; v[2] = vin[2];
+                v[ax] = -v[ax];
+            } else {
+                const U2 ua = draw2(e.seed, (uint32_t)key, (uint32_t)(key >> 32), (uint32_t)e.step,
+                                    (TAG_SECONDARY << 24) | (uint32_t)(2 + m));
+                const double dep = asin(2.0 * ua.a - 1.0), az = 2.0 * 3.14159265358979323846 * ua.b;
+                const double sgn = vin[ax] > 0.0 ? -1.0 : 1.0;
+                const double cn = speed * cos(dep) * sgn, sa = speed * sin(dep) * cos(az), sb = speed * sin(dep) * sin(az);
+                if (ax == 0) { v[0] = cn; v[1] = sa; v[2] = sb; }
+                else if (ax == 1) { v[0] = sb; v[1] = cn; v[2] = sa; }
+                else { v[0] = sa; v[1] = sb; v[2] = cn; }
+            }
+            const double x[3] = {cp[0] + trem * v[0], cp[1] + trem * v[1], cp[2] + trem * v[2]};
+            DPos pos;
+            pos.set(x[0], x[1], x[2]);
+            long long* tmp = b.charge_tmp[obj] + (long long)sec * b.n_cmat[obj];
+            if (cell_in(b, obj, pos.i, pos.j, pos.k)) {
+                DPos hp;
+                double hc[3];
+                const int hax = find_body_face(b, obj, x[0], x[1], x[2], v[0], v[1], v[2], ax, hp, hc);
+                if (hax >= 0) {
+                    const int oa = hax == 0 ? 1 : 0, ob = hax == 2 ? 1 : 2;
+                    if (!surface_charge(b.g, b.node_cmat, obj, tmp, hax, hp.i, hp.j, hp.k, hp.d1[oa], hp.d1[ob], 1))
+                        atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_BAD_CMAT_NODE);
+                } else {
+                    atomicAdd(&a.sc->not_found, 1ull);
+                    atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_SURFACE_NOT_FOUND);
+                }
+                atomicAdd(&a.sc->absorbed_by[obj][sec], 1ull);
+                continue;
+            }
+            // Particle::getNext{X,Y,Z}CrossPoint (particle.cpp:206-255) of the position one step back
+            double o[3] = {x[0] - v[0], x[1] - v[1], x[2] - v[2]}, c[3] = {o[0], o[1], o[2]};
+            const double fo = floor(o[ax]), d1 = o[ax] - fo, d2 = 1.0 - d1;
+            if (v[ax] > 0.0) {
+                const double mv = d2 / v[ax];
+                for (int r = 0; r < 3; ++r) c[r] = (r == ax) ? ceil(o[r]) : o[r] + v[r] * mv;
+            } else if (v[ax] < 0.0) {
+                const double mv = d1 / (-v[ax]);
+                for (int r = 0; r < 3; ++r) c[r] = (r == ax) ? floor(o[r]) : o[r] + v[r] * mv;
+            }
+            DPos np;
+            np.set(c[0], c[1], c[2]);
+            const int oa = ax == 0 ? 1 : 0, ob = ax == 2 ? 1 : 2;
+            if (!surface_charge(b.g, b.node_cmat, obj, tmp, ax, np.i, np.j, np.k, np.d1[oa], np.d1[ob], -1))
+                atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_BAD_CMAT_NODE);
+            atomicAdd(&a.sc->emitted_by[obj][sec], 1ull);
+            finish_source(a, sec, x[0], x[1], x[2], v[0], v[1], v[2], true, true, s_energy);
+        }
+    }
+    energy_flush(a, s_energy);
 }
 
 // ------------------------------------------------------------------ loading
@@ -1802,6 +2011,7 @@ void launch_emit(Ctx& c, bool fused) {
         else emit_kernel<<<grid_for(add), kThreads, 0, c.st>>>(source_args<float>(c, fused), e);
         FOPIS_LAUNCH_CHECK();
     }
+    launch_secondary(c, fused);
 }
 
 static int node_size(const Ctx& c, int axis) {
@@ -1852,15 +2062,59 @@ void launch_inject(Ctx& c, bool fused) {
     FOPIS_LAUNCH_CHECK();
 }
 
-void launch_absorb(Ctx& c) {
-    if (c.objs.empty()) return;
+static AbsorbArgs absorb_args(const Ctx& c) {
     AbsorbArgs a;
     a.ab = c.ab; a.g = make_grid(c); a.cellmap = c.cellmap; a.node_cmat = c.node_cmat; a.sc = c.d_sc;
-    for (int o = 0; o < FOPIS_MAX_OBJECTS; ++o) { a.charge_tmp[o] = nullptr; a.n_cmat[o] = 0; }
-    for (size_t o = 0; o < c.objs.size(); ++o) { a.charge_tmp[o] = c.objs[o].charge_tmp; a.n_cmat[o] = c.objs[o].n; }
+    a.inc = c.inc;
+    for (int o = 0; o < FOPIS_MAX_OBJECTS; ++o) { a.charge_tmp[o] = nullptr; a.n_cmat[o] = 0; a.secondary[o] = 0; }
+    for (size_t o = 0; o < c.objs.size(); ++o) {
+        a.charge_tmp[o] = c.objs[o].charge_tmp;
+        a.n_cmat[o] = c.objs[o].n;
+        a.secondary[o] = c.objs[o].secondary_species >= 0 && c.inc.cap > 0 ? 1 : 0;
+    }
+    return a;
+}
+
+void launch_absorb(Ctx& c) {
+    if (c.objs.empty()) return;
     ++c.launches;
-    absorb_kernel<<<148 * 4, kThreads, 0, c.st>>>(a);
+    absorb_kernel<<<148 * 4, kThreads, 0, c.st>>>(absorb_args(c));
     FOPIS_LAUNCH_CHECK();
+}
+
+// The secondaries of the incidents the last absorption recorded, then the
+// list is cleared (Spacecraft::clearIncidentEvents, SecondaryEmission.cpp:31-33).
+void launch_secondary(Ctx& c, bool fused) {
+    if (c.inc.cap == 0) return;
+    sync_scalars(c);
+    const long long n = (long long)std::min<unsigned long long>(c.h_sc->incident_n, (unsigned long long)c.inc.cap);
+    if (n > 0) {
+        SecondaryArgs e;
+        e.inc = c.inc; e.n = n; e.energy_ev = c.p.energy_ev; e.seed = c.p.seed; e.step = c.timestep;
+        for (int o = 0; o < FOPIS_MAX_OBJECTS; ++o) e.sec[o] = -1;
+        for (size_t o = 0; o < c.objs.size(); ++o) e.sec[o] = c.objs[o].secondary_species;
+        for (int s = 0; s < FOPIS_MAX_SPECIES; ++s) {
+            e.mass[s] = s < c.nsp ? c.p.species[s].mass : 1.0;
+            e.charge[s] = s < c.nsp ? c.p.species[s].charge * c.p.species[s].size : 0.0;
+            e.vth[s] = s < c.nsp ? c.p.species[s].thermal_velocity : 0.0;
+        }
+        FOPIS_CUDA(cudaMemsetAsync(&c.d_sc->secondary_n, 0, sizeof(unsigned long long), c.st));
+        ++c.launches;
+        see_count_kernel<<<grid_for(n), kThreads, 0, c.st>>>(e, c.d_sc);
+        FOPIS_LAUNCH_CHECK();
+        sync_scalars(c);
+        const int64_t add = (int64_t)c.h_sc->secondary_n;
+        for (size_t o = 0; o < c.objs.size(); ++o) {
+            const int s = c.objs[o].secondary_species;
+            if (s >= 0 && c.nslots[s] + add > c.cap[s])
+                particles_alloc(c, s, (int64_t)((c.nslots[s] + add) * 1.5) + 65536);
+        }
+        ++c.launches;
+        if (c.fp64) see_emit_kernel<<<grid_for(n), kThreads, 0, c.st>>>(source_args<double>(c, fused), e, absorb_args(c));
+        else see_emit_kernel<<<grid_for(n), kThreads, 0, c.st>>>(source_args<float>(c, fused), e, absorb_args(c));
+        FOPIS_LAUNCH_CHECK();
+    }
+    FOPIS_CUDA(cudaMemsetAsync(&c.d_sc->incident_n, 0, sizeof(unsigned long long), c.st));
 }
 
 void launch_energy(Ctx& c) {

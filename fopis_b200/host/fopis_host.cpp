@@ -45,7 +45,8 @@ void calc_flux(double vth, double density_norm, double size, const double drift[
 
 fopis_species ParticleType::to_abi(const Normalizer& norm, double dx) const {
     fopis_species s{};
-    s.kind = type == "ambient" ? FOPIS_SPECIES_AMBIENT : FOPIS_SPECIES_PHOTOELECTRON;
+    s.kind = type == "ambient" ? FOPIS_SPECIES_AMBIENT
+             : type == "photoelectron" ? FOPIS_SPECIES_PHOTOELECTRON : FOPIS_SPECIES_SECONDARY;
     s.particle_per_cell = particle_per_cell;
     s.charge = charge;
     s.mass = mass;
@@ -58,7 +59,7 @@ fopis_species ParticleType::to_abi(const Normalizer& norm, double dx) const {
     if (type == "ambient") {
         const double dens_norm = density * std::pow(dx, 3.0);                         // normalizeDensity
         calc_flux(s.thermal_velocity, dens_norm, s.size, s.drift, s.injection_axis, s.flux);
-    } else {
+    } else if (type == "photoelectron") {
         const double j = norm.current_density(current_density);
         s.emission_amount = 1.0 * j / (std::fabs(charge) * s.size);                   // dx^2 = 1 (Spacecraft.cpp:876-877)
     }
@@ -82,6 +83,43 @@ void parse_obj(const std::string& path, int nx, int ny, int nz, ObjectSpec& o) {
     o.cells.assign(cells, cells + 3 * (size_t)nc);
     fopis_free(nodes);
     fopis_free(cells);
+}
+
+// Per-node texture lists of the same file (ObjectDataFromFile::textures), turned
+// into the dielectric capacitance map of Spacecraft::construct (Spacecraft.cpp:
+// 117-149): per node the mean over its quads of normalizeCapacitance(4 pi eps0
+// eps_r) of the quad's material; an unknown material name is an error there too.
+void node_capacitance(const std::string& path, int nx, int ny, int nz, const std::map<int, std::string>& materials,
+                      const Normalizer& norm, ObjectSpec& o) {
+    // Spacecraft::material_property_list (SpacecraftMaterialPropertyList.cpp:3-34)
+    static const std::map<std::string, double> eps_r = {{"Silicon", 12.0}, {"Aluminum", 9.5}, {"EpoxyGlass", 5.0},
+                                                        {"Bakelite", 4.8}, {"GlassReinforcedTeflon", 2.32},
+                                                        {"Teflon", 2.1}};
+    int32_t *start = nullptr, *tex = nullptr;
+    int n = 0;
+    const int rc = fopis_parse_obj_textures(path.c_str(), nx, ny, nz, &start, &tex, &n);
+    if (rc != FOPIS_OK) throw Error(rc, "cannot parse " + path);
+    o.capacitance.assign(n, 0.0);
+    try {
+        for (int m = 0; m < n; ++m) {
+            double acc = 0.0;
+            for (int t = start[m]; t < start[m + 1]; ++t) {
+                const auto it = materials.find(tex[t]);
+                const auto pe = it == materials.end() ? eps_r.end() : eps_r.find(it->second);
+                if (pe == eps_r.end())
+                    throw Error(FOPIS_ERR_ARG, "Invalid material name " + (it == materials.end() ? std::string("") : it->second) +
+                                                   " is specified to be assigned the texture index " + std::to_string(tex[t]) + ".");
+                acc += 4.0 * M_PI * kEps0 * pe->second * norm.V_unit / kE;   // normalizeCapacitance
+            }
+            o.capacitance[m] = acc / (start[m + 1] - start[m]);
+        }
+    } catch (...) {
+        fopis_free(start);
+        fopis_free(tex);
+        throw;
+    }
+    fopis_free(start);
+    fopis_free(tex);
 }
 
 }  // namespace
@@ -108,7 +146,7 @@ Input load_input(const std::string& path) {
         ParticleType p;
         p.name = kv.first;
         p.type = pl["type"].str();
-        if (p.type != "ambient" && p.type != "photoelectron")
+        if (p.type != "ambient" && p.type != "photoelectron" && p.type != "secondary")
             throw Error(FOPIS_ERR_ARG, "species type " + p.type + " is outside the ES hot path");
         p.mass = pl["mass"].number();
         p.charge = pl["charge"].number();
@@ -122,8 +160,9 @@ Input load_input(const std::string& path) {
         p.current_density = pl.number_or("current_density", 0.0);
         species.push_back(p);
     }
-    // Environment::resetParticleTypeOrder: ambient first, then photoelectrons
+    // Environment::resetParticleTypeOrder (Environment.cpp:360-377): ambient, photoelectron, secondary
     std::stable_partition(species.begin(), species.end(), [](const ParticleType& p) { return p.type == "ambient"; });
+    std::stable_partition(species.begin(), species.end(), [](const ParticleType& p) { return p.type != "secondary"; });
     in.species = species;
 
     double bfield[3] = {0.0, 0.0, 0.0}, shine[3] = {0.0, 0.0, 0.0};
@@ -153,13 +192,15 @@ Input load_input(const std::string& path) {
     p.capacity_factor = 1.5;
     p.precision = FOPIS_MIXED;
     p.seed = 12345;
+    p.energy_ev = norm.unenergy(1.0) / kE;   // Normalizer::unnormalizeEnergy(1, "eV")
 
     if (js.has("Object")) {
         const std::string base = dir_of(path);
         for (const auto& kv : js["Object"].items()) {
             const Value& o = kv.second;
-            if (o.str_or("surface_type", "perfect") != "perfect")
-                throw Error(FOPIS_ERR_ARG, "only perfect conductors are on the ES hot path");
+            const std::string surface = o.str_or("surface_type", "perfect");
+            if (surface != "perfect" && surface != "dielectric")
+                throw Error(FOPIS_ERR_ARG, "surface_type " + surface + " is not perfect or dielectric");
             ObjectSpec spec;
             spec.name = kv.first;
             std::string file = o["file_name"].str();
@@ -171,8 +212,17 @@ Input load_input(const std::string& path) {
             spec.initial_potential_offset = norm.potential(o.number_or("initial_potential_offset", 0.0));
             if (o.has("emit_particles"))
                 for (const auto& e : o["emit_particles"].items())
-                    for (size_t s = 0; s < species.size(); ++s)
+                    for (size_t s = 0; s < species.size(); ++s) {
                         if (species[s].name == e.first && species[s].type == "photoelectron") spec.emit_species = (int)s;
+                        if (species[s].name == e.first && species[s].type == "secondary") spec.secondary_species = (int)s;
+                    }
+            if (surface == "dielectric") {
+                std::map<int, std::string> mats;
+                if (o.has("materials"))
+                    for (const auto& m : o["materials"].items()) mats[std::stoi(m.first)] = m.second.str();
+                spec.dielectric = 1;
+                node_capacitance(file, nxyz[0], nxyz[1], nxyz[2], mats, norm, spec);
+            }
             in.objects.push_back(spec);
         }
     }
@@ -218,6 +268,9 @@ RootGrid::RootGrid(const Input& in, int device) : in_(in) {
         d.fixed_potential = o.fixed_potential;
         d.initial_potential_offset = o.initial_potential_offset;
         d.emit_species = o.emit_species;
+        d.secondary_species = o.secondary_species;
+        d.dielectric = o.dielectric;
+        d.capacitance = o.dielectric ? o.capacitance.data() : nullptr;
         int id = -1;
         check(fopis_add_object(ctx_, &d, &id));
         object_ids_.push_back(id);

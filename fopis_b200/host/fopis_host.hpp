@@ -41,7 +41,7 @@ struct Normalizer {
 // ParticleType / AmbientParticleType / PhotoElectronParticleType (the fields the ES path reads).
 struct ParticleType {
     std::string name;
-    std::string type;              // "ambient" | "photoelectron"
+    std::string type;              // "ambient" | "photoelectron" | "secondary"
     double mass = 1.0;             // m_e
     double charge = -1.0;          // e
     double density = 0.0;          // m^-3
@@ -67,6 +67,9 @@ struct ObjectSpec {
     double fixed_potential = 0.0;  // normalised
     double initial_potential_offset = 0.0;
     int emit_species = -1;
+    int secondary_species = -1;    // secondary-electron species the body emits
+    int dielectric = 0;            // surface_type "dielectric"
+    std::vector<double> capacitance;   // [n_cmat] normalised node capacitance (dielectric)
     int n_cmat() const { return (int)(nodes.size() / 3); }
 };
 
@@ -74,7 +77,7 @@ struct ObjectSpec {
 struct Input {
     fopis_params params{};
     Normalizer norm;
-    std::vector<ParticleType> species;   // ABI order: ambient first, then photoelectrons
+    std::vector<ParticleType> species;   // ABI order: ambient, photoelectron, secondary
     std::vector<ObjectSpec> objects;
     int max_timestep = 0;
     double dx = 1.0, dt = 1.0;

@@ -39,6 +39,10 @@ void dump_params(const Input& in, const std::string& file) {
         f.write(reinterpret_cast<const char*>(pot), sizeof pot);
         f.write(reinterpret_cast<const char*>(o.nodes.data()), sizeof(int32_t) * o.nodes.size());
         f.write(reinterpret_cast<const char*>(o.cells.data()), sizeof(int32_t) * o.cells.size());
+        const int32_t extra[2] = {o.secondary_species, o.dielectric};
+        f.write(reinterpret_cast<const char*>(extra), sizeof extra);
+        if (o.dielectric)
+            f.write(reinterpret_cast<const char*>(o.capacitance.data()), sizeof(double) * o.capacitance.size());
     }
 }
 }  // namespace

@@ -64,7 +64,10 @@ typedef enum fopis_status {
 
 typedef enum fopis_species_kind {
     FOPIS_SPECIES_AMBIENT = 0,        /* AmbientParticleType */
-    FOPIS_SPECIES_PHOTOELECTRON = 1   /* PhotoElectronParticleType */
+    FOPIS_SPECIES_PHOTOELECTRON = 1,  /* PhotoElectronParticleType */
+    FOPIS_SPECIES_SECONDARY = 2       /* SecondaryParticleType (src/Particle/SecondaryParticleType.cpp):
+                                         emitted where other species hit a body; thermal_velocity
+                                         is the true-secondary emission speed sqrt(2T/m) */
 } fopis_species_kind;
 
 /* One particle species; fields mirror ParticleType (include/particle_type.hpp:13-120). */
@@ -121,6 +124,8 @@ typedef struct fopis_params {
     int precision;               /* fopis_precision */
     int reserved0;
     uint64_t seed;               /* Philox key for loading, injection and emission */
+    double energy_ev;            /* Normalizer::unnormalizeEnergy(1, "eV") = m_e dx^2 / (e dt^2): eV per
+                                    normalised energy unit (secondary-emission yields); 0 without them */
 } fopis_params;
 
 /* A voxel conductor; replaces the ObjectDataFromFile + Spacecraft construction
@@ -134,6 +139,12 @@ typedef struct fopis_object_desc {
     double fixed_potential;      /* normalised */
     double initial_potential_offset; /* normalised (Spacecraft::initializeChargeMapOffset) */
     int emit_species;            /* photoelectron species emitted from the lit face, -1 = none */
+    int secondary_species;       /* secondary-electron species emitted where particles hit the body,
+                                    -1 = none (Spacecraft::hasSecondaryParticles, SecondaryEmission.cpp:5-12) */
+    int dielectric;              /* surface_type "dielectric" (Spacecraft::isDielectricSurface) */
+    const double* capacitance;   /* [n_cmat] normalised node capacitance of a dielectric surface, the mean
+                                    over the node's faces of normalizeCapacitance(4 pi eps0 eps_r) of the
+                                    face's material (Spacecraft.cpp:117-149); 0 where none */
 } fopis_object_desc;
 
 /* Field selectors for fopis_get_field / fopis_set_field. */
@@ -239,6 +250,15 @@ int fopis_step(void* ctx, int n);
 /* Phase entry points, for parity checks between phases. */
 int fopis_update_velocity(void* ctx);        /* Grid::updateParticleVelocityES (GridParticleTreatmentES.cpp:13-88) */
 int fopis_emit_particles(void* ctx);         /* RootGrid::emitParticlesFromObjects (RootGridObject.cpp:175-181) */
+/* Spacecraft::incident_events (SecondaryEmission.cpp:14-33): the hits recorded by the last
+ * absorption, consumed by the next emission. One record of FOPIS_INCIDENT_DOUBLES doubles:
+ * object, incident species, surface axis (0 x, 1 y, 2 z), remaining time (the move ratio
+ * since the crossing), crossing point x, y, z, velocity vx, vy, vz. get copies at most cap
+ * records out (*n gets the count); set replaces the pending list (n <= the absorbed-list
+ * capacity). */
+#define FOPIS_INCIDENT_DOUBLES 10
+int fopis_get_incidents(void* ctx, double* records, int64_t cap, int64_t* n);
+int fopis_set_incidents(void* ctx, const double* records, int64_t n);
 int fopis_update_position(void* ctx);        /* RootGrid::updateParticlePositionES (GridParticleTreatmentES.cpp:90-181) */
 int fopis_inject_particles(void* ctx);       /* RootGrid::injectParticlesFromBoundary (RootGridParticle.cpp:3-130) */
 int fopis_update_rho(void* ctx);             /* RootGrid::updateRho (RootGridField.cpp:1153-1252), incl. the
@@ -352,6 +372,12 @@ int fopis_efield_energy_noalloc(const double* phi, int nx, int ny, int nz, doubl
  * allocated with malloc; release them with fopis_free. */
 int fopis_parse_obj(const char* path, int nx, int ny, int nz,
                     int32_t** cmat_nodes, int* n_cmat, int32_t** cells, int* n_cells);
+/* The same file's face textures per surface node (ObjectDataFromFile::textures,
+ * ObjectUtils.cpp:65-160): node c (cmat order) lists the texture index of every quad
+ * covering it, tex[start[c] .. start[c+1]), start has n_cmat + 1 entries. The
+ * texture index is the vt number of the quad's first vertex (f v/vt/vn ...). */
+int fopis_parse_obj_textures(const char* path, int nx, int ny, int nz,
+                             int32_t** start, int32_t** tex, int* n_cmat);
 void fopis_free(void* p);
 
 #ifdef __cplusplus

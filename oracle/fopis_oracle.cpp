@@ -87,7 +87,7 @@ static inline void box_muller(double u1, double u2, double& n0, double& n1) {
     n1 = r * std::sin(t);
 }
 
-enum : uint32_t { TAG_LOAD = 1u, TAG_INJECT = 2u, TAG_EMIT = 3u };
+enum : uint32_t { TAG_LOAD = 1u, TAG_INJECT = 2u, TAG_EMIT = 3u, TAG_SECONDARY = 4u };
 
 // ---------------------------------------------------------------- containers
 struct Arr3 {
@@ -143,7 +143,16 @@ struct Object {
     int is_potential_fixed = 0;
     double fixed_potential = 0.0, initial_potential_offset = 0.0;
     int emit_species = -1;
+    int secondary_species = -1;                // SecondaryParticleType emitted by this body
+    int dielectric = 0;                        // surface_type "dielectric"
+    std::vector<double> capacitance;           // capacitance_map [n]
     bool has_C = false;
+};
+
+// IncidentInfo_t (src/Spacecraft/Incident.cpp) plus the object it hit.
+struct Incident {
+    int obj, s, axis;
+    double trem, x, y, z, vx, vy, vz;
 };
 
 struct Ctx {
@@ -156,6 +165,8 @@ struct Ctx {
     std::vector<Arr3> rho;       // rho[0] total, rho[1+s]
     Arr3 phi, poisson_error, ex, ey, ez, exref, eyref, ezref;
     std::vector<Object> objects;
+    std::vector<Incident> incidents;            // Spacecraft::incident_events of all objects
+    std::vector<std::vector<Incident>> incidents_by_species;   // filled per species in update_rho
     std::vector<std::array<double, 6>> inject_residual;
     int64_t timestep = 1;        // Environment::timestep starts at 1 (Initialize.cpp:161)
     // solver
@@ -466,22 +477,42 @@ static bool surface_charge(const Ctx& c, Object& o, int axis, const Pos& pos, in
     return true;
 }
 
-// Spacecraft::distributeInnerParticleCharge (Spacecraft.cpp:512-592), non-secondary
-// branch. Returns 1 if absorbed.
-static int absorb(Ctx& c, Object& o, Particle& p, int& bad) {
+// The first of a particle's crossing points that is a body face on an axis
+// other than `skip` (-1: any), in the order of Spacecraft::distribute
+// InnerParticleCharge (Spacecraft.cpp:512-592) and, with skip, of
+// distributeInnerParticleChargeForSecondary (SecondaryEmission.cpp:35-110).
+static int first_face(const Ctx& c, const Object& o, const Particle& p, int skip, Pos& hit) {
+    const int isign = (p.vx > 0.0) ? 1 : -1, jsign = (p.vy > 0.0) ? 1 : -1, ksign = (p.vz > 0.0) ? 1 : -1;
+    Pos cps[3];
+    const int ncp = computeCrossPoints(p, cps);
+    for (int t = 0; t < ncp; ++t) {
+        const Pos& cp = cps[t];
+        if (skip != 0 && isXsurfacePoint(c, o, cp, isign)) { hit = cp; return 0; }
+        if (skip != 1 && isYsurfacePoint(c, o, cp, jsign)) { hit = cp; return 1; }
+        if (skip != 2 && isZsurfacePoint(c, o, cp, ksign)) { hit = cp; return 2; }
+    }
+    return -1;
+}
+
+// Spacecraft::distributeInnerParticleCharge (Spacecraft.cpp:512-592). A body that
+// emits secondaries keeps the hit as an incident event (its move ratio along the
+// face axis is the remaining time, SecondaryEmission.cpp:14-33). Returns 1 if
+// absorbed.
+static int absorb(Ctx& c, int oi, Particle& p, int& bad, std::vector<Incident>* inc) {
+    Object& o = c.objects[oi];
     const Pos pos = posXYZ(p.x, p.y, p.z);
     if (!isContaining(c, o, pos)) return 0;
     const int id = p.typeId;
     const double q = c.p.species[id].charge * c.p.species[id].size;
-    const int isign = (p.vx > 0.0) ? 1 : -1, jsign = (p.vy > 0.0) ? 1 : -1, ksign = (p.vz > 0.0) ? 1 : -1;
-    Pos cps[3];
-    const int ncp = computeCrossPoints(p, cps);
-    bool found = false;
-    for (int t = 0; t < ncp && !found; ++t) {
-        const Pos& cp = cps[t];
-        if (isXsurfacePoint(c, o, cp, isign)) { if (!surface_charge(c, o, 0, cp, id, q)) bad = 1; found = true; }
-        else if (isYsurfacePoint(c, o, cp, jsign)) { if (!surface_charge(c, o, 1, cp, id, q)) bad = 1; found = true; }
-        else if (isZsurfacePoint(c, o, cp, ksign)) { if (!surface_charge(c, o, 2, cp, id, q)) bad = 1; found = true; }
+    Pos cp;
+    const int ax = first_face(c, o, p, -1, cp);
+    if (ax >= 0) {
+        if (!surface_charge(c, o, ax, cp, id, q)) bad = 1;
+        if (o.secondary_species >= 0 && inc) {
+            const double d1[3] = {pos.dx1, pos.dy1, pos.dz1}, d2[3] = {pos.dx2, pos.dy2, pos.dz2};
+            const double v[3] = {p.vx, p.vy, p.vz};
+            inc->push_back(Incident{oi, id, ax, moveRatio(d1[ax], d2[ax], v[ax]), cp.x, cp.y, cp.z, p.vx, p.vy, p.vz});
+        }
     }
     o.current[id] += q;
     p.isValid = 0;
@@ -501,6 +532,29 @@ static double total_charge(const Ctx& c, const Object& o) {
     return q;
 }
 
+// Spacecraft::redistributeChargeForDielectric (Spacecraft.cpp:641-706): a node j
+// with capacitance c_j > 0 enters with phi_j - Q_j / c_j, Q_j its charge summed
+// over the species, in both the potential and delta rho. d holds V - phi_j on
+// entry; the potential and d are recomputed here.
+static void redistribute_dielectric(Ctx& c, Object& o, std::vector<double>& d) {
+    const int n = o.n_cmat;
+    std::vector<double> pe(n);
+    for (int j = 0; j < n; ++j) {
+        const auto& nd = o.cmat[j];
+        pe[j] = c.phi(nd[0], nd[1], nd[2]);
+        if (o.capacitance[j] > 0.0) {
+            double qn = 0.0;
+            for (int pid = 0; pid < c.nsp; ++pid) qn += o.charge_map[(size_t)pid * n + j];
+            pe[j] -= qn / o.capacitance[j];
+        }
+    }
+    double ctp = 0.0;
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) ctp += o.C[(size_t)i * n + j] * pe[j];
+    o.potential = o.is_potential_fixed ? o.fixed_potential : (ctp + o.total_charge) / o.total_cmat_value;
+    for (int j = 0; j < n; ++j) d[j] = o.potential - pe[j];
+}
+
 // Spacecraft::redistributeChargeForPerfectConductor (Spacecraft.cpp:708-758).
 static void redistribute(Ctx& c, Object& o) {
     o.total_charge = total_charge(c, o);
@@ -514,6 +568,7 @@ static void redistribute(Ctx& c, Object& o) {
     o.potential = o.is_potential_fixed ? o.fixed_potential : (ctp + o.total_charge) / o.total_cmat_value;
     std::vector<double> d(n);
     for (int j = 0; j < n; ++j) { const auto& nd = o.cmat[j]; d[j] = o.potential - c.phi(nd[0], nd[1], nd[2]); }
+    if (o.dielectric) redistribute_dielectric(c, o, d);
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < n; ++i) {
         double dr = 0.0;
@@ -754,13 +809,18 @@ static int update_rho(Ctx& c) {
     for (auto& r : c.rho) r.zero();
     int bad = 0;
     int64_t absorbed = 0;
+    c.incidents_by_species.assign(c.nsp, {});
 #pragma omp parallel for schedule(static) reduction(| : bad) reduction(+ : absorbed)
     for (int pid = 0; pid < c.nsp; ++pid) {
         const double q = c.p.species[pid].charge * c.p.species[pid].size;
         Arr3& r = c.rho[pid + 1];
         for (auto& p : c.particles[pid]) {
             if (!p.isValid) continue;
-            for (auto& o : c.objects) { int b = 0; absorbed += absorb(c, o, p, b); bad |= b; }
+            for (int oi = 0; oi < (int)c.objects.size(); ++oi) {
+                int b = 0;
+                absorbed += absorb(c, oi, p, b, &c.incidents_by_species[pid]);
+                bad |= b;
+            }
             if (p.isValid) {
                 const Pos pos = posXYZ(p.x, p.y, p.z);
                 const int i = pos.i, j = pos.j, k = pos.k;
@@ -776,6 +836,7 @@ static int update_rho(Ctx& c) {
         }
     }
     c.absorbed_step = absorbed;
+    for (auto& v : c.incidents_by_species) c.incidents.insert(c.incidents.end(), v.begin(), v.end());
     for (auto& o : c.objects) sum_whole_charge(c, o);
     for (int pid = 1; pid <= c.nsp; ++pid)
         for (size_t t = 0; t < c.rho[0].v.size(); ++t) c.rho[0].v[t] += c.rho[pid].v[t];
@@ -1033,6 +1094,142 @@ static int emit(Ctx& c) {
     c.emitted_step = emitted;
     return bad;
 }
+static int emit_secondaries(Ctx& c);
+// RootGrid::emitParticlesFromObjects: photoelectrons, then secondaries.
+static int emit_all(Ctx& c) {
+    const int a = emit(c);
+    if (a < 0) return a;
+    return a | emit_secondaries(c);
+}
+
+// ---------------------------------------------------------------- secondary electrons
+// Spacecraft::emitParticles, secondary branch (Spacecraft.cpp:901-937), with
+// SecondaryParticleType::generateNewParticles and Whipple's coefficients
+// (src/Particle/SecondaryParticleType.cpp:16-194) on the reference's hard-coded
+// test material. Deviation: the draws are Philox keyed by the incident's own
+// content (crossing point and velocity rounded to 2^-24, species, axis, object)
+// and the step, the same function as the GPU path's, not the std::mt19937_64
+// streams of the reference, whose values depend on how many incidents came
+// before.
+static const double kSeeFermi = 9.1, kSeeDeltaMax = 3.0, kSeeEpsMax = 420.0, kSeeZ = 13.0;
+
+static inline uint64_t see_mix(uint64_t h, uint64_t w) {
+    h ^= w;
+    h *= 0x100000001B3ull;
+    h ^= h >> 29;
+    return h;
+}
+static uint64_t incident_key(const Incident& e) {
+    const double d[6] = {e.x, e.y, e.z, e.vx, e.vy, e.vz};
+    uint64_t h = 0xCBF29CE484222325ull;
+    for (int q = 0; q < 6; ++q) h = see_mix(h, (uint64_t)std::llrint(d[q] * 16777216.0));
+    return see_mix(h, (uint64_t)e.s | ((uint64_t)e.axis << 8) | ((uint64_t)e.obj << 16));
+}
+static inline U2 see_draw(const Ctx& c, uint64_t key, uint32_t idx) {
+    return draw2(c.p.seed, (uint32_t)key, (uint32_t)(key >> 32), (uint32_t)c.timestep, (TAG_SECONDARY << 24) | idx);
+}
+
+// SecondaryParticleType::computeWhipple{TrueSecondary,Inelastic,Elastic}Coeff.
+static double whipple_true(double E, double th) {
+    return (1.114 * kSeeDeltaMax / std::cos(th)) * std::pow(kSeeEpsMax / E, 0.35) *
+           (1.0 - std::exp(-2.28 * std::cos(th) * std::pow(E / kSeeEpsMax, 1.35)));
+}
+static double whipple_inelastic(double E, double th) {
+    const double eta1 = 1.0 - std::pow(2.0 / E, 0.037 * kSeeZ);
+    const double eta2 = 0.1 * std::exp(-E / 5000.0);
+    double eta0 = 0.0;
+    if (E > 50.0 && E < 1000.0) eta0 = std::log(E / 50.0) / std::log(20.0);
+    else if (E > 1000.0) eta0 = 1.0;
+    return eta0 * (eta1 + eta2) * (7.37 * std::pow(kSeeZ, -0.56875)) * (1.0 - std::cos(th));
+}
+static double whipple_elastic(double E) {
+    return (1.0 / 13.54) * std::pow(kSeeFermi, 4) / (16.0 * (std::pow(E + kSeeFermi, 3) + std::pow(kSeeFermi, 3)));
+}
+
+// SecondaryParticleType::generateNewParticles for one incident.
+static void see_generate(const Ctx& c, const Incident& e, int sec, std::vector<Particle>& out) {
+    const uint64_t key = incident_key(e);
+    const double m_in = c.p.species[e.s].mass, q_in = c.p.species[e.s].charge;
+    const double v2 = e.vx * e.vx + e.vy * e.vy + e.vz * e.vz;
+    const double vin[3] = {e.vx, e.vy, e.vz};
+    const double E = 0.5 * m_in * v2 * c.p.energy_ev;                  // getIncidentEnergyInElectronVolt
+    const double th = std::acos(std::fabs(vin[e.axis]) / std::sqrt(v2));    // getIncidentAngle
+    const double r = q_in < 0.0 ? whipple_elastic(E) : 0.0;
+    const double eta = q_in < 0.0 ? whipple_inelastic(E, th) : 0.0;
+    double delta = whipple_true(E, th);
+    const U2 u = see_draw(c, key, 0);
+    int kind, count;
+    if (u.a < r) { kind = 1; count = 1; }
+    else if (u.a < r + eta) { kind = 2; count = 1; }
+    else {
+        delta /= (1.0 - r - eta);
+        kind = 3;
+        count = (int)std::floor(delta) + ((u.b < delta - std::floor(delta)) ? 1 : 0);
+    }
+    double speed = c.p.species[sec].thermal_velocity;                   // true secondaries
+    if (kind == 2) {
+        const double share = see_draw(c, key, 1).a;                        // of the incident energy
+        speed = std::sqrt(2.0 * (share * 0.5 * m_in * v2) / c.p.species[sec].mass);
+    }
+    for (int m = 0; m < count; ++m) {
+        double v[3] = {vin[0], vin[1], vin[2]};
+        if (kind == 1) {
+            v[e.axis] = -v[e.axis];
+        } else {
+            const U2 ua = see_draw(c, key, (uint32_t)(2 + m));
+            const double dep = std::asin(2.0 * ua.a - 1.0), az = 2.0 * M_PI * ua.b;
+            const double sgn = vin[e.axis] > 0.0 ? -1.0 : 1.0;
+            const double cn = speed * std::cos(dep) * sgn;
+            const double sa = speed * std::sin(dep) * std::cos(az), sb = speed * std::sin(dep) * std::sin(az);
+            if (e.axis == 0) { v[0] = cn; v[1] = sa; v[2] = sb; }
+            else if (e.axis == 1) { v[0] = sb; v[1] = cn; v[2] = sa; }
+            else { v[0] = sa; v[1] = sb; v[2] = cn; }
+        }
+        Particle p;
+        p.vx = v[0]; p.vy = v[1]; p.vz = v[2];
+        p.x = e.x + e.trem * v[0]; p.y = e.y + e.trem * v[1]; p.z = e.z + e.trem * v[2];
+        p.typeId = sec; p.isValid = 1;
+        out.push_back(p);
+    }
+}
+
+// The pending incidents' secondaries: a secondary inside the body is absorbed at
+// once on a face of another axis (its incident, recorded by the reference into
+// the list it is iterating and cleared right after, emits nothing); the others
+// take their charge off the face they left, at the next crossing of their
+// back-dated position along the incident axis, and are appended. The list is
+// then cleared (Spacecraft::clearIncidentEvents).
+static int emit_secondaries(Ctx& c) {
+    int bad = 0;
+    int64_t emitted = 0;
+    for (const Incident& e : c.incidents) {
+        Object& o = c.objects[e.obj];
+        const int sec = o.secondary_species;
+        if (sec < 0) continue;
+        const double q = c.p.species[sec].charge * c.p.species[sec].size;
+        std::vector<Particle> gen;
+        see_generate(c, e, sec, gen);
+        for (Particle& p : gen) {
+            if (isContaining(c, o, posXYZ(p.x, p.y, p.z))) {
+                Pos hit;
+                const int ax = first_face(c, o, p, e.axis, hit);
+                if (ax >= 0 && !surface_charge(c, o, ax, hit, sec, q)) bad = 1;
+                o.current[sec] += q;
+                continue;
+            }
+            Particle old = p;
+            old.x -= p.vx; old.y -= p.vy; old.z -= p.vz;
+            const Pos ep = next_cross(old, e.axis);
+            if (!surface_charge(c, o, e.axis, ep, sec, -q)) bad = 1;
+            o.current[sec] -= q;
+            c.particles[sec].push_back(p);
+            ++emitted;
+        }
+    }
+    c.incidents.clear();
+    c.emitted_step += emitted;
+    return bad;
+}
 
 // Grid::removeInvalidParticles (src/Grid/GridParticleTreatment.cpp:93-102).
 static void remove_invalid(Ctx& c) {
@@ -1049,7 +1246,7 @@ static void reset_objects(Ctx& c) {
 static int main_loop(Ctx& c) {
     reset_objects(c);
     update_velocity(c);
-    int bad = emit(c);
+    int bad = emit_all(c);
     update_position(c);
     inject(c, nullptr);
     bad |= update_rho(c);
@@ -1274,6 +1471,9 @@ int orc_add_object(void* h, const fopis_object_desc* d) {
     o.fixed_potential = d->fixed_potential;
     o.initial_potential_offset = d->initial_potential_offset;
     o.emit_species = d->emit_species;
+    o.secondary_species = d->secondary_species;
+    o.dielectric = d->dielectric;
+    if (o.dielectric) o.capacitance.assign(d->capacitance, d->capacitance + d->n_cmat);
     c->objects.push_back(std::move(o));
     return (int)c->objects.size() - 1;
 }
@@ -1327,7 +1527,28 @@ void orc_generate_ambient(void* h) { generate_ambient(*(Ctx*)h); }
 
 void orc_reset_objects(void* h) { reset_objects(*(Ctx*)h); }
 void orc_update_velocity(void* h) { update_velocity(*(Ctx*)h); }
-int orc_emit(void* h) { return emit(*(Ctx*)h); }
+int orc_emit(void* h) { return emit_all(*(Ctx*)h); }
+// The pending incident list as records of 10 doubles (object, species, axis,
+// remaining time, x, y, z, vx, vy, vz), the layout of fopis_get_incidents.
+int64_t orc_get_incidents(void* h, double* out, int64_t cap) {
+    Ctx* c = (Ctx*)h;
+    const int64_t n = (int64_t)c->incidents.size();
+    for (int64_t t = 0; t < std::min(n, cap); ++t) {
+        const Incident& e = c->incidents[t];
+        double* r = out + 10 * t;
+        r[0] = e.obj; r[1] = e.s; r[2] = e.axis; r[3] = e.trem;
+        r[4] = e.x; r[5] = e.y; r[6] = e.z; r[7] = e.vx; r[8] = e.vy; r[9] = e.vz;
+    }
+    return n;
+}
+void orc_set_incidents(void* h, const double* in, int64_t n) {
+    Ctx* c = (Ctx*)h;
+    c->incidents.clear();
+    for (int64_t t = 0; t < n; ++t) {
+        const double* r = in + 10 * t;
+        c->incidents.push_back(Incident{(int)r[0], (int)r[1], (int)r[2], r[3], r[4], r[5], r[6], r[7], r[8], r[9]});
+    }
+}
 void orc_update_position(void* h) { update_position(*(Ctx*)h); }
 void orc_inject(void* h, int64_t* counts) { inject(*(Ctx*)h, counts); }
 int orc_update_rho(void* h) { return update_rho(*(Ctx*)h); }

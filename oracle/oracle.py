@@ -61,6 +61,8 @@ def lib():
             "orc_fixed_deposit": (None, [vp, vp, vp, vp, vp, C.c_int64, vp]),
             "orc_fixed_fold": (None, [vp, vp]),
             "orc_position": (None, [vp, C.c_int64, vp, vp]),
+            "orc_get_incidents": (C.c_int64, [vp, dp, C.c_int64]),
+            "orc_set_incidents": (None, [vp, dp, C.c_int64]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -210,7 +212,25 @@ class Oracle:
         d.fixed_potential = o.fixed_potential
         d.initial_potential_offset = o.initial_potential_offset
         d.emit_species = o.emit_species
+        d.secondary_species = getattr(o, "secondary_species", -1)
+        d.dielectric = getattr(o, "dielectric", 0)
+        if d.dielectric:
+            cap = np.ascontiguousarray(o.capacitance, np.float64)
+            self._keep.append(cap)
+            d.capacitance = cap.ctypes.data_as(C.POINTER(C.c_double))
         return self.L.orc_add_object(self.h, C.addressof(d))
+
+    def get_incidents(self):
+        """Spacecraft::incident_events as an [n, 10] array (object, species, axis,
+        remaining time, x, y, z, vx, vy, vz)."""
+        n = self.L.orc_get_incidents(self.h, None, 0)
+        out = np.zeros((max(n, 1), 10))
+        self.L.orc_get_incidents(self.h, out.ctypes.data_as(C.POINTER(C.c_double)), n)
+        return out[:n]
+
+    def set_incidents(self, recs):
+        recs = np.ascontiguousarray(recs, np.float64).reshape(-1, 10)
+        self.L.orc_set_incidents(self.h, recs.ctypes.data_as(C.POINTER(C.c_double)), len(recs))
 
     def set_solver(self, mode: int, max_post_loop: int = 1000, exact_tol: float = 1e-13):
         self.L.orc_set_solver(self.h, mode, max_post_loop, exact_tol)

@@ -7,11 +7,18 @@ from pathlib import Path
 from fopis_b200 import config
 
 
-def write_input(dirpath, n=25, ppc=4, photo=True, steps=5, drift=(0.0, 0.0, 0.0)):
+def write_input(dirpath, n=25, ppc=4, photo=True, steps=5, drift=(0.0, 0.0, 0.0), secondary=False, dielectric=None):
+    """dielectric: the materials map (texture index -> material name) of a dielectric
+    cube whose +x face carries texture 2 and the other faces texture 1."""
     d = Path(dirpath)
     d.mkdir(parents=True, exist_ok=True)
     (d / "objects").mkdir(exist_ok=True)
-    (d / "objects" / "cube.obj").write_text(config.box_obj_text([((-2, -2, -2), (2, 2, 2))]))
+    text = config.box_obj_text([((-2, -2, -2), (2, 2, 2))])
+    if dielectric:
+        # box_obj_text writes f a/1/n ...; the normal index n = 2 is the +x face
+        text = "\n".join(l.replace("/1/2", "/2/2") if l.startswith("f ") else l for l in text.splitlines()) + "\n"
+        text = text.replace("vt 0.5 0.5\n", "vt 0.5 0.5\nvt 0.25 0.5\n")
+    (d / "objects" / "cube.obj").write_text(text)
     dx, dt = config.plasma_units()
     plasma = {
         "Electron": {"type": "ambient", "mass": 1.0, "charge": -1.0, "density": 1.0e7, "temperature": 1.0,
@@ -26,15 +33,20 @@ def write_input(dirpath, n=25, ppc=4, photo=True, steps=5, drift=(0.0, 0.0, 0.0)
         plasma["Photo"] = {"type": "photoelectron", "mass": 1.0, "charge": -1.0, "density": 1.0e7, "temperature": 0.2,
                            "particle_per_cell": ppc, "current_density": 10.0 * config.E * 1.0e7 * vbar / 4.0}
         emit = {"Photo": {}}
+    if secondary:
+        plasma["Secondary"] = {"type": "secondary", "mass": 1.0, "charge": -1.0, "density": 1.0e7, "temperature": 2.0,
+                               "particle_per_cell": ppc}
+        emit["Secondary"] = {}
     js = {
         "Environment": {"max_timestep": steps, "job_type": "new", "solver_type": "ES", "boundary": "DDDDDD",
                         "dimension": "3D", "nx": n, "ny": n, "nz": n, "proc_x": 1, "proc_y": 1, "proc_z": 1,
                         "dx": dx, "dt": dt},
         "Plasma": plasma,
         "Field": {"static_bfield": [0.0, 0.0, 0.0], "shine_vector": [-1.0, 0.0, 0.0]},
-        "Object": {"Spacecraft": {"file_name": "objects/cube.obj", "surface_type": "perfect", "emit_particles": emit,
+        "Object": {"Spacecraft": {"file_name": "objects/cube.obj",
+                                  "surface_type": "dielectric" if dielectric else "perfect", "emit_particles": emit,
                                   "is_potential_fixed": False, "fixed_potential": 0.0,
-                                  "initial_potential_offset": 0.0}},
+                                  "initial_potential_offset": 0.0, **({"materials": dielectric} if dielectric else {})}},
         "Options": {"use_existing_capacity_matrix": False},
     }
     path = d / "input.json"

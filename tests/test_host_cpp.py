@@ -39,7 +39,13 @@ def dump(path, tmp_path):
         off += 12 * nn
         cells = np.frombuffer(raw, np.int32, 3 * nc, off).reshape(-1, 3)
         off += 12 * nc
-        objs.append((nodes, cells, int(fixed), int(emit), pot))
+        sec, diel = np.frombuffer(raw, np.int32, 2, off)
+        off += 8
+        cap = None
+        if diel:
+            cap = np.frombuffer(raw, np.float64, nn, off)
+            off += 8 * nn
+        objs.append((nodes, cells, int(fixed), int(emit), pot, int(sec), int(diel), cap))
     return p, objs
 
 
@@ -49,10 +55,13 @@ def compare(cpp, py):
     assert bytes(p) == bytes(q), [(f, getattr(p, f), getattr(q, f)) for f, _ in q._fields_ if
                                   not isinstance(getattr(q, f), (int, float)) or getattr(p, f) != getattr(q, f)]
     assert len(objs) == len(py.objects)
-    for (nodes, cells, fixed, emit, pot), o in zip(objs, py.objects):
+    for (nodes, cells, fixed, emit, pot, sec, diel, cap), o in zip(objs, py.objects):
         assert np.array_equal(nodes, o.nodes) and np.array_equal(cells, o.cells)
         assert fixed == o.is_potential_fixed and emit == o.emit_species
         assert pot[0] == o.fixed_potential and pot[1] == o.initial_potential_offset
+        assert sec == o.secondary_species and diel == o.dielectric
+        if diel:
+            assert np.array_equal(cap, o.capacitance)
 
 
 @pytest.fixture(scope="module")
@@ -66,6 +75,16 @@ def built():
 def test_cpp_loader_matches_python(built, tmp_path, photo):
     path = write_input(tmp_path, photo=photo, drift=(50.0, 0.0, -20.0))
     compare(dump(path, tmp_path), config.load_input(str(path)))
+
+
+def test_cpp_loader_dielectric_and_secondary(built, tmp_path):
+    # a dielectric cube of two materials emitting photoelectrons and secondaries
+    path = write_input(tmp_path, photo=True, secondary=True, dielectric={"1": "Teflon", "2": "Aluminum"})
+    py = config.load_input(str(path))
+    assert [s.kind for s in py.species] == ["ambient", "ambient", "photoelectron", "secondary"]
+    o = py.objects[0]
+    assert o.dielectric == 1 and o.secondary_species == 3 and o.emit_species == 2
+    compare(dump(path, tmp_path), py)
 
 
 def test_cpp_loader_on_reference_sample(built, tmp_path):

@@ -54,8 +54,11 @@ def test_abi_library_exports_every_declared_symbol():
 def test_abi_struct_layout_matches_header():
     import ctypes as C
     assert C.sizeof(_abi.Species) == 152
-    assert C.sizeof(_abi.Params) == 1352
+    assert C.sizeof(_abi.Params) == 1360
     assert _abi.Params.seed.offset == 1344
+    assert _abi.Params.energy_ev.offset == 1352
+    assert C.sizeof(_abi.ObjectDesc) == 80
+    assert _abi.ObjectDesc.capacitance.offset == 72
 
 
 def _write(tmp_path, text):
