@@ -1,6 +1,7 @@
 // tc.cuh — sm_100a building blocks for the tensor-core kernels: 16-byte
-// cp.async staging, mbarriers with bounded waits, tensor-memory (TMEM)
-// allocation, tcgen05.mma with shared-memory descriptors, tcgen05.ld.
+// cp.async and bulk (TMA engine) staging, mbarriers with bounded waits,
+// tensor-memory (TMEM) allocation, tcgen05.mma with shared-memory descriptors,
+// tcgen05.ld.
 //
 // Operand layouts are the canonical no-swizzle ("interleaved") forms: a core
 // matrix is 8 rows x 16 bytes stored as 128 contiguous bytes.
@@ -55,6 +56,18 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint32_
 }
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+// Arrives on the barrier and adds `bytes` to the transfer count its phase waits for.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// Bulk copy (TMA engine, no tensor map) of `bytes` from this GPU's global memory
+// into this CTA's shared memory; both addresses 16-byte aligned, bytes a
+// multiple of 16. Completion counts `bytes` on the mbarrier.
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
 }
 
 // Tensor memory: one warp allocates / frees; ncols is a power of two >= 32.

@@ -207,29 +207,41 @@ __device__ __forceinline__ void conv_epilogue(const ConvArgs& a, uint32_t tmem, 
 
 template <int CIN, int COUT>
 struct ConvShape {
-    static constexpr int NST = 4, LA = 2;
     static constexpr int KB = CIN / 16;
     static constexpr int A_PL = 130 * 16;
     static constexpr int A_BYTES = (CIN / 8) * A_PL;
     static constexpr int W_TAP = CIN * COUT * 2;
     static constexpr int B_BYTES = 3 * W_TAP;
     static constexpr int ST = A_BYTES + B_BYTES;
+    // stages in the ring (about 48 KB of it, 2 to 8), and the copies kept in flight ahead of the MMAs
+    static constexpr int NST = ST * 8 <= 49152 ? 8 : (ST * 2 >= 49152 ? 2 : 49152 / ST);
+    static constexpr int LA = NST > 2 ? NST - 2 : 1;   // one stage of slack for the MMAs to release a buffer
     static constexpr int COLS = COUT < 32 ? 32 : COUT;
-    static constexpr int SMEM = NST * ST + (NST + 1) * 8 + 16;
+    static constexpr int SMEM = NST * ST + (2 * NST + 1) * 8 + 16;
+    static constexpr uint32_t STAGE_TX = (CIN / 8) * A_PL + B_BYTES;   // bytes one stage's bulk copies bring
 };
 
+// One implicit-GEMM convolution tile loop. Thread 0 produces and issues: for
+// stage q it waits until the MMAs of stage q - NST have released the buffer,
+// then brings the CIN/8 contiguous 2,080-byte plane segments of the shifted
+// positions and the three taps' weight block in with bulk copies (TMA engine,
+// completion counted on the stage's full barrier); for stage q - LA it waits on
+// that full barrier and issues the tcgen05 MMAs into the TMEM accumulator. The
+// four warps run the epilogue once a tile's nine stages are committed.
 template <int CIN, int COUT, int EPI>
 __global__ void __launch_bounds__(128) conv_kernel(ConvArgs a) {
     using S = ConvShape<CIN, COUT>;
     static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 64, "channel counts");
     constexpr uint32_t IDESC = tc::idesc_bf16(128, COUT, false, false);
     extern __shared__ __align__(128) uint8_t sm[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + S::NST * S::ST);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + S::NST + 1);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + S::NST * S::ST);   // [NST] MMAs done, [NST] tile done
+    uint64_t* full = bar + S::NST + 1;                                   // [NST] stage data landed
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(full + S::NST);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == 0) tc::tmem_alloc(tc::saddr(tslot), S::COLS);
     if (tid == 0) {
         for (int b = 0; b <= S::NST; ++b) tc::mbar_init(tc::saddr(bar + b), 1);
+        for (int b = 0; b < S::NST; ++b) tc::mbar_init(tc::saddr(full + b), 1);
         tc::fence_mbar_init();
     }
     tc::fence_before();
@@ -240,50 +252,50 @@ __global__ void __launch_bounds__(128) conv_kernel(ConvArgs a) {
     const int ntl = (int)blockIdx.x < a.tiles ? (a.tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     const int total = ntl * 9;
     for (int q = 0; q < total + S::LA; ++q) {
-        if (q < total) {
-            const int b = q % S::NST;
-            if (q >= S::NST && !tc::mbar_wait(tc::saddr(bar + b), (uint32_t)((q / S::NST) - 1) & 1u)) report(a.err, 1u);
-            const int tl = q / 9, s = q - tl * 9;
-            const long long p0 = ((long long)blockIdx.x + (long long)tl * gridDim.x) * 128;
-            const int di = s / 3 - 1, dj = s % 3 - 1;
-            const long long pb = p0 + di * a.Si + dj * a.Sj - 1;
-            const uint32_t sA = sbase + b * S::ST, sB = sA + S::A_BYTES;
-            for (int e = tid; e < (CIN / 8) * 130; e += 128) {
-                const int pl = e / 130, rr = e - pl * 130;
-                tc::cp16(sA + pl * S::A_PL + rr * 16, a.x.p + ((long long)pl * a.x.stride + pb + rr) * 8);
-            }
-            const uint8_t* wsrc = reinterpret_cast<const uint8_t*>(a.w) + (size_t)(s * 3) * S::W_TAP;
-            for (int e = tid; e < S::B_BYTES / 16; e += 128) tc::cp16(sB + e * 16, wsrc + (size_t)e * 16);
-        }
-        tc::cp_commit();
         const int cq = q - S::LA;
-        if (cq < 0) continue;
-        tc::cp_wait<S::LA>();
-        tc::fence_async_smem();
-        __syncthreads();
-        const int b = cq % S::NST, tl = cq / 9, s = cq - tl * 9;
         if (tid == 0) {
-            tc::fence_after();
-            const uint32_t sA = sbase + b * S::ST, sB = sA + S::A_BYTES;
+            if (q < total) {
+                const int b = q % S::NST;
+                if (q >= S::NST && !tc::mbar_wait(tc::saddr(bar + b), (uint32_t)((q / S::NST) - 1) & 1u)) report(a.err, 1u);
+                const int tl = q / 9, s = q - tl * 9;
+                const long long p0 = ((long long)blockIdx.x + (long long)tl * gridDim.x) * 128;
+                const int di = s / 3 - 1, dj = s % 3 - 1;
+                const long long pb = p0 + di * a.Si + dj * a.Sj - 1;
+                const uint32_t sA = sbase + b * S::ST, sB = sA + S::A_BYTES, fb = tc::saddr(full + b);
+                tc::mbar_arrive_expect_tx(fb, S::STAGE_TX);
 #pragma unroll
-            for (int dk = 0; dk < 3; ++dk)
+                for (int pl = 0; pl < CIN / 8; ++pl)
+                    tc::bulk_g2s(sA + pl * S::A_PL, a.x.p + ((long long)pl * a.x.stride + pb) * 8, S::A_PL, fb);
+                tc::bulk_g2s(sB, reinterpret_cast<const uint8_t*>(a.w) + (size_t)(s * 3) * S::W_TAP, S::B_BYTES, fb);
+            }
+            if (cq >= 0) {
+                const int b = cq % S::NST, s = cq % 9;
+                if (!tc::mbar_wait(tc::saddr(full + b), (uint32_t)(cq / S::NST) & 1u)) report(a.err, 4u);
+                tc::fence_after();
+                const uint32_t sA = sbase + b * S::ST, sB = sA + S::A_BYTES;
 #pragma unroll
-                for (int kb = 0; kb < S::KB; ++kb) {
-                    const uint64_t ad = tc::sdesc(sA + (2 * kb) * S::A_PL + dk * 16, S::A_PL, 128);
-                    const uint64_t bd = tc::sdesc(sB + dk * S::W_TAP + kb * COUT * 32, COUT * 16, 128);
-                    tc::mma(tmem, ad, bd, IDESC, (s | dk | kb) != 0 ? 1u : 0u);
-                }
-            tc::commit(tc::saddr(bar + b));
-            if (s == 8) tc::commit(tc::saddr(bar + S::NST));
+                for (int dk = 0; dk < 3; ++dk)
+#pragma unroll
+                    for (int kb = 0; kb < S::KB; ++kb) {
+                        const uint64_t ad = tc::sdesc(sA + (2 * kb) * S::A_PL + dk * 16, S::A_PL, 128);
+                        const uint64_t bd = tc::sdesc(sB + dk * S::W_TAP + kb * COUT * 32, COUT * 16, 128);
+                        tc::mma(tmem, ad, bd, IDESC, (s | dk | kb) != 0 ? 1u : 0u);
+                    }
+                tc::commit(tc::saddr(bar + b));
+                if (s == 8) tc::commit(tc::saddr(bar + S::NST));
+            }
         }
-        if (s == 8) {
+        if (cq >= 0 && cq % 9 == 8) {
+            const int tl = cq / 9;
             if (!tc::mbar_wait(tc::saddr(bar + S::NST), (uint32_t)tl & 1u)) report(a.err, 2u);
             tc::fence_after();
             conv_epilogue<COUT, EPI>(a, tmem, ((long long)blockIdx.x + (long long)tl * gridDim.x) * 128, warp, lane);
             tc::fence_before();
+            __syncthreads();   // every warp's TMEM reads done before the next tile's MMAs overwrite it
+            tc::fence_after();
         }
     }
-    __syncthreads();
+    __syncthreads();   // every issued stage was consumed: no copy is in flight
     tc::fence_after();
     if (warp == 0) tc::tmem_dealloc(tmem, S::COLS);
 }
