@@ -204,14 +204,41 @@ class RootGrid:
         self._check(self.lib.fopis_advance_timestep(self.h))
 
     # ------------------------------------------------------------ fields
+    def field_shape(self, which: int):
+        """(first index, extent) per axis of a field; the EM Yee arrays start
+        below 0 on axes with damping layers (boost::multi_array index bases)."""
+        lo, n = (C.c_int * 3)(), (C.c_int * 3)()
+        self._check(self.lib.fopis_field_shape(self.h, which, lo, n))
+        return tuple(lo), tuple(n)
+
     def get_field(self, which: int) -> np.ndarray:
-        out = np.empty(self.shape)
+        _, n = self.field_shape(which)
+        out = np.empty(n)
         self._check(self.lib.fopis_get_field(self.h, which, _dp(out), out.size))
         return out
 
     def set_field(self, which: int, a: np.ndarray):
-        a = np.ascontiguousarray(a, dtype=np.float64).reshape(self.shape)
+        _, n = self.field_shape(which)
+        a = np.ascontiguousarray(a, dtype=np.float64).reshape(n)
         self._check(self.lib.fopis_set_field(self.h, which, _dp(a), a.size))
+
+    def updateBfield(self):
+        """RootGrid::updateBfield (EM mode)."""
+        self._check(self.lib.fopis_update_bfield(self.h))
+
+    def mainLoopEM(self, n: int = 1):
+        """n calls of RootGrid::mainLoopEM (fopis_step of a context created with solver EM)."""
+        if self.p.solver != _abi.SOLVER_EM:
+            raise _abi.FopisError(_abi.ERR_STATE, "the context runs the ES solver")
+        return self.mainLoopES(n)
+
+    def getBref(self):
+        return tuple(self.get_field(w) for w in (_abi.FIELD_BXREF, _abi.FIELD_BYREF, _abi.FIELD_BZREF))
+
+    def getBfieldEnergy(self) -> float:
+        e = C.c_double()
+        self._check(self.lib.fopis_get_bfield_energy(self.h, C.byref(e)))
+        return e.value
 
     def getPhi(self):
         return self.get_field(_abi.FIELD_PHI)

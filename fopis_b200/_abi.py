@@ -41,13 +41,30 @@ GUESS_ZERO = 0
 GUESS_WARM = 1
 GUESS_LEARNED = 2
 GUESS_HISTORY = 3
+SOLVER_ES = 0
+SOLVER_EM = 1
 
 FIELD_PHI = 0
 FIELD_RHO0 = 1
 FIELD_EXREF = 2
 FIELD_EYREF = 3
 FIELD_EZREF = 4
+FIELD_BXREF = 5
+FIELD_BYREF = 6
+FIELD_BZREF = 7
+FIELD_JXREF = 8
+FIELD_JYREF = 9
+FIELD_JZREF = 10
 FIELD_RHO_SPECIES = 16
+FIELD_EX = 32
+FIELD_EY = 33
+FIELD_EZ = 34
+FIELD_BX = 35
+FIELD_BY = 36
+FIELD_BZ = 37
+FIELD_JX = 38
+FIELD_JY = 39
+FIELD_JZ = 40
 
 
 class Species(C.Structure):
@@ -84,9 +101,10 @@ class Params(C.Structure):
         ("remove_interval", C.c_int),
         ("capacity_factor", C.c_double),
         ("precision", C.c_int),
-        ("reserved0", C.c_int),
+        ("solver", C.c_int),
         ("seed", C.c_uint64),
         ("energy_ev", C.c_double),
+        ("mu0", C.c_double),
     ]
 
 
@@ -161,6 +179,9 @@ SIGNATURES = {
     "fopis_update_rho": (C.c_int, [_VP]),
     "fopis_solve_poisson": (C.c_int, [_VP]),
     "fopis_update_efield": (C.c_int, [_VP]),
+    "fopis_update_bfield": (C.c_int, [_VP]),
+    "fopis_field_shape": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "fopis_get_bfield_energy": (C.c_int, [_VP, _DP]),
     "fopis_remove_invalid_particles": (C.c_int, [_VP]),
     "fopis_advance_timestep": (C.c_int, [_VP]),
     "fopis_get_field": (C.c_int, [_VP, C.c_int, _DP, C.c_size_t]),

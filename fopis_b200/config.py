@@ -39,6 +39,8 @@ class Normalizer:
         self.V_unit = dx * dx * ME / (E * dt * dt)
         self.A_unit = E / dt
         self.eps0 = EPS0 * (dx ** 3 * ME) / (E * E * dt * dt)   # normalizeEpsilon
+        self.mu0 = MU0 * E * E / (ME * dx)                       # normalizeMu
+        self.c = self.velocity(CLIGHT)                           # normalizeVelocity(c): the Courant number
 
     def velocity(self, v):
         return self.t * v / self.x
@@ -164,8 +166,14 @@ def _species_struct(sp: SpeciesInfo, norm: Normalizer, dx: float) -> _abi.Specie
 def make_params(nxyz: Tuple[int, int, int], boundary: str, dx: float, dt: float, species: List[SpeciesInfo],
                 bfield_nT=(0.0, 0.0, 0.0), shine=(0.0, 0.0, 0.0), seed: int = 12345, tol: float = 1e-8,
                 max_vcycles: int = 100, sort_interval: int = 8, guess: int = _abi.GUESS_WARM,
-                capacity_factor: float = 1.5, precision: int = _abi.MIXED) -> Tuple[_abi.Params, Normalizer]:
+                capacity_factor: float = 1.5, precision: int = _abi.MIXED,
+                solver: str = "ES") -> Tuple[_abi.Params, Normalizer]:
     norm = Normalizer(dx, dt)
+    if solver not in ("ES", "EM"):
+        raise ValueError(f"solver_type {solver} is neither ES nor EM")
+    if solver == "EM" and norm.c > 1.0:
+        # Environment::checkCFLCondition (src/Misc/Environment.cpp:193-203) aborts the run
+        raise ValueError(f"Courant number exceeds 1.0 (c dt / dx = {norm.c:.6g})")
     p = _abi.Params()
     p.nx, p.ny, p.nz = (int(v) for v in nxyz)
     p.boundary = boundary.encode()
@@ -188,6 +196,8 @@ def make_params(nxyz: Tuple[int, int, int], boundary: str, dx: float, dt: float,
     p.precision = precision
     p.seed = seed
     p.energy_ev = norm.unenergy(1.0) / E                       # Normalizer::unnormalizeEnergy(1, "eV")
+    p.solver = _abi.SOLVER_EM if solver == "EM" else _abi.SOLVER_ES
+    p.mu0 = norm.mu0
     return p, norm
 
 
@@ -394,7 +404,8 @@ def load_input(path: str) -> SimConfig:
     bfield = field_in.get("static_bfield", (0.0, 0.0, 0.0))
     shine = field_in.get("shine_vector", (0.0, 0.0, 0.0))
     opts = js.get("Options", {})
-    p, norm = make_params(nxyz, env["boundary"], dx, dt, species, bfield_nT=bfield, shine=shine)
+    p, norm = make_params(nxyz, env["boundary"], dx, dt, species, bfield_nT=bfield, shine=shine,
+                          solver=str(env.get("solver_type", "ES")))
     objs = []
     names = [s.name for s in species]
     for oname in sorted(js.get("Object", {})):

@@ -216,6 +216,50 @@ int one_step(Ctx& c) {
     return rc2;
 }
 
+// RootGrid::mainLoopEM (RootGrid.cpp:145-191): velocity (E and B gather),
+// emission, position with the edge currents, injection, rho (with the first
+// solve and the redistribution when objects exist), then the FDTD E and B
+// updates. ms_phase: velocity, emit, position + inject, -, rho, E, B, sort.
+int em_step(Ctx& c) {
+    step_begin(c);
+    FOPIS_CUDA(cudaMemsetAsync(c.d_sc->pushed, 0, 3 * sizeof(c.d_sc->pushed), c.st));
+    FOPIS_CUDA(cudaMemsetAsync(&c.d_sc->absorbed_n, 0, sizeof(unsigned long long), c.st));
+    record(c, 0);
+    launch_em_velocity(c);
+    record(c, 1);
+    launch_emit(c, false);
+    record(c, 2);
+    launch_em_position(c);
+    launch_inject(c, false);
+    record(c, 3);
+    rho_zero(c);
+    launch_deposit_all(c);
+    int rc1 = FOPIS_OK;
+    rho_tail(c, &rc1);
+    record(c, 5);
+    em_update_efield(c);
+    record(c, 6);
+    em_update_bfield(c);
+    record(c, 7);
+    const int si = c.p.sort_interval > 0 ? c.p.sort_interval : 8;
+    if (c.timestep % si == 0) particles_sort(c);
+    record(c, 8);
+    const int rc = check_device(c);
+    update_currents(c);
+    c.energy_valid = false;
+    c.timestep += 1;
+    if (c.ev[0]) {
+        FOPIS_CUDA(cudaEventSynchronize(c.ev[8]));
+        float ms = 0.f;
+        const int map[8][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 3}, {3, 5}, {5, 6}, {6, 7}, {7, 8}};
+        for (int q = 0; q < 8; ++q) {
+            cudaEventElapsedTime(&ms, c.ev[map[q][0]], c.ev[map[q][1]]);
+            c.ms_phase[q] = ms;
+        }
+    }
+    return rc != FOPIS_OK ? rc : rc1;
+}
+
 }  // namespace
 
 extern "C" {
@@ -246,6 +290,17 @@ int fopis_create(const fopis_params* p, int device, void** out) {
         if (p->precision != FOPIS_MIXED && p->precision != FOPIS_FP64)
             throw ApiError{FOPIS_ERR_ARG, "precision must be FOPIS_MIXED or FOPIS_FP64"};
         x.fp64 = p->precision == FOPIS_FP64;
+        if (p->solver != FOPIS_SOLVER_ES && p->solver != FOPIS_SOLVER_EM)
+            throw ApiError{FOPIS_ERR_ARG, "solver must be FOPIS_SOLVER_ES or FOPIS_SOLVER_EM"};
+        if (p->solver == FOPIS_SOLVER_EM) {
+            if (!(p->mu0 > 0.0)) throw ApiError{FOPIS_ERR_ARG, "the EM solver needs params.mu0"};
+            // Environment::checkCFLCondition (Environment.cpp:193-203): Normalizer::c = 1/sqrt(eps0 mu0)
+            if (1.0 / std::sqrt(p->eps0 * p->mu0) > 1.0 + 1e-9)
+                throw ApiError{FOPIS_ERR_ARG, "Courant number exceeds 1.0"};
+            for (int a = 0; a < 3; ++a)
+                if ((p->boundary[2 * a] == 'P') != (p->boundary[2 * a + 1] == 'P'))
+                    throw ApiError{FOPIS_ERR_ARG, "the EM solver needs each axis periodic on both sides or on neither"};
+        }
         for (int s = 0; s < p->nspecies; ++s)
             if (!(p->species[s].mass > 0.0)) throw ApiError{FOPIS_ERR_ARG, "species mass must be positive"};
         int ndev = 0;
@@ -307,6 +362,7 @@ int fopis_create(const fopis_params* p, int device, void** out) {
         FOPIS_CUDA(cudaMallocHost(&x.h_sc, sizeof(DevScalars)));
         std::memset(x.h_sc, 0, sizeof(DevScalars));
         for (auto& e : x.ev) FOPIS_CUDA(cudaEventCreate(&e));
+        if (p->solver == FOPIS_SOLVER_EM) em_alloc(x);
         mg_setup(x);
         mg_prepare(x);
         FOPIS_CUDA(cudaDeviceSynchronize());
@@ -326,6 +382,7 @@ void fopis_destroy(void* h) {
     if (!c) return;
     if (c->st) cudaStreamSynchronize(c->st);
     unet_free(*c);
+    em_free(*c);
     for (int s = 0; s < FOPIS_MAX_SPECIES; ++s) {
         Soa* v[2] = {&c->sp[s], &c->sp2[s]};
         for (Soa* q : v) {
@@ -572,7 +629,12 @@ int fopis_initialize(void* h) {
         int rc1 = FOPIS_OK;
         rho_tail(c, &rc1);
         const int rc2 = solve(c, solve_kind_after_rho(c));
-        efield_update(c);
+        if (c.em.on) {
+            em_efield_from_phi(c);
+            em_update_bfield(c);
+        } else {
+            efield_update(c);
+        }
         const int rc = check_device(c);
         update_currents(c);
         c.energy_valid = false;
@@ -585,7 +647,7 @@ int fopis_step(void* h, int n) {
     return guarded(h, [&](Ctx& c) -> int {
         int rc = FOPIS_OK;
         for (int t = 0; t < n; ++t) {
-            rc = one_step(c);
+            rc = c.em.on ? em_step(c) : one_step(c);
             if (rc != FOPIS_OK && rc != FOPIS_ERR_NOT_CONVERGED) return rc;
         }
         return rc;
@@ -595,7 +657,8 @@ int fopis_step(void* h, int n) {
 int fopis_update_velocity(void* h) {
     return guarded(h, [&](Ctx& c) -> int {
         step_begin(c);   // RootGrid::resetObjects precedes it in mainLoopES
-        launch_push(c, true, false, false);
+        if (c.em.on) launch_em_velocity(c);
+        else launch_push(c, true, false, false);
         c.energy_valid = false;
         return check_device(c);
     });
@@ -611,7 +674,8 @@ int fopis_emit_particles(void* h) {
 
 int fopis_update_position(void* h) {
     return guarded(h, [&](Ctx& c) -> int {
-        launch_push(c, false, true, false);
+        if (c.em.on) launch_em_position(c);
+        else launch_push(c, false, true, false);
         c.energy_valid = false;
         return check_device(c);
     });
@@ -645,8 +709,43 @@ int fopis_solve_poisson(void* h) {
 
 int fopis_update_efield(void* h) {
     return guarded(h, [&](Ctx& c) -> int {
-        efield_update(c);
+        if (c.em.on) em_update_efield(c);
+        else efield_update(c);
         FOPIS_CUDA(cudaStreamSynchronize(c.st));
+        return FOPIS_OK;
+    });
+}
+
+int fopis_update_bfield(void* h) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (!c.em.on) throw ApiError{FOPIS_ERR_STATE, "updateBfield belongs to the EM solver"};
+        em_update_bfield(c);
+        FOPIS_CUDA(cudaStreamSynchronize(c.st));
+        return FOPIS_OK;
+    });
+}
+
+int fopis_field_shape(void* h, int which, int lo[3], int n[3]) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (!lo || !n) throw ApiError{FOPIS_ERR_ARG, "null shape output"};
+        const int cc[3] = {c.cx, c.cy, c.cz};
+        for (int a = 0; a < 3; ++a) { lo[a] = 0; n[a] = cc[a]; }
+        if (const YeeArr* y = em_array(c, which)) {
+            for (int a = 0; a < 3; ++a) { lo[a] = y->lo[a]; n[a] = y->n[a]; }
+        } else if (which >= FOPIS_FIELD_JX && which <= FOPIS_FIELD_JZ) {
+            if (!c.em.on) throw ApiError{FOPIS_ERR_ARG, "edge currents exist in the EM mode only"};
+            n[which - FOPIS_FIELD_JX] -= 1;
+        } else if (which >= FOPIS_FIELD_EX && which <= FOPIS_FIELD_BZ) {
+            throw ApiError{FOPIS_ERR_ARG, "Yee arrays exist in the EM mode only"};
+        }
+        return FOPIS_OK;
+    });
+}
+
+int fopis_get_bfield_energy(void* h, double* energy) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (!energy) throw ApiError{FOPIS_ERR_ARG, "null output"};
+        *energy = c.em.on ? em_bfield_energy(c) : 0.0;
         return FOPIS_OK;
     });
 }
@@ -660,16 +759,43 @@ int fopis_advance_timestep(void* h) {
     });
 }
 
+// Elements of a field selector's array: the Yee arrays and edge currents of the
+// EM mode have their own extents, every other field the node grid's.
+static size_t field_elements(Ctx& c, int which) {
+    if (const YeeArr* y = em_array(c, which)) return y->size();
+    if (c.em.on && which >= FOPIS_FIELD_JX && which <= FOPIS_FIELD_JZ) {
+        const int d = which - FOPIS_FIELD_JX;
+        return (size_t)(c.cx - (d == 0)) * (c.cy - (d == 1)) * (c.cz - (d == 2));
+    }
+    return c.N;
+}
+
 int fopis_get_field(void* h, int which, double* out, size_t n) {
     return guarded(h, [&](Ctx& c) -> int {
-        if (!out || n != c.N) throw ApiError{FOPIS_ERR_ARG, "output size must be (nx+2)(ny+2)(nz+2)"};
-        field_export(c, which, out);
+        if (!out || n != field_elements(c, which))
+            throw ApiError{FOPIS_ERR_ARG, "output size must be the field's element count (fopis_field_shape)"};
+        const bool em_field = c.em.on && ((which >= FOPIS_FIELD_EXREF && which <= FOPIS_FIELD_JZREF) ||
+                                          (which >= FOPIS_FIELD_EX && which <= FOPIS_FIELD_JZ));
+        if (em_field) em_field_export(c, which, out);
+        else if (which >= FOPIS_FIELD_BXREF && which <= FOPIS_FIELD_JZREF)
+            throw ApiError{FOPIS_ERR_ARG, "magnetic field and current exist in the EM mode only"};
+        else field_export(c, which, out);
         return FOPIS_OK;
     });
 }
 
 int fopis_set_field(void* h, int which, const double* in, size_t n) {
     return guarded(h, [&](Ctx& c) -> int {
+        if (const YeeArr* y = em_array(c, which)) {
+            if (!in || n != y->size()) throw ApiError{FOPIS_ERR_ARG, "input size must be the Yee array's element count"};
+            FOPIS_CUDA(cudaMemcpy(y->v, in, sizeof(double) * n, cudaMemcpyHostToDevice));
+            return FOPIS_OK;
+        }
+        if (c.em.on && which >= FOPIS_FIELD_JX && which <= FOPIS_FIELD_JZ) {
+            if (!in || n != field_elements(c, which)) throw ApiError{FOPIS_ERR_ARG, "input size must be the current's element count"};
+            FOPIS_CUDA(cudaMemcpy(c.em.j[which - FOPIS_FIELD_JX], in, sizeof(double) * n, cudaMemcpyHostToDevice));
+            return FOPIS_OK;
+        }
         if (!in || n != c.N) throw ApiError{FOPIS_ERR_ARG, "input size must be (nx+2)(ny+2)(nz+2)"};
         double* dst = which == FOPIS_FIELD_PHI ? c.phi : (which == FOPIS_FIELD_RHO0 ? c.rho0 : nullptr);
         if (!dst) throw ApiError{FOPIS_ERR_ARG, "only PHI and RHO0 can be set"};
@@ -684,7 +810,7 @@ int fopis_get_energy(void* h, double* pe, double* fe) {
         double e = 0.0;
         for (int s = 0; s < c.nsp; ++s) e += 0.5 * c.p.species[s].mass * c.h_sc->energy[s] * c.p.species[s].size;
         if (pe) *pe = e;
-        if (fe) *fe = efield_energy(c);
+        if (fe) *fe = c.em.on ? em_efield_energy(c) : efield_energy(c);
         return FOPIS_OK;
     });
 }

@@ -181,6 +181,29 @@ struct MGLevel {
     size_t size() const { return (size_t)n[0] * n[1] * n[2]; }
 };
 
+// A Yee array of the EM mode: boost::multi_array with index bases, C order,
+// element (i, j, k) at ((i - lo0) n1 + (j - lo1)) n2 + (k - lo2).
+struct YeeArr {
+    double* v = nullptr;
+    int lo[3] = {0, 0, 0};
+    int n[3] = {0, 0, 0};
+    size_t size() const { return (size_t)n[0] * n[1] * n[2]; }
+};
+
+// Device state of the EM solver (FOPIS_SOLVER_EM).
+struct EMState {
+    bool on = false;
+    int L[3] = {1, 1, 1};            // Environment::damping_length: the node counts
+    int lo[3] = {0, 0, 0};           // x_low.. of RootGrid::initializeField
+    int up[3] = {0, 0, 0};           // x_up..
+    YeeArr f[6];                     // ex, ey, ez, bx, by, bz
+    double* j[3] = {nullptr, nullptr, nullptr};   // jx [cx-1][cy][cz], jy [cx][cy-1][cz], jz [cx][cy][cz-1]
+    double* eref = nullptr;          // [3][N] nodal E (FP64, the export copy)
+    double* bref = nullptr;          // [3][N] nodal B (FP64)
+    float4* B = nullptr;             // nodal B (FP32) for the gather of the mixed mode
+    Vec4d* B64 = nullptr;            // nodal B (FP64) for the FP64 mode
+};
+
 struct Ctx {
     fopis_params p{};
     int device = 0;
@@ -263,6 +286,8 @@ struct Ctx {
     bool hist_ok = false;
     // learned guess (allocated on demand)
     void* unet = nullptr;
+    // EM mode
+    EMState em;
 };
 
 // ------------------------------------------------------------------ launchers
@@ -277,6 +302,8 @@ void particles_sort(Ctx& c);
 int64_t brick_keys(const Ctx& c);
 void launch_push(Ctx& c, bool vel, bool pos, bool dep);
 void launch_deposit_all(Ctx& c);
+void launch_em_velocity(Ctx& c);
+void launch_em_position(Ctx& c);
 void launch_emit(Ctx& c, bool fused);
 void launch_inject(Ctx& c, bool fused);
 void launch_absorb(Ctx& c);
@@ -293,6 +320,17 @@ double efield_energy(Ctx& c);
 void phi_boundary(Ctx& c);
 void phi_axpy(Ctx& c, double* dst, const double* a, const double* b, double sb);   // dst = a + sb * b over all nodes
 void glue_copy(Ctx& c, double* a);
+// em.cu (FDTD solver of the EM mode)
+void em_alloc(Ctx& c);
+void em_free(Ctx& c);
+void em_fold_currents(Ctx& c);
+void em_efield_from_phi(Ctx& c);   // RootGrid::updateEfield in the EM mode (start-up)
+void em_update_efield(Ctx& c);     // RootGrid::updateEfieldFDTD
+void em_update_bfield(Ctx& c);     // RootGrid::updateBfield
+double em_efield_energy(Ctx& c);
+double em_bfield_energy(Ctx& c);
+const YeeArr* em_array(const Ctx& c, int which);   // FOPIS_FIELD_EX..BZ, or null
+void em_field_export(Ctx& c, int which, double* host);
 // multigrid.cu
 void mg_setup(Ctx& c);
 void mg_free(Ctx& c);

@@ -379,6 +379,132 @@ __global__ void __launch_bounds__(kThreads) push_kernel(PushArgsT<T> a) {
     }
 }
 
+// ------------------------------------------------------------------ EM particle phases
+// Grid::updateParticleVelocityEM (src/Grid/GridParticleTreatmentEM.cpp:13-105):
+// the CIC gather of the nodal E and B, both scaled by 0.5 q/m, then Boris with
+// the gathered b, boris = 2 / (1 + |b|^2). One particle per thread.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) em_velocity_kernel(PushArgsT<T> a, const typename NodeE<T>::type* B) {
+    const long long n = (long long)min(*a.count, (unsigned long long)a.cap);
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int32_t cell = a.p.cell[idx];
+        if (cell < 0) continue;
+        int i, j, k;
+        unpack_cell(cell, i, j, k);
+        const T x1 = a.p.ox[idx], y1 = a.p.oy[idx], z1 = a.p.oz[idx];
+        const T x2 = (T)1 - x1, y2 = (T)1 - y1, z2 = (T)1 - z1;
+        const T w[8] = {a.qm * x2 * y2 * z2, a.qm * x1 * y2 * z2, a.qm * x2 * y1 * z2, a.qm * x1 * y1 * z2,
+                        a.qm * x2 * y2 * z1, a.qm * x1 * y2 * z1, a.qm * x2 * y1 * z1, a.qm * x1 * y1 * z1};
+        const int b = lin(a.g, i, j, k), sj = (int)a.g.sj, si = (int)a.g.si;
+        const int off[8] = {0, si, sj, si + sj, 1, si + 1, sj + 1, si + sj + 1};
+        T e[3] = {(T)0, (T)0, (T)0}, m[3] = {(T)0, (T)0, (T)0};
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            const auto ev = load_e(a.E + b + off[t]);
+            const auto bv = load_e(B + b + off[t]);
+            e[0] += w[t] * ev.x; e[1] += w[t] * ev.y; e[2] += w[t] * ev.z;
+            m[0] += w[t] * bv.x; m[1] += w[t] * bv.y; m[2] += w[t] * bv.z;
+        }
+        const T boris = (T)2 / ((T)1 + (m[0] * m[0] + m[1] * m[1] + m[2] * m[2]));
+        const T vx1 = a.p.vx[idx] + e[0], vy1 = a.p.vy[idx] + e[1], vz1 = a.p.vz[idx] + e[2];
+        const T vxt = vx1 + vy1 * m[2] - vz1 * m[1];
+        const T vyt = vy1 + vz1 * m[0] - vx1 * m[2];
+        const T vzt = vz1 + vx1 * m[1] - vy1 * m[0];
+        a.p.vx[idx] = vx1 + e[0] + boris * (vyt * m[2] - vzt * m[1]);
+        a.p.vy[idx] = vy1 + e[1] + boris * (vzt * m[0] - vxt * m[2]);
+        a.p.vz[idx] = vz1 + e[2] + boris * (vxt * m[1] - vyt * m[0]);
+    }
+}
+
+// Edge currents of the EM mode, FP64, glue-layout edges of the node grid.
+struct EdgeJ {
+    double *x, *y, *z;     // jx [cx-1][cy][cz], jy [cx][cy-1][cz], jz [cx][cy][cz-1]
+    int cx, cy, cz;
+};
+
+// The zigzag relay point of Position::getReferencePosition
+// (include/position.hpp:88-96) on one axis, in a frame whose cell index is
+// floor(x) + 1: the shared face when the two cells differ, else the midpoint.
+__device__ __forceinline__ double em_relay(int i_new, int i_old, double x_new, double x_old) {
+    return fmin((double)min(i_new, i_old), fmax((double)max(i_new, i_old) - 1.0, 0.5 * (x_new + x_old)));
+}
+
+// One half of Particle::distributeCurrentAtOldPosition / AtNewPosition
+// (src/Particle/particle.cpp:258-338) on the edges of cell (i, j, k): flux f
+// and in-cell weights w (the mean of the half's two points in the cell's frame).
+__device__ __forceinline__ void em_current_half(const EdgeJ& J, int i, int j, int k, const double f[3],
+                                                const double w[3]) {
+    const long long ax = ((long long)i * J.cy + j) * J.cz + k;                 // jx [cx-1][cy][cz]
+    atomicAdd(J.x + ax, f[0] * (1.0 - w[1]) * (1.0 - w[2]));
+    atomicAdd(J.x + ax + J.cz, f[0] * w[1] * (1.0 - w[2]));
+    atomicAdd(J.x + ax + 1, f[0] * (1.0 - w[1]) * w[2]);
+    atomicAdd(J.x + ax + J.cz + 1, f[0] * w[1] * w[2]);
+    const long long ay = ((long long)i * (J.cy - 1) + j) * J.cz + k;           // jy [cx][cy-1][cz]
+    const long long syi = (long long)(J.cy - 1) * J.cz;
+    atomicAdd(J.y + ay, f[1] * (1.0 - w[0]) * (1.0 - w[2]));
+    atomicAdd(J.y + ay + syi, f[1] * w[0] * (1.0 - w[2]));
+    atomicAdd(J.y + ay + 1, f[1] * (1.0 - w[0]) * w[2]);
+    atomicAdd(J.y + ay + syi + 1, f[1] * w[0] * w[2]);
+    const long long az = ((long long)i * J.cy + j) * (J.cz - 1) + k;           // jz [cx][cy][cz-1]
+    const long long szi = (long long)J.cy * (J.cz - 1);
+    atomicAdd(J.z + az, f[2] * (1.0 - w[0]) * (1.0 - w[1]));
+    atomicAdd(J.z + az + szi, f[2] * w[0] * (1.0 - w[1]));
+    atomicAdd(J.z + az + (J.cz - 1), f[2] * (1.0 - w[0]) * w[1]);
+    atomicAdd(J.z + az + szi + (J.cz - 1), f[2] * w[0] * w[1]);
+}
+
+// RootGrid::updateParticlePositionEM's per-particle part
+// (src/Grid/GridParticleTreatmentEM.cpp:107-139): the old-cell half of the
+// charge-conserving current (from x to x + v), the move with the boundary rules
+// and, while still valid, the new-cell half (from x - v to x in the frame of
+// the cell the particle lands in, a periodic crossing included). Positions
+// enter the current in the cell's frame (offset in [0, 1)), the reference's
+// global coordinates shifted by the cell's lower node. q is the super-particle
+// charge per step.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) em_position_kernel(PushArgsT<T> a, EdgeJ J, double q) {
+    const long long n = (long long)min(*a.count, (unsigned long long)a.cap);
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int32_t cell = a.p.cell[idx];
+        if (cell < 0) continue;
+        PStateT<T> st;
+        unpack_cell(cell, st.i, st.j, st.k);
+        st.ox = a.p.ox[idx]; st.oy = a.p.oy[idx]; st.oz = a.p.oz[idx];
+        st.vx = a.p.vx[idx]; st.vy = a.p.vy[idx]; st.vz = a.p.vz[idx];
+        {
+            const T o[3] = {st.ox, st.oy, st.oz}, v[3] = {st.vx, st.vy, st.vz};
+            double f[3], w[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const double x1 = (double)o[d], x2 = (double)(T)(o[d] + v[d]);   // the move's own sum
+                const int i2 = (int)floor(x2) + 1;
+                const double r = em_relay(i2, 1, x2, x1);
+                f[d] = q * (r - x1);
+                w[d] = 0.5 * (r + x1);
+            }
+            em_current_half(J, st.i, st.j, st.k, f, w);
+        }
+        const bool live = move_boundary(a, st);
+        if (live) {
+            const T o[3] = {st.ox, st.oy, st.oz}, v[3] = {st.vx, st.vy, st.vz};
+            double f[3], w[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const double x2 = (double)o[d], x1 = x2 - (double)v[d];
+                const int i1 = (int)floor(x1) + 1;
+                const double r = em_relay(1, i1, x2, x1);
+                f[d] = q * (x2 - r);
+                w[d] = 0.5 * (r + x2);
+            }
+            em_current_half(J, st.i, st.j, st.k, f, w);
+        }
+        a.p.cell[idx] = live ? pack_cell(st.i, st.j, st.k) : -1;
+        a.p.ox[idx] = st.ox; a.p.oy[idx] = st.oy; a.p.oz[idx] = st.oz;
+    }
+}
+
 // ------------------------------------------------------------------ brick push
 // push_brick_kernel: the fused push (gather + Boris + move + boundaries +
 // absorption flag + deposit + kinetic energy) over the brick-sorted particles,
@@ -1921,6 +2047,9 @@ void particles_sort(Ctx& c) {
 template <typename T> const typename NodeE<T>::type* node_e(const Ctx& c);
 template <> const float4* node_e<float>(const Ctx& c) { return c.E; }
 template <> const Vec4d* node_e<double>(const Ctx& c) { return c.E64; }
+template <typename T> const typename NodeE<T>::type* node_b(const Ctx& c);
+template <> const float4* node_b<float>(const Ctx& c) { return c.em.B; }
+template <> const Vec4d* node_b<double>(const Ctx& c) { return c.em.B64; }
 
 template <typename T>
 static PushArgsT<T> push_args(Ctx& c, int s) {
@@ -1974,6 +2103,37 @@ void launch_push(Ctx& c, bool vel, bool pos, bool dep) {
 }
 
 void launch_deposit_all(Ctx& c) { launch_push(c, false, false, true); }
+
+// Grid::updateParticleVelocityEM for every species.
+void launch_em_velocity(Ctx& c) {
+    for (int s = 0; s < c.nsp; ++s) {
+        if (c.cap[s] == 0) continue;
+        ++c.launches;
+        if (c.fp64) em_velocity_kernel<double><<<grid_for(c.cap[s]), kThreads, 0, c.st>>>(push_args<double>(c, s), node_b<double>(c));
+        else em_velocity_kernel<float><<<grid_for(c.cap[s]), kThreads, 0, c.st>>>(push_args<float>(c, s), node_b<float>(c));
+        FOPIS_LAUNCH_CHECK();
+    }
+}
+
+// RootGrid::updateParticlePositionEM: J = 0 (Field::initializeCurrent), the
+// moves with their edge currents, then the periodic folds of the currents.
+void launch_em_position(Ctx& c) {
+    const size_t nx = (size_t)(c.cx - 1) * c.cy * c.cz, ny = (size_t)c.cx * (c.cy - 1) * c.cz,
+                 nz = (size_t)c.cx * c.cy * (c.cz - 1);
+    FOPIS_CUDA(cudaMemsetAsync(c.em.j[0], 0, sizeof(double) * nx, c.st));
+    FOPIS_CUDA(cudaMemsetAsync(c.em.j[1], 0, sizeof(double) * ny, c.st));
+    FOPIS_CUDA(cudaMemsetAsync(c.em.j[2], 0, sizeof(double) * nz, c.st));
+    const EdgeJ J{c.em.j[0], c.em.j[1], c.em.j[2], c.cx, c.cy, c.cz};
+    for (int s = 0; s < c.nsp; ++s) {
+        if (c.cap[s] == 0) continue;
+        const double q = c.p.species[s].charge * c.p.species[s].size;   // getChargeOfSuperParticle() / dt
+        ++c.launches;
+        if (c.fp64) em_position_kernel<double><<<grid_for(c.cap[s]), kThreads, 0, c.st>>>(push_args<double>(c, s), J, q);
+        else em_position_kernel<float><<<grid_for(c.cap[s]), kThreads, 0, c.st>>>(push_args<float>(c, s), J, q);
+        FOPIS_LAUNCH_CHECK();
+    }
+    em_fold_currents(c);
+}
 
 template <typename T>
 static SourceArgsT<T> source_args(Ctx& c, bool fused) {

@@ -21,6 +21,8 @@ Normalizer::Normalizer(double dx, double dt) : x(dx), t(dt) {
     V_unit = dx * dx * kMe / (kE * dt * dt);
     A_unit = kE / dt;
     eps0 = kEps0 * (std::pow(dx, 3.0) * kMe) / (kE * kE * dt * dt);   // Normalizer::normalizeEpsilon
+    mu0 = kMu0 * kE * kE / (kMe * dx);                                // Normalizer::normalizeMu
+    c = velocity(kClight);                                            // Normalizer::normalizeVelocity(c)
 }
 
 void calc_flux(double vth, double density_norm, double size, const double drift[3], const int injection_axis[6],
@@ -139,6 +141,11 @@ Input load_input(const std::string& path) {
         throw Error(FOPIS_ERR_ARG, "Unknown jobtype, neither ``new'' or ``load'', was inputted.");   // Initialize.cpp:97-99
     in.norm = Normalizer(in.dx, in.dt);
     const Normalizer& norm = in.norm;
+    const std::string solver = env.str_or("solver_type", "ES");
+    if (solver != "ES" && solver != "EM") throw Error(FOPIS_ERR_ARG, "solver_type " + solver + " is neither ES nor EM");
+    // Environment::checkCFLCondition (src/Misc/Environment.cpp:193-203) aborts an EM run
+    if (solver == "EM" && norm.c > 1.0)
+        throw Error(FOPIS_ERR_ARG, "Courant number exceeds 1.0 (c dt / dx = " + std::to_string(norm.c) + ")");
 
     std::vector<ParticleType> species;
     for (const auto& kv : js["Plasma"].items()) {        // std::map order, as picojson's
@@ -193,6 +200,8 @@ Input load_input(const std::string& path) {
     p.precision = FOPIS_MIXED;
     p.seed = 12345;
     p.energy_ev = norm.unenergy(1.0) / kE;   // Normalizer::unnormalizeEnergy(1, "eV")
+    p.solver = solver == "EM" ? FOPIS_SOLVER_EM : FOPIS_SOLVER_ES;
+    p.mu0 = norm.mu0;
 
     if (js.has("Object")) {
         const std::string base = dir_of(path);

@@ -5,6 +5,7 @@
 // C ABI (include/fopis_gpu.h); no device code lives here.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 #include <memory>
 #include <stdexcept>
@@ -19,12 +20,14 @@ namespace host {
 // Physical constants of include/normalizer.hpp.
 constexpr double kE = 1.60217733e-19;
 constexpr double kEps0 = 8.854187817e-12;
+constexpr double kMu0 = 4.0 * M_PI * 1.0e-7;
+constexpr double kClight = 2.99792458e8;
 constexpr double kMe = 9.1093818872e-31;
 
 // Normalizer (include/normalizer.hpp): x_unit = dx, t_unit = dt, m_unit = m_e, e_unit = e.
 struct Normalizer {
     double x = 1.0, t = 1.0, m = kMe, e = kE;
-    double V_unit = 1.0, A_unit = 1.0, eps0 = 1.0;
+    double V_unit = 1.0, A_unit = 1.0, eps0 = 1.0, mu0 = 1.0, c = 1.0;
     Normalizer() = default;
     Normalizer(double dx, double dt);
     double velocity(double v) const { return t * v / x; }

@@ -122,11 +122,21 @@ typedef struct fopis_params {
     int remove_interval;         /* removeInvalidParticles period (RootGrid.cpp:136-140); 0 -> 50 */
     double capacity_factor;      /* particle capacity / initial count; 0 -> 1.5 */
     int precision;               /* fopis_precision */
-    int reserved0;
+    int solver;                  /* fopis_solver: Environment::solver_type */
     uint64_t seed;               /* Philox key for loading, injection and emission */
     double energy_ev;            /* Normalizer::unnormalizeEnergy(1, "eV") = m_e dx^2 / (e dt^2): eV per
                                     normalised energy unit (secondary-emission yields); 0 without them */
+    double mu0;                  /* Normalizer::mu0 = mu0 e^2 / (m_e dx) (include/normalizer.hpp:219-221);
+                                    used by the EM solver only. Normalizer::c = 1/sqrt(eps0 mu0) must not
+                                    exceed 1 (Environment::checkCFLCondition, Environment.cpp:193-203) */
 } fopis_params;
+
+typedef enum fopis_solver {
+    FOPIS_SOLVER_ES = 0,   /* RootGrid::mainLoopES: Poisson solve each step */
+    FOPIS_SOLVER_EM = 1    /* RootGrid::mainLoopEM (RootGrid.cpp:145-191): FDTD on a Yee grid with
+                              damping layers of the grid's own size beyond every non-periodic face,
+                              charge-conserving (zigzag) edge currents */
+} fopis_solver;
 
 /* A voxel conductor; replaces the ObjectDataFromFile + Spacecraft construction
  * (src/Spacecraft/ObjectUtils.cpp:9-333, Spacecraft.cpp:16-152). */
@@ -154,7 +164,24 @@ typedef enum fopis_field {
     FOPIS_FIELD_EXREF = 2,   /* Field::exref (nodal E) */
     FOPIS_FIELD_EYREF = 3,
     FOPIS_FIELD_EZREF = 4,
-    FOPIS_FIELD_RHO_SPECIES = 16 /* + species id: Field::rho[1 + s] */
+    FOPIS_FIELD_BXREF = 5,   /* Field::bxref (nodal B, EM) */
+    FOPIS_FIELD_BYREF = 6,
+    FOPIS_FIELD_BZREF = 7,
+    FOPIS_FIELD_JXREF = 8,   /* Field::jxref (nodal current, EM; RootGrid::updateReferenceCurrent,
+                                RootGridField.cpp:1256-1285) */
+    FOPIS_FIELD_JYREF = 9,
+    FOPIS_FIELD_JZREF = 10,
+    FOPIS_FIELD_RHO_SPECIES = 16, /* + species id: Field::rho[1 + s] */
+    /* EM Yee arrays in their own extents (fopis_field_shape): */
+    FOPIS_FIELD_EX = 32,     /* Field::ex .. ez, edges, damping layers included */
+    FOPIS_FIELD_EY = 33,
+    FOPIS_FIELD_EZ = 34,
+    FOPIS_FIELD_BX = 35,     /* Field::bx .. bz, faces, damping layers included */
+    FOPIS_FIELD_BY = 36,
+    FOPIS_FIELD_BZ = 37,
+    FOPIS_FIELD_JX = 38,     /* Field::jx .. jz, edges of the glue grid */
+    FOPIS_FIELD_JY = 39,
+    FOPIS_FIELD_JZ = 40
 } fopis_field;
 
 typedef struct fopis_stats {
@@ -242,13 +269,16 @@ int fopis_sort_particles(void* ctx);
 
 /* ---- the ES step and its phases (RootGrid::mainLoopES order) ------------ */
 
-/* Grid::initialize (Grid.cpp:23-36): updateRho, solvePoisson, updateEfield. */
+/* Grid::initialize (Grid.cpp:23-36): updateRho, solvePoisson, updateEfield, and in
+ * the EM mode updateBfield. */
 int fopis_initialize(void* ctx);
 /* n calls of RootGrid::mainLoopES (RootGrid.cpp:82-143), fused: the push kernel
- * gathers, pushes, moves, applies boundaries and deposits in one pass. */
+ * gathers, pushes, moves, applies boundaries and deposits in one pass. With
+ * solver FOPIS_SOLVER_EM, n calls of RootGrid::mainLoopEM (RootGrid.cpp:145-191). */
 int fopis_step(void* ctx, int n);
 /* Phase entry points, for parity checks between phases. */
-int fopis_update_velocity(void* ctx);        /* Grid::updateParticleVelocityES (GridParticleTreatmentES.cpp:13-88) */
+int fopis_update_velocity(void* ctx);        /* Grid::updateParticleVelocityES (GridParticleTreatmentES.cpp:13-88);
+                                                EM: updateParticleVelocityEM (GridParticleTreatmentEM.cpp:13-105) */
 int fopis_emit_particles(void* ctx);         /* RootGrid::emitParticlesFromObjects (RootGridObject.cpp:175-181) */
 /* Spacecraft::incident_events (SecondaryEmission.cpp:14-33): the hits recorded by the last
  * absorption, consumed by the next emission. One record of FOPIS_INCIDENT_DOUBLES doubles:
@@ -259,12 +289,17 @@ int fopis_emit_particles(void* ctx);         /* RootGrid::emitParticlesFromObjec
 #define FOPIS_INCIDENT_DOUBLES 10
 int fopis_get_incidents(void* ctx, double* records, int64_t cap, int64_t* n);
 int fopis_set_incidents(void* ctx, const double* records, int64_t n);
-int fopis_update_position(void* ctx);        /* RootGrid::updateParticlePositionES (GridParticleTreatmentES.cpp:90-181) */
+int fopis_update_position(void* ctx);        /* RootGrid::updateParticlePositionES (GridParticleTreatmentES.cpp:90-181);
+                                                EM: updateParticlePositionEM with the edge currents
+                                                (GridParticleTreatmentEM.cpp:107-201) */
 int fopis_inject_particles(void* ctx);       /* RootGrid::injectParticlesFromBoundary (RootGridParticle.cpp:3-130) */
 int fopis_update_rho(void* ctx);             /* RootGrid::updateRho (RootGridField.cpp:1153-1252), incl. the
                                                 first solve and Spacecraft::redistributeCharge when objects exist */
 int fopis_solve_poisson(void* ctx);          /* RootGrid::solvePoisson (RootGridField.cpp:41-63) */
-int fopis_update_efield(void* ctx);          /* RootGrid::updateEfield + updateReferenceEfield (RootGridField.cpp:456-582) */
+int fopis_update_efield(void* ctx);          /* ES: RootGrid::updateEfield + updateReferenceEfield (RootGridField.cpp:456-582);
+                                                EM: RootGrid::updateEfieldFDTD (damping form, :584-710) */
+int fopis_update_bfield(void* ctx);          /* EM: RootGrid::updateBfield (damping form, RootGridField.cpp:589-820)
+                                                and updateReferenceBfield (:1102-1127); FOPIS_ERR_STATE in ES */
 int fopis_remove_invalid_particles(void* ctx); /* Grid::removeInvalidParticles */
 /* Ends a step driven through the phase entry points: ++Environment::timestep
  * (src/main.cpp:33), which keys the Philox draws of injection and emission. */
@@ -281,10 +316,19 @@ int fopis_set_injection_carry(void* ctx, const double* carry, int n);
 
 /* ---- fields and diagnostics --------------------------------------------- */
 
-/* Copies a node field out in the reference layout (n = (nx+2)(ny+2)(nz+2)). */
+/* Copies a field out in the reference's C order [i][j][k] over its own extent:
+ * n = (nx+2)(ny+2)(nz+2) for node fields, the product of fopis_field_shape's
+ * extents for the EM Yee arrays (FOPIS_FIELD_EX .. JZ). */
 int fopis_get_field(void* ctx, int which, double* out, size_t n);
-/* Overwrites PHI or RHO0 (for solver-only use and warm starts). */
+/* Overwrites PHI or RHO0 (for solver-only use and warm starts) or, in the EM
+ * mode, one Yee array or edge current (EX .. JZ: initial fields of a run or a
+ * resume; the next position update recomputes J). */
 int fopis_set_field(void* ctx, int which, const double* in, size_t n);
+/* First index (the multi_array index base: below 0 on axes with damping
+ * layers) and extent per axis of a field. */
+int fopis_field_shape(void* ctx, int which, int lo[3], int n[3]);
+/* Field::getBfieldEnergy (src/Grid/Field.cpp:215-234), normalised; 0 in ES. */
+int fopis_get_bfield_energy(void* ctx, double* energy);
 /* Grid::getParticleEnergy (GridParticleTreatment.cpp:104-118) and
  * Field::getEfieldEnergy (Field.cpp:194-213), normalised. */
 int fopis_get_energy(void* ctx, double* particle_energy, double* efield_energy);

@@ -99,6 +99,25 @@ struct Arr3 {
     void zero() { std::fill(v.begin(), v.end(), 0.0); }
 };
 
+// boost::multi_array with index bases: the EM Yee arrays extended by the damping
+// layers (RootGrid::initializeField, src/Grid/RootGrid/RootGridField.cpp:7-39).
+struct ArrB {
+    int lo[3] = {0, 0, 0}, n[3] = {0, 0, 0};
+    std::vector<double> v;
+    void resize(int l0, int u0, int l1, int u1, int l2, int u2) {   // half-open [l, u)
+        lo[0] = l0; lo[1] = l1; lo[2] = l2;
+        n[0] = u0 - l0; n[1] = u1 - l1; n[2] = u2 - l2;
+        v.assign((size_t)n[0] * n[1] * n[2], 0.0);
+    }
+    inline double& operator()(int i, int j, int k) {
+        return v[((size_t)(i - lo[0]) * n[1] + (j - lo[1])) * n[2] + (k - lo[2])];
+    }
+    inline double operator()(int i, int j, int k) const {
+        return v[((size_t)(i - lo[0]) * n[1] + (j - lo[1])) * n[2] + (k - lo[2])];
+    }
+    int up(int a) const { return lo[a] + n[a]; }   // one past the last index
+};
+
 // include/particle.hpp:14-20 — 56 bytes.
 struct Particle {
     double x, y, z;
@@ -176,6 +195,12 @@ struct Ctx {
     int last_iterations = 0;
     double last_residual = 0.0;
     int64_t injected_step = 0, emitted_step = 0, absorbed_step = 0;
+    // EM mode (Environment::solver_type == "EM"): Yee E and B with damping layers,
+    // edge currents, nodal B
+    bool em = false;
+    int L[3] = {1, 1, 1};        // Environment::damping_length (L_dx, L_dy, L_dz)
+    ArrB fex, fey, fez, fbx, fby, fbz;
+    Arr3 jx, jy, jz, bxref, byref, bzref;
     char err[256] = {0};
 };
 
@@ -211,6 +236,31 @@ static void init_ctx(Ctx& c, const fopis_params* p) {
     c.eyref.resize(c.cx, c.cy, c.cz);
     c.ezref.resize(c.cx, c.cy, c.cz);
     c.inject_residual.assign(c.nsp, {0, 0, 0, 0, 0, 0});
+    c.em = p->solver == FOPIS_SOLVER_EM;
+    if (c.em) {
+        // RootGrid::initializeField (RootGridField.cpp:7-39): damping length = node count per
+        // axis, the arrays reach that far beyond every non-periodic face.
+        c.L[0] = c.nx; c.L[1] = c.ny; c.L[2] = c.nz;
+        const int cc[3] = {c.cx, c.cy, c.cz};
+        int lo[3], up[3];
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = isBoundary(c, a, 0) ? -c.L[a] : 0;
+            up[a] = isBoundary(c, a, 1) ? cc[a] + c.L[a] : cc[a];
+        }
+        c.fex.resize(lo[0], up[0] - 1, lo[1], up[1], lo[2], up[2]);
+        c.fey.resize(lo[0], up[0], lo[1], up[1] - 1, lo[2], up[2]);
+        c.fez.resize(lo[0], up[0], lo[1], up[1], lo[2], up[2] - 1);
+        c.fbx.resize(lo[0], up[0], lo[1], up[1] - 1, lo[2], up[2] - 1);
+        c.fby.resize(lo[0], up[0] - 1, lo[1], up[1], lo[2], up[2] - 1);
+        c.fbz.resize(lo[0], up[0] - 1, lo[1], up[1] - 1, lo[2], up[2]);
+        // Grid::initializeField (src/Grid/Grid.cpp:170-194): edge currents, nodal B
+        c.jx.resize(c.cx - 1, c.cy, c.cz);
+        c.jy.resize(c.cx, c.cy - 1, c.cz);
+        c.jz.resize(c.cx, c.cy, c.cz - 1);
+        c.bxref.resize(c.cx, c.cy, c.cz);
+        c.byref.resize(c.cx, c.cy, c.cz);
+        c.bzref.resize(c.cx, c.cy, c.cz);
+    }
 }
 
 // ---------------------------------------------------------------- halo semantics
@@ -903,6 +953,352 @@ static void update_efield(Ctx& c) {
     copy_field_glue(c, c.ezref);
 }
 
+// ---------------------------------------------------------------- EM mode
+// Communicator::sendRecvFieldX/Y/Z self branch on an array with index bases
+// (src/MPI/Communicator.cpp:265-343): along a periodic axis (base 0 there)
+// index 0 <- index max-2, index max-1 <- index 1, over the whole extent of the
+// other two axes; x, then y, then z.
+static void copy_field_glue_b(const Ctx& c, ArrB& a) {
+    for (int axis = 0; axis < 3; ++axis) {
+        if (!c.notb[2 * axis]) continue;
+        const int a1 = axis == 0 ? 1 : 0, a2 = axis == 2 ? 1 : 2;
+        const int m = a.up(axis);
+        for (int u = a.lo[a1]; u < a.up(a1); ++u)
+            for (int w = a.lo[a2]; w < a.up(a2); ++w) {
+                int p0[3], p1[3], pm2[3], pm1[3];
+                p0[a1] = p1[a1] = pm2[a1] = pm1[a1] = u;
+                p0[a2] = p1[a2] = pm2[a2] = pm1[a2] = w;
+                p0[axis] = 0; p1[axis] = 1; pm2[axis] = m - 2; pm1[axis] = m - 1;
+                const double lo = a(p1[0], p1[1], p1[2]);
+                a(p0[0], p0[1], p0[2]) = a(pm2[0], pm2[1], pm2[2]);
+                a(pm1[0], pm1[1], pm1[2]) = lo;
+            }
+    }
+}
+
+// MPIw::Environment::sendRecvEdgeScalar (src/MPI/Environment.cpp:74-130) with
+// Communicator::sendRecvScalarX/Y/Z's self branch (Communicator.cpp:497-574):
+// along each periodic axis the glue planes g-1-t and size-1-t (t < g) both
+// become their sum, g = 2 along the current's own direction, 1 across it.
+static void fold_edge_scalar(const Ctx& c, Arr3& a, int dir) {
+    const int dims[3] = {a.cx, a.cy, a.cz};
+    for (int axis = 0; axis < 3; ++axis) {
+        if (!c.notb[2 * axis]) continue;
+        const int g = axis == dir ? 2 : 1, size = dims[axis];
+        const int a1 = axis == 0 ? 1 : 0, a2 = axis == 2 ? 1 : 2;
+        for (int u = 0; u < dims[a1]; ++u)
+            for (int w = 0; w < dims[a2]; ++w)
+                for (int t = 0; t < g; ++t) {
+                    int pl[3], pu[3];
+                    pl[a1] = pu[a1] = u; pl[a2] = pu[a2] = w;
+                    pl[axis] = g - 1 - t; pu[axis] = size - 1 - t;
+                    const double s = a(pl[0], pl[1], pl[2]) + a(pu[0], pu[1], pu[2]);
+                    a(pl[0], pl[1], pl[2]) = s; a(pu[0], pu[1], pu[2]) = s;
+                }
+    }
+}
+
+// RootGrid::updateReferenceEfield (RootGridField.cpp:489-582) on the Yee edges
+// of the EM mode: nodal means of the two edges, the one-sided phi difference on
+// the node next to a non-periodic face and zero on its glue node.
+static void reference_efield_em(Ctx& c) {
+    const int X = c.cx, Y = c.cy, Z = c.cz;
+    Arr3& phi = c.phi;
+    for (int i = 1; i < X - 1; ++i)
+        for (int j = 1; j < Y - 1; ++j)
+            for (int k = 1; k < Z - 1; ++k) {
+                c.exref(i, j, k) = 0.5 * (c.fex(i - 1, j, k) + c.fex(i, j, k));
+                c.eyref(i, j, k) = 0.5 * (c.fey(i, j - 1, k) + c.fey(i, j, k));
+                c.ezref(i, j, k) = 0.5 * (c.fez(i, j, k - 1) + c.fez(i, j, k));
+            }
+    if (isBoundary(c, 0, 0))
+        for (int j = 1; j < Y - 1; ++j) for (int k = 1; k < Z - 1; ++k) {
+            c.exref(0, j, k) = 0.0;
+            c.exref(1, j, k) = 0.5 * (phi(3, j, k) - 4.0 * phi(2, j, k) + 3.0 * phi(1, j, k));
+        }
+    if (isBoundary(c, 0, 1))
+        for (int j = 1; j < Y - 1; ++j) for (int k = 1; k < Z - 1; ++k) {
+            c.exref(X - 1, j, k) = 0.0;
+            c.exref(X - 2, j, k) = 0.5 * (-phi(X - 4, j, k) + 4.0 * phi(X - 3, j, k) - 3.0 * phi(X - 2, j, k));
+        }
+    if (isBoundary(c, 1, 0))
+        for (int i = 1; i < X - 1; ++i) for (int k = 1; k < Z - 1; ++k) {
+            c.eyref(i, 0, k) = 0.0;
+            c.eyref(i, 1, k) = 0.5 * (phi(i, 3, k) - 4.0 * phi(i, 2, k) + 3.0 * phi(i, 1, k));
+        }
+    if (isBoundary(c, 1, 1))
+        for (int i = 1; i < X - 1; ++i) for (int k = 1; k < Z - 1; ++k) {
+            c.eyref(i, Y - 1, k) = 0.0;
+            c.eyref(i, Y - 2, k) = 0.5 * (-phi(i, Y - 4, k) + 4.0 * phi(i, Y - 3, k) - 3.0 * phi(i, Y - 2, k));
+        }
+    if (isBoundary(c, 2, 0))
+        for (int i = 1; i < X - 1; ++i) for (int j = 1; j < Y - 1; ++j) {
+            c.ezref(i, j, 0) = 0.0;
+            c.ezref(i, j, 1) = 0.5 * (phi(i, j, 3) - 4.0 * phi(i, j, 2) + 3.0 * phi(i, j, 1));
+        }
+    if (isBoundary(c, 2, 1))
+        for (int i = 1; i < X - 1; ++i) for (int j = 1; j < Y - 1; ++j) {
+            c.ezref(i, j, Z - 1) = 0.0;
+            c.ezref(i, j, Z - 2) = 0.5 * (-phi(i, j, Z - 4) + 4.0 * phi(i, j, Z - 3) - 3.0 * phi(i, j, Z - 2));
+        }
+    copy_field_glue(c, c.exref);
+    copy_field_glue(c, c.eyref);
+    copy_field_glue(c, c.ezref);
+}
+
+// RootGrid::updateEfield (RootGridField.cpp:456-487) in the EM mode: the edges of
+// the real grid from phi (the damping layers keep their values), then the
+// nodal reference.
+static void update_efield_em_from_phi(Ctx& c) {
+    const int X = c.cx, Y = c.cy, Z = c.cz;
+    const Arr3& phi = c.phi;
+    for (int i = 0; i < X; ++i)
+        for (int j = 0; j < Y; ++j)
+            for (int k = 0; k < Z; ++k) {
+                if (i < X - 1) c.fex(i, j, k) = phi(i, j, k) - phi(i + 1, j, k);
+                if (j < Y - 1) c.fey(i, j, k) = phi(i, j, k) - phi(i, j + 1, k);
+                if (k < Z - 1) c.fez(i, j, k) = phi(i, j, k) - phi(i, j, k + 1);
+            }
+    reference_efield_em(c);
+}
+
+// RootGrid::updateReferenceBfield (RootGridField.cpp:1102-1127): nodal means of
+// the four faces around each node, then the periodic glue copies.
+static void reference_bfield(Ctx& c) {
+    const int X = c.cx, Y = c.cy, Z = c.cz;
+    for (int i = 1; i < X - 1; ++i)
+        for (int j = 1; j < Y - 1; ++j)
+            for (int k = 1; k < Z - 1; ++k) {
+                c.bxref(i, j, k) = 0.25 * (c.fbx(i, j, k) + c.fbx(i, j - 1, k) + c.fbx(i, j, k - 1) + c.fbx(i, j - 1, k - 1));
+                c.byref(i, j, k) = 0.25 * (c.fby(i, j, k) + c.fby(i - 1, j, k) + c.fby(i, j, k - 1) + c.fby(i - 1, j, k - 1));
+                c.bzref(i, j, k) = 0.25 * (c.fbz(i, j, k) + c.fbz(i - 1, j, k) + c.fbz(i, j - 1, k) + c.fbz(i - 1, j - 1, k));
+            }
+    copy_field_glue(c, c.bxref);
+    copy_field_glue(c, c.byref);
+    copy_field_glue(c, c.bzref);
+}
+
+// The damping mask of updateEfieldFDTDDamping / updateBfieldDamping
+// (RootGridField.cpp:628-642, 742-756): 1 - (d/L)^2 with d the distance of an
+// index from the real grid [1, real-2] (masking_parameter 1).
+static inline double damp1(double r, double L, int real) {
+    const double d = (r <= 0) ? -r + 1 : (r >= real - 1) ? r - static_cast<double>(real) + 2.0 : 0.0;
+    return 1.0 - std::pow(1.0 * d / L, 2);
+}
+static inline double damp(const Ctx& c, int i, int j, int k) {
+    return damp1(i, c.L[0], c.cx) * damp1(j, c.L[1], c.cy) * damp1(k, c.L[2], c.cz);
+}
+static inline bool real_region(const Ctx& c, int i, int j, int k) {
+    return i > 0 && i < c.cx - 1 && j > 0 && j < c.cy - 1 && k > 0 && k < c.cz - 1;
+}
+
+// RootGrid::updateEfieldFDTDDamping (RootGridField.cpp:594-710): E += dt/eps0
+// (curl B / mu0 - J) on the real edges, the damped update without J on the
+// last real edge of each direction and throughout the damping layers, then the
+// periodic glue copies and the nodal reference.
+static void update_efield_fdtd(Ctx& c) {
+    ArrB &ex = c.fex, &ey = c.fey, &ez = c.fez;
+    const ArrB &bx = c.fbx, &by = c.fby, &bz = c.fbz;
+    const double dte = 1.0 / c.p.eps0;              // dt / eps0, dt = 1
+    const double C = dte / (c.p.mu0 * 1.0);        // dt / (mu0 eps0 dx)
+    const int i0 = ex.lo[0] + 1, i1 = ex.up(0), j0 = ex.lo[1] + 1, j1 = ex.up(1) - 1;
+    const int k0 = ex.lo[2] + 1, k1 = ex.up(2) - 1;
+    const int xmax = ex.up(0) + 1, ymax = ex.up(1), zmax = ex.up(2);   // max_x/y/z_index
+#pragma omp parallel for schedule(static)
+    for (int i = i0; i < i1; ++i)
+        for (int j = j0; j < j1; ++j)
+            for (int k = k0; k < k1; ++k) {
+                const double cx_ = bz(i, j, k) - bz(i, j - 1, k) - by(i, j, k) + by(i, j, k - 1);
+                if (real_region(c, i, j, k)) {
+                    if (i < c.cx - 2) ex(i, j, k) = ex(i, j, k) - c.jx(i, j, k) * dte + C * cx_;
+                    else ex(i, j, k) = 0.5 * (damp(c, i, j, k) + damp(c, i + 1, j, k)) * (ex(i, j, k) + C * cx_);
+                } else if (i < xmax - 2) {
+                    ex(i, j, k) = 0.5 * (damp(c, i, j, k) + damp(c, i + 1, j, k)) * (ex(i, j, k) + C * cx_);
+                }
+            }
+#pragma omp parallel for schedule(static)
+    for (int i = i0; i < i1; ++i)
+        for (int j = j0; j < j1; ++j)
+            for (int k = k0; k < k1; ++k) {
+                const double cy_ = bx(i, j, k) - bx(i, j, k - 1) - bz(i, j, k) + bz(i - 1, j, k);
+                const double cz_ = by(i, j, k) - by(i - 1, j, k) - bx(i, j, k) + bx(i, j - 1, k);
+                if (real_region(c, i, j, k)) {
+                    if (j < c.cy - 2) ey(i, j, k) = ey(i, j, k) - c.jy(i, j, k) * dte + C * cy_;
+                    else ey(i, j, k) = 0.5 * (damp(c, i, j, k) + damp(c, i, j + 1, k)) * (ey(i, j, k) + C * cy_);
+                    if (k < c.cz - 2) ez(i, j, k) = ez(i, j, k) - c.jz(i, j, k) * dte + C * cz_;
+                    else ez(i, j, k) = 0.5 * (damp(c, i, j, k) + damp(c, i, j, k + 1)) * (ez(i, j, k) + C * cz_);
+                } else {
+                    if (j < ymax - 2)
+                        ey(i, j, k) = 0.5 * (damp(c, i, j, k) + damp(c, i, j + 1, k)) * (ey(i, j, k) + C * cy_);
+                    if (k < zmax - 2)
+                        ez(i, j, k) = 0.5 * (damp(c, i, j, k) + damp(c, i, j, k + 1)) * (ez(i, j, k) + C * cz_);
+                }
+            }
+    copy_field_glue_b(c, ex);
+    copy_field_glue_b(c, ey);
+    copy_field_glue_b(c, ez);
+    reference_efield_em(c);
+}
+
+// RootGrid::updateBfieldDamping (RootGridField.cpp:712-820): B -= dt curl E / dx on
+// the real faces, damped on the last real face and in the damping layers,
+// then the periodic glue copies and the nodal reference.
+static void update_bfield(Ctx& c) {
+    ArrB &bx = c.fbx, &by = c.fby, &bz = c.fbz;
+    const ArrB &ex = c.fex, &ey = c.fey, &ez = c.fez;
+    const double d = 1.0;                           // dt / dx
+    const int xmax = bx.up(0), ymax = bx.up(1) + 1, zmax = bx.up(2) + 1;   // max_x/y/z_index
+    const int X = c.cx, Y = c.cy, Z = c.cz;
+#pragma omp parallel for schedule(static)
+    for (int i = bx.lo[0] + 1; i < xmax - 1; ++i)
+        for (int j = bx.lo[1] + 1; j < ymax - 1; ++j)
+            for (int k = bx.lo[2] + 1; k < zmax - 1; ++k) {
+                const double gx = (ey(i, j, k + 1) - ey(i, j, k)) - (ez(i, j + 1, k) - ez(i, j, k));
+                const double gy = (ez(i + 1, j, k) - ez(i, j, k)) - (ex(i, j, k + 1) - ex(i, j, k));
+                const double gz = (ex(i, j + 1, k) - ex(i, j, k)) - (ey(i + 1, j, k) - ey(i, j, k));
+                const double mx = 0.25 * (damp(c, i, j, k) + damp(c, i, j + 1, k) + damp(c, i, j, k + 1) + damp(c, i, j + 1, k + 1));
+                const double my = 0.25 * (damp(c, i, j, k) + damp(c, i + 1, j, k) + damp(c, i, j, k + 1) + damp(c, i + 1, j, k + 1));
+                const double mz = 0.25 * (damp(c, i, j, k) + damp(c, i + 1, j, k) + damp(c, i, j + 1, k) + damp(c, i + 1, j + 1, k));
+                if (real_region(c, i, j, k)) {
+                    if (j != Y - 2 && k != Z - 2) bx(i, j, k) = bx(i, j, k) + d * gx;
+                    else bx(i, j, k) = mx * (bx(i, j, k) + d * gx);
+                    if (i != X - 2 && k != Z - 2) by(i, j, k) = by(i, j, k) + d * gy;
+                    else by(i, j, k) = my * (by(i, j, k) + d * gy);
+                    if (i != X - 2 && j != Y - 2) bz(i, j, k) = bz(i, j, k) + d * gz;
+                    else bz(i, j, k) = mz * (bz(i, j, k) + d * gz);
+                } else {
+                    if (j != ymax - 2 && k != zmax - 2) bx(i, j, k) = mx * (bx(i, j, k) + d * gx);
+                    if (i != xmax - 2 && k != zmax - 2) by(i, j, k) = my * (by(i, j, k) + d * gy);
+                    if (i != xmax - 2 && j != ymax - 2) bz(i, j, k) = mz * (bz(i, j, k) + d * gz);
+                }
+            }
+    copy_field_glue_b(c, bx);
+    copy_field_glue_b(c, by);
+    copy_field_glue_b(c, bz);
+    reference_bfield(c);
+}
+
+// Grid::updateParticleVelocityEM (src/Grid/GridParticleTreatmentEM.cpp:13-105):
+// CIC gather of the nodal E and B, both scaled by 0.5 q/m, and the Boris
+// kick/rotate/kick with the gathered b (boris = 2 / (1 + |b|^2)).
+static void update_velocity_em(Ctx& c) {
+    for (int pid = 0; pid < c.nsp; ++pid) {
+        const double qm = 0.5 * c.p.species[pid].charge / c.p.species[pid].mass;
+        auto& parray = c.particles[pid];
+        const long n = (long)parray.size();
+#pragma omp parallel for schedule(static)
+        for (long pn = 0; pn < n; ++pn) {
+            Particle& p = parray[pn];
+            if (!p.isValid) continue;
+            Pos pos = posXYZ(p.x, p.y, p.z);
+            const int i = pos.i, j = pos.j, k = pos.k;
+            const double v1 = qm * pos.dx2 * pos.dy2 * pos.dz2, v2 = qm * pos.dx1 * pos.dy2 * pos.dz2;
+            const double v3 = qm * pos.dx2 * pos.dy1 * pos.dz2, v4 = qm * pos.dx1 * pos.dy1 * pos.dz2;
+            const double v5 = qm * pos.dx2 * pos.dy2 * pos.dz1, v6 = qm * pos.dx1 * pos.dy2 * pos.dz1;
+            const double v7 = qm * pos.dx2 * pos.dy1 * pos.dz1, v8 = qm * pos.dx1 * pos.dy1 * pos.dz1;
+            auto g = [&](const Arr3& e) {
+                return v1 * e(i, j, k) + v2 * e(i + 1, j, k) + v3 * e(i, j + 1, k) + v4 * e(i + 1, j + 1, k) +
+                       v5 * e(i, j, k + 1) + v6 * e(i + 1, j, k + 1) + v7 * e(i, j + 1, k + 1) +
+                       v8 * e(i + 1, j + 1, k + 1);
+            };
+            const double exv = g(c.exref), eyv = g(c.eyref), ezv = g(c.ezref);
+            const double bx = g(c.bxref), by = g(c.byref), bz = g(c.bzref);
+            const double boris = 2.0 / (1.0 + (bx * bx + by * by + bz * bz));
+            const double vx1 = p.vx + exv, vy1 = p.vy + eyv, vz1 = p.vz + ezv;
+            const double vxt = vx1 + vy1 * bz - vz1 * by;
+            const double vyt = vy1 + vz1 * bx - vx1 * bz;
+            const double vzt = vz1 + vx1 * by - vy1 * bx;
+            p.vx = vx1 + exv + boris * (vyt * bz - vzt * by);
+            p.vy = vy1 + eyv + boris * (vzt * bx - vxt * bz);
+            p.vz = vz1 + ezv + boris * (vxt * by - vyt * bx);
+        }
+    }
+}
+
+// Position::getReferencePosition (include/position.hpp:88-96): the zigzag's
+// relay point, on the shared cell face when the cells differ, else the midpoint.
+static inline double relay(int i_new, int i_old, double x_new, double x_old) {
+    return std::min(static_cast<double>(std::min(i_new, i_old)),
+                    std::max(static_cast<double>(std::max(i_new, i_old)) - 1.0, 0.5 * (x_new + x_old)));
+}
+
+// One half of the charge-conserving current of Particle::distributeCurrentAt
+// OldPosition / AtNewPosition (src/Particle/particle.cpp:258-338): flux f on
+// the edges of the cell of `at`, weights w = mean of the half's two points
+// minus the cell's lower node.
+static void current_half(Ctx& c, const Pos& at, const double f[3], const double w[3]) {
+    const int i = at.i, j = at.j, k = at.k;
+    c.jx(i, j, k) += f[0] * (1.0 - w[1]) * (1.0 - w[2]);
+    c.jx(i, j + 1, k) += f[0] * w[1] * (1.0 - w[2]);
+    c.jx(i, j, k + 1) += f[0] * (1.0 - w[1]) * w[2];
+    c.jx(i, j + 1, k + 1) += f[0] * w[1] * w[2];
+    c.jy(i, j, k) += f[1] * (1.0 - w[0]) * (1.0 - w[2]);
+    c.jy(i + 1, j, k) += f[1] * w[0] * (1.0 - w[2]);
+    c.jy(i, j, k + 1) += f[1] * (1.0 - w[0]) * w[2];
+    c.jy(i + 1, j, k + 1) += f[1] * w[0] * w[2];
+    c.jz(i, j, k) += f[2] * (1.0 - w[0]) * (1.0 - w[1]);
+    c.jz(i + 1, j, k) += f[2] * w[0] * (1.0 - w[1]);
+    c.jz(i, j + 1, k) += f[2] * (1.0 - w[0]) * w[1];
+    c.jz(i + 1, j + 1, k) += f[2] * w[0] * w[1];
+}
+
+// RootGrid::updateParticlePositionEM (src/Grid/GridParticleTreatmentEM.cpp:107-201):
+// J = 0 (Field::initializeCurrent), for every valid particle the old-cell half
+// of the current (from x to x + v), the move and the boundary rules, and for a
+// particle still valid the new-cell half (from x - v to x, in the wrapped frame
+// after a periodic crossing); then the periodic folds of the edge currents.
+// The single-rank migration appends crossing particles in the reference;
+// wrapping them in place leaves the same set and the same sums.
+static void update_position_em(Ctx& c) {
+    c.jx.zero(); c.jy.zero(); c.jz.zero();
+    const double slx = c.nx, sly = c.ny, slz = c.nz;
+    for (int pid = 0; pid < c.nsp; ++pid) {
+        const double q = c.p.species[pid].charge * c.p.species[pid].size / 1.0;   // per dt
+        for (auto& p : c.particles[pid]) {
+            if (!p.isValid) continue;
+            {
+                const Pos o = posXYZ(p.x, p.y, p.z);
+                const Pos nw = posXYZ(p.x + p.vx, p.y + p.vy, p.z + p.vz);
+                const Pos r = posXYZ(relay(nw.i, o.i, nw.x, o.x), relay(nw.j, o.j, nw.y, o.y), relay(nw.k, o.k, nw.z, o.z));
+                const double f[3] = {q * (r.x - o.x), q * (r.y - o.y), q * (r.z - o.z)};
+                const double w[3] = {0.5 * (r.x + o.x) - (static_cast<double>(o.i) - 1.0),
+                                     0.5 * (r.y + o.y) - (static_cast<double>(o.j) - 1.0),
+                                     0.5 * (r.z + o.z) - (static_cast<double>(o.k) - 1.0)};
+                current_half(c, o, f, w);
+            }
+            p.x += p.vx; p.y += p.vy; p.z += p.vz;
+            boundary_axis(c, p.x, p.isValid, 0, slx);
+            boundary_axis(c, p.y, p.isValid, 1, sly);
+            boundary_axis(c, p.z, p.isValid, 2, slz);
+            if (p.isValid) {
+                const Pos o = posXYZ(p.x - p.vx, p.y - p.vy, p.z - p.vz);
+                const Pos nw = posXYZ(p.x, p.y, p.z);
+                const Pos r = posXYZ(relay(nw.i, o.i, nw.x, o.x), relay(nw.j, o.j, nw.y, o.y), relay(nw.k, o.k, nw.z, o.z));
+                const double f[3] = {q * (nw.x - r.x), q * (nw.y - r.y), q * (nw.z - r.z)};
+                const double w[3] = {0.5 * (r.x + nw.x) - (static_cast<double>(nw.i) - 1.0),
+                                     0.5 * (r.y + nw.y) - (static_cast<double>(nw.j) - 1.0),
+                                     0.5 * (r.z + nw.z) - (static_cast<double>(nw.k) - 1.0)};
+                current_half(c, nw, f, w);
+            }
+        }
+    }
+    fold_edge_scalar(c, c.jx, 0);
+    fold_edge_scalar(c, c.jy, 1);
+    fold_edge_scalar(c, c.jz, 2);
+}
+
+// Field::getBfieldEnergy (src/Grid/Field.cpp:215-234), normalised.
+static double bfield_energy(const Ctx& c) {
+    const int X = c.cx, Y = c.cy, Z = c.cz;
+    double en = 0.0;
+    for (int i = 1; i < X - 1; ++i) for (int j = 1; j < Y - 1; ++j) for (int k = 1; k < Z - 1; ++k) {
+        if (j < Y - 2 && k < Z - 2) en += std::pow(c.fbx(i, j, k), 2);
+        if (i < X - 2 && k < Z - 2) en += std::pow(c.fby(i, j, k), 2);
+        if (i < X - 2 && j < Y - 2) en += std::pow(c.fbz(i, j, k), 2);
+    }
+    return 0.5 * en / c.p.mu0;
+}
+
 // ---------------------------------------------------------------- sources
 static inline double max_extent(const Ctx& c, int axis) {
     const int n = axis == 0 ? c.nx : (axis == 1 ? c.ny : c.nz);
@@ -1242,8 +1638,24 @@ static void reset_objects(Ctx& c) {
     for (auto& o : c.objects) std::fill(o.current.begin(), o.current.end(), 0.0);
 }
 
+// RootGrid::mainLoopEM (src/Grid/RootGrid/RootGrid.cpp:145-191).
+static int main_loop_em(Ctx& c) {
+    reset_objects(c);
+    update_velocity_em(c);
+    int bad = emit_all(c);
+    update_position_em(c);
+    inject(c, nullptr);
+    bad |= update_rho(c);
+    update_efield_fdtd(c);
+    update_bfield(c);
+    if (c.timestep % 50 == 0) remove_invalid(c);
+    ++c.timestep;
+    return bad;
+}
+
 // RootGrid::mainLoopES (src/Grid/RootGrid/RootGrid.cpp:82-143).
 static int main_loop(Ctx& c) {
+    if (c.em) return main_loop_em(c);
     reset_objects(c);
     update_velocity(c);
     int bad = emit_all(c);
@@ -1526,7 +1938,10 @@ int64_t orc_get_particles(void* h, int s, void* aos, int64_t cap) {
 void orc_generate_ambient(void* h) { generate_ambient(*(Ctx*)h); }
 
 void orc_reset_objects(void* h) { reset_objects(*(Ctx*)h); }
-void orc_update_velocity(void* h) { update_velocity(*(Ctx*)h); }
+void orc_update_velocity(void* h) {
+    Ctx* c = (Ctx*)h;
+    if (c->em) update_velocity_em(*c); else update_velocity(*c);
+}
 int orc_emit(void* h) { return emit_all(*(Ctx*)h); }
 // The pending incident list as records of 10 doubles (object, species, axis,
 // remaining time, x, y, z, vx, vy, vz), the layout of fopis_get_incidents.
@@ -1549,11 +1964,19 @@ void orc_set_incidents(void* h, const double* in, int64_t n) {
         c->incidents.push_back(Incident{(int)r[0], (int)r[1], (int)r[2], r[3], r[4], r[5], r[6], r[7], r[8], r[9]});
     }
 }
-void orc_update_position(void* h) { update_position(*(Ctx*)h); }
+void orc_update_position(void* h) {
+    Ctx* c = (Ctx*)h;
+    if (c->em) update_position_em(*c); else update_position(*c);
+}
 void orc_inject(void* h, int64_t* counts) { inject(*(Ctx*)h, counts); }
 int orc_update_rho(void* h) { return update_rho(*(Ctx*)h); }
 void orc_solve_poisson(void* h) { solve_poisson(*(Ctx*)h); }
-void orc_update_efield(void* h) { update_efield(*(Ctx*)h); }
+void orc_update_efield(void* h) {
+    Ctx* c = (Ctx*)h;
+    if (c->em) update_efield_fdtd(*c); else update_efield(*c);
+}
+void orc_update_bfield(void* h) { if (((Ctx*)h)->em) update_bfield(*(Ctx*)h); }
+double orc_bfield_energy(void* h) { return ((Ctx*)h)->em ? bfield_energy(*(Ctx*)h) : 0.0; }
 void orc_remove_invalid(void* h) { remove_invalid(*(Ctx*)h); }
 int orc_main_loop(void* h, int n) { int bad = 0; for (int t = 0; t < n; ++t) bad |= main_loop(*(Ctx*)h); return bad; }
 // Grid::initialize (src/Grid/Grid.cpp:23-36).
@@ -1561,7 +1984,12 @@ int orc_initialize(void* h) {
     Ctx* c = (Ctx*)h;
     int bad = update_rho(*c);
     solve_poisson(*c);
-    update_efield(*c);
+    if (c->em) {
+        update_efield_em_from_phi(*c);
+        update_bfield(*c);
+    } else {
+        update_efield(*c);
+    }
     return bad;
 }
 void orc_set_timestep(void* h, int64_t t) { ((Ctx*)h)->timestep = t; }
@@ -1570,9 +1998,41 @@ void orc_step_counts(void* h, int64_t* injected, int64_t* emitted, int64_t* abso
     Ctx* c = (Ctx*)h; *injected = c->injected_step; *emitted = c->emitted_step; *absorbed = c->absorbed_step;
 }
 
-// which: 0 phi, 1 rho0, 2..4 E ref, 16+s rho species, 32..34 edge E (their own shapes)
+// The EM Yee array of a field selector (32..37), or null.
+static ArrB* yee_array(Ctx* c, int which) {
+    if (!c->em) return nullptr;
+    switch (which) {
+        case 32: return &c->fex;
+        case 33: return &c->fey;
+        case 34: return &c->fez;
+        case 35: return &c->fbx;
+        case 36: return &c->fby;
+        case 37: return &c->fbz;
+    }
+    return nullptr;
+}
+
+// which: 0 phi, 1 rho0, 2..4 E ref, 5..7 B ref, 8..10 J ref, 16+s rho species,
+// 32..34 edge E, 35..37 face B, 38..40 edge J (their own shapes, fopis_field numbering)
 int orc_get_field(void* h, int which, double* out) {
     Ctx* c = (Ctx*)h;
+    if (ArrB* b = yee_array(c, which)) {
+        std::memcpy(out, b->v.data(), sizeof(double) * b->v.size());
+        return 0;
+    }
+    if (which >= 8 && which <= 10) {
+        if (!c->em) return -1;
+        // RootGrid::updateReferenceCurrent (RootGridField.cpp:1256-1285)
+        Arr3 r;
+        r.resize(c->cx, c->cy, c->cz);
+        for (int i = 1; i < c->cx - 1; ++i) for (int j = 1; j < c->cy - 1; ++j) for (int k = 1; k < c->cz - 1; ++k)
+            r(i, j, k) = which == 8 ? 0.5 * (c->jx(i - 1, j, k) + c->jx(i, j, k))
+                                    : (which == 9 ? 0.5 * (c->jy(i, j - 1, k) + c->jy(i, j, k))
+                                                  : 0.5 * (c->jz(i, j, k - 1) + c->jz(i, j, k)));
+        copy_field_glue(*c, r);
+        std::memcpy(out, r.v.data(), sizeof(double) * r.v.size());
+        return 0;
+    }
     const Arr3* a = nullptr;
     switch (which) {
         case 0: a = &c->phi; break;
@@ -1580,9 +2040,15 @@ int orc_get_field(void* h, int which, double* out) {
         case 2: a = &c->exref; break;
         case 3: a = &c->eyref; break;
         case 4: a = &c->ezref; break;
+        case 5: a = c->em ? &c->bxref : nullptr; break;
+        case 6: a = c->em ? &c->byref : nullptr; break;
+        case 7: a = c->em ? &c->bzref : nullptr; break;
         case 32: a = &c->ex; break;
         case 33: a = &c->ey; break;
         case 34: a = &c->ez; break;
+        case 38: a = c->em ? &c->jx : nullptr; break;
+        case 39: a = c->em ? &c->jy : nullptr; break;
+        case 40: a = c->em ? &c->jz : nullptr; break;
         default:
             if (which >= 16 && which < 16 + c->nsp) a = &c->rho[which - 15];
     }
@@ -1590,9 +2056,30 @@ int orc_get_field(void* h, int which, double* out) {
     std::memcpy(out, a->v.data(), sizeof(double) * a->v.size());
     return 0;
 }
+
+// First index and extent per axis of a field (index bases of the EM arrays).
+int orc_field_shape(void* h, int which, int* lo, int* n) {
+    Ctx* c = (Ctx*)h;
+    if (ArrB* b = yee_array(c, which)) {
+        for (int a = 0; a < 3; ++a) { lo[a] = b->lo[a]; n[a] = b->n[a]; }
+        return 0;
+    }
+    const Arr3* a = nullptr;
+    if (which >= 32 && which <= 34) a = which == 32 ? &c->ex : (which == 33 ? &c->ey : &c->ez);
+    if (which >= 38 && which <= 40 && c->em) a = which == 38 ? &c->jx : (which == 39 ? &c->jy : &c->jz);
+    lo[0] = lo[1] = lo[2] = 0;
+    if (a) { n[0] = a->cx; n[1] = a->cy; n[2] = a->cz; }
+    else { n[0] = c->cx; n[1] = c->cy; n[2] = c->cz; }
+    return 0;
+}
 int orc_set_field(void* h, int which, const double* in) {
     Ctx* c = (Ctx*)h;
+    if (ArrB* b = yee_array(c, which)) {
+        std::memcpy(b->v.data(), in, sizeof(double) * b->v.size());
+        return 0;
+    }
     Arr3* a = which == 0 ? &c->phi : (which == 1 ? &c->rho[0] : nullptr);
+    if (c->em && which >= 38 && which <= 40) a = which == 38 ? &c->jx : (which == 39 ? &c->jy : &c->jz);
     if (!a) return -1;
     std::memcpy(a->v.data(), in, sizeof(double) * a->v.size());
     return 0;
@@ -1612,6 +2099,12 @@ void orc_energy(void* h, double* pe, double* fe) {
     double en = 0.0;
     const int X = c->cx, Y = c->cy, Z = c->cz;
     for (int i = 1; i < X - 1; ++i) for (int j = 1; j < Y - 1; ++j) for (int k = 1; k < Z - 1; ++k) {
+        if (c->em) {   // the Yee edges of the EM mode
+            if (i < X - 2) en += c->fex(i, j, k) * c->fex(i, j, k);
+            if (j < Y - 2) en += c->fey(i, j, k) * c->fey(i, j, k);
+            if (k < Z - 2) en += c->fez(i, j, k) * c->fez(i, j, k);
+            continue;
+        }
         if (i < X - 2) en += c->ex(i, j, k) * c->ex(i, j, k);
         if (j < Y - 2) en += c->ey(i, j, k) * c->ey(i, j, k);
         if (k < Z - 2) en += c->ez(i, j, k) * c->ez(i, j, k);

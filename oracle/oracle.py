@@ -62,6 +62,8 @@ def lib():
             "orc_fixed_fold": (None, [vp, vp]),
             "orc_position": (None, [vp, C.c_int64, vp, vp]),
             "orc_get_incidents": (C.c_int64, [vp, dp, C.c_int64]),
+            "orc_update_bfield": (None, [vp]), "orc_bfield_energy": (C.c_double, [vp]),
+            "orc_field_shape": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
             "orc_set_incidents": (None, [vp, dp, C.c_int64]),
         }
         for name, (res, args) in sig.items():
@@ -332,17 +334,29 @@ class Oracle:
         self.L.orc_step_counts(self.h, C.byref(a), C.byref(b), C.byref(c))
         return a.value, b.value, c.value
 
+    def field_shape(self, which):
+        """(first index, extent) per axis; the EM Yee arrays start below 0 on
+        axes with damping layers."""
+        lo, n = (C.c_int * 3)(), (C.c_int * 3)()
+        assert self.L.orc_field_shape(self.h, which, lo, n) == 0
+        return tuple(lo), tuple(n)
+
     def field(self, which):
-        shapes = {32: (self.shape[0] - 1, self.shape[1], self.shape[2]),
-                  33: (self.shape[0], self.shape[1] - 1, self.shape[2]),
-                  34: (self.shape[0], self.shape[1], self.shape[2] - 1)}
-        out = np.zeros(shapes.get(which, self.shape))
+        _, n = self.field_shape(which)
+        out = np.zeros(n)
         assert self.L.orc_get_field(self.h, which, out.ctypes.data_as(C.POINTER(C.c_double))) == 0
         return out
 
     def set_field(self, which, a):
-        a = np.ascontiguousarray(a, np.float64).reshape(self.shape)
+        _, n = self.field_shape(which)
+        a = np.ascontiguousarray(a, np.float64).reshape(n)
         assert self.L.orc_set_field(self.h, which, a.ctypes.data_as(C.POINTER(C.c_double))) == 0
+
+    def update_bfield(self):
+        self.L.orc_update_bfield(self.h)
+
+    def bfield_energy(self):
+        return self.L.orc_bfield_energy(self.h)
 
     def energy(self):
         pe, fe = C.c_double(), C.c_double()

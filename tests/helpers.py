@@ -45,3 +45,32 @@ def match(a, b, vscale=10.0):
 def rel_err(a, b):
     den = np.max(np.abs(b))
     return float(np.max(np.abs(a - b)) / (den if den > 0 else 1.0))
+
+
+def em_config(n=13, boundary="DDDDDD", ppc=4, te_ev=5.0e3, density=1.0e12, courant=0.5, precision=None,
+              boxes=None, photo=False, obj_parser=None):
+    """An EM-mode configuration: electrons of te_ev and 1 eV ions (mass 100) at
+    `density`, dx = 0.5 m (below the Debye length of those electrons), dt =
+    courant * dx / c (Environment::checkCFLCondition needs c dt / dx <= 1);
+    electrons move ~0.05 cells per step. boxes: voxel conductors (as
+    config.objects_from_boxes)."""
+    from fopis_b200 import _abi, config
+    from fopis_b200.config import SpeciesInfo, make_params
+    dx = 0.5
+    dt = courant * dx / config.CLIGHT
+    sp = [SpeciesInfo("Electron", "ambient", 1.0, -1.0, density, te_ev, ppc),
+          SpeciesInfo("Ion", "ambient", 100.0, 1.0, density, 1.0, ppc)]
+    shine = (0.0, 0.0, 0.0)
+    if photo:
+        import math
+        vbar = math.sqrt(8.0 * 10.0 * config.E / (math.pi * config.ME))
+        sp.append(SpeciesInfo("Photo", "photoelectron", 1.0, -1.0, density, 10.0, ppc,
+                              current_density=10.0 * config.E * density * vbar / 4.0))
+        shine = (-1.0, 0.0, 0.0)
+    p, norm = make_params((n, n, n), boundary, dx, dt, sp, tol=1e-10, sort_interval=1000000, shine=shine,
+                          precision=_abi.FP64 if precision is None else precision, solver="EM")
+    objs = []
+    if boxes:
+        emit = next((k for k, s in enumerate(sp) if s.kind == "photoelectron"), -1)
+        objs.append(config.objects_from_boxes(boxes, (n, n, n), emit_species=emit, obj_parser=obj_parser))
+    return config.SimConfig(params=p, norm=norm, species=sp, objects=objs, dx=dx, dt=dt)

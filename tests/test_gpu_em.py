@@ -1,0 +1,179 @@
+"""GPU parity of the EM mode (RootGrid::mainLoopEM, src/Grid/RootGrid/RootGrid.cpp:145-191)
+against the FP64 oracle:
+
+* the FDTD updates alone (RootGrid::updateEfieldFDTDDamping / updateBfieldDamping,
+  src/Grid/RootGrid/RootGridField.cpp:594-820, with the periodic glue copies and the
+  nodal references of :489-582 and :1102-1127) on random fields and currents, on
+  D, mixed and periodic boxes: every Yee array and nodal field to 1e-12 of its
+  largest value over three updates;
+* the phases of one step on the FP64 GPU path: the E and B gather with Boris
+  (GridParticleTreatmentEM.cpp:13-105) to 1e-12, the edge currents of
+  updateParticlePositionEM (:107-201, particle.cpp:258-338) to 1e-12 of the largest;
+* whole mainLoopEM runs, FP64: a D box with injection and a periodic box (20
+  steps) and a floating conductor with photoemission (10 steps): particle sets to
+  1e-9 cells, fields to 1e-8 of their largest, the three energies to 1e-9
+  (the oracle solves Poisson exactly, the GPU to 1e-10, so the start-up E differs
+  at that level and is carried along);
+* the mixed mode (FP32 particles) against the same oracle: fields to 1e-4 of their
+  largest after 10 steps.
+"""
+import numpy as np
+import pytest
+
+import oracle as orc
+from fopis_b200 import RootGrid, _abi
+
+from helpers import as_f32_state, em_config, match, random_particles, rel_err
+
+pytestmark = pytest.mark.gpu
+
+YEE = list(range(_abi.FIELD_EX, _abi.FIELD_BZ + 1))
+NODAL = [_abi.FIELD_EXREF, _abi.FIELD_EYREF, _abi.FIELD_EZREF, _abi.FIELD_BXREF, _abi.FIELD_BYREF, _abi.FIELD_BZREF]
+CURRENTS = [_abi.FIELD_JX, _abi.FIELD_JY, _abi.FIELD_JZ]
+
+
+@pytest.mark.parametrize("boundary", ["DDDDDD", "PPDDPP", "PPPPPP"])
+def test_fdtd_updates_match_oracle(gpu_available, boundary):
+    cfg = em_config(n=10, boundary=boundary)
+    g = RootGrid(cfg)
+    o = orc.Oracle(cfg.params)
+    rng = np.random.default_rng(7)
+    for which in YEE + CURRENTS:
+        assert g.field_shape(which) == o.field_shape(which)
+        a = rng.standard_normal(o.field_shape(which)[1]) * (1e-3 if which in CURRENTS else 1.0)
+        g.set_field(which, a)
+        o.set_field(which, a)
+    phi = rng.standard_normal((12, 12, 12))
+    g.set_field(_abi.FIELD_PHI, phi)
+    o.set_field(0, phi)
+    for _ in range(3):
+        g.updateEfield()
+        o.update_efield()
+        g.updateBfield()
+        o.update_bfield()
+    for which in YEE + NODAL:
+        assert rel_err(g.get_field(which), o.field(which)) <= 1e-12, which
+    assert g.getBfieldEnergy() == pytest.approx(o.bfield_energy(), rel=1e-12)
+    assert g.getEnergy()[1] == pytest.approx(o.energy()[1], rel=1e-12)
+    g.close()
+    o.close()
+
+
+def load_pair(cfg, seed=30, ppc_fill=4, f32=False):
+    p = cfg.params
+    g = RootGrid(cfg)
+    if cfg.objects:
+        g.initializeObjectsCmatrix(0)
+    o = orc.Oracle(p, cfg.objects)
+    o.set_solver(1, exact_tol=1e-13)
+    if cfg.objects:
+        o.set_cmatrix(0, g.get_cmatrix(0))
+    hi = [p.nx - 1 if cfg.params.boundary[2 * a] != b"P"[0] else p.nx for a in range(3)]
+    for s in range(2):
+        recs = random_particles(int(np.prod(hi)) * ppc_fill, (0, 0, 0), hi, p.species[s].deviation, seed + s, s)
+        if cfg.objects:
+            cells = {tuple(c) for c in cfg.objects[0].cells}
+            keep = np.array([tuple(int(np.floor(v)) + 1 for v in (r["x"], r["y"], r["z"])) not in cells for r in recs])
+            recs = recs[keep]
+        g.load_particles(s, recs)
+        o.load_particles(s, as_f32_state(recs) if f32 else recs)
+    g.initialize()
+    o.initialize()
+    return g, o
+
+
+def compare_particles(g, o, tol_x, tol_v):
+    for s in range(g.nspecies):
+        a, b, _ = match(g.getParticles(s), o.particles(s))
+        for key in ("x", "y", "z"):
+            assert np.max(np.abs(a[key] - b[key]), initial=0.0) <= tol_x, (s, key)
+        vmax = max(np.max(np.abs(b[k]), initial=0.0) for k in ("vx", "vy", "vz"))
+        for key in ("vx", "vy", "vz"):
+            assert np.max(np.abs(a[key] - b[key]), initial=0.0) <= tol_v * vmax, (s, key)
+
+
+def test_em_phases_match_oracle(gpu_available):
+    cfg = em_config(n=13)
+    g, o = load_pair(cfg)
+    for which in NODAL[:3]:
+        assert rel_err(g.get_field(which), o.field(which)) <= 1e-8, which
+    # B after Grid::initialize is the curl of a gradient: rounding on both sides
+    emax = max(np.max(np.abs(o.field(w))) for w in NODAL[:3])
+    for which in NODAL[3:]:
+        assert np.max(np.abs(g.get_field(which))) <= 1e-12 * emax
+        assert np.max(np.abs(o.field(which))) <= 1e-12 * emax
+    g.updateParticleVelocity()
+    o.update_velocity()
+    compare_particles(g, o, 1e-12, 1e-9)
+    g.updateParticlePosition()
+    o.update_position()
+    for which in CURRENTS:
+        assert rel_err(g.get_field(which), o.field(which)) <= 1e-9, which
+    compare_particles(g, o, 1e-12, 1e-9)
+    g.injectParticlesFromBoundary()
+    o.inject()
+    g.updateRho()
+    o.update_rho()
+    assert rel_err(g.getRho(), o.field(1)) <= 1e-11
+    g.updateEfield()
+    o.update_efield()
+    g.updateBfield()
+    o.update_bfield()
+    for which in YEE + NODAL:
+        assert rel_err(g.get_field(which), o.field(which)) <= 1e-8, which
+    g.close()
+    o.close()
+
+
+@pytest.mark.parametrize("boundary,steps", [("DDDDDD", 20), ("PPPPPP", 20)])
+def test_em_main_loop_fp64_tracks_oracle(gpu_available, boundary, steps):
+    cfg = em_config(n=13, boundary=boundary)
+    g, o = load_pair(cfg)
+    hist = []
+    for _ in range(steps):
+        g.mainLoopEM(1)
+        o.main_loop(1)
+        pe_g, fe_g = g.getEnergy()
+        pe_o, fe_o = o.energy()
+        hist.append((pe_g / pe_o - 1, fe_g / fe_o - 1, g.getBfieldEnergy() / o.bfield_energy() - 1))
+    hist = np.abs(np.array(hist))
+    assert np.max(hist) <= 1e-8, hist.max(0)
+    compare_particles(g, o, 1e-9, 1e-8)
+    for which in YEE + NODAL + CURRENTS:
+        assert rel_err(g.get_field(which), o.field(which)) <= 1e-8, which
+    print(f"\nEM {boundary}: {steps} steps, worst relative energy differences (particles, E, B) "
+          f"{hist.max(0)}, B energy {o.bfield_energy():.3e}")
+    g.close()
+    o.close()
+
+
+def test_em_conductor_run_tracks_oracle(gpu_available):
+    cfg = em_config(n=17, boxes=[((-2, -2, -2), (2, 2, 2))], photo=True, obj_parser=orc.parse_obj)
+    g, o = load_pair(cfg)
+    V = []
+    for _ in range(10):
+        g.mainLoopEM(1)
+        o.main_loop(1)
+        V.append((g.getObject(0)[0], o.get_object(0)[0]))
+    V = np.array(V)
+    assert np.max(np.abs(V[:, 0] - V[:, 1]) / np.abs(V[:, 1])) <= 1e-8
+    compare_particles(g, o, 1e-9, 1e-8)
+    for which in YEE + NODAL:
+        assert rel_err(g.get_field(which), o.field(which)) <= 1e-8, which
+    g.close()
+    o.close()
+
+
+def test_em_mixed_precision_tracks_oracle(gpu_available):
+    cfg = em_config(n=13, precision=_abi.MIXED)
+    g, o = load_pair(cfg, f32=True)
+    for _ in range(10):
+        g.mainLoopEM(1)
+        o.main_loop(1)
+    for which in YEE + NODAL + CURRENTS:
+        assert rel_err(g.get_field(which), o.field(which)) <= 1e-4, which
+    pe_g, fe_g = g.getEnergy()
+    pe_o, fe_o = o.energy()
+    assert pe_g == pytest.approx(pe_o, rel=1e-5)
+    g.close()
+    o.close()

@@ -51,14 +51,30 @@ def test_abi_library_exports_every_declared_symbol():
     assert lib.fopis_version().startswith(b"fopis-b200")
 
 
-def test_abi_struct_layout_matches_header():
+def test_abi_struct_layout_matches_header(tmp_path):
+    """Every field offset and struct size of the ctypes mirror against the C
+    compiler's offsetof/sizeof on include/fopis_gpu.h."""
     import ctypes as C
-    assert C.sizeof(_abi.Species) == 152
-    assert C.sizeof(_abi.Params) == 1360
-    assert _abi.Params.seed.offset == 1344
-    assert _abi.Params.energy_ev.offset == 1352
-    assert C.sizeof(_abi.ObjectDesc) == 80
-    assert _abi.ObjectDesc.capacitance.offset == 72
+    import subprocess
+    structs = {"fopis_species": _abi.Species, "fopis_params": _abi.Params,
+               "fopis_object_desc": _abi.ObjectDesc, "fopis_stats": _abi.Stats}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{ROOT / "include" / "fopis_gpu.h"}"',
+             "int main(void) {"]
+    for cname, cls in structs.items():
+        lines.append(f'printf("{cname} __sizeof__ %zu\\n", sizeof({cname}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l}
+    for cname, cls in structs.items():
+        assert got[(cname, "__sizeof__")] == C.sizeof(cls), cname
+        for fname, _ in cls._fields_:
+            assert got[(cname, fname)] == getattr(cls, fname).offset, (cname, fname)
 
 
 def _write(tmp_path, text):
