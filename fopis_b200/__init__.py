@@ -222,6 +222,10 @@ class RootGrid:
         a = np.ascontiguousarray(a, dtype=np.float64).reshape(n)
         self._check(self.lib.fopis_set_field(self.h, which, _dp(a), a.size))
 
+    def updateReferenceFields(self):
+        """Nodal E (and in the EM mode B) from the current fields, as Grid::initializeForLoad."""
+        self._check(self.lib.fopis_update_reference_fields(self.h))
+
     def updateBfield(self):
         """RootGrid::updateBfield (EM mode)."""
         self._check(self.lib.fopis_update_bfield(self.h))

@@ -180,6 +180,7 @@ SIGNATURES = {
     "fopis_solve_poisson": (C.c_int, [_VP]),
     "fopis_update_efield": (C.c_int, [_VP]),
     "fopis_update_bfield": (C.c_int, [_VP]),
+    "fopis_update_reference_fields": (C.c_int, [_VP]),
     "fopis_field_shape": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "fopis_get_bfield_energy": (C.c_int, [_VP, _DP]),
     "fopis_remove_invalid_particles": (C.c_int, [_VP]),

@@ -716,6 +716,15 @@ int fopis_update_efield(void* h) {
     });
 }
 
+int fopis_update_reference_fields(void* h) {
+    return guarded(h, [&](Ctx& c) -> int {
+        if (c.em.on) em_reference_fields(c);
+        else efield_update(c);
+        FOPIS_CUDA(cudaStreamSynchronize(c.st));
+        return FOPIS_OK;
+    });
+}
+
 int fopis_update_bfield(void* h) {
     return guarded(h, [&](Ctx& c) -> int {
         if (!c.em.on) throw ApiError{FOPIS_ERR_STATE, "updateBfield belongs to the EM solver"};

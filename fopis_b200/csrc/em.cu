@@ -479,6 +479,11 @@ void em_update_bfield(Ctx& c) {
     reference_bfield(c);
 }
 
+void em_reference_fields(Ctx& c) {
+    reference_efield(c);
+    reference_bfield(c);
+}
+
 double em_efield_energy(Ctx& c) { return 0.5 * c.p.eps0 * em_energy(c, 0); }
 double em_bfield_energy(Ctx& c) { return 0.5 * em_energy(c, 1) / c.p.mu0; }
 

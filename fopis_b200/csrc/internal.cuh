@@ -327,6 +327,7 @@ void em_fold_currents(Ctx& c);
 void em_efield_from_phi(Ctx& c);   // RootGrid::updateEfield in the EM mode (start-up)
 void em_update_efield(Ctx& c);     // RootGrid::updateEfieldFDTD
 void em_update_bfield(Ctx& c);     // RootGrid::updateBfield
+void em_reference_fields(Ctx& c);  // updateReferenceEfield + updateReferenceBfield
 double em_efield_energy(Ctx& c);
 double em_bfield_energy(Ctx& c);
 const YeeArr* em_array(const Ctx& c, int which);   // FOPIS_FIELD_EX..BZ, or null

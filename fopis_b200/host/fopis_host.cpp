@@ -338,6 +338,17 @@ void RootGrid::saveResumeData(const std::string& dir) const {
     f.put_f64("Efield/exref", shape, getField(FOPIS_FIELD_EXREF).data());
     f.put_f64("Efield/eyref", shape, getField(FOPIS_FIELD_EYREF).data());
     f.put_f64("Efield/ezref", shape, getField(FOPIS_FIELD_EZREF).data());
+    if (in_.params.solver == FOPIS_SOLVER_EM) {
+        // RootGrid::saveResumeFieldData (RootGridIO.cpp:236-271): the Yee E and B, damping layers included
+        const char* names[6] = {"Efield/ex", "Efield/ey", "Efield/ez", "Bfield/bx", "Bfield/by", "Bfield/bz"};
+        for (int q = 0; q < 6; ++q) {
+            int lo[3], n[3];
+            check(fopis_field_shape(ctx_, FOPIS_FIELD_EX + q, lo, n));
+            std::vector<double> v((size_t)n[0] * n[1] * n[2]);
+            check(fopis_get_field(ctx_, FOPIS_FIELD_EX + q, v.data(), v.size()));
+            f.put_f64(names[q], {(uint64_t)n[0], (uint64_t)n[1], (uint64_t)n[2]}, v.data());
+        }
+    }
     for (size_t k = 0; k < in_.objects.size(); ++k) {
         const int n = in_.objects[k].n_cmat();
         std::vector<double> cm((size_t)nsp * n);
@@ -375,6 +386,17 @@ void RootGrid::loadResumeData(const std::string& dir) {
     const size_t N = (size_t)(in_.params.nx + 2) * (in_.params.ny + 2) * (in_.params.nz + 2);
     if (phi.size() != N) throw std::runtime_error("resume data: Potential/phi has the wrong size");
     check(fopis_set_field(ctx_, FOPIS_FIELD_PHI, phi.data(), N));
+    if (in_.params.solver == FOPIS_SOLVER_EM) {   // RootGrid::loadResumeFieldData (RootGridIO.cpp:181-234)
+        const char* names[6] = {"Efield/ex", "Efield/ey", "Efield/ez", "Bfield/bx", "Bfield/by", "Bfield/bz"};
+        for (int q = 0; q < 6; ++q) {
+            int lo[3], n[3];
+            check(fopis_field_shape(ctx_, FOPIS_FIELD_EX + q, lo, n));
+            const std::vector<double> v = f.f64(names[q]);
+            if (v.size() != (size_t)n[0] * n[1] * n[2])
+                throw std::runtime_error(std::string("resume data: ") + names[q] + " has the wrong size");
+            check(fopis_set_field(ctx_, FOPIS_FIELD_EX + q, v.data(), v.size()));
+        }
+    }
     for (size_t k = 0; k < in_.objects.size(); ++k) {
         const int n = in_.objects[k].n_cmat();
         const std::vector<double> cm = f.f64(in_.objects[k].name + "/charge_map");
@@ -387,6 +409,13 @@ void RootGrid::loadResumeData(const std::string& dir) {
 // (the reference reads its saved edge E), then updateRho, which with objects
 // runs the first solve and the redistribution of the restored charge map.
 void RootGrid::initializeForLoad() {
+    if (in_.params.solver == FOPIS_SOLVER_EM) {
+        // EM: updateRho, then the nodal E and B from the restored Yee arrays
+        check(fopis_sort_particles(ctx_));
+        updateRho();
+        check(fopis_update_reference_fields(ctx_));
+        return;
+    }
     updateEfield();
     check(fopis_sort_particles(ctx_));
     updateRho();
@@ -418,6 +447,12 @@ double RootGrid::getEFieldEnergy() const {
     check(fopis_get_energy(ctx_, &pe, &fe));
     return fe;
 }
+double RootGrid::getBFieldEnergy() const {
+    double be = 0.0;
+    check(fopis_get_bfield_energy(ctx_, &be));
+    return be;
+}
+void RootGrid::updateBfield() { check(fopis_update_bfield(ctx_)); }
 fopis_stats RootGrid::stats() const {
     fopis_stats st{};
     check(fopis_get_stats(ctx_, &st));
@@ -482,9 +517,11 @@ void plot_energy(const RootGrid& g, int timestep, const std::string& dir) {
         std::snprintf(h, sizeof h, "%16s %16s %16s %16s", "Energy [J]", "Particle [J]", "EField [J]", "BField [J]");
         put_header(file, h);
     }
-    const double pe = g.getParticleEnergy(), fe = g.getEFieldEnergy();
+    // IO::plotEnergy (src/Misc/IO.cpp:170-194): the B column is nonzero in the EM mode only
+    const double pe = g.getParticleEnergy(), fe = g.getEFieldEnergy(), be = g.getBFieldEnergy();
     char e[128];
-    std::snprintf(e, sizeof e, "%16.7e %16.7e %16.7e %16.7e", n.unenergy(pe + fe), n.unenergy(pe), n.unenergy(fe), 0.0);
+    std::snprintf(e, sizeof e, "%16.7e %16.7e %16.7e %16.7e", n.unenergy(pe + fe + be), n.unenergy(pe), n.unenergy(fe),
+                  n.unenergy(be));
     put_log(file, timestep, timestep * g.input().dt, e);
 }
 

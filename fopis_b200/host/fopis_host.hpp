@@ -162,6 +162,8 @@ public:
 
     double getParticleEnergy() const;                // Grid::getParticleEnergy
     double getEFieldEnergy() const;                  // Field::getEfieldEnergy
+    double getBFieldEnergy() const;                  // Field::getBfieldEnergy (0 in the ES mode)
+    void updateBfield();                             // RootGrid::updateBfield (EM mode)
     std::vector<int64_t> getValidParticleNumbers() const;
     std::vector<Particle> getParticles(int species) const;
     std::vector<double> getField(int which) const;   // fopis_field, glue layout (nx+2)(ny+2)(nz+2)

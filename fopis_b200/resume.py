@@ -160,6 +160,9 @@ def load_info(cfg, resume_dir) -> int:
     return int(d["timestep"])
 
 
+EM_SETS = ("Efield/ex", "Efield/ey", "Efield/ez", "Bfield/bx", "Bfield/by", "Bfield/bz")
+
+
 def save_resume(grid, resume_dir) -> None:
     """Environment::saveInfo + RootGrid::saveResumeData for a fopis_b200.RootGrid."""
     cfg = grid.cfg
@@ -180,6 +183,10 @@ def save_resume(grid, resume_dir) -> None:
     sets["Potential/phi"] = grid.getPhi()
     ex, ey, ez = grid.getEref()
     sets["Efield/exref"], sets["Efield/eyref"], sets["Efield/ezref"] = ex, ey, ez
+    if cfg.params.solver == _abi.SOLVER_EM:
+        # RootGrid::saveResumeFieldData (RootGridIO.cpp:236-271): the Yee E and B
+        for name, which in zip(EM_SETS, range(_abi.FIELD_EX, _abi.FIELD_BZ + 1)):
+            sets[name] = grid.get_field(which)
     for k, o in enumerate(cfg.objects):
         sets[o.name + "/charge_map"] = grid.getChargeMap(k)
     os.makedirs(resume_dir, exist_ok=True)
@@ -213,11 +220,20 @@ def load_resume(grid, resume_dir) -> int:
             carry[6 * s:6 * s + 6] = d[g + "injection_carry"]
     grid._check(lib.fopis_set_injection_carry(grid.h, carry.ctypes.data_as(C.POINTER(C.c_double)), 6 * nsp))
     grid.set_field(_abi.FIELD_PHI, d["Potential/phi"])
+    em = cfg.params.solver == _abi.SOLVER_EM
+    if em:   # RootGrid::loadResumeFieldData (RootGridIO.cpp:181-234)
+        for name, which in zip(EM_SETS, range(_abi.FIELD_EX, _abi.FIELD_BZ + 1)):
+            grid.set_field(which, d[name])
     for k, o in enumerate(cfg.objects):
         cm = np.ascontiguousarray(d[o.name + "/charge_map"], np.float64)
         grid._check(lib.fopis_set_charge_map(grid.h, grid.object_ids[k], cm.ctypes.data_as(C.POINTER(C.c_double)),
                                              cm.size))
     # Grid::initializeForLoad (Grid.cpp:38-50)
+    if em:
+        grid.sort()
+        grid.updateRho()
+        grid.updateReferenceFields()
+        return ts
     grid.updateEfield()
     grid.sort()
     grid.updateRho()

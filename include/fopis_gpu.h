@@ -298,6 +298,10 @@ int fopis_update_rho(void* ctx);             /* RootGrid::updateRho (RootGridFie
 int fopis_solve_poisson(void* ctx);          /* RootGrid::solvePoisson (RootGridField.cpp:41-63) */
 int fopis_update_efield(void* ctx);          /* ES: RootGrid::updateEfield + updateReferenceEfield (RootGridField.cpp:456-582);
                                                 EM: RootGrid::updateEfieldFDTD (damping form, :584-710) */
+int fopis_update_reference_fields(void* ctx);  /* ES: the nodal E from phi (updateReferenceEfield on the edges of
+                                                updateEfield); EM: RootGrid::updateReferenceEfield and
+                                                updateReferenceBfield on the current Yee arrays (RootGridField.cpp:
+                                                489-582, 1102-1127), as Grid::initializeForLoad (Grid.cpp:38-50) */
 int fopis_update_bfield(void* ctx);          /* EM: RootGrid::updateBfield (damping form, RootGridField.cpp:589-820)
                                                 and updateReferenceBfield (:1102-1127); FOPIS_ERR_STATE in ES */
 int fopis_remove_invalid_particles(void* ctx); /* Grid::removeInvalidParticles */

@@ -177,3 +177,69 @@ def test_em_mixed_precision_tracks_oracle(gpu_available):
     assert pe_g == pytest.approx(pe_o, rel=1e-5)
     g.close()
     o.close()
+
+
+def test_em_resume_tracks_uninterrupted_run(gpu_available, tmp_path):
+    """Resume data of the EM mode (RootGrid::saveResumeFieldData / loadResumeFieldData,
+    RootGridIO.cpp:181-271: the Yee E and B under Efield/ex.. and Bfield/bx..) and
+    Grid::initializeForLoad: 3 steps, save, continue 3 steps in a fresh context,
+    against 6 uninterrupted steps."""
+    from fopis_b200 import resume as R
+    cfg = em_config(n=13)
+
+    def fresh():
+        g, o = load_pair(cfg)
+        o.close()
+        return g
+
+    def hist(g, steps):
+        out = []
+        for _ in range(steps):
+            g.mainLoopEM(1)
+            out.append(g.getEnergy() + (g.getBfieldEnergy(),))
+        return np.array(out)
+
+    a = fresh()
+    ha = hist(a, 6)
+    b = fresh()
+    hist(b, 3)
+    R.save_resume(b, tmp_path)
+    c = RootGrid(cfg)
+    assert R.load_resume(c, tmp_path) == int(b.stats().timestep)
+    hc = hist(c, 3)
+    assert np.max(np.abs(hc / ha[3:] - 1)) <= 1e-9, hc / ha[3:] - 1
+    for which in YEE:
+        assert rel_err(c.get_field(which), a.get_field(which)) <= 1e-9, which
+    for g in (a, b, c):
+        g.close()
+
+
+def test_fopis_run_em_matches_python_driver(gpu_available, tmp_path):
+    """fopis_run on an "EM" input.json: data/energy.txt carries the B-field column
+    of IO::plotEnergy (src/Misc/IO.cpp:170-194) and matches the Python driver."""
+    import subprocess
+    from pathlib import Path
+    from fopis_b200 import config
+    from host_input import write_input
+    run = Path(__file__).resolve().parent.parent / "fopis_b200" / "fopis_run"
+    steps = 4
+    path = write_input(tmp_path / "case", n=17, ppc=4, photo=True, steps=steps, em=True)
+    out = tmp_path / "data"
+    r = subprocess.run([str(run), str(path), "--out", str(out), "--resume", str(tmp_path / "resume")],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    energy = np.loadtxt(out / "energy.txt", skiprows=1)
+    cfg = config.load_input(str(path))
+    g = RootGrid(cfg)
+    g.initializeObjectsCmatrix(0)
+    g.generate_ambient()
+    g.initialize()
+    n = cfg.norm
+    for t in range(steps):
+        g.mainLoopEM(1)
+        pe, fe = g.getEnergy()
+        be = g.getBfieldEnergy()
+        np.testing.assert_allclose(energy[t, 3:6], [n.unenergy(pe), n.unenergy(fe), n.unenergy(be)], rtol=1e-6)
+        np.testing.assert_allclose(energy[t, 2], n.unenergy(pe + fe + be), rtol=1e-6)
+    assert energy[-1, 5] > 0.0
+    g.close()

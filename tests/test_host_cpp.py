@@ -91,3 +91,19 @@ def test_cpp_loader_on_reference_sample(built, tmp_path):
     if SAMPLE is None or not SAMPLE.exists():
         pytest.skip("reference sample input not available")
     compare(dump(SAMPLE, tmp_path), config.load_input(str(SAMPLE)))
+
+
+def test_cpp_loader_em_mode(built, tmp_path):
+    """solver_type "EM": the solver and the normalised mu0 (include/normalizer.hpp:219-221)
+    in the parameters; a time step above the Courant limit is refused by both loaders
+    (Environment::checkCFLCondition, src/Misc/Environment.cpp:193-203)."""
+    path = write_input(tmp_path / "ok", photo=True, em=True)
+    py = config.load_input(str(path))
+    assert py.params.solver == _abi.SOLVER_EM and py.params.mu0 > 0
+    compare(dump(path, tmp_path), py)
+    bad = write_input(tmp_path / "bad", photo=False, em=True, courant=1.5)
+    with pytest.raises(ValueError, match="Courant number exceeds 1.0"):
+        config.load_input(str(bad))
+    r = subprocess.run([str(RUN), str(bad), "--dump-params", str(tmp_path / "x.bin")], capture_output=True,
+                       text=True, timeout=120)
+    assert r.returncode != 0 and "Courant number exceeds 1.0" in (r.stderr + r.stdout)
