@@ -229,11 +229,23 @@ int em_step(Ctx& c) {
     record(c, 1);
     launch_emit(c, false);
     record(c, 2);
-    launch_em_position(c);
-    launch_inject(c, false);
+    if (c.fp64) {
+        // FP64: the current (FP64 atomics) and the move, the injection, then the rho pass
+        launch_em_position(c);
+        launch_inject(c, false);
+        rho_zero(c);
+        launch_deposit_all(c);
+    } else {
+        // mixed: one particle pass moves, adds the fixed-point current halves, tests the
+        // bodies and deposits; injected particles deposit as they are created
+        const size_t per = (size_t)(c.cx - 1) * c.cy * c.cz + (size_t)c.cx * (c.cy - 1) * c.cz +
+                           (size_t)c.cx * c.cy * (c.cz - 1);
+        FOPIS_CUDA(cudaMemsetAsync(c.em.jfix, 0, sizeof(unsigned long long) * per * c.nsp, c.st));
+        rho_zero(c);
+        launch_em_move(c);
+        launch_inject(c, true);
+    }
     record(c, 3);
-    rho_zero(c);
-    launch_deposit_all(c);
     int rc1 = FOPIS_OK;
     rho_tail(c, &rc1);
     record(c, 5);
@@ -246,6 +258,9 @@ int em_step(Ctx& c) {
     record(c, 8);
     const int rc = check_device(c);
     update_currents(c);
+    if (!c.fp64)
+        for (int s = 0; s < c.nsp; ++s)
+            if (c.timestep % si != 0) c.valid[s] = (int64_t)(c.h_sc->survived[s] + c.h_sc->added[s]);
     c.energy_valid = false;
     c.timestep += 1;
     if (c.ev[0]) {

@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <vector>
 
 namespace fopis {
 
@@ -37,12 +38,16 @@ struct Geo {
     int lo[3];     // first index of the extended grid per axis
     int up[3];     // one past the last
     int per[3];    // axis periodic
+    const double* mask[3];   // per-axis damping factor of index i at mask[a][i - lo[a]]
 };
 Geo make_geo(const Ctx& c) {
     Geo g;
     g.c[0] = c.cx; g.c[1] = c.cy; g.c[2] = c.cz;
+    size_t off = 0;
     for (int a = 0; a < 3; ++a) {
         g.L[a] = c.em.L[a]; g.lo[a] = c.em.lo[a]; g.up[a] = c.em.up[a]; g.per[a] = c.per[2 * a];
+        g.mask[a] = c.em.mask + off;
+        off += (size_t)(g.up[a] - g.lo[a]);
     }
     return g;
 }
@@ -54,14 +59,15 @@ int blocks(long long n) {
 
 // The masking factor of the damping forms (RootGridField.cpp:628-642, 742-756):
 // per axis 1 - (d / L)^2, d = the index's distance from the real grid [1, real-2]
-// (masking_parameter 1), multiplied over the three axes.
-__device__ __forceinline__ double damp1(int r, int L, int real) {
+// (masking_parameter 1), evaluated once per index into a table on the host
+// (damp1), multiplied over the three axes on the device.
+double damp1(int r, int L, int real) {
     const double d = (r <= 0) ? -(double)r + 1.0 : (r >= real - 1) ? (double)r - (double)real + 2.0 : 0.0;
     const double q = 1.0 * d / (double)L;
     return 1.0 - q * q;
 }
 __device__ __forceinline__ double damp(const Geo& g, int i, int j, int k) {
-    return damp1(i, g.L[0], g.c[0]) * damp1(j, g.L[1], g.c[1]) * damp1(k, g.L[2], g.c[2]);
+    return __ldg(g.mask[0] + (i - g.lo[0])) * __ldg(g.mask[1] + (j - g.lo[1])) * __ldg(g.mask[2] + (k - g.lo[2]));
 }
 __device__ __forceinline__ bool real_region(const Geo& g, int i, int j, int k) {
     return i > 0 && i < g.c[0] - 1 && j > 0 && j < g.c[1] - 1 && k > 0 && k < g.c[2] - 1;
@@ -410,10 +416,22 @@ void em_alloc(Ctx& c) {
         FOPIS_CUDA(cudaMalloc(&e.j[a], sizeof(double) * nj[a]));
         FOPIS_CUDA(cudaMemset(e.j[a], 0, sizeof(double) * nj[a]));
     }
+    {   // damping factors per axis and index, [x extent][y extent][z extent] back to back
+        std::vector<double> m;
+        for (int a = 0; a < 3; ++a)
+            for (int r = e.lo[a]; r < e.up[a]; ++r) m.push_back(damp1(r, e.L[a], cc[a]));
+        FOPIS_CUDA(cudaMalloc(&e.mask, sizeof(double) * m.size()));
+        FOPIS_CUDA(cudaMemcpy(e.mask, m.data(), sizeof(double) * m.size(), cudaMemcpyHostToDevice));
+    }
     FOPIS_CUDA(cudaMalloc(&e.eref, sizeof(double) * 3 * c.N));
     FOPIS_CUDA(cudaMemset(e.eref, 0, sizeof(double) * 3 * c.N));
     FOPIS_CUDA(cudaMalloc(&e.bref, sizeof(double) * 3 * c.N));
     FOPIS_CUDA(cudaMemset(e.bref, 0, sizeof(double) * 3 * c.N));
+    if (!c.fp64) {
+        const size_t per = nj[0] + nj[1] + nj[2];
+        FOPIS_CUDA(cudaMalloc(&e.jfix, sizeof(unsigned long long) * per * c.nsp));
+        FOPIS_CUDA(cudaMemset(e.jfix, 0, sizeof(unsigned long long) * per * c.nsp));
+    }
     if (c.fp64) {
         FOPIS_CUDA(cudaMalloc(&e.B64, sizeof(Vec4d) * c.N));
         FOPIS_CUDA(cudaMemset(e.B64, 0, sizeof(Vec4d) * c.N));
@@ -427,8 +445,10 @@ void em_free(Ctx& c) {
     EMState& e = c.em;
     for (auto& y : e.f) { if (y.v) cudaFree(y.v); y.v = nullptr; }
     for (auto& p : e.j) { if (p) cudaFree(p); p = nullptr; }
-    for (void* p : {(void*)e.eref, (void*)e.bref, (void*)e.B, (void*)e.B64}) if (p) cudaFree(p);
-    e.eref = e.bref = nullptr;
+    for (void* p : {(void*)e.eref, (void*)e.bref, (void*)e.B, (void*)e.B64, (void*)e.mask, (void*)e.jfix})
+        if (p) cudaFree(p);
+    e.eref = e.bref = e.mask = nullptr;
+    e.jfix = nullptr;
     e.B = nullptr;
     e.B64 = nullptr;
     e.on = false;

@@ -202,6 +202,8 @@ struct EMState {
     double* bref = nullptr;          // [3][N] nodal B (FP64)
     float4* B = nullptr;             // nodal B (FP32) for the gather of the mixed mode
     Vec4d* B64 = nullptr;            // nodal B (FP64) for the FP64 mode
+    double* mask = nullptr;          // damping factor per axis and index (x, y, z extents back to back)
+    unsigned long long* jfix = nullptr;   // mixed mode: [nsp][jx | jy | jz] fixed-point current sums (2^-40)
 };
 
 struct Ctx {
@@ -304,6 +306,7 @@ void launch_push(Ctx& c, bool vel, bool pos, bool dep);
 void launch_deposit_all(Ctx& c);
 void launch_em_velocity(Ctx& c);
 void launch_em_position(Ctx& c);
+void launch_em_move(Ctx& c);
 void launch_emit(Ctx& c, bool fused);
 void launch_inject(Ctx& c, bool fused);
 void launch_absorb(Ctx& c);

@@ -505,6 +505,201 @@ __global__ void __launch_bounds__(kThreads) em_position_kernel(PushArgsT<T> a, E
     }
 }
 
+// Edge currents of the mixed mode in fixed point: per species the sum of
+// J / (q size) in units of 2^-24 of one particle crossing a cell (the FP32
+// resolution of the particle offsets), int64 two's complement sums (exact,
+// independent of the order of the additions), converted to the FP64 J of
+// Field::jx.. once per step.
+constexpr float kCurrentScale = 16777216.0f;   // 2^24
+struct EdgeFix {
+    unsigned long long *x = nullptr, *y = nullptr, *z = nullptr;   // this species' jx, jy, jz sums
+    int cx = 0, cy = 0, cz = 0;
+};
+
+__device__ __forceinline__ float em_relay_f(int i_new, int i_old, float x_new, float x_old) {
+    return fminf((float)min(i_new, i_old), fmaxf((float)max(i_new, i_old) - 1.0f, 0.5f * (x_new + x_old)));
+}
+
+// The old-cell half of the zigzag (the move from x to x + v) in the cell's frame,
+// unit charge: flux f and weights w (src/Particle/particle.cpp:258-298), FP32.
+__device__ __forceinline__ void em_half_old(const PState& st, float f[3], float w[3]) {
+    const float o[3] = {st.ox, st.oy, st.oz}, v[3] = {st.vx, st.vy, st.vz};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const float x1 = o[d], x2 = o[d] + v[d];   // the move's own sum
+        const float r = em_relay_f((int)floorf(x2) + 1, 1, x2, x1);
+        f[d] = r - x1;
+        w[d] = 0.5f * (r + x1);
+    }
+}
+// The new-cell half (from x - v to x) in the frame of the cell the particle
+// landed in (particle.cpp:300-338).
+__device__ __forceinline__ void em_half_new(const PState& st, float f[3], float w[3]) {
+    const float o[3] = {st.ox, st.oy, st.oz}, v[3] = {st.vx, st.vy, st.vz};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const float x2 = o[d], x1 = x2 - v[d];
+        const float r = em_relay_f(1, (int)floorf(x1) + 1, x2, x1);
+        f[d] = x2 - r;
+        w[d] = 0.5f * (r + x2);
+    }
+}
+
+// The twelve edge terms of one half in fixed point (|term| <= 2^24), in the edge
+// order of em_current_half, and the address of term q of cell (i, j, k).
+__device__ __forceinline__ void em_terms(const float f[3], const float w[3], int t[12]) {
+    const float s0 = kCurrentScale * f[0], s1 = kCurrentScale * f[1], s2 = kCurrentScale * f[2];
+    t[0] = __float2int_rn(s0 * (1.0f - w[1]) * (1.0f - w[2]));
+    t[1] = __float2int_rn(s0 * w[1] * (1.0f - w[2]));
+    t[2] = __float2int_rn(s0 * (1.0f - w[1]) * w[2]);
+    t[3] = __float2int_rn(s0 * w[1] * w[2]);
+    t[4] = __float2int_rn(s1 * (1.0f - w[0]) * (1.0f - w[2]));
+    t[5] = __float2int_rn(s1 * w[0] * (1.0f - w[2]));
+    t[6] = __float2int_rn(s1 * (1.0f - w[0]) * w[2]);
+    t[7] = __float2int_rn(s1 * w[0] * w[2]);
+    t[8] = __float2int_rn(s2 * (1.0f - w[0]) * (1.0f - w[1]));
+    t[9] = __float2int_rn(s2 * w[0] * (1.0f - w[1]));
+    t[10] = __float2int_rn(s2 * (1.0f - w[0]) * w[1]);
+    t[11] = __float2int_rn(s2 * w[0] * w[1]);
+}
+__device__ __forceinline__ unsigned long long* em_term_ptr(const EdgeFix& J, int i, int j, int k, int q) {
+    const int e = q & 3;
+    if (q < 4) return J.x + ((long long)i * J.cy + j) * J.cz + k + ((e & 1) ? J.cz : 0) + ((e >> 1) ? 1 : 0);
+    if (q < 8) return J.y + ((long long)i * (J.cy - 1) + j) * J.cz + k + ((e & 1) ? (long long)(J.cy - 1) * J.cz : 0) +
+                      ((e >> 1) ? 1 : 0);
+    return J.z + ((long long)i * J.cy + j) * (J.cz - 1) + k + ((e & 1) ? (long long)J.cy * (J.cz - 1) : 0) +
+           ((e >> 1) ? (J.cz - 1) : 0);
+}
+
+// Warp-aggregated fixed-point current terms t[12] of cell (i, j, k). When every
+// depositing lane shares one cell the warp sums each term with one redux.sync
+// (32 terms of at most 2^25 stay below 2^30) and lane 0 adds; otherwise lanes
+// whose cell is unique add their terms directly and lanes sharing a cell are
+// summed per cell, their leader adding. Every lane of the warp calls it.
+__device__ __forceinline__ void em_warp_add(const EdgeFix& J, bool dep, int i, int j, int k, const int t[12]) {
+    const int lane = threadIdx.x & 31;
+    const int key = dep ? (i * J.cy + j) * J.cz + k : -1;   // node cells stay below 2^31
+    const unsigned deps = __ballot_sync(kFull, dep);
+    if (!deps) return;
+    const int key0 = __shfl_sync(kFull, key, __ffs(deps) - 1);
+    if (__all_sync(kFull, !dep || key == key0)) {
+        const int first = __ffs(deps) - 1;
+#pragma unroll
+        for (int q = 0; q < 12; ++q) {
+            const int sum = __reduce_add_sync(kFull, dep ? t[q] : 0);
+            if (lane == first && sum) atomicAdd(em_term_ptr(J, i, j, k, q), (unsigned long long)(long long)sum);
+        }
+        return;
+    }
+    const unsigned grp = __match_any_sync(kFull, dep ? key : -1 - lane);
+    const bool single = __popc(grp) == 1;
+    if (dep && single) {
+#pragma unroll
+        for (int q = 0; q < 12; ++q)
+            if (t[q]) atomicAdd(em_term_ptr(J, i, j, k, q), (unsigned long long)(long long)t[q]);
+    }
+    unsigned multi = __ballot_sync(kFull, dep && !single);
+    while (multi) {
+        const int leader = __ffs(multi) - 1;
+        const unsigned members = __shfl_sync(kFull, grp, leader);
+        const bool in = (members >> lane) & 1u;
+#pragma unroll
+        for (int q = 0; q < 12; ++q) {
+            const int sum = __reduce_add_sync(kFull, in ? t[q] : 0);
+            if (lane == leader && sum) atomicAdd(em_term_ptr(J, i, j, k, q), (unsigned long long)(long long)sum);
+        }
+        multi &= ~members;
+    }
+}
+
+// The current of one particle move: the old-cell half from f_old/w_old at
+// cell (oi, oj, ok) and, when the particle is still valid, the new-cell half at
+// its new cell; a particle that stayed in its cell adds both halves in one
+// warp sum. Every lane of the warp calls it.
+__device__ __forceinline__ void em_warp_move_current(const EdgeFix& J, bool had, int oi, int oj, int ok,
+                                                     const float fo[3], const float wo[3], bool live, int ni, int nj,
+                                                     int nk, const float fn[3], const float wn[3]) {
+    int t[12];
+    const bool same = live && ni == oi && nj == oj && nk == ok;
+    if (had) em_terms(fo, wo, t);
+    else {
+#pragma unroll
+        for (int q = 0; q < 12; ++q) t[q] = 0;
+    }
+    if (same) {
+        int u[12];
+        em_terms(fn, wn, u);
+#pragma unroll
+        for (int q = 0; q < 12; ++q) t[q] += u[q];
+    }
+    em_warp_add(J, had, oi, oj, ok, t);
+    const bool cross = live && !same;
+    if (__any_sync(kFull, cross)) {
+        if (cross) em_terms(fn, wn, t);
+        else {
+#pragma unroll
+            for (int q = 0; q < 12; ++q) t[q] = 0;
+        }
+        em_warp_add(J, cross, ni, nj, nk, t);
+    }
+}
+
+// The mixed mode's particle pass of the EM step over the unsorted slots
+// [a.lo, count): the old-cell half of the current, the move with the boundary
+// rules, the new-cell half, the body test and the rho deposit
+// (updateParticlePositionEM, then updateRho's per-particle part,
+// RootGridField.cpp:1168-1196). push_brick_kernel<.., true> takes the sorted bricks.
+__global__ void __launch_bounds__(kThreads) em_tail_kernel(PushArgs a, EdgeFix J) {
+    const long long n = (long long)min(*a.count, (unsigned long long)a.cap);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    double npushed = 0.0, nkept = 0.0;
+    for (long long base = a.lo + (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        const long long idx = base + (threadIdx.x & 31);
+        const int32_t cell = idx < n ? a.p.cell[idx] : -1;
+        bool live = cell >= 0;
+        PState st{0, 0, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        float fo[3] = {0.f, 0.f, 0.f}, wo[3] = {0.f, 0.f, 0.f}, fn[3] = {0.f, 0.f, 0.f}, wn[3] = {0.f, 0.f, 0.f};
+        if (live) {
+            unpack_cell(cell, st.i, st.j, st.k);
+            st.ox = a.p.ox[idx]; st.oy = a.p.oy[idx]; st.oz = a.p.oz[idx];
+            st.vx = a.p.vx[idx]; st.vy = a.p.vy[idx]; st.vz = a.p.vz[idx];
+            em_half_old(st, fo, wo);
+        }
+        const int oi = st.i, oj = st.j, ok = st.k;
+        if (live) live = move_boundary(a, st);
+        if (live) em_half_new(st, fn, wn);
+        em_warp_move_current(J, cell >= 0, oi, oj, ok, fo, wo, live, st.i, st.j, st.k, fn, wn);
+        if (absorb_check(a, st, live)) live = false;
+        if (warp_deposit(a.rho, a.g, live, live ? lin(a.g, st.i, st.j, st.k) : 0, st.ox, st.oy, st.oz))
+            atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_RHO_OVERFLOW);
+        npushed += cell >= 0 ? 1.0 : 0.0;
+        nkept += live ? 1.0 : 0.0;
+        if (cell >= 0) {
+            a.p.cell[idx] = live ? pack_cell(st.i, st.j, st.k) : -1;
+            a.p.ox[idx] = st.ox; a.p.oy[idx] = st.oy; a.p.oz[idx] = st.oz;
+        }
+    }
+    const double np = block_sum(npushed), nk = block_sum(nkept);
+    if (threadIdx.x == 0) {
+        if (np > 0.0) atomicAdd(&a.sc->pushed[a.s], (unsigned long long)np);
+        if (nk > 0.0) atomicAdd(&a.sc->survived[a.s], (unsigned long long)nk);
+    }
+}
+
+// J_d = sum_s q_s size_s 2^-40 (fixed-point sums), FP64, for the three edge arrays.
+struct FixScales { double v[FOPIS_MAX_SPECIES]; };
+__global__ void em_j_convert_kernel(const unsigned long long* fix, long long per_species, int nsp, FixScales sc,
+                                    double* jx, long long nx, double* jy, long long ny, double* jz) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < per_species;
+         t += (long long)gridDim.x * blockDim.x) {   // the three arrays back to back
+        double v = 0.0;
+        for (int s = 0; s < nsp; ++s) v += sc.v[s] * (double)(long long)fix[(long long)s * per_species + t];
+        if (t < nx) jx[t] = v;
+        else if (t < nx + ny) jy[t - nx] = v;
+        else jz[t - nx - ny] = v;
+    }
+}
+
 // ------------------------------------------------------------------ brick push
 // push_brick_kernel: the fused push (gather + Boris + move + boundaries +
 // absorption flag + deposit + kinetic energy) over the brick-sorted particles,
@@ -626,8 +821,9 @@ __device__ __forceinline__ void corners_from_moments(unsigned long long M[8]) {
             if (!(T & axis)) M[T] = (M[T] << kDepositBits) - M[T | axis];
 }
 
-template <int MINB>
-__global__ void __launch_bounds__(kBrickThreads, MINB) push_brick_kernel(PushArgs a, const int32_t* brick_start) {
+template <int MINB, bool EM>
+__global__ void __launch_bounds__(kBrickThreads, MINB) push_brick_kernel(PushArgs a, const int32_t* brick_start,
+                                                                         EdgeFix J) {
     __shared__ __align__(16) unsigned s_mom[kPlanes * kWinCells];
     __shared__ __align__(16) unsigned long long s_batch[kBatchPad];    // batch entries; node tile in the epilogue
     unsigned* const t_lo = reinterpret_cast<unsigned*>(s_batch);
@@ -675,7 +871,23 @@ __global__ void __launch_bounds__(kBrickThreads, MINB) push_brick_kernel(PushArg
                     const long long idx = c0 + q;
                     bool live = cell[r] >= 0;
                     PState st{0, 0, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-                    if (live) {
+                    if constexpr (EM) {
+                        // the EM step: velocities were updated by em_velocity_kernel; the move
+                        // carries the two halves of the charge-conserving current
+                        float fo[3] = {0.f, 0.f, 0.f}, wo[3] = {0.f, 0.f, 0.f};
+                        float fn[3] = {0.f, 0.f, 0.f}, wn[3] = {0.f, 0.f, 0.f};
+                        const bool had = live;
+                        if (live) {
+                            unpack_cell(cell[r], st.i, st.j, st.k);
+                            st.ox = f[r][0]; st.oy = f[r][1]; st.oz = f[r][2];
+                            st.vx = f[r][3]; st.vy = f[r][4]; st.vz = f[r][5];
+                            em_half_old(st, fo, wo);
+                        }
+                        const int oi = st.i, oj = st.j, ok = st.k;
+                        if (live) live = move_boundary(a, st);
+                        if (live) em_half_new(st, fn, wn);
+                        em_warp_move_current(J, had, oi, oj, ok, fo, wo, live, st.i, st.j, st.k, fn, wn);
+                    } else if (live) {
                         unpack_cell(cell[r], st.i, st.j, st.k);
                         st.ox = f[r][0]; st.oy = f[r][1]; st.oz = f[r][2];
                         st.vx = f[r][3]; st.vy = f[r][4]; st.vz = f[r][5];
@@ -2090,7 +2302,7 @@ void launch_push(Ctx& c, bool vel, bool pos, bool dep) {
         } else if (vel && pos && dep && c.sorted_n[s] > 0 && c.brick_start[s]) {
             PushArgs a = push_args<float>(c, s);
             ++c.launches;
-            push_brick_kernel<4><<<brick_count(c), kBrickThreads, 0, c.st>>>(a, c.brick_start[s]);
+            push_brick_kernel<4, false><<<brick_count(c), kBrickThreads, 0, c.st>>>(a, c.brick_start[s], EdgeFix{});
             a.lo = c.sorted_n[s];
             ++c.launches;
             push_kernel<float, true, true, true><<<grid_for(std::max<int64_t>(c.cap[s] - a.lo, 1)), kThreads, 0, c.st>>>(a);
@@ -2113,6 +2325,36 @@ void launch_em_velocity(Ctx& c) {
         else em_velocity_kernel<float><<<grid_for(c.cap[s]), kThreads, 0, c.st>>>(push_args<float>(c, s), node_b<float>(c));
         FOPIS_LAUNCH_CHECK();
     }
+}
+
+// The mixed mode's EM particle pass: per species the brick-sorted slots with
+// push_brick_kernel<.., true> and the appended tail with em_tail_kernel (move,
+// fixed-point current halves, body test, rho deposit), then J in FP64 and its
+// periodic folds. The caller zeroes rho and the fixed-point sums.
+void launch_em_move(Ctx& c) {
+    const long long nxe = (long long)(c.cx - 1) * c.cy * c.cz, nye = (long long)c.cx * (c.cy - 1) * c.cz;
+    const long long per = nxe + nye + (long long)c.cx * c.cy * (c.cz - 1);
+    FixScales sc{};
+    for (int s = 0; s < c.nsp; ++s) {
+        sc.v[s] = c.p.species[s].charge * c.p.species[s].size / (double)kCurrentScale;
+        if (c.cap[s] == 0) continue;
+        unsigned long long* base = c.em.jfix + (size_t)s * per;
+        const EdgeFix J{base, base + nxe, base + nxe + nye, c.cx, c.cy, c.cz};
+        PushArgs a = push_args<float>(c, s);
+        if (c.sorted_n[s] > 0 && c.brick_start[s]) {
+            ++c.launches;
+            push_brick_kernel<3, true><<<brick_count(c), kBrickThreads, 0, c.st>>>(a, c.brick_start[s], J);
+            a.lo = c.sorted_n[s];
+        }
+        ++c.launches;
+        em_tail_kernel<<<grid_for(std::max<int64_t>(c.cap[s] - a.lo, 1)), kThreads, 0, c.st>>>(a, J);
+        FOPIS_LAUNCH_CHECK();
+    }
+    ++c.launches;
+    em_j_convert_kernel<<<grid_for(per), kThreads, 0, c.st>>>(c.em.jfix, per, c.nsp, sc, c.em.j[0], nxe, c.em.j[1], nye,
+                                                              c.em.j[2]);
+    FOPIS_LAUNCH_CHECK();
+    em_fold_currents(c);
 }
 
 // RootGrid::updateParticlePositionEM: J = 0 (Field::initializeCurrent), the
