@@ -188,11 +188,15 @@ WORKLOADS = {
     "cube128_plain": ("128^3 cells Dirichlet + 6-face injection, e+i mass ratio 100, 16^3 conductor cube", 32),
     "craft256": ("256^3 cells Dirichlet + 6-face injection, e+i mass ratio 100, 32x16x16 body + 48x4x16 panel "
                  "with +x photoemission", 32),
+    "em128": ("EM solver (FDTD with damping layers), 128^3 cells Dirichlet + 6-face injection, e+i mass ratio 100, "
+              "Te = 5 keV, n = 1e12 m^-3, Courant 0.5, no object", 32),
 }
 
 
 def workload_desc(name: str, ppc) -> str:
     text, default_ppc = WORKLOADS[name]
+    if name == "em128":
+        return f"{name}: {text}, {ppc or default_ppc} ppc/species, one Poisson solve at start-up (MG to 1e-8)"
     solves = "1 solve/step" if name == "periodic32" else "2 solves/step"
     return f"{name}: {text}, {ppc or default_ppc} ppc/species, MG to ||r||/||f|| <= 1e-8, {solves}"
 
@@ -496,6 +500,65 @@ def craft256_block(args, local, steps: int = 8, warmup: int = 2):
     return out
 
 
+# Algorithmic bytes of one FDTD update per interior index of the extended Yee
+# grid: three edge (face) components read and written, three of the other
+# field read (the neighbours come from cache).
+FDTD_BYTES_PER_INDEX = 72
+
+
+def em128_block(args, local, steps: int = 6, warmup: int = 2):
+    """The EM solver's step (RootGrid::mainLoopEM) on the em128 workload: ms/step,
+    particle-steps/s, phase times, and the HBM fractions of the FDTD updates
+    (72 B per interior index of the 389^3 extended grid) and of the particle
+    passes (velocity 40 B, move + current + deposit 44 B per particle: the
+    state read, the position part written). Timed with CUDA events on the
+    library stream."""
+    import torch
+    from fopis_b200 import RootGrid, config
+    cfg = config.workload("em128", seed=20251203, sort_interval=args.sort_interval)
+    g = RootGrid(cfg, device=local)
+    g.generate_ambient()
+    g.initialize()
+    for _ in range(warmup):
+        g.mainLoopEM(1)
+    stream = torch.cuda.ExternalStream(g.stream_ptr(), device=torch.device("cuda", local))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    psteps, ph = 0, np.zeros(8)
+    torch.cuda.synchronize(local)
+    e0.record(stream)
+    for _ in range(steps):
+        g.mainLoopEM(1)
+        st = g.stats()
+        psteps += total_particles(st, cfg.params.nspecies)
+        ph += np.array(st.ms_phase[:8])
+    e1.record(stream)
+    torch.cuda.synchronize(local)
+    ms = e0.elapsed_time(e1)
+    ph /= steps
+    hbm, _ = peaks()
+    _, n = g.field_shape(32)                                  # ex: one shorter than the grid along x
+    interior = (n[0] - 1) * (n[1] - 2) * (n[2] - 2)          # the updates' index range [lo+1, up-1)^3
+    npart = psteps / steps
+    gbs = lambda b, t: b / (t * 1e-3) / 1e9
+    out = {"workload": workload_desc("em128", None), "steps": steps, "warmup": warmup,
+           "ms_per_step": ms / steps, "particle_steps_per_s": psteps / (ms * 1e-3), "particles": int(npart),
+           "yee_grid": [n[0] + 1, n[1], n[2]],
+           "phases_ms": {k: round(float(v), 4) for k, v in zip(
+               ["velocity", "emit", "move_current_deposit_inject", "-", "rho_tail", "efield_fdtd", "bfield_fdtd",
+                "sort"], ph)},
+           "roofline": {
+               "efield_fdtd": {"achieved": gbs(FDTD_BYTES_PER_INDEX * interior, ph[5]), "peak": hbm, "unit": "GB/s",
+                               "frac": gbs(FDTD_BYTES_PER_INDEX * interior, ph[5]) / hbm},
+               "bfield_fdtd": {"achieved": gbs(FDTD_BYTES_PER_INDEX * interior, ph[6]), "peak": hbm, "unit": "GB/s",
+                               "frac": gbs(FDTD_BYTES_PER_INDEX * interior, ph[6]) / hbm},
+               "velocity": {"achieved": gbs(40 * npart, ph[0]), "peak": hbm, "unit": "GB/s",
+                            "frac": gbs(40 * npart, ph[0]) / hbm},
+               "move_current_deposit": {"achieved": gbs(44 * npart, ph[2]), "peak": hbm, "unit": "GB/s",
+                                        "frac": gbs(44 * npart, ph[2]) / hbm}}}
+    g.close()
+    return out
+
+
 def reference_cmatrix(cfg):
     """Capacity matrix for the CPU arms, as the reference's use_existing_capacity_matrix
     would load it: the exact sine-basis build of the oracle (host only, untimed)."""
@@ -559,6 +622,8 @@ def main():
     ap.add_argument("--learned-lr", type=float, default=1e-3)
     ap.add_argument("--mixed-vs-fp64", type=int, default=100,
                     help="steps of the mixed-precision run against the FP64 GPU mode on the same seed (0: skip)")
+    ap.add_argument("--no-em128", dest="em128", action="store_false",
+                    help="skip the EM-solver block (em128 workload)")
     ap.add_argument("--no-craft256", dest="craft256", action="store_false",
                     help="skip the 256^3 spacecraft block")
     ap.add_argument("--guess", default="history", choices=["warm", "history"],
@@ -653,6 +718,8 @@ def main():
         line["mixed_vs_fp64"] = mixed_vs_fp64(args, local, res["cmatrix"], args.mixed_vs_fp64)
     if args.craft256 and world == 1 and args.workload != "craft256":
         line["craft256"] = craft256_block(args, local)
+    if args.em128 and world == 1 and args.workload != "em128":
+        line["em128"] = em128_block(args, local)
     if rank == 0 and res["cmatrix"] is not None:
         try:
             Cx = reference_cmatrix(cfg)

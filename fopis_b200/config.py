@@ -338,14 +338,20 @@ def workload(name: str, ppc: Optional[int] = None, seed: int = 20251203, obj_par
     cube64       64^3 cells Dirichlet + injection, 8^3 cube conductor, 32 ppc;
     cube128      128^3 cells Dirichlet + injection, 16^3 cube, photoemission from +x;
     cube128_plain same without photoemission;
-    craft256     256^3 cells, 32x16x16 body + 48x4x16 panel, photoemission.
-    Electrons + ions (mass ratio 100), Te = Ti = 1 eV, n = 1e7 m^-3."""
+    craft256     256^3 cells, 32x16x16 body + 48x4x16 panel, photoemission;
+    em128        the EM solver on 128^3 cells Dirichlet + injection, no object,
+                 Te = 5 keV, n = 1e12 m^-3, dx = 0.5 m, dt = dx / (2 c) (Courant 0.5).
+    Electrons + ions (mass ratio 100), Te = Ti = 1 eV, n = 1e7 m^-3 (em128 as stated)."""
     dx, dt = plasma_units()
     n0, te = 1e7, 1.0
+    if name == "em128":
+        dx, n0, te = 0.5, 1e12, 5e3
+        dt = 0.5 * dx / CLIGHT
+        kw.setdefault("solver", "EM")
     if ppc is None:
         ppc = 16 if name == "periodic32" else 32
     e_sp = SpeciesInfo("Electron", "ambient", 1.0, -1.0, n0, te, ppc)
-    i_sp = SpeciesInfo("Ion", "ambient", 100.0, 1.0, n0, te, ppc)
+    i_sp = SpeciesInfo("Ion", "ambient", 100.0, 1.0, n0, 1.0 if name == "em128" else te, ppc)
     species = [e_sp, i_sp]
     shine = (0.0, 0.0, 0.0)
     boxes = []
@@ -359,6 +365,8 @@ def workload(name: str, ppc: Optional[int] = None, seed: int = 20251203, obj_par
         nxyz, boundary = (129, 129, 129), "DDDDDD"
         boxes = [((-8, -8, -8), (8, 8, 8))]
         photo = name == "cube128"
+    elif name == "em128":
+        nxyz, boundary = (129, 129, 129), "DDDDDD"
     elif name == "craft256":
         nxyz, boundary = (257, 257, 257), "DDDDDD"
         boxes = [((-16, -8, -8), (16, 8, 8)), ((-24, 8, -8), (24, 12, 8))]
