@@ -263,7 +263,8 @@ def run_gpu(args, world, rank, local):
             n = pushed_particles(st, nsp)
             psteps += n
             pushed.append(n)
-            push_ms.append(st.ms_phase[0])
+            # the push phase: the fused ES push, or the EM step's move + current + deposit pass
+            push_ms.append(st.ms_phase[2] if args.workload == "em128" else st.ms_phase[0])
             phases_all.append([round(x, 3) for x in st.ms_phase])
             vcyc.append(st.vcycles_step)
             pointwise.append(st.residual_pointwise)
@@ -674,10 +675,13 @@ def main():
     res, cfg = run_gpu(args, world, rank, local)
     value = res["psteps"] / (res["ms"] * 1e-3)
     push_bytes = PUSH_BYTES_PER_PARTICLE if args.precision == "mixed" else PUSH_BYTES_FP64
+    em = args.workload == "em128"
+    if em:
+        push_bytes = 44.0 if args.precision == "mixed" else 2 * PUSH_BYTES_FP64
     achieved = push_bytes * res["pushed"] / (res["push_ms"] * 1e-3) / 1e9
     traffic = None
     prof = ROOT / "profiles" / "push_kernel_cube64.md"
-    if prof.exists() and args.precision == "mixed":
+    if prof.exists() and args.precision == "mixed" and not em:
         # DRAM bytes per particle of one push_brick_kernel launch, from the committed ncu summary
         m = re.search(r"\| dram_bytes_per_particle \| ([0-9.]+) \|", prof.read_text())
         if m:
@@ -685,7 +689,8 @@ def main():
     line = dict(base, value=value, steps=args.steps, warmup=args.warmup, ms_per_step=res["ms"] / args.steps)
     line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                         "traffic": traffic,
-                        "kernel": ("push_brick_kernel + tail push_kernel (all species)" if args.precision == "mixed"
+                        "kernel": ("push_brick_kernel<3, true> + em_tail_kernel (move, current, deposit)" if em
+                                   else "push_brick_kernel + tail push_kernel (all species)" if args.precision == "mixed"
                                    else "push_kernel<double> (all species)"),
                         "peak_kind": peak_kind,
                         "bytes_per_particle": push_bytes}
@@ -700,8 +705,9 @@ def main():
     line["solve_mode"] = res["solve_mode"]
     line["vcycles_per_step"] = res["vcycles_per_step"]
     line["particles"] = res["particles"]
-    line["phases_ms_last_step"] = dict(zip(["push", "emit", "inject", "absorb", "rho+solve1", "solve2", "efield",
-                                            "sort"], [round(x, 4) for x in res["phases_last"]]))
+    names = (["velocity", "emit", "move_current_deposit_inject", "-", "rho_tail", "efield_fdtd", "bfield_fdtd", "sort"]
+             if em else ["push", "emit", "inject", "absorb", "rho+solve1", "solve2", "efield", "sort"])
+    line["phases_ms_last_step"] = dict(zip(names, [round(x, 4) for x in res["phases_last"]]))
     line["spacecraft_potential_V"] = res["potential_V"]
     line["step_ms"] = res["step_ms"]
     if args.phases:

@@ -258,9 +258,11 @@ int em_step(Ctx& c) {
     record(c, 8);
     const int rc = check_device(c);
     update_currents(c);
-    if (!c.fp64)
-        for (int s = 0; s < c.nsp; ++s)
-            if (c.timestep % si != 0) c.valid[s] = (int64_t)(c.h_sc->survived[s] + c.h_sc->added[s]);
+    for (int s = 0; s < c.nsp; ++s) {
+        // the mixed pass counts the particles it moved; the FP64 path's in-use slots stand in
+        c.pushed_step[s] = c.fp64 ? (int64_t)c.h_sc->count[s] : (int64_t)c.h_sc->pushed[s];
+        if (!c.fp64 && c.timestep % si != 0) c.valid[s] = (int64_t)(c.h_sc->survived[s] + c.h_sc->added[s]);
+    }
     c.energy_valid = false;
     c.timestep += 1;
     if (c.ev[0]) {
