@@ -1837,6 +1837,17 @@ void orc_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
 }
 
 // The oracle's Position::setXYZ on n points: ijk[3n], d[6n] = dx1,dy1,dz1,dx2,dy2,dz2.
+// The oracle's zigzag relay point (relay, used by update_position_em) per pair of
+// new and old positions.
+void orc_relay(const double* new_xyz, const double* old_xyz, int64_t n, double* out) {
+    for (int64_t t = 0; t < n; ++t) {
+        const Pos nw = posXYZ(new_xyz[3 * t], new_xyz[3 * t + 1], new_xyz[3 * t + 2]);
+        const Pos od = posXYZ(old_xyz[3 * t], old_xyz[3 * t + 1], old_xyz[3 * t + 2]);
+        out[3 * t] = relay(nw.i, od.i, nw.x, od.x);
+        out[3 * t + 1] = relay(nw.j, od.j, nw.y, od.y);
+        out[3 * t + 2] = relay(nw.k, od.k, nw.z, od.z);
+    }
+}
 void orc_position(const double* xyz, int64_t n, int32_t* ijk, double* d) {
     for (int64_t t = 0; t < n; ++t) {
         const Pos p = posXYZ(xyz[3 * t], xyz[3 * t + 1], xyz[3 * t + 2]);

@@ -63,6 +63,7 @@ def lib():
             "orc_position": (None, [vp, C.c_int64, vp, vp]),
             "orc_get_incidents": (C.c_int64, [vp, dp, C.c_int64]),
             "orc_update_bfield": (None, [vp]), "orc_bfield_energy": (C.c_double, [vp]),
+            "orc_relay": (None, [vp, vp, C.c_int64, vp]),
             "orc_field_shape": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
             "orc_set_incidents": (None, [vp, dp, C.c_int64]),
         }
@@ -112,6 +113,29 @@ def position(xyz: np.ndarray):
     d = np.zeros((n, 6), np.float64)
     lib().orc_position(xyz.ctypes.data, n, ijk.ctypes.data, d.ctypes.data)
     return ijk, d
+
+
+def relay(new_xyz: np.ndarray, old_xyz: np.ndarray) -> np.ndarray:
+    """The oracle's zigzag relay points for pairs of positions."""
+    a = np.ascontiguousarray(new_xyz, np.float64)
+    b = np.ascontiguousarray(old_xyz, np.float64)
+    out = np.zeros_like(a)
+    lib().orc_relay(a.ctypes.data, b.ctypes.data, len(a), out.ctypes.data)
+    return out
+
+
+def ref_relay(new_xyz: np.ndarray, old_xyz: np.ndarray):
+    """The reference's own Position::getReferencePosition (oracle/_ref), or None
+    where the reference sources were absent at build time."""
+    if not REF_PIN.exists():
+        return None
+    L = C.CDLL(str(REF_PIN))
+    L.ref_relay.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+    a = np.ascontiguousarray(new_xyz, np.float64)
+    b = np.ascontiguousarray(old_xyz, np.float64)
+    out = np.zeros_like(a)
+    L.ref_relay(a.ctypes.data, b.ctypes.data, len(a), out.ctypes.data)
+    return out
 
 
 def ref_position(xyz: np.ndarray):

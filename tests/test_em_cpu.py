@@ -296,3 +296,26 @@ def test_oracle_fdtd_matches_numpy(boundary):
         assert err <= 1e-13, (which, err)
         assert np.max(np.abs(got - f[q])) > 1e-3          # the update changed it
     o.close()
+
+
+def test_relay_point_pinned_to_reference():
+    """The oracle's zigzag relay point against the reference's own
+    Position::getReferencePosition (include/position.hpp:88-96, compiled into
+    oracle/_ref): moves within a cell, across one face, across two and three
+    faces, onto and off exact integer coordinates, below zero (periodic glue)."""
+    rng = np.random.default_rng(4)
+    old = rng.uniform(-1.0, 20.0, (20000, 3))
+    step = rng.uniform(-0.99, 0.99, (20000, 3))
+    new = old + step
+    old[:500] = np.floor(old[:500])                 # start on a node
+    new[500:1000] = np.floor(new[500:1000])         # end on a node
+    new[1000:1500] = old[1000:1500]                 # no move
+    want = orc.ref_relay(new, old)
+    if want is None:
+        pytest.skip("oracle/_ref was not built (reference sources absent)")
+    got = orc.relay(new, old)
+    assert np.array_equal(got, want)
+    # the relay sits on the shared face when the cells differ
+    cross = np.floor(new[:, 0]) != np.floor(old[:, 0])
+    assert cross.sum() > 1000
+    assert np.all(got[cross, 0] == np.maximum(np.floor(new[cross, 0]), np.floor(old[cross, 0])))
