@@ -602,7 +602,7 @@ def run_oracle(cfg, Cm, threads: int, steps: int, warmup: int = 0, budget_s: flo
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fopis", choices=["fopis", "reference"])
     ap.add_argument("--workload", default="cube128")
