@@ -612,35 +612,65 @@ __device__ __forceinline__ void em_warp_add(const EdgeFix& J, bool dep, int i, i
     }
 }
 
-// The current of one particle move: the old-cell half from f_old/w_old at
-// cell (oi, oj, ok) and, when the particle is still valid, the new-cell half at
-// its new cell; a particle that stayed in its cell adds both halves in one
-// warp sum. Every lane of the warp calls it.
+// Both halves of a move that stays in its cell, summed in closed form: with the
+// midpoint m = x + v/2 and d = v/4 per axis, the two halves' x-edge terms
+// (v/2)[(1 - m_y - d_y)(1 - m_z - d_z) + (1 - m_y + d_y)(1 - m_z + d_z)] ... are
+// v_x [(1 - m_y)(1 - m_z) + d_y d_z], v_x [m_y (1 - m_z) - d_y d_z], ... (the
+// relay point of both halves is the midpoint, include/position.hpp:88-96).
+__device__ __forceinline__ void em_terms_same(const float o[3], const float v[3], int t[12]) {
+    float m[3], d[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) { m[a] = o[a] + 0.5f * v[a]; d[a] = 0.25f * v[a]; }
+    const float s0 = kCurrentScale * v[0], s1 = kCurrentScale * v[1], s2 = kCurrentScale * v[2];
+    const float dyz = d[1] * d[2], dxz = d[0] * d[2], dxy = d[0] * d[1];
+    t[0] = __float2int_rn(s0 * ((1.0f - m[1]) * (1.0f - m[2]) + dyz));
+    t[1] = __float2int_rn(s0 * (m[1] * (1.0f - m[2]) - dyz));
+    t[2] = __float2int_rn(s0 * ((1.0f - m[1]) * m[2] - dyz));
+    t[3] = __float2int_rn(s0 * (m[1] * m[2] + dyz));
+    t[4] = __float2int_rn(s1 * ((1.0f - m[0]) * (1.0f - m[2]) + dxz));
+    t[5] = __float2int_rn(s1 * (m[0] * (1.0f - m[2]) - dxz));
+    t[6] = __float2int_rn(s1 * ((1.0f - m[0]) * m[2] - dxz));
+    t[7] = __float2int_rn(s1 * (m[0] * m[2] + dxz));
+    t[8] = __float2int_rn(s2 * ((1.0f - m[0]) * (1.0f - m[1]) + dxy));
+    t[9] = __float2int_rn(s2 * (m[0] * (1.0f - m[1]) - dxy));
+    t[10] = __float2int_rn(s2 * ((1.0f - m[0]) * m[1] - dxy));
+    t[11] = __float2int_rn(s2 * (m[0] * m[1] + dxy));
+}
+
+// The current of one particle move, from the start offsets o0 and velocity of
+// the particle in cell (oi, oj, ok) and its state after the move (st, live):
+// a move that stays in its cell adds both halves at once (em_terms_same);
+// otherwise the old-cell half goes to the old cell and, while the particle is
+// still valid, the new-cell half to the new one. Every lane of the warp calls it.
 __device__ __forceinline__ void em_warp_move_current(const EdgeFix& J, bool had, int oi, int oj, int ok,
-                                                     const float fo[3], const float wo[3], bool live, int ni, int nj,
-                                                     int nk, const float fn[3], const float wn[3]) {
+                                                     const float o0[3], const PState& st, bool live) {
+    const float v[3] = {st.vx, st.vy, st.vz};
     int t[12];
-    const bool same = live && ni == oi && nj == oj && nk == ok;
-    if (had) em_terms(fo, wo, t);
-    else {
+    const bool same = live && st.i == oi && st.j == oj && st.k == ok;
+    if (same) {
+        em_terms_same(o0, v, t);
+    } else if (had) {
+        PState s0 = st;
+        s0.ox = o0[0]; s0.oy = o0[1]; s0.oz = o0[2];
+        float f[3], w[3];
+        em_half_old(s0, f, w);
+        em_terms(f, w, t);
+    } else {
 #pragma unroll
         for (int q = 0; q < 12; ++q) t[q] = 0;
-    }
-    if (same) {
-        int u[12];
-        em_terms(fn, wn, u);
-#pragma unroll
-        for (int q = 0; q < 12; ++q) t[q] += u[q];
     }
     em_warp_add(J, had, oi, oj, ok, t);
     const bool cross = live && !same;
     if (__any_sync(kFull, cross)) {
-        if (cross) em_terms(fn, wn, t);
-        else {
+        if (cross) {
+            float f[3], w[3];
+            em_half_new(st, f, w);
+            em_terms(f, w, t);
+        } else {
 #pragma unroll
             for (int q = 0; q < 12; ++q) t[q] = 0;
         }
-        em_warp_add(J, cross, ni, nj, nk, t);
+        em_warp_add(J, cross, st.i, st.j, st.k, t);
     }
 }
 
@@ -658,17 +688,15 @@ __global__ void __launch_bounds__(kThreads) em_tail_kernel(PushArgs a, EdgeFix J
         const int32_t cell = idx < n ? a.p.cell[idx] : -1;
         bool live = cell >= 0;
         PState st{0, 0, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        float fo[3] = {0.f, 0.f, 0.f}, wo[3] = {0.f, 0.f, 0.f}, fn[3] = {0.f, 0.f, 0.f}, wn[3] = {0.f, 0.f, 0.f};
         if (live) {
             unpack_cell(cell, st.i, st.j, st.k);
             st.ox = a.p.ox[idx]; st.oy = a.p.oy[idx]; st.oz = a.p.oz[idx];
             st.vx = a.p.vx[idx]; st.vy = a.p.vy[idx]; st.vz = a.p.vz[idx];
-            em_half_old(st, fo, wo);
         }
         const int oi = st.i, oj = st.j, ok = st.k;
+        const float o0[3] = {st.ox, st.oy, st.oz};
         if (live) live = move_boundary(a, st);
-        if (live) em_half_new(st, fn, wn);
-        em_warp_move_current(J, cell >= 0, oi, oj, ok, fo, wo, live, st.i, st.j, st.k, fn, wn);
+        em_warp_move_current(J, cell >= 0, oi, oj, ok, o0, st, live);
         if (absorb_check(a, st, live)) live = false;
         if (warp_deposit(a.rho, a.g, live, live ? lin(a.g, st.i, st.j, st.k) : 0, st.ox, st.oy, st.oz))
             atomicOr(&a.sc->status, (unsigned)FOPIS_DEV_RHO_OVERFLOW);
@@ -874,19 +902,16 @@ __global__ void __launch_bounds__(kBrickThreads, MINB) push_brick_kernel(PushArg
                     if constexpr (EM) {
                         // the EM step: velocities were updated by em_velocity_kernel; the move
                         // carries the two halves of the charge-conserving current
-                        float fo[3] = {0.f, 0.f, 0.f}, wo[3] = {0.f, 0.f, 0.f};
-                        float fn[3] = {0.f, 0.f, 0.f}, wn[3] = {0.f, 0.f, 0.f};
                         const bool had = live;
                         if (live) {
                             unpack_cell(cell[r], st.i, st.j, st.k);
                             st.ox = f[r][0]; st.oy = f[r][1]; st.oz = f[r][2];
                             st.vx = f[r][3]; st.vy = f[r][4]; st.vz = f[r][5];
-                            em_half_old(st, fo, wo);
                         }
                         const int oi = st.i, oj = st.j, ok = st.k;
+                        const float o0[3] = {st.ox, st.oy, st.oz};
                         if (live) live = move_boundary(a, st);
-                        if (live) em_half_new(st, fn, wn);
-                        em_warp_move_current(J, had, oi, oj, ok, fo, wo, live, st.i, st.j, st.k, fn, wn);
+                        em_warp_move_current(J, had, oi, oj, ok, o0, st, live);
                     } else if (live) {
                         unpack_cell(cell[r], st.i, st.j, st.k);
                         st.ox = f[r][0]; st.oy = f[r][1]; st.oz = f[r][2];
