@@ -319,3 +319,49 @@ def test_relay_point_pinned_to_reference():
     cross = np.floor(new[:, 0]) != np.floor(old[:, 0])
     assert cross.sum() > 1000
     assert np.all(got[cross, 0] == np.maximum(np.floor(new[cross, 0]), np.floor(old[cross, 0])))
+
+
+def test_oracle_em_velocity_matches_restatement():
+    """Grid::updateParticleVelocityEM (src/Grid/GridParticleTreatmentEM.cpp:13-105)
+    restated in numpy on the oracle's own nodal E and B: CIC weights times 0.5 q/m,
+    boris = 2 / (1 + |b|^2) with the gathered b."""
+    cfg = em_config(n=9)
+    p = cfg.params
+    o = orc.Oracle(p)
+    rng = np.random.default_rng(12)
+    for which in range(32, 38):               # random Yee fields, then the nodal references
+        o.set_field(which, rng.standard_normal(o.field_shape(which)[1]))
+    o.set_field(0, rng.standard_normal((11, 11, 11)))
+    o.update_efield()
+    o.update_bfield()
+    recs = random_particles(500, (0, 0, 0), (8, 8, 8), 0.05, 3, 0)
+    o.load_particles(0, recs)
+    E = [o.field(w) for w in (2, 3, 4)]
+    B = [o.field(w) for w in (5, 6, 7)]
+    assert max(np.max(np.abs(b)) for b in B) > 0.1
+    o.update_velocity()
+    got = o.particles(0)
+    qm = 0.5 * p.species[0].charge / p.species[0].mass
+    x, y, z = recs["x"], recs["y"], recs["z"]
+    i, j, k = (np.floor(c).astype(int) + 1 for c in (x, y, z))
+    dx1, dy1, dz1 = x - (i - 1), y - (j - 1), z - (k - 1)
+    dx2, dy2, dz2 = 1 - dx1, 1 - dy1, 1 - dz1
+    w = [qm * dx2 * dy2 * dz2, qm * dx1 * dy2 * dz2, qm * dx2 * dy1 * dz2, qm * dx1 * dy1 * dz2,
+         qm * dx2 * dy2 * dz1, qm * dx1 * dy2 * dz1, qm * dx2 * dy1 * dz1, qm * dx1 * dy1 * dz1]
+    corners = [(0, 0, 0), (1, 0, 0), (0, 1, 0), (1, 1, 0), (0, 0, 1), (1, 0, 1), (0, 1, 1), (1, 1, 1)]
+
+    def gather(a):
+        return sum(wc * a[i + c[0], j + c[1], k + c[2]] for wc, c in zip(w, corners))
+
+    ex, ey, ez = (gather(a) for a in E)
+    bx, by, bz = (gather(a) for a in B)
+    boris = 2.0 / (1.0 + (bx * bx + by * by + bz * bz))
+    vx1, vy1, vz1 = recs["vx"] + ex, recs["vy"] + ey, recs["vz"] + ez
+    vxt = vx1 + vy1 * bz - vz1 * by
+    vyt = vy1 + vz1 * bx - vx1 * bz
+    vzt = vz1 + vx1 * by - vy1 * bx
+    want = (vx1 + ex + boris * (vyt * bz - vzt * by), vy1 + ey + boris * (vzt * bx - vxt * bz),
+            vz1 + ez + boris * (vxt * by - vyt * bx))
+    for key, wv in zip(("vx", "vy", "vz"), want):
+        assert np.max(np.abs(got[key] - wv)) <= 1e-12 * np.max(np.abs(wv)), key
+    o.close()
