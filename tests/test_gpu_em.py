@@ -32,7 +32,7 @@ NODAL = [_abi.FIELD_EXREF, _abi.FIELD_EYREF, _abi.FIELD_EZREF, _abi.FIELD_BXREF,
 CURRENTS = [_abi.FIELD_JX, _abi.FIELD_JY, _abi.FIELD_JZ]
 
 
-@pytest.mark.parametrize("boundary", ["DDDDDD", "PPDDPP", "PPPPPP"])
+@pytest.mark.parametrize("boundary", ["DDDDDD", "PPDDPP", "PPPPPP", "NDPPDN"])
 def test_fdtd_updates_match_oracle(gpu_available, boundary):
     cfg = em_config(n=10, boundary=boundary)
     g = RootGrid(cfg)
@@ -164,8 +164,11 @@ def test_em_conductor_run_tracks_oracle(gpu_available):
     o.close()
 
 
-def test_em_mixed_precision_tracks_oracle(gpu_available):
-    cfg = em_config(n=13, precision=_abi.MIXED)
+@pytest.mark.parametrize("boundary", ["DDDDDD", "PPPPPP"])
+def test_em_mixed_precision_tracks_oracle(gpu_available, boundary):
+    """The mixed mode's one-pass move with the fixed-point current (the periodic
+    folds included on the P box) against the FP64 oracle."""
+    cfg = em_config(n=13, boundary=boundary, precision=_abi.MIXED)
     g, o = load_pair(cfg, f32=True)
     for _ in range(10):
         g.mainLoopEM(1)
@@ -175,6 +178,29 @@ def test_em_mixed_precision_tracks_oracle(gpu_available):
     pe_g, fe_g = g.getEnergy()
     pe_o, fe_o = o.energy()
     assert pe_g == pytest.approx(pe_o, rel=1e-5)
+    g.close()
+    o.close()
+
+
+def test_em_mixed_conductor_run_tracks_oracle(gpu_available):
+    """The mixed mode with a floating conductor and photoemission: emitted particles
+    move with their current in the tail pass, injected ones deposit as they are
+    created, absorption and the redistribution as in the ES step."""
+    cfg = em_config(n=17, boxes=[((-2, -2, -2), (2, 2, 2))], photo=True, obj_parser=orc.parse_obj,
+                    precision=_abi.MIXED)
+    g, o = load_pair(cfg, f32=True)
+    V = []
+    for _ in range(10):
+        g.mainLoopEM(1)
+        o.main_loop(1)
+        V.append((g.getObject(0)[0], o.get_object(0)[0]))
+    V = np.array(V)
+    assert np.max(np.abs(V[:, 0] - V[:, 1]) / np.abs(V[:, 1])) <= 1e-4
+    for s in range(3):       # FP32 trajectories may cross a face where the FP64 ones do not
+        ng, no = len(g.getParticles(s)), len(o.particles(s))
+        assert abs(ng - no) <= max(5, 2e-3 * no), (s, ng, no)
+    for which in YEE + NODAL:
+        assert rel_err(g.get_field(which), o.field(which)) <= 1e-4, which
     g.close()
     o.close()
 
