@@ -264,7 +264,7 @@ def run_gpu(args, world, rank, local):
             psteps += n
             pushed.append(n)
             # the push phase: the fused ES push, or the EM step's move + current + deposit pass
-            push_ms.append(st.ms_phase[2] if args.workload == "em128" else st.ms_phase[0])
+            push_ms.append(st.ms_phase[0] + st.ms_phase[2] if args.workload == "em128" else st.ms_phase[0])
             phases_all.append([round(x, 3) for x in st.ms_phase])
             vcyc.append(st.vcycles_step)
             pointwise.append(st.residual_pointwise)
@@ -511,9 +511,9 @@ def em128_block(args, local, steps: int = 6, warmup: int = 2):
     """The EM solver's step (RootGrid::mainLoopEM) on the em128 workload: ms/step,
     particle-steps/s, phase times, and the HBM fractions of the FDTD updates
     (72 B per interior index of the 389^3 extended grid) and of the particle
-    passes (velocity 40 B, move + current + deposit 44 B per particle: the
-    state read, the position part written). Timed with CUDA events on the
-    library stream."""
+    pass (the velocity update, the move, the current and the deposit in one
+    pass when no body emits, as here: 56 B per particle, the state read and
+    written). Timed with CUDA events on the library stream."""
     import torch
     from fopis_b200 import RootGrid, config
     cfg = config.workload("em128", seed=20251203, sort_interval=args.sort_interval)
@@ -552,10 +552,8 @@ def em128_block(args, local, steps: int = 6, warmup: int = 2):
                                "frac": gbs(FDTD_BYTES_PER_INDEX * interior, ph[5]) / hbm},
                "bfield_fdtd": {"achieved": gbs(FDTD_BYTES_PER_INDEX * interior, ph[6]), "peak": hbm, "unit": "GB/s",
                                "frac": gbs(FDTD_BYTES_PER_INDEX * interior, ph[6]) / hbm},
-               "velocity": {"achieved": gbs(40 * npart, ph[0]), "peak": hbm, "unit": "GB/s",
-                            "frac": gbs(40 * npart, ph[0]) / hbm},
-               "move_current_deposit": {"achieved": gbs(44 * npart, ph[2]), "peak": hbm, "unit": "GB/s",
-                                        "frac": gbs(44 * npart, ph[2]) / hbm}}}
+               "kick_move_current_deposit": {"achieved": gbs(56 * npart, ph[0] + ph[2]), "peak": hbm, "unit": "GB/s",
+                                             "frac": gbs(56 * npart, ph[0] + ph[2]) / hbm}}}
     g.close()
     return out
 
@@ -677,7 +675,7 @@ def main():
     push_bytes = PUSH_BYTES_PER_PARTICLE if args.precision == "mixed" else PUSH_BYTES_FP64
     em = args.workload == "em128"
     if em:
-        push_bytes = 44.0 if args.precision == "mixed" else 2 * PUSH_BYTES_FP64
+        push_bytes = 56.0 if args.precision == "mixed" else 2 * PUSH_BYTES_FP64
     achieved = push_bytes * res["pushed"] / (res["push_ms"] * 1e-3) / 1e9
     traffic = None
     prof = ROOT / "profiles" / "push_kernel_cube64.md"
@@ -689,7 +687,7 @@ def main():
     line = dict(base, value=value, steps=args.steps, warmup=args.warmup, ms_per_step=res["ms"] / args.steps)
     line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                         "traffic": traffic,
-                        "kernel": ("push_brick_kernel<3, true> + em_tail_kernel (move, current, deposit)" if em
+                        "kernel": ("push_brick_kernel<3, true> + em_tail_kernel (velocity, move, current, deposit)" if em
                                    else "push_brick_kernel + tail push_kernel (all species)" if args.precision == "mixed"
                                    else "push_kernel<double> (all species)"),
                         "peak_kind": peak_kind,

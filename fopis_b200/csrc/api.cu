@@ -224,8 +224,13 @@ int em_step(Ctx& c) {
     step_begin(c);
     FOPIS_CUDA(cudaMemsetAsync(c.d_sc->pushed, 0, 3 * sizeof(c.d_sc->pushed), c.st));
     FOPIS_CUDA(cudaMemsetAsync(&c.d_sc->absorbed_n, 0, sizeof(unsigned long long), c.st));
+    // the mixed pass can give the velocity update itself when no body emits: then no
+    // particle is created between the velocity and the position updates
+    bool emits = false;
+    for (const auto& o : c.objs) emits = emits || o.emit_species >= 0 || o.secondary_species >= 0;
+    const bool kick_in_pass = !c.fp64 && !emits;
     record(c, 0);
-    launch_em_velocity(c);
+    if (!kick_in_pass) launch_em_velocity(c);
     record(c, 1);
     launch_emit(c, false);
     record(c, 2);
@@ -242,7 +247,7 @@ int em_step(Ctx& c) {
                            (size_t)c.cx * c.cy * (c.cz - 1);
         FOPIS_CUDA(cudaMemsetAsync(c.em.jfix, 0, sizeof(unsigned long long) * per * c.nsp, c.st));
         rho_zero(c);
-        launch_em_move(c);
+        launch_em_move(c, kick_in_pass);
         launch_inject(c, true);
     }
     record(c, 3);

@@ -306,7 +306,7 @@ void launch_push(Ctx& c, bool vel, bool pos, bool dep);
 void launch_deposit_all(Ctx& c);
 void launch_em_velocity(Ctx& c);
 void launch_em_position(Ctx& c);
-void launch_em_move(Ctx& c);
+void launch_em_move(Ctx& c, bool kick);
 void launch_emit(Ctx& c, bool fused);
 void launch_inject(Ctx& c, bool fused);
 void launch_absorb(Ctx& c);

@@ -384,36 +384,44 @@ __global__ void __launch_bounds__(kThreads) push_kernel(PushArgsT<T> a) {
 // the CIC gather of the nodal E and B, both scaled by 0.5 q/m, then Boris with
 // the gathered b, boris = 2 / (1 + |b|^2). One particle per thread.
 template <typename T>
+__device__ __forceinline__ void em_kick(const PushArgsT<T>& a, const typename NodeE<T>::type* B, PStateT<T>& st) {
+    const T x1 = st.ox, y1 = st.oy, z1 = st.oz;
+    const T x2 = (T)1 - x1, y2 = (T)1 - y1, z2 = (T)1 - z1;
+    const T w[8] = {a.qm * x2 * y2 * z2, a.qm * x1 * y2 * z2, a.qm * x2 * y1 * z2, a.qm * x1 * y1 * z2,
+                    a.qm * x2 * y2 * z1, a.qm * x1 * y2 * z1, a.qm * x2 * y1 * z1, a.qm * x1 * y1 * z1};
+    const int b = lin(a.g, st.i, st.j, st.k), sj = (int)a.g.sj, si = (int)a.g.si;
+    const int off[8] = {0, si, sj, si + sj, 1, si + 1, sj + 1, si + sj + 1};
+    T e[3] = {(T)0, (T)0, (T)0}, m[3] = {(T)0, (T)0, (T)0};
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        const auto ev = load_e(a.E + b + off[t]);
+        const auto bv = load_e(B + b + off[t]);
+        e[0] += w[t] * ev.x; e[1] += w[t] * ev.y; e[2] += w[t] * ev.z;
+        m[0] += w[t] * bv.x; m[1] += w[t] * bv.y; m[2] += w[t] * bv.z;
+    }
+    const T boris = (T)2 / ((T)1 + (m[0] * m[0] + m[1] * m[1] + m[2] * m[2]));
+    const T vx1 = st.vx + e[0], vy1 = st.vy + e[1], vz1 = st.vz + e[2];
+    const T vxt = vx1 + vy1 * m[2] - vz1 * m[1];
+    const T vyt = vy1 + vz1 * m[0] - vx1 * m[2];
+    const T vzt = vz1 + vx1 * m[1] - vy1 * m[0];
+    st.vx = vx1 + e[0] + boris * (vyt * m[2] - vzt * m[1]);
+    st.vy = vy1 + e[1] + boris * (vzt * m[0] - vxt * m[2]);
+    st.vz = vz1 + e[2] + boris * (vxt * m[1] - vyt * m[0]);
+}
+
+template <typename T>
 __global__ void __launch_bounds__(kThreads) em_velocity_kernel(PushArgsT<T> a, const typename NodeE<T>::type* B) {
     const long long n = (long long)min(*a.count, (unsigned long long)a.cap);
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n;
          idx += (long long)gridDim.x * blockDim.x) {
         const int32_t cell = a.p.cell[idx];
         if (cell < 0) continue;
-        int i, j, k;
-        unpack_cell(cell, i, j, k);
-        const T x1 = a.p.ox[idx], y1 = a.p.oy[idx], z1 = a.p.oz[idx];
-        const T x2 = (T)1 - x1, y2 = (T)1 - y1, z2 = (T)1 - z1;
-        const T w[8] = {a.qm * x2 * y2 * z2, a.qm * x1 * y2 * z2, a.qm * x2 * y1 * z2, a.qm * x1 * y1 * z2,
-                        a.qm * x2 * y2 * z1, a.qm * x1 * y2 * z1, a.qm * x2 * y1 * z1, a.qm * x1 * y1 * z1};
-        const int b = lin(a.g, i, j, k), sj = (int)a.g.sj, si = (int)a.g.si;
-        const int off[8] = {0, si, sj, si + sj, 1, si + 1, sj + 1, si + sj + 1};
-        T e[3] = {(T)0, (T)0, (T)0}, m[3] = {(T)0, (T)0, (T)0};
-#pragma unroll
-        for (int t = 0; t < 8; ++t) {
-            const auto ev = load_e(a.E + b + off[t]);
-            const auto bv = load_e(B + b + off[t]);
-            e[0] += w[t] * ev.x; e[1] += w[t] * ev.y; e[2] += w[t] * ev.z;
-            m[0] += w[t] * bv.x; m[1] += w[t] * bv.y; m[2] += w[t] * bv.z;
-        }
-        const T boris = (T)2 / ((T)1 + (m[0] * m[0] + m[1] * m[1] + m[2] * m[2]));
-        const T vx1 = a.p.vx[idx] + e[0], vy1 = a.p.vy[idx] + e[1], vz1 = a.p.vz[idx] + e[2];
-        const T vxt = vx1 + vy1 * m[2] - vz1 * m[1];
-        const T vyt = vy1 + vz1 * m[0] - vx1 * m[2];
-        const T vzt = vz1 + vx1 * m[1] - vy1 * m[0];
-        a.p.vx[idx] = vx1 + e[0] + boris * (vyt * m[2] - vzt * m[1]);
-        a.p.vy[idx] = vy1 + e[1] + boris * (vzt * m[0] - vxt * m[2]);
-        a.p.vz[idx] = vz1 + e[2] + boris * (vxt * m[1] - vyt * m[0]);
+        PStateT<T> st;
+        unpack_cell(cell, st.i, st.j, st.k);
+        st.ox = a.p.ox[idx]; st.oy = a.p.oy[idx]; st.oz = a.p.oz[idx];
+        st.vx = a.p.vx[idx]; st.vy = a.p.vy[idx]; st.vz = a.p.vz[idx];
+        em_kick(a, B, st);
+        a.p.vx[idx] = st.vx; a.p.vy[idx] = st.vy; a.p.vz[idx] = st.vz;
     }
 }
 
@@ -514,6 +522,7 @@ constexpr float kCurrentScale = 16777216.0f;   // 2^24
 struct EdgeFix {
     unsigned long long *x = nullptr, *y = nullptr, *z = nullptr;   // this species' jx, jy, jz sums
     int cx = 0, cy = 0, cz = 0;
+    const float4* B = nullptr;   // nodal B: the pass also gives the velocity update first (em_kick)
 };
 
 __device__ __forceinline__ float em_relay_f(int i_new, int i_old, float x_new, float x_old) {
@@ -692,6 +701,7 @@ __global__ void __launch_bounds__(kThreads) em_tail_kernel(PushArgs a, EdgeFix J
             unpack_cell(cell, st.i, st.j, st.k);
             st.ox = a.p.ox[idx]; st.oy = a.p.oy[idx]; st.oz = a.p.oz[idx];
             st.vx = a.p.vx[idx]; st.vy = a.p.vy[idx]; st.vz = a.p.vz[idx];
+            if (J.B) em_kick(a, J.B, st);
         }
         const int oi = st.i, oj = st.j, ok = st.k;
         const float o0[3] = {st.ox, st.oy, st.oz};
@@ -705,6 +715,7 @@ __global__ void __launch_bounds__(kThreads) em_tail_kernel(PushArgs a, EdgeFix J
         if (cell >= 0) {
             a.p.cell[idx] = live ? pack_cell(st.i, st.j, st.k) : -1;
             a.p.ox[idx] = st.ox; a.p.oy[idx] = st.oy; a.p.oz[idx] = st.oz;
+            if (J.B) { a.p.vx[idx] = st.vx; a.p.vy[idx] = st.vy; a.p.vz[idx] = st.vz; }
         }
     }
     const double np = block_sum(npushed), nk = block_sum(nkept);
@@ -907,6 +918,7 @@ __global__ void __launch_bounds__(kBrickThreads, MINB) push_brick_kernel(PushArg
                             unpack_cell(cell[r], st.i, st.j, st.k);
                             st.ox = f[r][0]; st.oy = f[r][1]; st.oz = f[r][2];
                             st.vx = f[r][3]; st.vy = f[r][4]; st.vz = f[r][5];
+                            if (J.B) em_kick(a, J.B, st);
                         }
                         const int oi = st.i, oj = st.j, ok = st.k;
                         const float o0[3] = {st.ox, st.oy, st.oz};
@@ -2355,8 +2367,10 @@ void launch_em_velocity(Ctx& c) {
 // The mixed mode's EM particle pass: per species the brick-sorted slots with
 // push_brick_kernel<.., true> and the appended tail with em_tail_kernel (move,
 // fixed-point current halves, body test, rho deposit), then J in FP64 and its
-// periodic folds. The caller zeroes rho and the fixed-point sums.
-void launch_em_move(Ctx& c) {
+// periodic folds. With kick the same pass gives the velocity update first
+// (the caller's choice when no particle is emitted between the two updates).
+// The caller zeroes rho and the fixed-point sums.
+void launch_em_move(Ctx& c, bool kick) {
     const long long nxe = (long long)(c.cx - 1) * c.cy * c.cz, nye = (long long)c.cx * (c.cy - 1) * c.cz;
     const long long per = nxe + nye + (long long)c.cx * c.cy * (c.cz - 1);
     FixScales sc{};
@@ -2364,7 +2378,7 @@ void launch_em_move(Ctx& c) {
         sc.v[s] = c.p.species[s].charge * c.p.species[s].size / (double)kCurrentScale;
         if (c.cap[s] == 0) continue;
         unsigned long long* base = c.em.jfix + (size_t)s * per;
-        const EdgeFix J{base, base + nxe, base + nxe + nye, c.cx, c.cy, c.cz};
+        const EdgeFix J{base, base + nxe, base + nxe + nye, c.cx, c.cy, c.cz, kick ? c.em.B : nullptr};
         PushArgs a = push_args<float>(c, s);
         if (c.sorted_n[s] > 0 && c.brick_start[s]) {
             ++c.launches;
