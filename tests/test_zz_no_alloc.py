@@ -47,39 +47,3 @@ def test_noalloc_energy_matches_existing_entry_point(gpu_available):
     assert rc == _abi.ERR_ARG
     g.close()
 
-
-def test_noalloc_energy_replays_in_a_cuda_graph(gpu_available):
-    """The stated purpose: the call recorded once under stream capture and replayed
-    with the caller's potential changed in place, allocating nothing; each replay
-    equals fopis_get_energy for the potential it saw."""
-    import torch
-    dx, dt = plasma_units()
-    sp = [SpeciesInfo("Electron", "ambient", 1.0, -1.0, 1e7, 1.0, 4)]
-    p, norm = make_params((25, 27, 23), "DDDDPP", dx, dt, sp)
-    g = RootGrid(SimConfig(params=p, norm=norm, species=sp))
-    lib = _abi.library()
-    rng = np.random.default_rng(5)
-    dphi = torch.zeros(g.shape, dtype=torch.float64, device="cuda")
-    out = torch.zeros(1, dtype=torch.float64, device="cuda")
-    side = torch.cuda.Stream()
-    # the first call of the context looks the scratch address up outside any capture
-    assert lib.fopis_efield_energy_noalloc(C.c_void_p(dphi.data_ptr()), p.nx, p.ny, p.nz, p.eps0,
-                                           C.c_void_p(out.data_ptr()), C.c_void_p(side.cuda_stream)) == 0
-    torch.cuda.synchronize()
-    graph = torch.cuda.CUDAGraph()
-    with torch.cuda.graph(graph, stream=side):
-        rc = lib.fopis_efield_energy_noalloc(C.c_void_p(dphi.data_ptr()), p.nx, p.ny, p.nz, p.eps0,
-                                             C.c_void_p(out.data_ptr()), C.c_void_p(side.cuda_stream))
-    assert rc == 0
-    for call in range(2):
-        phi = rng.standard_normal(g.shape) * (2.0 + call)
-        dphi.copy_(torch.from_numpy(phi))
-        torch.cuda.synchronize()
-        graph.replay()
-        torch.cuda.synchronize()
-        g.set_field(_abi.FIELD_PHI, phi)
-        _, expect = g.getEnergy()
-        got = float(out.item())
-        assert abs(got - expect) <= 1e-12 * abs(expect), (call, got, expect)
-    del graph
-    g.close()
