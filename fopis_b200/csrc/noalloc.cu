@@ -40,7 +40,7 @@ constexpr long long kNodesPerPartial = 8192;
 constexpr int kThreadsNA = 256;
 constexpr int kMaxContexts = 64;
 
-__device__ __align__(256) double g_energy_partials[kMaxPartials];
+static __device__ __align__(256) double g_energy_partials[kMaxPartials];
 
 // The scratch address of each context met so far, by the context's unique id
 // (cuCtxGetId never hands out an id twice in a process, so a context created
