@@ -200,7 +200,10 @@ typedef struct fopis_stats {
     int64_t emitted_step;
     uint32_t device_status;      /* FOPIS_DEV_* bits */
     int learned_used;            /* the learned guess seeded the last step's solves */
-    double ms_phase[8];          /* last step: push, emit, inject, absorb, rho, solve, efield, sort */
+    double ms_phase[8];          /* last step, ES: push, emit, inject, absorb, rho + first solve, second
+                                    solve, efield, sort; EM: velocity (0 when the particle pass gives
+                                    it), emit, position with the currents + inject, 0, rho, E update,
+                                    B update, sort */
     int64_t kernel_launches;     /* kernels this context has launched since creation */
     int solve_mode;              /* 0: host-driven V-cycle loop; 1: one CUDA graph with a device-side
                                     loop; 2: the same graph with programmatic dependent launches */
