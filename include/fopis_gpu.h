@@ -1,10 +1,12 @@
 /*
  * fopis_gpu.h — C ABI of libfopis_gpu.so, the B200 (sm_100a) electrostatic
- * particle-in-cell timestep of FOPIS ("TDPIC").
+ * particle-in-cell timestep of FOPIS ("TDPIC"), and its electromagnetic (FDTD)
+ * variant.
  *
  * The reference has no plugin or FFI layer: its ES path is the RootGrid phase
  * methods that RootGrid::mainLoopES calls in order (src/Grid/RootGrid/RootGrid.cpp:82-143)
- * plus the start-up in Initializer::initTDPIC (src/Misc/Initialize.cpp:16-107).
+ * plus the start-up in Initializer::initTDPIC (src/Misc/Initialize.cpp:16-107);
+ * RootGrid::mainLoopEM (RootGrid.cpp:145-191) is the EM path.
  * Each entry point below replaces one of those methods; the citation beside it
  * names the reference function whose behaviour it keeps.
  *
