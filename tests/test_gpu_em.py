@@ -125,6 +125,24 @@ def test_em_phases_match_oracle(gpu_available):
     o.close()
 
 
+def test_em_mixed_phases_match_oracle(gpu_available):
+    """The phase entry points in the mixed mode (FP32 particles): velocity, then the
+    position update with the edge currents (FP64 atomics of the FP32 terms), against
+    the FP64 oracle on the same FP32-rounded start."""
+    cfg = em_config(n=13, precision=_abi.MIXED)
+    g, o = load_pair(cfg, f32=True)
+    g.updateParticleVelocity()
+    o.update_velocity()
+    compare_particles(g, o, 1e-6, 1e-5)
+    g.updateParticlePosition()
+    o.update_position()
+    for which in CURRENTS:
+        assert rel_err(g.get_field(which), o.field(which)) <= 1e-5, which
+    compare_particles(g, o, 1e-5, 1e-5)
+    g.close()
+    o.close()
+
+
 @pytest.mark.parametrize("boundary,steps", [("DDDDDD", 20), ("PPPPPP", 20)])
 def test_em_main_loop_fp64_tracks_oracle(gpu_available, boundary, steps):
     cfg = em_config(n=13, boundary=boundary)
