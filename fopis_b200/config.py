@@ -32,15 +32,19 @@ class Normalizer:
     """include/normalizer.hpp: x_unit = dx, t_unit = dt, m_unit = m_e, e_unit = e."""
 
     def __init__(self, dx: float, dt: float):
+        # Normalizer::updatePhysicalConstants (include/normalizer.hpp:24-38) in the
+        # reference's operation order, so every factor is the reference's to the bit:
+        # pow(u, 2) is the product u * u (the compiler's form of it), pow(u, 3) the libm pow
         self.x = dx
         self.t = dt
         self.m = ME
         self.e = E
-        self.V_unit = dx * dx * ME / (E * dt * dt)
+        self.x_pow_3 = dx ** 3
+        self.V_unit = (dx * dx) * ME / (E * (dt * dt))
         self.A_unit = E / dt
-        self.eps0 = EPS0 * (dx ** 3 * ME) / (E * E * dt * dt)   # normalizeEpsilon
-        self.mu0 = MU0 * E * E / (ME * dx)                       # normalizeMu
-        self.c = self.velocity(CLIGHT)                           # normalizeVelocity(c): the Courant number
+        self.eps0 = EPS0 * (self.x_pow_3 * ME) / ((E * E) * (dt * dt))   # normalizeEpsilon
+        self.mu0 = MU0 * (E * E) / (ME * dx)                              # normalizeMu
+        self.c = self.velocity(CLIGHT)                                    # normalizeVelocity(c): the Courant number
 
     def velocity(self, v):
         return self.t * v / self.x
@@ -67,7 +71,11 @@ class Normalizer:
         return i * self.A_unit
 
     def unenergy(self, en):
-        return en * self.m * self.x ** 2 / self.t ** 2
+        return en * self.m * (self.x * self.x) / (self.t * self.t)
+
+    def unenergy_ev(self, en):
+        """unnormalizeEnergy(en, "eV")."""
+        return en * self.m * (self.x * self.x) / (self.e * (self.t * self.t))
 
 
 def calc_flux(vth: float, density_norm: float, size: float, drift: Sequence[float],
@@ -149,7 +157,7 @@ def _species_struct(sp: SpeciesInfo, norm: Normalizer, dx: float) -> _abi.Specie
     s.thermal_velocity = norm.velocity(math.sqrt(2.0 * T / (sp.mass * ME)))
     s.deviation = norm.velocity(math.sqrt(T / (sp.mass * ME)))
     for a in range(3):
-        s.drift[a] = sp.drift_kms[a] * 1e3 * norm.velocity(1.0)
+        s.drift[a] = sp.drift_kms[a] * (1e3 * norm.velocity(1.0))      # Initialize.cpp:353-355
     for a in range(6):
         s.injection_axis[a] = int(sp.injection_axis[a])
     if sp.kind == "ambient":
@@ -179,7 +187,7 @@ def make_params(nxyz: Tuple[int, int, int], boundary: str, dx: float, dt: float,
     p.boundary = boundary.encode()
     p.eps0 = norm.eps0
     for a in range(3):
-        p.static_bfield[a] = bfield_nT[a] * norm.bfield(1.0) * 1e-9
+        p.static_bfield[a] = bfield_nT[a] * (norm.bfield(1.0) * 1e-9)   # Initialize.cpp:314-318
         p.shine_vector[a] = float(shine[a])
     # Environment::resetParticleTypeOrder (Environment.cpp:360-377): ambient, photoelectron, secondary
     ordered = [s for k in ("ambient", "photoelectron", "secondary") for s in species if s.kind == k]
@@ -195,7 +203,7 @@ def make_params(nxyz: Tuple[int, int, int], boundary: str, dx: float, dt: float,
     p.capacity_factor = capacity_factor
     p.precision = precision
     p.seed = seed
-    p.energy_ev = norm.unenergy(1.0) / E                       # Normalizer::unnormalizeEnergy(1, "eV")
+    p.energy_ev = norm.unenergy_ev(1.0)                        # Normalizer::unnormalizeEnergy(1, "eV")
     p.solver = _abi.SOLVER_EM if solver == "EM" else _abi.SOLVER_ES
     p.mu0 = norm.mu0
     return p, norm

@@ -17,12 +17,16 @@ namespace fopis {
 namespace host {
 
 // ---------------------------------------------------------------- units
+// Normalizer::updatePhysicalConstants (include/normalizer.hpp:24-38) in the
+// reference's operation order, so every factor is the reference's to the bit:
+// pow(u, 2) is the product u * u (the compiler's form of it), pow(u, 3) the libm pow.
 Normalizer::Normalizer(double dx, double dt) : x(dx), t(dt) {
-    V_unit = dx * dx * kMe / (kE * dt * dt);
+    const double x_pow_3 = std::pow(dx, 3.0);
+    V_unit = (dx * dx) * kMe / (kE * (dt * dt));
     A_unit = kE / dt;
-    eps0 = kEps0 * (std::pow(dx, 3.0) * kMe) / (kE * kE * dt * dt);   // Normalizer::normalizeEpsilon
-    mu0 = kMu0 * kE * kE / (kMe * dx);                                // Normalizer::normalizeMu
-    c = velocity(kClight);                                            // Normalizer::normalizeVelocity(c)
+    eps0 = kEps0 * (x_pow_3 * kMe) / ((kE * kE) * (dt * dt));   // Normalizer::normalizeEpsilon
+    mu0 = kMu0 * (kE * kE) / (kMe * dx);                         // Normalizer::normalizeMu
+    c = velocity(kClight);                                       // Normalizer::normalizeVelocity(c)
 }
 
 void calc_flux(double vth, double density_norm, double size, const double drift[3], const int injection_axis[6],
@@ -56,7 +60,7 @@ fopis_species ParticleType::to_abi(const Normalizer& norm, double dx) const {
     const double T = kE * temperature;                                               // setTemperature: e * T[eV]
     s.thermal_velocity = norm.velocity(std::sqrt(2.0 * T / (mass * kMe)));
     s.deviation = norm.velocity(std::sqrt(T / (mass * kMe)));
-    for (int a = 0; a < 3; ++a) s.drift[a] = drift_kms[a] * 1e3 * norm.velocity(1.0);
+    for (int a = 0; a < 3; ++a) s.drift[a] = drift_kms[a] * (1e3 * norm.velocity(1.0));   // Initialize.cpp:353-355
     for (int a = 0; a < 6; ++a) s.injection_axis[a] = injection_axis[a];
     if (type == "ambient") {
         const double dens_norm = density * std::pow(dx, 3.0);                         // normalizeDensity
@@ -185,7 +189,7 @@ Input load_input(const std::string& path) {
     std::snprintf(p.boundary, sizeof p.boundary, "%s", env["boundary"].str().c_str());
     p.eps0 = norm.eps0;
     for (int a = 0; a < 3; ++a) {
-        p.static_bfield[a] = bfield[a] * norm.bfield(1.0) * 1e-9;   // nT
+        p.static_bfield[a] = bfield[a] * (norm.bfield(1.0) * 1e-9);   // nT (Initialize.cpp:314-318)
         p.shine_vector[a] = shine[a];
     }
     if ((int)species.size() > FOPIS_MAX_SPECIES) throw Error(FOPIS_ERR_ARG, "too many species");
@@ -199,7 +203,7 @@ Input load_input(const std::string& path) {
     p.capacity_factor = 1.5;
     p.precision = FOPIS_MIXED;
     p.seed = 12345;
-    p.energy_ev = norm.unenergy(1.0) / kE;   // Normalizer::unnormalizeEnergy(1, "eV")
+    p.energy_ev = norm.unenergy_ev(1.0);   // Normalizer::unnormalizeEnergy(1, "eV")
     p.solver = solver == "EM" ? FOPIS_SOLVER_EM : FOPIS_SOLVER_ES;
     p.mu0 = norm.mu0;
 

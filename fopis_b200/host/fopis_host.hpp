@@ -38,7 +38,8 @@ struct Normalizer {
     double unpotential(double phi) const { return phi * V_unit; }
     double uncharge(double q) const { return q * e; }
     double uncurrent(double i) const { return i * A_unit; }
-    double unenergy(double en) const { return en * m * x * x / (t * t); }
+    double unenergy(double en) const { return en * m * (x * x) / (t * t); }
+    double unenergy_ev(double en) const { return en * m * (x * x) / (e * (t * t)); }   // unnormalizeEnergy(en, "eV")
 };
 
 // ParticleType / AmbientParticleType / PhotoElectronParticleType (the fields the ES path reads).

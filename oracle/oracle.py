@@ -17,6 +17,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
 REF_PIN = HERE / "_ref" / "libpin_position.so"
+REF_NORM = HERE / "_ref" / "libpin_normalizer.so"
 
 PARTICLE_DTYPE = np.dtype([("x", "<f8"), ("y", "<f8"), ("z", "<f8"), ("vx", "<f8"), ("vy", "<f8"), ("vz", "<f8"),
                            ("typeId", "<i4"), ("isValid", "<i4")])
@@ -135,6 +136,39 @@ def ref_relay(new_xyz: np.ndarray, old_xyz: np.ndarray):
     b = np.ascontiguousarray(old_xyz, np.float64)
     out = np.zeros_like(a)
     L.ref_relay(a.ctypes.data, b.ctypes.data, len(a), out.ctypes.data)
+    return out
+
+
+NORMALIZER_UNITS = ("eps0", "mu0", "c", "V_unit", "A_unit", "velocity", "bfield", "current_density", "density",
+                    "energy", "energy_ev", "capacitance")
+NORMALIZER_APPLY = {"velocity": 0, "unvelocity": 1, "potential": 2, "unpotential": 3, "current_density": 4,
+                    "uncurrent": 5, "uncharge": 6, "unenergy": 7, "capacitance": 8, "density": 9, "bfield": 10}
+
+
+def ref_normalizer_units(dx: float, dt: float):
+    """The reference's own Normalizer (include/normalizer.hpp, src/Misc/Normalizer.cpp)
+    after Initializer's unit set-up with dx and dt: a dict over NORMALIZER_UNITS, or None."""
+    if not REF_NORM.exists():
+        return None
+    L = C.CDLL(str(REF_NORM))
+    L.ref_normalizer_units.argtypes = [C.c_double, C.c_double, C.c_void_p, C.c_int]
+    L.ref_normalizer_units.restype = C.c_int
+    out = np.zeros(len(NORMALIZER_UNITS), np.float64)
+    m = L.ref_normalizer_units(dx, dt, out.ctypes.data, len(out))
+    return dict(zip(NORMALIZER_UNITS[:m], out[:m].tolist()))
+
+
+def ref_normalizer_apply(dx: float, dt: float, kind: str, values: np.ndarray):
+    """One of the reference Normalizer's conversions (NORMALIZER_APPLY) on values, or None."""
+    if not REF_NORM.exists():
+        return None
+    L = C.CDLL(str(REF_NORM))
+    L.ref_normalizer_apply.argtypes = [C.c_double, C.c_double, C.c_int, C.c_void_p, C.c_int64, C.c_void_p]
+    L.ref_normalizer_apply.restype = C.c_int
+    x = np.ascontiguousarray(values, np.float64)
+    out = np.zeros_like(x)
+    if L.ref_normalizer_apply(dx, dt, NORMALIZER_APPLY[kind], x.ctypes.data, len(x), out.ctypes.data) != 0:
+        raise ValueError(kind)
     return out
 
 
