@@ -1,12 +1,12 @@
 """Parity on the named workloads at their stated sizes, against the FP64
-oracle, at the tolerances of the north-star contract:
+oracle, at these tolerances:
 
-* config 1 (32^3 cells fully periodic, electrons + ions, 16 particles per
+* the periodic box (32^3 cells fully periodic, electrons + ions, 16 particles per
   cell per species, 100 steps): after the first step every particle's
   position and velocity within 1e-5 relative of the oracle's; over 100 steps
   the kinetic- and field-energy histories within 1 % (mixed precision), and
   much tighter in the FP64 mode;
-* config 2 (64^3 cells, Dirichlet faces with injection, 8^3-cell cube
+* the 64^3 spacecraft box (64^3 cells, Dirichlet faces with injection, 8^3-cell cube
   conductor, 32 particles per cell per species, FP64 on the GPU): the
   spacecraft potential within 1e-6 relative of the oracle's for 50 steps;
 * a grid with Dirichlet, Neumann and periodic faces: phi (held Neumann faces
@@ -74,7 +74,7 @@ def test_config1_periodic32(gpu_available, precision):
     fe = np.abs(h[:, 1] - h[:, 3]) / np.max(h[:, 3])
     tol = 0.01 if precision == _abi.MIXED else 1e-4
     assert pe.max() <= tol and fe.max() <= tol, (pe.max(), fe.max())
-    print(f"\nconfig 1 ({'mixed' if precision == _abi.MIXED else 'fp64'}): step-1 max |dx|/|x| {ex:.2e}, |dv|/|v| {ev:.2e};"
+    print(f"\nperiodic 32^3 box ({'mixed' if precision == _abi.MIXED else 'fp64'}): step-1 max |dx|/|x| {ex:.2e}, |dv|/|v| {ev:.2e};"
           f" 100 steps: kinetic energy {pe.max():.2e}, field energy {fe.max():.2e} of its max")
     g.close()
     o.close()
@@ -101,7 +101,7 @@ def test_config2_cube64_fp64_potential(gpu_available):
     Vg, Vo = np.array(Vg), np.array(Vo)
     err = np.abs(Vg - Vo) / np.abs(Vo)
     assert err.max() <= 1e-6, err.max()
-    print(f"\nconfig 2 (fp64, 50 steps): spacecraft potential max rel. error {err.max():.2e}")
+    print(f"\n64^3 spacecraft box (fp64, 50 steps): spacecraft potential max rel. error {err.max():.2e}")
     pg, _ = g.getEnergy()
     po, _ = o.energy()
     assert abs(pg - po) <= 1e-6 * po
