@@ -143,6 +143,7 @@ class SimConfig:
     dt: float = 1.0
     use_existing_capacity_matrix: bool = False
     maximum_poisson_post_loop: int = 1000
+    plot_energy_width: int = 0       # IO.plot_energy_width: energy log every this many steps, 0 = never
 
 
 def _species_struct(sp: SpeciesInfo, norm: Normalizer, dx: float) -> _abi.Species:
@@ -450,4 +451,5 @@ def load_input(path: str) -> SimConfig:
                                dielectric=int(surface == "dielectric"), capacitance=cap))
     return SimConfig(params=p, norm=norm, species=species, objects=objs, max_timestep=int(env.get("max_timestep", 0)),
                      dx=dx, dt=dt, use_existing_capacity_matrix=bool(opts.get("use_existing_capacity_matrix", False)),
-                     maximum_poisson_post_loop=int(opts.get("maximum_poisson_post_loop", 1000)))
+                     maximum_poisson_post_loop=int(opts.get("maximum_poisson_post_loop", 1000)),
+                     plot_energy_width=int(float(js.get("IO", {}).get("plot_energy_width", 0))))

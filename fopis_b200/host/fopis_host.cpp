@@ -183,6 +183,9 @@ Input load_input(const std::string& path) {
         if (f.has("shine_vector")) for (int a = 0; a < 3; ++a) shine[a] = f["shine_vector"][a].number();
     }
     if (js.has("Options")) in.use_existing_capacity_matrix = js["Options"].boolean_or("use_existing_capacity_matrix", false);
+    // the IO section's energy-log width (Initialize.cpp:219-250, cast from a number as there);
+    // the other widths select field files, which are not written here
+    if (js.has("IO")) in.plot_energy_width = static_cast<int>(js["IO"].number_or("plot_energy_width", 0.0));
 
     fopis_params& p = in.params;
     p.nx = nxyz[0]; p.ny = nxyz[1]; p.nz = nxyz[2];

@@ -87,6 +87,7 @@ struct Input {
     double dx = 1.0, dt = 1.0;
     bool use_existing_capacity_matrix = false;
     std::string job_type = "new";        // Environment.job_type: "new" or "load"
+    int plot_energy_width = 0;           // IO.plot_energy_width: energy log every this many steps, 0 = never
 };
 
 // Initializer::initTDPIC's parsing (src/Initializer/Initialize.cpp:158-421) for

@@ -4,7 +4,8 @@
 // for job_type "new" load the ambient plasma and initialize, for "load" read
 // <resume>/environment.bin and grid_id_0.bin and Grid::initializeForLoad
 // (Initialize.cpp:75-99); per step RootGrid::mainLoop and the energy / object /
-// particle-number logs; at the end Environment::saveInfo and
+// particle-number logs (the energy log every IO.plot_energy_width steps, never
+// when it is 0 or absent); at the end Environment::saveInfo and
 // RootGrid::saveResumeData into <resume>.
 //
 //   fopis_run [input.json] [--steps N] [--out DIR] [--resume DIR] [--device D]
@@ -44,6 +45,8 @@ void dump_params(const Input& in, const std::string& file) {
         if (o.dielectric)
             f.write(reinterpret_cast<const char*>(o.capacitance.data()), sizeof(double) * o.capacitance.size());
     }
+    const int32_t io[1] = {in.plot_energy_width};
+    f.write(reinterpret_cast<const char*>(io), sizeof io);
 }
 }  // namespace
 
@@ -102,7 +105,8 @@ int main(int argc, char** argv) {
         std::cout << "===== Begin Main Loop =====" << std::endl;
         for (int64_t t = first; t <= last; ++t) {
             grid.mainLoop();
-            io::plot_energy(grid, (int)t, out);
+            // Environment::plotEnergy (include/environment.hpp:242, :266-278)
+            if (in.plot_energy_width != 0 && t % in.plot_energy_width == 0) io::plot_energy(grid, (int)t, out);
             io::plot_objects(grid, (int)t, out);
             io::plot_particle_numbers(grid, (int)t, out);
         }

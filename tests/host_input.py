@@ -56,6 +56,7 @@ def write_input(dirpath, n=25, ppc=4, photo=True, steps=5, drift=(0.0, 0.0, 0.0)
                                   "is_potential_fixed": False, "fixed_potential": 0.0,
                                   "initial_potential_offset": 0.0, **({"materials": dielectric} if dielectric else {})}},
         "Options": {"use_existing_capacity_matrix": False},
+        "IO": {"plot_energy_width": 1},
     }
     path = d / "input.json"
     path.write_text(json.dumps(js, indent=2))

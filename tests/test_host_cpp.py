@@ -46,6 +46,7 @@ def dump(path, tmp_path):
             cap = np.frombuffer(raw, np.float64, nn, off)
             off += 8 * nn
         objs.append((nodes, cells, int(fixed), int(emit), pot, int(sec), int(diel), cap))
+    p.plot_energy_width = int(np.frombuffer(raw, np.int32, 1, off)[0])
     return p, objs
 
 
@@ -54,6 +55,7 @@ def compare(cpp, py):
     q = py.params
     assert bytes(p) == bytes(q), [(f, getattr(p, f), getattr(q, f)) for f, _ in q._fields_ if
                                   not isinstance(getattr(q, f), (int, float)) or getattr(p, f) != getattr(q, f)]
+    assert p.plot_energy_width == py.plot_energy_width
     assert len(objs) == len(py.objects)
     for (nodes, cells, fixed, emit, pot, sec, diel, cap), o in zip(objs, py.objects):
         assert np.array_equal(nodes, o.nodes) and np.array_equal(cells, o.cells)
@@ -84,6 +86,22 @@ def test_cpp_loader_dielectric_and_secondary(built, tmp_path):
     assert [s.kind for s in py.species] == ["ambient", "ambient", "photoelectron", "secondary"]
     o = py.objects[0]
     assert o.dielectric == 1 and o.secondary_species == 3 and o.emit_species == 2
+    compare(dump(path, tmp_path), py)
+
+
+@pytest.mark.parametrize("io", [{"plot_energy_width": 7}, {"plot_energy_width": 3.0, "plot_rho_width": 0}, None])
+def test_cpp_loader_energy_log_width(built, tmp_path, io):
+    """IO.plot_energy_width, cast from a number as Initializer does (Initialize.cpp:219-250);
+    without it the energy log is never written (Environment::isPlotTimestep, environment.hpp:266-278)."""
+    import json
+    path = write_input(tmp_path, photo=False)
+    js = json.loads(path.read_text())
+    js.pop("IO", None)
+    if io is not None:
+        js["IO"] = io
+    path.write_text(json.dumps(js))
+    py = config.load_input(str(path))
+    assert py.plot_energy_width == (int(io["plot_energy_width"]) if io else 0)
     compare(dump(path, tmp_path), py)
 
 
